@@ -1,0 +1,221 @@
+"""Python host binding of libcof.so (ctypes over include/cof.h).
+
+Mirrors cas-offinder-lib's public search API:
+
+    search(devices, max_mismatches, max_dna_bulges, max_rna_bulges,
+           search_filter_ascii, pattern_len, patterns_ascii, recv, dest)
+    (cas-offinder-lib/src/search.rs:1490-1500)
+
+The genome (the `recv` channel of ChromChunkInfo) is a `Genome` object that
+is filled once and stays resident on the GPU; the result (the `dest` channel,
+rendered by the CLI writer, cas-offinder-cli/src/main.rs:122-247) is the
+8-column row text.  The CUDA library must be present: importing this module
+without libcof.so raises, there is no CPU fallback.
+"""
+import ctypes
+import os
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libcof.so")
+
+COF_OK = 0
+COF_E_BADINPUT = -1
+COF_E_OOM = -2
+COF_E_CUDA = -3
+COF_E_IO = -4
+COF_E_UNSUPPORTED = -5
+COF_E_STATE = -6
+COF_E_TIMEOUT = -7
+COF_F_ADD_REVCOMP = 1
+
+HEADER = "#Bulge type\tcrRNA\tDNA\tChromosome\tPosition\tDirection\tMismatches\tBulge Size\n"
+
+# Every symbol include/cof.h declares.
+EXPORTS = (
+    "cof_genome_create", "cof_genome_add_chunk", "cof_genome_load", "cof_genome_upload",
+    "cof_genome_n_nucl", "cof_genome_n_chunks", "cof_genome_free", "cof_search",
+    "cof_search_batch", "cof_result_free", "cof_genome_last_stats", "cof_last_error",
+    "cof_abi_version",
+)
+
+
+class CofError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"cof error {code}: {msg}")
+        self.code = code
+
+
+class _Request(ctypes.Structure):
+    _fields_ = [
+        ("search_filter", ctypes.c_char_p),
+        ("pattern_len", ctypes.c_size_t),
+        ("patterns", ctypes.POINTER(ctypes.c_char_p)),
+        ("n_patterns", ctypes.c_size_t),
+        ("max_mismatches", ctypes.c_uint32),
+        ("max_dna_bulges", ctypes.c_uint32),
+        ("max_rna_bulges", ctypes.c_uint32),
+        ("flags", ctypes.c_uint32),
+        ("chunks_per_search", ctypes.c_uint32),
+    ]
+
+
+class _Result(ctypes.Structure):
+    _fields_ = [
+        ("text", ctypes.c_void_p),
+        ("text_len", ctypes.c_size_t),
+        ("n_rows", ctypes.c_uint64),
+        ("device_ms", ctypes.c_double),
+    ]
+
+
+_lib = None
+
+
+def load_library(path=LIB_PATH):
+    """Loads libcof.so (raises if it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise ImportError(f"{path} is missing: build it with cas-offinder-rust-old_b200/build.py")
+    lib = ctypes.CDLL(path)
+    vp, c = ctypes.c_void_p, ctypes
+    lib.cof_genome_create.argtypes = [c.c_int, c.POINTER(vp)]
+    lib.cof_genome_add_chunk.argtypes = [vp, c.c_char_p, c.c_void_p, c.c_uint64, c.c_uint64]
+    lib.cof_genome_load.argtypes = [vp, c.c_char_p]
+    lib.cof_genome_upload.argtypes = [vp]
+    lib.cof_genome_n_nucl.argtypes = [vp]
+    lib.cof_genome_n_nucl.restype = c.c_uint64
+    lib.cof_genome_n_chunks.argtypes = [vp]
+    lib.cof_genome_n_chunks.restype = c.c_uint64
+    lib.cof_genome_free.argtypes = [vp]
+    lib.cof_genome_free.restype = None
+    lib.cof_search.argtypes = [vp, c.POINTER(_Request), c.POINTER(_Result)]
+    lib.cof_search_batch.argtypes = [vp, c.POINTER(_Request), c.c_size_t, c.POINTER(_Result)]
+    lib.cof_result_free.argtypes = [c.POINTER(_Result)]
+    lib.cof_result_free.restype = None
+    lib.cof_genome_last_stats.argtypes = [vp, c.POINTER(c.c_double), c.POINTER(c.c_uint64)]
+    lib.cof_last_error.restype = c.c_char_p
+    lib.cof_abi_version.restype = c.c_int
+    _lib = lib
+    return lib
+
+
+def _check(rc):
+    if rc != COF_OK:
+        raise CofError(rc, _lib.cof_last_error().decode(errors="replace"))
+
+
+def _make_request(filt, patterns, mm, db, rb, add_revcomp, cps, keep):
+    fb = filt.encode() if isinstance(filt, str) else bytes(filt)
+    pb = [p.encode() if isinstance(p, str) else bytes(p) for p in patterns]
+    arr = (ctypes.c_char_p * len(pb))(*pb)
+    keep.extend([fb, pb, arr])
+    r = _Request()
+    r.search_filter = fb
+    r.pattern_len = len(fb)
+    r.patterns = arr
+    r.n_patterns = len(pb)
+    r.max_mismatches = mm
+    r.max_dna_bulges = db
+    r.max_rna_bulges = rb
+    r.flags = COF_F_ADD_REVCOMP if add_revcomp else 0
+    r.chunks_per_search = cps
+    return r
+
+
+class Genome:
+    """A genome resident on one GPU (replaces the ChromChunkInfo channel)."""
+
+    def __init__(self, path=None, device=0):
+        lib = load_library()
+        h = ctypes.c_void_p()
+        _check(lib.cof_genome_create(device, ctypes.byref(h)))
+        self._h = h
+        if path is not None:
+            self.load(path)
+
+    def load(self, path):
+        _check(_lib.cof_genome_load(self._h, os.fsencode(path)))
+
+    def add_chunk(self, name, bit4, chunk_start, chunk_end):
+        buf = bytes(bit4)
+        _check(_lib.cof_genome_add_chunk(self._h, name.encode() if isinstance(name, str) else name,
+                                         buf, chunk_start, chunk_end))
+
+    def upload(self):
+        _check(_lib.cof_genome_upload(self._h))
+
+    @property
+    def n_nucl(self):
+        return _lib.cof_genome_n_nucl(self._h)
+
+    @property
+    def n_chunks(self):
+        return _lib.cof_genome_n_chunks(self._h)
+
+    def search(self, search_filter, patterns, max_mismatches, max_dna_bulges=0,
+               max_rna_bulges=0, add_revcomp=True, chunks_per_search=0):
+        """Returns (rows_text, n_rows) for one request."""
+        return self.search_batch([dict(search_filter=search_filter, patterns=patterns,
+                                       max_mismatches=max_mismatches,
+                                       max_dna_bulges=max_dna_bulges,
+                                       max_rna_bulges=max_rna_bulges, add_revcomp=add_revcomp,
+                                       chunks_per_search=chunks_per_search)])[0]
+
+    def search_batch(self, requests):
+        """Many requests in one pass; returns [(rows_text, n_rows), ...]."""
+        keep = []
+        reqs = (_Request * len(requests))()
+        for i, r in enumerate(requests):
+            reqs[i] = _make_request(r["search_filter"], r["patterns"], r["max_mismatches"],
+                                    r.get("max_dna_bulges", 0), r.get("max_rna_bulges", 0),
+                                    r.get("add_revcomp", True), r.get("chunks_per_search", 0),
+                                    keep)
+        outs = (_Result * len(requests))()
+        _check(_lib.cof_search_batch(self._h, reqs, len(requests), outs))
+        res = []
+        for o in outs:
+            text = ctypes.string_at(o.text, o.text_len).decode("latin-1") if o.text_len else ""
+            res.append((text, o.n_rows))
+            _lib.cof_result_free(ctypes.byref(o))
+        return res
+
+    def last_stats(self):
+        ms = (ctypes.c_double * 5)()
+        cnt = (ctypes.c_uint64 * 5)()
+        _check(_lib.cof_genome_last_stats(self._h, ms, cnt))
+        return dict(scan_ms=ms[0], verify_ms=ms[1], format_ms=ms[2], d2h_ms=ms[3],
+                    total_ms=ms[4], candidates=cnt[0], pairs=cnt[1], raw_hits=cnt[2],
+                    rows=cnt[3], kernel_launches=cnt[4])
+
+    def close(self):
+        if getattr(self, "_h", None):
+            _lib.cof_genome_free(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+
+def search(devices, max_mismatches, max_dna_bulges, max_rna_bulges, search_filter_ascii,
+           pattern_len, patterns_ascii, genome):
+    """search() of search.rs:1490 with the genome as a resident Genome.
+
+    `devices` is accepted for signature parity (one GPU per Genome); the
+    patterns are the full fwd+rc list as main.rs passes them.  Returns the
+    writer's rows (list of str, without the header)."""
+    assert len(patterns_ascii) > 0
+    assert all(len(p) == pattern_len for p in patterns_ascii), "All patterns must have same length"
+    text, _ = genome.search(search_filter_ascii, patterns_ascii, max_mismatches, max_dna_bulges,
+                            max_rna_bulges, add_revcomp=False)
+    return text.splitlines()

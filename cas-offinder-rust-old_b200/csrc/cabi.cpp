@@ -1,0 +1,165 @@
+// cabi.cpp -- extern "C" entry points of libcof.so (declared in include/cof.h).
+#include <cstdlib>
+#include <cstring>
+#include <mutex>
+#include <new>
+#include <string>
+
+#include "../../include/cof.h"
+#include "cof_engine.h"
+
+struct cof_genome {
+    cof::Engine engine;
+    std::mutex mu;
+    explicit cof_genome(int dev) : engine(dev) {}
+};
+
+namespace {
+
+thread_local std::string g_last_error;
+
+int fail(int code, const std::string &msg) {
+    g_last_error = msg;
+    return code;
+}
+int fail(const cof::Error &e) { return fail(e.code, e.msg); }
+
+int to_requests(const cof_request *reqs, size_t n, std::vector<cof::Request> &out,
+                cof::Error &err) {
+    out.resize(n);
+    for (size_t i = 0; i < n; ++i) {
+        const cof_request &r = reqs[i];
+        if (cof::make_request(r.search_filter, r.pattern_len, r.patterns, r.n_patterns,
+                              r.max_mismatches, r.max_dna_bulges, r.max_rna_bulges, r.flags,
+                              r.chunks_per_search, out[i], err))
+            return err.code;
+    }
+    return 0;
+}
+
+int fill_result(const cof::Result &r, cof_result *out) {
+    out->text = (char *)std::malloc(r.text.size() + 1);
+    if (!out->text) return fail(COF_E_OOM, "out of host memory for result text");
+    std::memcpy(out->text, r.text.data(), r.text.size());
+    out->text[r.text.size()] = 0;
+    out->text_len = r.text.size();
+    out->n_rows = r.n_rows;
+    out->device_ms = r.device_ms;
+    return COF_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+COF_API int cof_abi_version(void) { return COF_ABI_VERSION; }
+
+COF_API const char *cof_last_error(void) { return g_last_error.c_str(); }
+
+COF_API int cof_genome_create(int device, cof_genome **out) {
+    if (!out) return fail(COF_E_BADINPUT, "null output handle");
+    *out = nullptr;
+    cof_genome *g = new (std::nothrow) cof_genome(device);
+    if (!g) return fail(COF_E_OOM, "out of host memory");
+    *out = g;
+    g_last_error.clear();
+    return COF_OK;
+}
+
+COF_API int cof_genome_add_chunk(cof_genome *g, const char *chr_name, const uint8_t *bit4,
+                                 uint64_t chunk_start, uint64_t chunk_end) {
+    if (!g || !chr_name || (!bit4 && chunk_end > chunk_start))
+        return fail(COF_E_BADINPUT, "null argument");
+    std::lock_guard<std::mutex> lk(g->mu);
+    if (g->engine.uploaded()) return fail(COF_E_STATE, "genome already uploaded");
+    cof::HostGenome &h = g->engine.host();
+    if (chunk_end == chunk_start) return COF_OK;  // empty chunks carry nothing
+    uint32_t name;
+    if (chunk_start != 0 && !h.name_idx.empty() && h.names[h.name_idx.back()] == chr_name)
+        name = h.name_idx.back();  // next chunk of the same record
+    else
+        name = h.add_name(chr_name, std::strlen(chr_name));
+    cof::Error err;
+    if (h.add_chunk(name, chunk_start, chunk_end, bit4, err)) return fail(err);
+    return COF_OK;
+}
+
+COF_API int cof_genome_load(cof_genome *g, const char *path) {
+    if (!g || !path) return fail(COF_E_BADINPUT, "null argument");
+    std::lock_guard<std::mutex> lk(g->mu);
+    if (g->engine.uploaded()) return fail(COF_E_STATE, "genome already uploaded");
+    cof::Error err;
+    if (cof::load_genome_path(g->engine.host(), path, err)) return fail(err);
+    return COF_OK;
+}
+
+COF_API int cof_genome_upload(cof_genome *g) {
+    if (!g) return fail(COF_E_BADINPUT, "null genome");
+    std::lock_guard<std::mutex> lk(g->mu);
+    cof::Error err;
+    if (g->engine.upload(err)) return fail(err);
+    return COF_OK;
+}
+
+COF_API uint64_t cof_genome_n_nucl(const cof_genome *g) {
+    return g ? g->engine.host().n_nucl() : 0;
+}
+
+COF_API uint64_t cof_genome_n_chunks(const cof_genome *g) {
+    return g ? g->engine.host().n_chunks() : 0;
+}
+
+COF_API void cof_genome_free(cof_genome *g) { delete g; }
+
+COF_API int cof_search_batch(cof_genome *g, const cof_request *reqs, size_t n_reqs,
+                             cof_result *outs) {
+    if (!g || (!reqs && n_reqs) || (!outs && n_reqs)) return fail(COF_E_BADINPUT, "null argument");
+    for (size_t i = 0; i < n_reqs; ++i) outs[i] = cof_result{nullptr, 0, 0, 0.0};
+    cof::Error err;
+    std::vector<cof::Request> rq;
+    if (to_requests(reqs, n_reqs, rq, err)) return fail(err);
+    std::vector<cof::Result> res;
+    std::lock_guard<std::mutex> lk(g->mu);
+    if (g->engine.search(rq, res, err)) return fail(err);
+    for (size_t i = 0; i < n_reqs; ++i) {
+        if (int rc = fill_result(res[i], &outs[i])) {
+            for (size_t j = 0; j < i; ++j) cof_result_free(&outs[j]);
+            return rc;
+        }
+    }
+    return COF_OK;
+}
+
+COF_API int cof_search(cof_genome *g, const cof_request *req, cof_result *out) {
+    return cof_search_batch(g, req, 1, out);
+}
+
+COF_API void cof_result_free(cof_result *r) {
+    if (!r) return;
+    std::free(r->text);
+    r->text = nullptr;
+    r->text_len = 0;
+    r->n_rows = 0;
+}
+
+// Stage timings of the last search on a genome (milliseconds / counts), for
+// benchmarking and profiling: scan, verify, format, d2h, total; PAM-passing
+// windows, window x pattern pairs, scan candidates, rows, kernel launches.
+// Not part of the reference interface.
+COF_API int cof_genome_last_stats(const cof_genome *g, double *ms5, uint64_t *counts5) {
+    if (!g || !ms5 || !counts5) return fail(COF_E_BADINPUT, "null argument");
+    const cof::StageTimes &t = g->engine.last_times();
+    ms5[0] = t.scan_ms;
+    ms5[1] = t.verify_ms;
+    ms5[2] = t.format_ms;
+    ms5[3] = t.d2h_ms;
+    ms5[4] = t.total_ms;
+    counts5[0] = t.candidates;
+    counts5[1] = t.pairs;
+    counts5[2] = t.raw_hits;
+    counts5[3] = t.rows;
+    counts5[4] = t.kernel_launches;
+    return COF_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,118 @@
+// cof_engine.h -- host-side engine of the B200 off-target search.
+//
+// Internal C++ interface shared by the C ABI (cabi.cpp), the command-line
+// front (cli.cpp) and the CUDA orchestration (engine.cu).
+#pragma once
+
+#include <cstddef>
+#include <cstdint>
+#include <string>
+#include <vector>
+
+namespace cof {
+
+constexpr uint32_t kChunkSize = 65536;           // chrom_chunk.rs:1
+constexpr uint32_t kChunkBytes = kChunkSize / 2;  // chrom_chunk.rs:2
+constexpr uint32_t kDefaultCps = 16384;          // search.rs:22 (GPU batch)
+constexpr uint32_t kMaxPatternLen = 32;          // one 32-bit word per plane
+
+// Status codes mirrored from include/cof.h.
+enum Status : int {
+    kOk = 0,
+    kBadInput = -1,
+    kOom = -2,
+    kCuda = -3,
+    kIo = -4,
+    kUnsupported = -5,
+    kState = -6,
+    kTimeout = -7,
+};
+
+struct Error {
+    int code = kOk;
+    std::string msg;
+};
+
+// bit4 one-hot code tables of cas-offinder-lib/src/bit4ops.rs:1-121.
+struct Bit4Tables {
+    uint8_t str2b4[2][256];  // [mixed_base][char]
+    char b4str[16];          // nibble -> uppercase IUPAC char (0 -> NUL)
+    Bit4Tables();
+};
+const Bit4Tables &bit4();
+inline uint8_t comp4(uint8_t v) { return (uint8_t)(((v << 2) | (v >> 2)) & 0xF); }
+char complement_char(char c);  // bit4ops.rs:211-221
+bool is_mixed_base(char c);    // bit4ops.rs:201-203
+
+// The chunk stream of the reference (ChromChunkInfo), tight-packed the way
+// chunks_to_searchchunk lays a search batch out (search.rs:1376-1427): chunk
+// k occupies bytes [boff[k], boff[k+1]) of `data`.
+struct HostGenome {
+    std::vector<std::string> names;
+    std::vector<uint32_t> name_idx;  // per chunk
+    std::vector<uint64_t> start, end, boff{0};
+    std::vector<uint8_t> data;
+    // staging for loaders
+    std::vector<uint8_t> cur;
+
+    size_t n_chunks() const { return start.size(); }
+    uint64_t n_nucl() const;
+    int add_chunk(uint32_t name, uint64_t cs, uint64_t ce, const uint8_t *bytes, Error &err);
+    uint32_t add_name(const char *s, size_t n);
+};
+
+// Genome loaders (read_fasta.rs, read_2bit.rs, read_fasta_folder.rs,
+// dispatch of main.rs:106-121).
+int load_genome_path(HostGenome &g, const std::string &path, Error &err);
+
+// One compiled search request.
+struct Request {
+    std::string filter;
+    std::vector<std::string> patterns;  // all patterns, fwd half then reverse half
+    uint32_t max_mm = 0, max_db = 0, max_rb = 0;
+    uint32_t cps = kDefaultCps;
+    uint64_t pam_len = 0;               // main.rs:80-91
+};
+// Validates a cof_request-like description and builds a Request.
+int make_request(const char *filter, size_t pattern_len, const char *const *patterns,
+                 size_t n_patterns, uint32_t mm, uint32_t db, uint32_t rb, uint32_t flags,
+                 uint32_t cps, Request &out, Error &err);
+
+struct Result {
+    std::string text;
+    uint64_t n_rows = 0;
+    double device_ms = 0;
+};
+
+// Per-stage device timings of the last search (milliseconds, CUDA events).
+struct StageTimes {
+    double scan_ms = 0, verify_ms = 0, format_ms = 0, d2h_ms = 0, total_ms = 0;
+    uint64_t candidates = 0, pairs = 0, raw_hits = 0, rows = 0, kernel_launches = 0;
+};
+
+class DeviceGenome;  // engine.cu
+
+// A genome bound to one GPU: host chunk stream + resident device copy.
+class Engine {
+  public:
+    explicit Engine(int device);
+    ~Engine();
+    Engine(const Engine &) = delete;
+    Engine &operator=(const Engine &) = delete;
+
+    HostGenome &host() { return host_; }
+    const HostGenome &host() const { return host_; }
+    bool uploaded() const { return dev_ != nullptr; }
+    int upload(Error &err);
+    int search(const std::vector<Request> &reqs, std::vector<Result> &out, Error &err);
+    const StageTimes &last_times() const { return times_; }
+    int device() const { return device_; }
+
+  private:
+    int device_;
+    HostGenome host_;
+    DeviceGenome *dev_ = nullptr;
+    StageTimes times_;
+};
+
+}  // namespace cof

@@ -1,0 +1,944 @@
+// engine.cu -- device side of the B200 off-target search (sm_100a).
+//
+// Data layout in HBM (resident per genome):
+//   bit4   : the reference's tight-packed chunk stream (two nucleotides per
+//            byte, one-hot T=1 C=2 A=4 G=8, N=0xF, IUPAC = union, 0 = pad),
+//            i.e. the concatenation of every search batch buffer
+//            (search.rs:1376-1427).  Used for exact verification, Myers/DP
+//            and site strings.
+//   planes : three bit planes per 32-nucleotide word, bit k = nucleotide
+//            32w+k: H and L (2-bit code A=00 C=01 G=10 T=11) and S (set when
+//            the nibble is not a single base: pad, N or IUPAC).  12 bytes per
+//            32 nt (0.375 B/nt).  Used by the PAM prefilter and the scan.
+//   chunk metadata (byte offset, record start/end, record name index) and
+//   the record names.
+//
+// Popcount path pipeline (db == rb == 0), one launch per stage:
+//   scan   : PAM prefilter on 32 window starts per lane from the planes,
+//            warp-ballot compaction of PAM-passing starts into a per-warp
+//            shared-memory queue, then every queued window x every pattern of
+//            the group: popc(((H^pH)|(L^pL)|S) & care) <= max_mm.  This is a
+//            superset of the reference's rows (see verify).
+//   verify : per candidate, the reference's exact decision: kernel popcount
+//            count with N masked to 0 (search.rs:378-463, :512-531), batch
+//            ownership and record-end drops (search.rs:540-546, :1428-1488),
+//            writer PAM filter and mismatch recount (main.rs:159-197).
+//   format : site strings with lowercase mismatches and the 8-column row text
+//            (main.rs:198-242), laid out by an exclusive scan of row lengths.
+#include <cub/cub.cuh>
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "cof_engine.h"
+
+namespace cof {
+
+// ---------------------------------------------------------------------------
+// error plumbing
+// ---------------------------------------------------------------------------
+
+#define CU(call)                                                                     \
+    do {                                                                             \
+        cudaError_t e_ = (call);                                                     \
+        if (e_ != cudaSuccess) {                                                     \
+            err = {e_ == cudaErrorMemoryAllocation ? kOom : kCuda,                   \
+                   std::string(#call) + ": " + cudaGetErrorString(e_)};              \
+            return err.code;                                                         \
+        }                                                                            \
+    } while (0)
+
+// ---------------------------------------------------------------------------
+// device structures
+// ---------------------------------------------------------------------------
+
+// One search batch of the reference (SearchChunkInfo, search.rs:57-90): the
+// chunks [first, first + nch) of the stream, starting at nucleotide `base`.
+struct BatchDev {
+    uint64_t base;         // global nucleotide index of the batch start
+    uint32_t valid;        // valid nucleotides (2 x tight-packed bytes)
+    uint32_t pad0;
+    uint32_t first;        // first chunk
+    uint32_t nch;          // chunks in the batch
+    uint32_t active_start; // Myers active start (search.rs:1087-1091)
+    uint32_t pad;
+};
+
+// PAM cell of a scan group: window cell index and allowed 2-bit codes as
+// full-word masks (all ones if the code is allowed).
+struct PamCell {
+    uint32_t cell, fa, fc, fg, ft;
+};
+
+constexpr int kMaxPamCells = 32;
+
+// One strand of one request: the windows whose non-N filter cells all hold
+// a single base of the filter's set are scanned against the patterns
+// [pat_begin, pat_end).
+struct ScanGroup {
+    uint32_t n_pam;
+    uint32_t pat_begin, pat_end;
+    uint32_t seg_begin, seg_end;  // scan segments of this group
+    uint32_t pad[3];
+    PamCell pam[kMaxPamCells];
+};
+
+// A contiguous range of window starts inside one batch.
+struct ScanSeg {
+    uint64_t lo, hi;        // global nucleotide range [lo, hi) of starts
+    uint64_t base;          // batch base
+    uint64_t w0;            // first plane word (lo / 32)
+    uint64_t tile_begin;    // prefix count of 1024-start tiles
+    uint32_t batch;
+    uint32_t pad;
+};
+
+// Scan-form pattern (window cells in bit positions 0..L-1).
+struct FastPattern {
+    uint32_t h, l, care;
+    int32_t k;  // max mismatches
+};
+
+// Exact-form pattern for verify / format.
+struct ExactPattern {
+    uint32_t request, strand, L, max_mm;
+    uint8_t b4[kMaxPatternLen];  // bit4 cells in scan orientation
+};
+
+struct RequestDev {
+    uint32_t L, max_mm, pam_len, first_pattern;
+    uint8_t fset[2][kMaxPatternLen];  // filter bit4 per strand, scan orientation
+    uint8_t fisn[2][kMaxPatternLen];  // filter char is N/n
+};
+
+struct Hit {
+    uint32_t s_local, pattern, batch, pad;
+};
+
+struct Row {
+    uint64_t s_global;   // window start
+    uint64_t clip;       // batch end (exclusive); cells at or past it read 0
+    uint64_t pos;        // chrom_idx (record coordinate)
+    uint32_t chunk;
+    uint32_t pattern;
+    uint32_t mm;
+    uint32_t pad;
+};
+
+struct Counters {
+    uint32_t hits;
+    uint32_t rows;
+    uint32_t overflow;
+    uint32_t pad;
+    unsigned long long candidates;
+    unsigned long long pairs;
+};
+
+__constant__ char c_b4str[16];
+
+__device__ __forceinline__ uint8_t nib(const uint8_t *__restrict__ g, uint64_t i) {
+    uint8_t b = __ldg(g + (i >> 1));
+    return (i & 1) ? (uint8_t)(b >> 4) : (uint8_t)(b & 0xF);
+}
+__device__ __forceinline__ uint8_t dcomp4(uint8_t v) {
+    return (uint8_t)(((v << 2) | (v >> 2)) & 0xF);
+}
+__device__ __forceinline__ bool single_base(uint8_t v) { return v && !(v & (v - 1)); }
+
+// ---------------------------------------------------------------------------
+// pack: bit4 stream -> H / L / S planes (one thread per 32 nt word)
+// ---------------------------------------------------------------------------
+
+__device__ __forceinline__ uint32_t gather_nibble_bit0(uint32_t v) {
+    // bits 0,4,...,28 -> bits 0..7
+    v &= 0x11111111u;
+    v = (v | (v >> 3)) & 0x03030303u;
+    v = (v | (v >> 6)) & 0x000F000Fu;
+    v = (v | (v >> 12)) & 0xFFu;
+    return v;
+}
+
+__global__ void pack_planes_kernel(const uint4 *__restrict__ bit4, uint64_t n_words,
+                                   uint32_t *__restrict__ H, uint32_t *__restrict__ L,
+                                   uint32_t *__restrict__ S) {
+    for (uint64_t w = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; w < n_words;
+         w += (uint64_t)gridDim.x * blockDim.x) {
+        uint4 q = bit4[w];
+        uint32_t x[4] = {q.x, q.y, q.z, q.w};
+        uint32_t h = 0, l = 0, s = 0;
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            uint32_t v = x[j];
+            uint32_t hb = (v >> 3) | v;                     // G or T
+            uint32_t lb = (v >> 1) | v;                     // C or T
+            uint32_t pc = v - ((v >> 1) & 0x55555555u);     // per-nibble popcount
+            pc = (pc & 0x33333333u) + ((pc >> 2) & 0x33333333u);
+            uint32_t t = pc ^ 0x11111111u;                  // zero nibble iff single base
+            uint32_t sb = t | (t >> 1) | (t >> 2);
+            h |= gather_nibble_bit0(hb) << (8 * j);
+            l |= gather_nibble_bit0(lb) << (8 * j);
+            s |= gather_nibble_bit0(sb) << (8 * j);
+        }
+        H[w] = h;
+        L[w] = l;
+        S[w] = s;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// scan: PAM prefilter + warp-queue compaction + popcount compare
+// ---------------------------------------------------------------------------
+
+constexpr int kScanWarps = 8;
+constexpr int kQCap = 256;             // flush threshold per warp queue
+constexpr int kQSlots = kQCap + 32;    // one drain step adds at most 32
+constexpr int kCpt = kQCap / 32;       // queued windows per lane in a flush
+constexpr int kSmemPatterns = 2048;    // patterns staged in shared memory
+constexpr int kMaxSegs = 64;
+
+struct ScanParams {
+    const uint32_t *H, *L, *S;
+    const ScanGroup *groups;
+    const ScanSeg *segs;
+    const FastPattern *pats;
+    Hit *hits;
+    uint32_t hit_cap;
+    Counters *ctr;
+};
+
+__device__ __forceinline__ void flush_queue(const uint4 *q, int n, const FastPattern *pt,
+                                            uint32_t pbeg, uint32_t npat, uint32_t batch,
+                                            const ScanParams &P, int lane) {
+    uint32_t ch[kCpt], cl[kCpt], cs[kCpt], sl[kCpt];
+#pragma unroll
+    for (int j = 0; j < kCpt; ++j) {
+        int idx = lane + 32 * j;
+        uint4 e = idx < n ? q[idx] : make_uint4(0xFFFFFFFFu, 0, 0, 0xFFFFFFFFu);
+        sl[j] = e.x;
+        ch[j] = e.y;
+        cl[j] = e.z;
+        cs[j] = e.w;
+    }
+    for (uint32_t p = 0; p < npat; ++p) {
+        FastPattern fp = pt[p];
+#pragma unroll
+        for (int j = 0; j < kCpt; ++j) {
+            uint32_t m = ((ch[j] ^ fp.h) | (cl[j] ^ fp.l) | cs[j]) & fp.care;
+            if ((int)__popc(m) <= fp.k) {
+                if (lane + 32 * j < n) {
+                    uint32_t i = atomicAdd(&P.ctr->hits, 1u);
+                    if (i < P.hit_cap) P.hits[i] = Hit{sl[j], pbeg + p, batch, 0};
+                    else P.ctr->overflow = 1;
+                }
+            }
+        }
+    }
+}
+
+__global__ void __launch_bounds__(kScanWarps * 32)
+scan_kernel(ScanParams P, uint64_t total_tiles_unused) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    uint4 *queues = reinterpret_cast<uint4 *>(smem_raw);
+    FastPattern *spat = reinterpret_cast<FastPattern *>(queues + kScanWarps * kQSlots);
+    __shared__ ScanGroup sg;
+    __shared__ ScanSeg ssegs[kMaxSegs];
+
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (threadIdx.x == 0) sg = P.groups[blockIdx.y];
+    __syncthreads();
+    const uint32_t nseg = sg.seg_end - sg.seg_begin;
+    for (uint32_t i = threadIdx.x; i < nseg; i += blockDim.x) ssegs[i] = P.segs[sg.seg_begin + i];
+    const uint32_t npat = sg.pat_end - sg.pat_begin;
+    const FastPattern *pt = P.pats + sg.pat_begin;
+    if (npat <= (uint32_t)kSmemPatterns) {
+        for (uint32_t i = threadIdx.x; i < npat; i += blockDim.x) spat[i] = pt[i];
+        pt = spat;
+    }
+    __syncthreads();
+    const uint64_t total_tiles = ssegs[nseg - 1].tile_begin +
+        ((ssegs[nseg - 1].hi - ssegs[nseg - 1].w0 * 32 + 1023) >> 10);
+
+    uint4 *q = queues + warp * kQSlots;
+    int qn = 0;
+    uint32_t qbatch = 0xFFFFFFFFu;
+    const uint32_t lt_mask = (1u << lane) - 1u;
+    unsigned long long ncand = 0;
+
+    const uint64_t gw = (uint64_t)blockIdx.x * kScanWarps + warp;
+    const uint64_t gstride = (uint64_t)gridDim.x * kScanWarps;
+    uint32_t sidx = 0;
+    for (uint64_t tile = gw; tile < total_tiles; tile += gstride) {
+        while (sidx + 1 < nseg && tile >= ssegs[sidx + 1].tile_begin) ++sidx;
+        const ScanSeg &sgm = ssegs[sidx];
+        if (sgm.batch != qbatch) {
+            if (qn) {
+                __syncwarp();
+                flush_queue(q, qn, pt, sg.pat_begin, npat, qbatch, P, lane);
+                __syncwarp();
+                qn = 0;
+            }
+            qbatch = sgm.batch;
+        }
+        const uint64_t w = sgm.w0 + (tile - sgm.tile_begin) * 32 + lane;
+        const uint32_t h0 = __ldg(P.H + w), h1 = __ldg(P.H + w + 1);
+        const uint32_t l0 = __ldg(P.L + w), l1 = __ldg(P.L + w + 1);
+        const uint32_t s0 = __ldg(P.S + w), s1 = __ldg(P.S + w + 1);
+        // window starts 32w + k in [lo, hi)
+        const uint64_t p0 = w * 32;
+        uint32_t m = 0xFFFFFFFFu;
+        if (p0 < sgm.lo) m = (sgm.lo - p0 >= 32) ? 0u : (m << (uint32_t)(sgm.lo - p0));
+        if (p0 + 32 > sgm.hi) m = (sgm.hi <= p0) ? 0u : (m & (0xFFFFFFFFu >> (uint32_t)(32 - (sgm.hi - p0))));
+        for (uint32_t c = 0; c < sg.n_pam && m; ++c) {
+            const PamCell pc = sg.pam[c];
+            const uint32_t h = __funnelshift_r(h0, h1, pc.cell);
+            const uint32_t l = __funnelshift_r(l0, l1, pc.cell);
+            const uint32_t s = __funnelshift_r(s0, s1, pc.cell);
+            const uint32_t t0 = (l & pc.fc) | (~l & pc.fa);
+            const uint32_t t1 = (l & pc.ft) | (~l & pc.fg);
+            m &= ((h & t1) | (~h & t0)) & ~s;
+        }
+        ncand += __popc(m);
+        // drain PAM-passing starts into the warp queue, one per lane per step
+        while (__any_sync(0xFFFFFFFFu, m)) {
+            const bool has = m != 0;
+            const uint32_t bal = __ballot_sync(0xFFFFFFFFu, has);
+            if (has) {
+                const uint32_t k = __ffs(m) - 1;
+                m &= m - 1;
+                const int slot = qn + __popc(bal & lt_mask);
+                q[slot] = make_uint4((uint32_t)(p0 + k - sgm.base), __funnelshift_r(h0, h1, k),
+                                     __funnelshift_r(l0, l1, k), __funnelshift_r(s0, s1, k));
+            }
+            qn += __popc(bal);
+            if (qn >= kQCap) {
+                __syncwarp();
+                flush_queue(q, qn, pt, sg.pat_begin, npat, qbatch, P, lane);
+                __syncwarp();
+                qn = 0;
+            }
+        }
+    }
+    if (qn) {
+        __syncwarp();
+        flush_queue(q, qn, pt, sg.pat_begin, npat, qbatch, P, lane);
+    }
+    // candidate count (for the roofline's algorithmic work)
+    for (int o = 16; o; o >>= 1) ncand += __shfl_down_sync(0xFFFFFFFFu, ncand, o);
+    if (lane == 0 && ncand) {
+        atomicAdd(&P.ctr->candidates, ncand);
+        atomicAdd(&P.ctr->pairs, ncand * (unsigned long long)npat);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// verify: the reference's exact decision per candidate hit
+// ---------------------------------------------------------------------------
+
+struct GenomeDev {
+    const uint8_t *bit4;
+    const uint64_t *boff, *start, *end;
+    const uint32_t *name_idx;
+    const char *names;
+    const uint32_t *name_off;
+    uint64_t n_chunks;
+};
+
+__global__ void verify_kernel(GenomeDev G, const BatchDev *__restrict__ batches,
+                              const ExactPattern *__restrict__ pats,
+                              const RequestDev *__restrict__ reqs, const Hit *__restrict__ hits,
+                              uint32_t n_hits, Row *__restrict__ rows, uint64_t *__restrict__ keys,
+                              uint32_t *__restrict__ vals, Counters *ctr,
+                              uint32_t *__restrict__ req_rows) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n_hits;
+         i += gridDim.x * blockDim.x) {
+        const Hit h = hits[i];
+        const BatchDev B = batches[h.batch];
+        const ExactPattern &P = pats[h.pattern];
+        const RequestDev &R = reqs[P.request];
+        const uint32_t L = P.L;
+        const uint64_t sg = B.base + h.s_local;
+        // search_chunk_cpu count on the N-masked batch buffer (zero past the
+        // batch's valid bytes)
+        uint8_t g[kMaxPatternLen];
+        int matches = 0;
+        for (uint32_t c = 0; c < L; ++c) {
+            uint8_t v = (h.s_local + c < B.valid) ? nib(G.bit4, sg + c) : 0;
+            if (v == 0xF) v = 0;
+            g[c] = v;
+            matches += __popc(v & P.b4[c]);
+        }
+        if ((int)L - matches > (int)R.max_mm) continue;
+        // convert_matches: owning chunk, record position, record-end drop
+        const uint64_t gbyte = sg >> 1;
+        uint32_t lo = B.first, hi = B.first + B.nch;  // boff[lo] <= gbyte < boff[hi]
+        while (hi - lo > 1) {
+            uint32_t mid = (lo + hi) >> 1;
+            if (G.boff[mid] <= gbyte) lo = mid; else hi = mid;
+        }
+        const uint32_t k = lo;
+        const uint64_t pos = G.start[k] + (sg - 2 * G.boff[k]);
+        const bool end_chrom = (k == B.first + B.nch - 1) || G.start[k + 1] == 0;
+        if (end_chrom && pos + L > G.end[k]) continue;
+        // writer: PAM filter and mismatch recount
+        const uint32_t st = P.strand;
+        uint32_t actual = 0;
+        bool pam_ok = true;
+        for (uint32_t c = 0; c < L; ++c) {
+            const bool sb = single_base(g[c]);
+            if (!R.fisn[st][c] && !(sb && (g[c] & R.fset[st][c]))) { pam_ok = false; break; }
+            if (P.b4[c] != 0xF && !(sb && (g[c] & P.b4[c]))) ++actual;
+        }
+        if (!pam_ok || actual > R.max_mm) continue;
+        const uint32_t r = atomicAdd(&ctr->rows, 1u);
+        rows[r] = Row{sg, B.base + B.valid, pos, k, h.pattern, actual, 0};
+        keys[r] = ((uint64_t)h.pattern << 34) | sg;
+        vals[r] = r;
+        atomicAdd(&req_rows[P.request], 1u);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// format: row lengths, then row text (main.rs:198-242)
+// ---------------------------------------------------------------------------
+
+__device__ __forceinline__ uint32_t ndigits(uint64_t v) {
+    uint32_t d = 1;
+    while (v >= 10) { v /= 10; ++d; }
+    return d;
+}
+__device__ __forceinline__ uint64_t pos_out(const Row &w, const RequestDev &R, uint32_t strand) {
+    uint64_t a = R.pam_len ? R.pam_len - 1 : 0;  // db == 0 on this path
+    return strand ? w.pos + a : w.pos;
+}
+
+__global__ void row_len_kernel(GenomeDev G, const Row *__restrict__ rows,
+                               const uint32_t *__restrict__ order, uint32_t n,
+                               const ExactPattern *__restrict__ pats,
+                               const RequestDev *__restrict__ reqs, uint32_t *__restrict__ len) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const Row w = rows[order[i]];
+        const ExactPattern &P = pats[w.pattern];
+        const RequestDev &R = reqs[P.request];
+        const uint32_t ni = G.name_idx[w.chunk];
+        const uint32_t name_len = G.name_off[ni + 1] - G.name_off[ni];
+        // "X\t" rna "\t" dna "\t" name "\t" pos "\t" dir "\t" mm "\t0\n"
+        len[i] = 2 + P.L + 1 + P.L + 1 + name_len + 1 + ndigits(pos_out(w, R, P.strand)) + 3 +
+                 ndigits(w.mm) + 3;
+    }
+}
+
+__device__ __forceinline__ char *put_u64(char *o, uint64_t v) {
+    char t[20];
+    int k = 0;
+    do { t[k++] = (char)('0' + v % 10); v /= 10; } while (v);
+    while (k) *o++ = t[--k];
+    return o;
+}
+
+__global__ void row_write_kernel(GenomeDev G, const Row *__restrict__ rows,
+                                 const uint32_t *__restrict__ order, uint32_t n,
+                                 const ExactPattern *__restrict__ pats,
+                                 const RequestDev *__restrict__ reqs,
+                                 const uint64_t *__restrict__ off, char *__restrict__ text) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const Row w = rows[order[i]];
+        const ExactPattern &P = pats[w.pattern];
+        const RequestDev &R = reqs[P.request];
+        const uint32_t L = P.L;
+        const bool fwd = P.strand == 0;
+        char *o = text + off[i];
+        *o++ = 'X';
+        *o++ = '\t';
+        char *rna = o;
+        char *dna = o + L + 1;
+        for (uint32_t c = 0; c < L; ++c) {
+            // output orientation: reverse strand strings are reverse complemented
+            const uint32_t sc = fwd ? c : L - 1 - c;
+            const uint64_t gi = w.s_global + sc;
+            uint8_t g = gi < w.clip ? nib(G.bit4, gi) : 0;
+            if (g == 0xF) g = 0;
+            uint8_t p = P.b4[sc];
+            if (!fwd) { g = dcomp4(g); p = dcomp4(p); }
+            rna[c] = c_b4str[p];
+            char d = c_b4str[g];
+            if (g == 0) d = (p == 0xF) ? 'N' : 'n';
+            else if (p == 0xF) {}
+            else if (!(single_base(g) && (g & p))) d = (char)(d | 0x20);
+            dna[c] = d;
+        }
+        o += L;
+        *o++ = '\t';
+        o += L;
+        *o++ = '\t';
+        const uint32_t ni = G.name_idx[w.chunk];
+        for (uint32_t c = G.name_off[ni]; c < G.name_off[ni + 1]; ++c) *o++ = G.names[c];
+        *o++ = '\t';
+        o = put_u64(o, pos_out(w, R, P.strand));
+        *o++ = '\t';
+        *o++ = fwd ? '+' : '-';
+        *o++ = '\t';
+        o = put_u64(o, w.mm);
+        *o++ = '\t';
+        *o++ = '0';
+        *o++ = '\n';
+    }
+}
+
+// ---------------------------------------------------------------------------
+// device genome + scratch
+// ---------------------------------------------------------------------------
+
+template <class T>
+struct DevBuf {
+    T *p = nullptr;
+    size_t cap = 0;
+    int ensure(size_t n, Error &err) {
+        if (n <= cap) return kOk;
+        if (p) cudaFree(p);
+        p = nullptr;
+        cap = 0;
+        size_t want = std::max<size_t>(n, 64);
+        CU(cudaMalloc((void **)&p, want * sizeof(T)));
+        cap = want;
+        return kOk;
+    }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        cap = 0;
+    }
+};
+
+class DeviceGenome {
+  public:
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev[8] = {};
+    int n_sm = 0;
+    DevBuf<uint8_t> bit4;
+    DevBuf<uint32_t> planes;
+    uint64_t n_words = 0;
+    DevBuf<uint64_t> boff, start, end;
+    DevBuf<uint32_t> name_idx, name_off;
+    DevBuf<char> names;
+    uint64_t n_chunks = 0;
+    // per-search scratch
+    DevBuf<unsigned char> tables;
+    DevBuf<Hit> hits;
+    DevBuf<Row> rows;
+    DevBuf<uint64_t> keys, keys2, offs;
+    DevBuf<uint32_t> vals, vals2, lens, req_rows;
+    DevBuf<Counters> ctr;
+    DevBuf<char> text;
+    DevBuf<unsigned char> cub_tmp;
+    char *h_text = nullptr;
+    size_t h_text_cap = 0;
+
+    ~DeviceGenome() {
+        bit4.release(); planes.release(); boff.release(); start.release(); end.release();
+        name_idx.release(); name_off.release(); names.release(); tables.release();
+        hits.release(); rows.release(); keys.release(); keys2.release(); offs.release();
+        vals.release(); vals2.release(); lens.release(); req_rows.release(); ctr.release();
+        text.release(); cub_tmp.release();
+        if (h_text) cudaFreeHost(h_text);
+        for (auto &e : ev)
+            if (e) cudaEventDestroy(e);
+        if (stream) cudaStreamDestroy(stream);
+    }
+    GenomeDev view() const {
+        return GenomeDev{bit4.p, boff.p, start.p, end.p, name_idx.p, names.p, name_off.p, n_chunks};
+    }
+};
+
+Engine::Engine(int device) : device_(device) {}
+Engine::~Engine() {
+    if (dev_) {
+        cudaSetDevice(device_);
+        delete dev_;
+    }
+}
+
+int Engine::upload(Error &err) {
+    if (dev_) return kOk;
+    CU(cudaSetDevice(device_));
+    std::unique_ptr<DeviceGenome> d(new DeviceGenome());
+    d->device = device_;
+    CU(cudaStreamCreateWithFlags(&d->stream, cudaStreamNonBlocking));
+    for (auto &e : d->ev) CU(cudaEventCreate(&e));
+    CU(cudaDeviceGetAttribute(&d->n_sm, cudaDevAttrMultiProcessorCount, device_));
+    CU(cudaMemcpyToSymbol(c_b4str, bit4().b4str, 16));  // per device context
+    const HostGenome &h = host_;
+    const uint64_t n_bytes = h.data.size();
+    const uint64_t n_nucl = 2 * n_bytes;
+    // 64 pad words (all non-single) so that a scan tile's last lanes and the
+    // funnel-shift neighbour word stay inside the planes
+    d->n_words = (n_nucl + 31) / 32 + 64;
+    if (d->bit4.ensure(d->n_words * 16 + 64, err)) return err.code;
+    CU(cudaMemsetAsync(d->bit4.p, 0, d->n_words * 16 + 64, d->stream));
+    if (n_bytes) CU(cudaMemcpyAsync(d->bit4.p, h.data.data(), n_bytes, cudaMemcpyHostToDevice, d->stream));
+    if (d->planes.ensure(3 * d->n_words, err)) return err.code;
+    {
+        int threads = 256;
+        uint64_t blocks = std::min<uint64_t>((d->n_words + threads - 1) / threads, 65535ull * 16);
+        pack_planes_kernel<<<(unsigned)std::max<uint64_t>(blocks, 1), threads, 0, d->stream>>>(
+            reinterpret_cast<const uint4 *>(d->bit4.p), d->n_words, d->planes.p,
+            d->planes.p + d->n_words, d->planes.p + 2 * d->n_words);
+        CU(cudaGetLastError());
+    }
+    const size_t nc = h.n_chunks();
+    d->n_chunks = nc;
+    if (d->boff.ensure(nc + 1, err) || d->start.ensure(nc + 1, err) ||
+        d->end.ensure(nc + 1, err) || d->name_idx.ensure(nc + 1, err))
+        return err.code;
+    std::vector<uint64_t> st(h.start), en(h.end);
+    st.push_back(0);  // sentinel: a record start after the last chunk
+    en.push_back(0);
+    std::vector<uint32_t> ni(h.name_idx);
+    ni.push_back(0);
+    CU(cudaMemcpyAsync(d->boff.p, h.boff.data(), (nc + 1) * 8, cudaMemcpyHostToDevice, d->stream));
+    CU(cudaMemcpyAsync(d->start.p, st.data(), (nc + 1) * 8, cudaMemcpyHostToDevice, d->stream));
+    CU(cudaMemcpyAsync(d->end.p, en.data(), (nc + 1) * 8, cudaMemcpyHostToDevice, d->stream));
+    CU(cudaMemcpyAsync(d->name_idx.p, ni.data(), (nc + 1) * 4, cudaMemcpyHostToDevice, d->stream));
+    std::vector<uint32_t> noff{0};
+    std::string all;
+    for (const auto &s : h.names) {
+        all += s;
+        noff.push_back((uint32_t)all.size());
+    }
+    if (d->names.ensure(all.size() + 1, err) || d->name_off.ensure(noff.size(), err)) return err.code;
+    if (!all.empty())
+        CU(cudaMemcpyAsync(d->names.p, all.data(), all.size(), cudaMemcpyHostToDevice, d->stream));
+    CU(cudaMemcpyAsync(d->name_off.p, noff.data(), noff.size() * 4, cudaMemcpyHostToDevice, d->stream));
+    CU(cudaStreamSynchronize(d->stream));
+    dev_ = d.release();
+    return kOk;
+}
+
+// ---------------------------------------------------------------------------
+// host orchestration
+// ---------------------------------------------------------------------------
+
+namespace {
+
+struct HostBatch {
+    size_t first, last;
+    bool has_head;
+};
+
+// Send thread of search.rs:1531-1572.
+std::vector<HostBatch> make_batches(size_t n_chunks, uint32_t cps) {
+    std::vector<HostBatch> out;
+    size_t bfirst = 0, blen = 0;
+    bool head = false;
+    for (size_t k = 0; k < n_chunks; ++k) {
+        if (blen == 0) bfirst = k;
+        ++blen;
+        if (blen == cps) {
+            out.push_back({bfirst, k, head});
+            bfirst = k;
+            blen = 1;
+            head = true;
+        }
+    }
+    if (blen && !(head && blen == 1)) out.push_back({bfirst, bfirst + blen - 1, head});
+    return out;
+}
+
+// Packs plain-old-data tables into one upload buffer.
+struct TablePack {
+    std::vector<unsigned char> buf;
+    template <class T>
+    size_t add(const std::vector<T> &v) {
+        size_t o = (buf.size() + 255) & ~size_t(255);
+        buf.resize(o + std::max<size_t>(v.size(), 1) * sizeof(T));
+        if (!v.empty()) std::memcpy(buf.data() + o, v.data(), v.size() * sizeof(T));
+        return o;
+    }
+};
+
+uint32_t code2(uint8_t b4) {  // single base one-hot -> 2-bit code A0 C1 G2 T3
+    switch (b4) {
+        case 4: return 0;
+        case 2: return 1;
+        case 8: return 2;
+        default: return 3;
+    }
+}
+
+}  // namespace
+
+int Engine::search(const std::vector<Request> &reqs, std::vector<Result> &out, Error &err) {
+    times_ = StageTimes();
+    out.assign(reqs.size(), Result());
+    if (reqs.empty()) return kOk;
+    for (const Request &r : reqs) {
+        if (r.max_db || r.max_rb) {
+            err = {kUnsupported, "bulge search is not available in this build"};
+            return err.code;
+        }
+        if (r.cps != reqs[0].cps) {
+            err = {kBadInput, "batched requests must share chunks_per_search"};
+            return err.code;
+        }
+    }
+    if (upload(err)) return err.code;
+    CU(cudaSetDevice(device_));
+    DeviceGenome &d = *dev_;
+    const HostGenome &h = host_;
+    const Bit4Tables &t = bit4();
+
+    // batches
+    const auto hb = make_batches(h.n_chunks(), reqs[0].cps);
+    std::vector<BatchDev> batches;
+    for (const HostBatch &b : hb) {
+        BatchDev x{};
+        x.base = 2 * h.boff[b.first];
+        x.valid = (uint32_t)(2 * (h.boff[b.last + 1] - h.boff[b.first]));
+        x.first = (uint32_t)b.first;
+        x.nch = (uint32_t)(b.last - b.first + 1);
+        const uint64_t c1 = b.has_head ? 2 * (h.boff[b.first + 1] - h.boff[b.first]) : 0;
+        x.active_start = (uint32_t)c1;
+        batches.push_back(x);
+    }
+
+    // requests -> groups, patterns, segments
+    std::vector<RequestDev> rdev;
+    std::vector<FastPattern> fpats;
+    std::vector<ExactPattern> epats;
+    std::vector<ScanGroup> groups;
+    std::vector<ScanSeg> segs;
+    std::vector<uint32_t> req_first_pat;
+    for (size_t ri = 0; ri < reqs.size(); ++ri) {
+        const Request &r = reqs[ri];
+        const uint32_t L = (uint32_t)r.filter.size();
+        RequestDev rd{};
+        rd.L = L;
+        rd.max_mm = r.max_mm;
+        rd.pam_len = (uint32_t)r.pam_len;
+        rd.first_pattern = (uint32_t)epats.size();
+        for (uint32_t c = 0; c < L; ++c) {
+            const char f = r.filter[c];
+            rd.fset[0][c] = t.str2b4[1][(uint8_t)f];
+            rd.fisn[0][c] = (f == 'N' || f == 'n');
+            const char fr = r.filter[L - 1 - c];
+            rd.fset[1][c] = comp4(t.str2b4[1][(uint8_t)fr]);
+            rd.fisn[1][c] = (fr == 'N' || fr == 'n');
+        }
+        rdev.push_back(rd);
+        req_first_pat.push_back((uint32_t)epats.size());
+        const size_t np = r.patterns.size(), nfwd = np / 2;
+        for (uint32_t strand = 0; strand < 2; ++strand) {
+            const size_t pb = strand ? nfwd : 0, pe = strand ? np : nfwd;
+            if (pb == pe) continue;
+            ScanGroup g{};
+            g.pat_begin = (uint32_t)fpats.size();
+            for (uint32_t c = 0; c < L; ++c) {
+                if (rd.fisn[strand][c]) continue;
+                if (g.n_pam == kMaxPamCells) break;
+                const uint8_t fs = rd.fset[strand][c];
+                PamCell pc{c, (fs & 4) ? ~0u : 0u, (fs & 2) ? ~0u : 0u, (fs & 8) ? ~0u : 0u,
+                           (fs & 1) ? ~0u : 0u};
+                g.pam[g.n_pam++] = pc;
+            }
+            for (size_t p = pb; p < pe; ++p) {
+                FastPattern fp{0, 0, 0, (int32_t)r.max_mm};
+                ExactPattern ep{};
+                ep.request = (uint32_t)ri;
+                ep.strand = strand;
+                ep.L = L;
+                ep.max_mm = r.max_mm;
+                for (uint32_t c = 0; c < L; ++c) {
+                    const uint8_t v = t.str2b4[1][(uint8_t)r.patterns[p][c]];
+                    ep.b4[c] = v;
+                    if (v && !(v & (v - 1))) {
+                        const uint32_t cd = code2(v);
+                        fp.care |= 1u << c;
+                        fp.h |= ((cd >> 1) & 1u) << c;
+                        fp.l |= (cd & 1u) << c;
+                    }
+                }
+                fpats.push_back(fp);
+                epats.push_back(ep);
+            }
+            g.pat_end = (uint32_t)fpats.size();
+            g.seg_begin = (uint32_t)segs.size();
+            uint64_t tiles = 0;
+            for (size_t bi = 0; bi < batches.size(); ++bi) {
+                const BatchDev &b = batches[bi];
+                // legacy_match_start_min_nucl (search.rs:540-546): starts in the
+                // head chunk that the previous batch already emitted
+                const uint64_t c1 = hb[bi].has_head ? b.active_start : 0;
+                const uint64_t msmin = c1 > L - 1 ? c1 - (L - 1) : 0;
+                ScanSeg s{};
+                s.lo = b.base + msmin;
+                s.hi = b.base + b.valid;
+                if (s.hi <= s.lo) continue;
+                s.base = b.base;
+                s.w0 = s.lo / 32;
+                s.tile_begin = tiles;
+                s.batch = (uint32_t)bi;
+                tiles += (s.hi - s.w0 * 32 + 1023) / 1024;
+                segs.push_back(s);
+            }
+            g.seg_end = (uint32_t)segs.size();
+            if (g.seg_end - g.seg_begin > (uint32_t)kMaxSegs) {
+                err = {kUnsupported, "too many search batches for one scan launch"};
+                return err.code;
+            }
+            if (g.seg_end > g.seg_begin) groups.push_back(g);
+        }
+    }
+
+    TablePack tp;
+    const size_t o_batch = tp.add(batches), o_rdev = tp.add(rdev), o_fp = tp.add(fpats),
+                 o_ep = tp.add(epats), o_grp = tp.add(groups), o_seg = tp.add(segs);
+    if (d.tables.ensure(tp.buf.size(), err)) return err.code;
+    cudaStream_t s = d.stream;
+    CU(cudaEventRecord(d.ev[0], s));
+    CU(cudaMemcpyAsync(d.tables.p, tp.buf.data(), tp.buf.size(), cudaMemcpyHostToDevice, s));
+    auto tab = [&](size_t o) { return (const void *)(d.tables.p + o); };
+    if (d.ctr.ensure(1, err) || d.req_rows.ensure(reqs.size(), err)) return err.code;
+    if (d.hits.cap == 0 && d.hits.ensure(1u << 22, err)) return err.code;
+
+    Counters hc{};
+    if (!groups.empty()) {
+        for (int attempt = 0; attempt < 2; ++attempt) {
+            CU(cudaMemsetAsync(d.ctr.p, 0, sizeof(Counters), s));
+            ScanParams sp;
+            sp.H = d.planes.p;
+            sp.L = d.planes.p + d.n_words;
+            sp.S = d.planes.p + 2 * d.n_words;
+            sp.groups = (const ScanGroup *)tab(o_grp);
+            sp.segs = (const ScanSeg *)tab(o_seg);
+            sp.pats = (const FastPattern *)tab(o_fp);
+            sp.hits = d.hits.p;
+            sp.hit_cap = (uint32_t)std::min<size_t>(d.hits.cap, 0xFFFFFFF0u);
+            sp.ctr = d.ctr.p;
+            const size_t smem = kScanWarps * kQSlots * sizeof(uint4) + kSmemPatterns * sizeof(FastPattern);
+            CU(cudaFuncSetAttribute(scan_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+            int occ = 0;
+            CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, scan_kernel, kScanWarps * 32, smem));
+            occ = std::max(occ, 1);
+            unsigned gx = (unsigned)std::max<int>(1, (d.n_sm * occ) / (int)groups.size());
+            CU(cudaEventRecord(d.ev[1], s));
+            scan_kernel<<<dim3(gx, (unsigned)groups.size()), kScanWarps * 32, smem, s>>>(sp, 0);
+            CU(cudaGetLastError());
+            CU(cudaEventRecord(d.ev[2], s));
+            ++times_.kernel_launches;
+            CU(cudaMemcpyAsync(&hc, d.ctr.p, sizeof(Counters), cudaMemcpyDeviceToHost, s));
+            CU(cudaStreamSynchronize(s));
+            if (!hc.overflow && hc.hits <= d.hits.cap) break;
+            if (attempt == 1) {
+                err = {kOom, "candidate buffer overflow after resize"};
+                return err.code;
+            }
+            if (d.hits.ensure((size_t)hc.hits + hc.hits / 4 + 1024, err)) return err.code;
+        }
+    } else {
+        CU(cudaEventRecord(d.ev[1], s));
+        CU(cudaEventRecord(d.ev[2], s));
+    }
+    times_.raw_hits = hc.hits;
+    times_.candidates = hc.candidates;
+    times_.pairs = hc.pairs;
+
+    // verify
+    const uint32_t n_hits = hc.hits;
+    if (d.rows.ensure(n_hits + 1, err) || d.keys.ensure(n_hits + 1, err) ||
+        d.keys2.ensure(n_hits + 1, err) || d.vals.ensure(n_hits + 1, err) ||
+        d.vals2.ensure(n_hits + 1, err))
+        return err.code;
+    CU(cudaMemsetAsync(d.req_rows.p, 0, reqs.size() * 4, s));
+    if (n_hits) {
+        unsigned vb = (unsigned)std::min<uint64_t>((n_hits + 255) / 256, (uint64_t)d.n_sm * 8);
+        verify_kernel<<<vb, 256, 0, s>>>(d.view(), (const BatchDev *)tab(o_batch),
+                                         (const ExactPattern *)tab(o_ep),
+                                         (const RequestDev *)tab(o_rdev), d.hits.p, n_hits,
+                                         d.rows.p, d.keys.p, d.vals.p, d.ctr.p, d.req_rows.p);
+        CU(cudaGetLastError());
+        ++times_.kernel_launches;
+    }
+    CU(cudaEventRecord(d.ev[3], s));
+    CU(cudaMemcpyAsync(&hc, d.ctr.p, sizeof(Counters), cudaMemcpyDeviceToHost, s));
+    std::vector<uint32_t> req_rows(reqs.size());
+    CU(cudaMemcpyAsync(req_rows.data(), d.req_rows.p, reqs.size() * 4, cudaMemcpyDeviceToHost, s));
+    CU(cudaStreamSynchronize(s));
+    const uint32_t n_rows = hc.rows;
+    times_.rows = n_rows;
+
+    // sort rows by (pattern, position), then lay out the text
+    const uint32_t *order = d.vals.p;
+    uint64_t text_bytes = 0;
+    if (n_rows) {
+        size_t tmp = 0;
+        CU(cub::DeviceRadixSort::SortPairs(nullptr, tmp, d.keys.p, d.keys2.p, d.vals.p, d.vals2.p,
+                                           (int)n_rows, 0, 64, s));
+        size_t tmp2 = 0;
+        CU(cub::DeviceScan::ExclusiveSum(nullptr, tmp2, d.lens.p, d.offs.p, (int)n_rows + 1, s));
+        if (d.cub_tmp.ensure(std::max(tmp, tmp2), err)) return err.code;
+        tmp = d.cub_tmp.cap;
+        CU(cub::DeviceRadixSort::SortPairs(d.cub_tmp.p, tmp, d.keys.p, d.keys2.p, d.vals.p,
+                                           d.vals2.p, (int)n_rows, 0, 64, s));
+        order = d.vals2.p;
+        if (d.lens.ensure(n_rows + 1, err) || d.offs.ensure(n_rows + 1, err)) return err.code;
+        unsigned fb = (unsigned)std::min<uint64_t>((n_rows + 255) / 256, (uint64_t)d.n_sm * 8);
+        row_len_kernel<<<fb, 256, 0, s>>>(d.view(), d.rows.p, order, n_rows,
+                                          (const ExactPattern *)tab(o_ep),
+                                          (const RequestDev *)tab(o_rdev), d.lens.p);
+        CU(cudaGetLastError());
+        CU(cudaMemsetAsync(d.lens.p + n_rows, 0, 4, s));
+        // widen lengths to 64-bit offsets
+        tmp2 = d.cub_tmp.cap;
+        CU(cub::DeviceScan::ExclusiveSum(d.cub_tmp.p, tmp2, d.lens.p, d.offs.p, (int)n_rows + 1, s));
+        CU(cudaMemcpyAsync(&text_bytes, d.offs.p + n_rows, 8, cudaMemcpyDeviceToHost, s));
+        CU(cudaStreamSynchronize(s));
+        if (d.text.ensure(text_bytes + 1, err)) return err.code;
+        row_write_kernel<<<fb, 256, 0, s>>>(d.view(), d.rows.p, order, n_rows,
+                                            (const ExactPattern *)tab(o_ep),
+                                            (const RequestDev *)tab(o_rdev), d.offs.p, d.text.p);
+        CU(cudaGetLastError());
+        times_.kernel_launches += 4;
+    }
+    CU(cudaEventRecord(d.ev[4], s));
+    if (text_bytes > d.h_text_cap) {
+        if (d.h_text) cudaFreeHost(d.h_text);
+        d.h_text = nullptr;
+        d.h_text_cap = 0;
+        CU(cudaMallocHost((void **)&d.h_text, text_bytes));
+        d.h_text_cap = text_bytes;
+    }
+    if (text_bytes) CU(cudaMemcpyAsync(d.h_text, d.text.p, text_bytes, cudaMemcpyDeviceToHost, s));
+    CU(cudaEventRecord(d.ev[5], s));
+    CU(cudaStreamSynchronize(s));
+
+    // split the text per request (rows are sorted request-major)
+    uint64_t r0 = 0, t0 = 0;
+    for (size_t ri = 0; ri < reqs.size(); ++ri) {
+        const uint64_t r1 = r0 + req_rows[ri];
+        uint64_t t1 = text_bytes;
+        if (r1 < n_rows) CU(cudaMemcpy(&t1, d.offs.p + r1, 8, cudaMemcpyDeviceToHost));
+        out[ri].n_rows = req_rows[ri];
+        if (t1 > t0) out[ri].text.assign(d.h_text + t0, d.h_text + t1);
+        r0 = r1;
+        t0 = t1;
+    }
+    float ms;
+    cudaEventElapsedTime(&ms, d.ev[1], d.ev[2]);
+    times_.scan_ms = ms;
+    cudaEventElapsedTime(&ms, d.ev[2], d.ev[3]);
+    times_.verify_ms = ms;
+    cudaEventElapsedTime(&ms, d.ev[3], d.ev[4]);
+    times_.format_ms = ms;
+    cudaEventElapsedTime(&ms, d.ev[4], d.ev[5]);
+    times_.d2h_ms = ms;
+    cudaEventElapsedTime(&ms, d.ev[0], d.ev[5]);
+    times_.total_ms = ms;
+    for (auto &r : out) r.device_ms = times_.total_ms;
+    return kOk;
+}
+
+}  // namespace cof

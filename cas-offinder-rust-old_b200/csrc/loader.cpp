@@ -1,0 +1,373 @@
+// loader.cpp -- genome loaders and request compiler (host side).
+//
+// Produces the reference's ChromChunkInfo stream (64 Knt chunks of bit4
+// one-hot nibbles) tight-packed into one byte stream, which is the layout the
+// device keeps resident.  Semantics follow:
+//   read_fasta        cas-offinder-lib/src/read_fasta.rs:9-71
+//   read_2bit         cas-offinder-lib/src/read_2bit.rs:33-118
+//   read_fasta_folder cas-offinder-lib/src/read_fasta_folder.rs:8-23
+//   path dispatch     cas-offinder-cli/src/main.rs:106-121
+#include <dirent.h>
+#include <sys/stat.h>
+
+#include <algorithm>
+#include <cerrno>
+#include <cstdio>
+#include <cstring>
+
+#include "cof_engine.h"
+
+namespace cof {
+
+Bit4Tables::Bit4Tables() {
+    // makebit4map / apply_lower (bit4ops.rs:17-47)
+    for (int mixed = 0; mixed < 2; ++mixed) {
+        uint8_t up[256] = {0};
+        up['G'] = 8; up['C'] = 2; up['A'] = 4; up['T'] = 1;
+        if (mixed) {
+            up['R'] = 12; up['Y'] = 3; up['S'] = 10; up['W'] = 5; up['K'] = 9;
+            up['M'] = 6; up['B'] = 11; up['D'] = 13; up['H'] = 7; up['V'] = 14;
+            up['N'] = 15;
+        }
+        std::memset(str2b4[mixed], 0, 256);
+        for (int i = 1; i <= 26; ++i) {
+            str2b4[mixed][64 + i] = up[64 + i];
+            str2b4[mixed][96 + i] = up[64 + i];
+        }
+    }
+    // invert_chrmap (bit4ops.rs:48-59): lowest character code wins
+    std::memset(b4str, 0, sizeof b4str);
+    for (int c = 255; c >= 0; --c)
+        if (str2b4[1][c]) b4str[str2b4[1][c]] = (char)c;
+}
+
+const Bit4Tables &bit4() {
+    static const Bit4Tables t;
+    return t;
+}
+
+char complement_char(char c) {
+    const Bit4Tables &t = bit4();
+    uint8_t v = t.str2b4[1][(uint8_t)c];
+    char out = v ? t.b4str[comp4(v)] : c;
+    return (char)(out | (c & 0x20));
+}
+
+bool is_mixed_base(char c) { return bit4().str2b4[1][(uint8_t)c] != 0; }
+
+uint64_t HostGenome::n_nucl() const {
+    uint64_t s = 0;
+    for (size_t k = 0; k < start.size(); ++k) s += end[k] - start[k];
+    return s;
+}
+
+uint32_t HostGenome::add_name(const char *s, size_t n) {
+    names.emplace_back(s, n);
+    return (uint32_t)(names.size() - 1);
+}
+
+int HostGenome::add_chunk(uint32_t name, uint64_t cs, uint64_t ce, const uint8_t *bytes,
+                          Error &err) {
+    if (ce < cs || ce - cs > kChunkSize) {
+        err = {kBadInput, "chunk must hold 0..65536 nucleotides"};
+        return err.code;
+    }
+    if (!start.empty() && cs != 0 && end.back() != cs) {
+        // search.rs:1396-1399
+        err = {kBadInput, "search expects chromosome chunks to arrive in order"};
+        return err.code;
+    }
+    size_t nb = (size_t)((ce - cs + 1) / 2);
+    name_idx.push_back(name);
+    start.push_back(cs);
+    end.push_back(ce);
+    data.insert(data.end(), bytes, bytes + nb);
+    boff.push_back(data.size());
+    return kOk;
+}
+
+namespace {
+
+struct File {
+    FILE *f = nullptr;
+    ~File() {
+        if (f) std::fclose(f);
+    }
+};
+
+// Reads a whole file.
+int slurp(const std::string &path, std::vector<char> &buf, Error &err) {
+    File fh;
+    fh.f = std::fopen(path.c_str(), "rb");
+    if (!fh.f) {
+        err = {kIo, "cannot open " + path + ": " + std::strerror(errno)};
+        return err.code;
+    }
+    std::fseek(fh.f, 0, SEEK_END);
+    long sz = std::ftell(fh.f);
+    std::fseek(fh.f, 0, SEEK_SET);
+    if (sz < 0) {
+        err = {kIo, "cannot size " + path};
+        return err.code;
+    }
+    buf.resize((size_t)sz);
+    if (sz && std::fread(buf.data(), 1, (size_t)sz, fh.f) != (size_t)sz) {
+        err = {kIo, "short read on " + path};
+        return err.code;
+    }
+    return kOk;
+}
+
+// read_fasta.rs:9-71 over an in-memory file.  Lines end at '\n' with one
+// preceding '\r' dropped (BufRead::lines).  Genome characters use the mixed
+// base map (N -> 0xF, IUPAC -> union, anything else -> 0).
+int parse_fasta(HostGenome &g, const std::vector<char> &buf, Error &err) {
+    const Bit4Tables &t = bit4();
+    const uint8_t *m = t.str2b4[1];
+    const char *p = buf.data(), *e = p + buf.size();
+    bool started = false, have_name = false;
+    uint32_t name = 0;
+    uint64_t cs = 0, ce = 0;
+    std::vector<uint8_t> &cur = g.cur;
+    cur.assign(kChunkBytes, 0);
+    while (p < e) {
+        const char *nl = (const char *)std::memchr(p, '\n', (size_t)(e - p));
+        const char *le = nl ? nl : e;
+        size_t len = (size_t)(le - p);
+        if (nl && len && p[len - 1] == '\r') --len;
+        if (len >= 1 && p[0] == '>') {
+            if (ce != cs && g.add_chunk(name, cs, ce, cur.data(), err)) return err.code;
+            name = g.add_name(p + 1, len - 1);
+            have_name = len > 1;
+            cs = ce = 0;
+            std::fill(cur.begin(), cur.end(), 0);
+            started = true;
+        } else {
+            if (!started) {
+                err = {kBadInput, "fasta file needs to start with >"};
+                return err.code;
+            }
+            if (!have_name) {
+                err = {kBadInput, "> must be followed by chromosome name"};
+                return err.code;
+            }
+            if (len + (size_t)(ce - cs) > kChunkSize) {
+                if (g.add_chunk(name, cs, ce, cur.data(), err)) return err.code;
+                cs = ce;
+                std::fill(cur.begin(), cur.end(), 0);
+            }
+            if (len > kChunkSize) {
+                err = {kBadInput, "line in fasta too long"};
+                return err.code;
+            }
+            size_t o = (size_t)(ce - cs);
+            const uint8_t *s = (const uint8_t *)p;
+            size_t i = 0;
+            if (o & 1) {
+                if (len) cur[o >> 1] |= (uint8_t)(m[s[0]] << 4);
+                i = 1;
+            }
+            for (; i + 1 < len; i += 2)
+                cur[(o + i) >> 1] = (uint8_t)(m[s[i]] | (m[s[i + 1]] << 4));
+            if (i < len) cur[(o + i) >> 1] |= m[s[i]];
+            ce += len;
+        }
+        p = nl ? nl + 1 : e;
+    }
+    if (ce > cs && g.add_chunk(name, cs, ce, cur.data(), err)) return err.code;
+    return kOk;
+}
+
+uint32_t rd32(const std::vector<char> &b, size_t &o, bool &ok) {
+    if (o + 4 > b.size()) {
+        ok = false;
+        return 0;
+    }
+    uint32_t v;
+    std::memcpy(&v, b.data() + o, 4);
+    o += 4;
+    return v;
+}
+
+// read_2bit.rs:33-118.  Sequences are taken one after the other in index
+// order (the stored offsets are skipped, as the reference does).
+int parse_2bit(HostGenome &g, const std::vector<char> &b, Error &err) {
+    bool ok = true;
+    size_t o = 0;
+    auto trunc = [&]() {
+        err = {kBadInput, "truncated .2bit file"};
+        return err.code;
+    };
+    if (rd32(b, o, ok) != 0x1A412743u || !ok) {
+        err = {kBadInput, ".2bit file badly formatted header"};
+        return err.code;
+    }
+    if (rd32(b, o, ok) != 0 || !ok) {
+        err = {kBadInput, "only supports version 0 of .2bit format"};
+        return err.code;
+    }
+    uint32_t cnt = rd32(b, o, ok);
+    o += 4;
+    if (!ok) return trunc();
+    std::vector<uint32_t> names(cnt);
+    for (uint32_t i = 0; i < cnt; ++i) {
+        if (o + 1 > b.size()) return trunc();
+        uint8_t nl = (uint8_t)b[o++];
+        if (o + nl + 4 > b.size()) return trunc();
+        names[i] = g.add_name(b.data() + o, nl);
+        o += nl + 4;
+    }
+    // BIT2_TO_BIT4 (bit4ops.rs:60-75): codes T=0 C=1 A=2 G=3, first base in
+    // the high bits of each byte.
+    uint16_t b2b4[256];
+    for (int i = 0; i < 256; ++i) {
+        uint16_t v = 0;
+        for (int j = 0; j < 4; ++j) v |= (uint16_t)((1u << ((i >> ((3 - j) * 2)) & 3)) << (4 * j));
+        b2b4[i] = v;
+    }
+    std::vector<uint8_t> &cur = g.cur;
+    cur.assign(kChunkBytes, 0);
+    for (uint32_t s = 0; s < cnt; ++s) {
+        uint32_t chrlen = rd32(b, o, ok);
+        uint32_t nbc = rd32(b, o, ok);
+        if (!ok) return trunc();
+        std::vector<std::pair<uint32_t, uint32_t>> nb(nbc);
+        for (uint32_t i = 0; i < nbc; ++i) nb[i].first = rd32(b, o, ok);
+        for (uint32_t i = 0; i < nbc; ++i) nb[i].second = rd32(b, o, ok);
+        if (!ok) return trunc();
+        std::stable_sort(nb.begin(), nb.end(),
+                         [](const std::pair<uint32_t, uint32_t> &x,
+                            const std::pair<uint32_t, uint32_t> &y) { return x.first < y.first; });
+        uint32_t mbc = rd32(b, o, ok);
+        if (!ok) return trunc();
+        o += (uint32_t)(mbc * 8u + 4u);
+        size_t pos = 0;
+        int64_t bmi = 0;
+        while (pos < chrlen) {
+            size_t rs = std::min<size_t>(chrlen - pos, kChunkSize);
+            size_t nbytes = (rs + 3) / 4;
+            if (o + nbytes > b.size()) return trunc();
+            const uint8_t *raw = (const uint8_t *)b.data() + o;
+            o += nbytes;
+            std::fill(cur.begin(), cur.end(), 0);
+            for (size_t i = 0; i < nbytes; ++i) {
+                uint16_t v = b2b4[raw[i]];
+                cur[2 * i] = (uint8_t)v;
+                cur[2 * i + 1] = (uint8_t)(v >> 8);
+            }
+            auto setn = [&](size_t a, size_t z, uint8_t v) {  // memsetbit4
+                for (size_t i = a; i < z; ++i) {
+                    if (i & 1) cur[i >> 1] = (uint8_t)((cur[i >> 1] & 0x0F) | (v << 4));
+                    else cur[i >> 1] = (uint8_t)((cur[i >> 1] & 0xF0) | v);
+                }
+            };
+            if (rs % 4) setn(rs, nbytes * 4, 0);
+            bmi = std::max<int64_t>(bmi - 1, 0);
+            while (bmi < (int64_t)nbc) {
+                int64_t bs = (int64_t)nb[bmi].first - (int64_t)pos;
+                int64_t be = (int64_t)(uint32_t)(nb[bmi].first + nb[bmi].second) - (int64_t)pos;
+                if (bs > (int64_t)rs) break;
+                int64_t a = std::max<int64_t>(bs, 0);
+                int64_t z = std::min<int64_t>(std::max<int64_t>(be, 0), (int64_t)rs);
+                if (a < z) setn((size_t)a, (size_t)z, 0xF);
+                ++bmi;
+            }
+            if (g.add_chunk(names[s], pos, pos + rs, cur.data(), err)) return err.code;
+            pos += rs;
+        }
+    }
+    return kOk;
+}
+
+}  // namespace
+
+int load_genome_path(HostGenome &g, const std::string &path, Error &err) {
+    struct stat st;
+    if (::stat(path.c_str(), &st)) {
+        err = {kIo, "cannot stat " + path};
+        return err.code;
+    }
+    std::vector<char> buf;
+    if (S_ISDIR(st.st_mode)) {
+        DIR *d = ::opendir(path.c_str());
+        if (!d) {
+            err = {kIo, "cannot open folder " + path};
+            return err.code;
+        }
+        int rc = kOk;
+        while (struct dirent *e = ::readdir(d)) {
+            std::string nm = e->d_name;
+            if (nm == "." || nm == "..") continue;
+            std::string p = path;
+            if (p.empty() || p.back() != '/') p += '/';
+            p += nm;
+            struct stat fs;
+            if (::stat(p.c_str(), &fs) || !S_ISREG(fs.st_mode)) continue;
+            if (p.size() >= 3 && p.compare(p.size() - 3, 3, ".fa") == 0) {
+                if ((rc = slurp(p, buf, err))) break;
+                if ((rc = parse_fasta(g, buf, err))) break;
+            }
+        }
+        ::closedir(d);
+        return rc;
+    }
+    if (int rc = slurp(path, buf, err)) return rc;
+    if (buf.empty()) {
+        err = {kIo, "cannot read " + path};
+        return err.code;
+    }
+    return buf[0] == '>' ? parse_fasta(g, buf, err) : parse_2bit(g, buf, err);
+}
+
+int make_request(const char *filter, size_t pattern_len, const char *const *patterns,
+                 size_t n_patterns, uint32_t mm, uint32_t db, uint32_t rb, uint32_t flags,
+                 uint32_t cps, Request &out, Error &err) {
+    auto bad = [&](const std::string &m, int code = kBadInput) {
+        err = {code, m};
+        return code;
+    };
+    if (!filter || !patterns || n_patterns == 0) return bad("no patterns");  // search.rs:1502
+    if (std::strlen(filter) != pattern_len) return bad("search filter length != pattern_len");
+    if (pattern_len == 0) return bad("empty pattern");
+    for (size_t i = 0; i < pattern_len; ++i)
+        if (!is_mixed_base(filter[i])) return bad("search filter must be a mixed base string");
+    out = Request();
+    out.filter = filter;
+    out.max_mm = mm;
+    out.max_db = db;
+    out.max_rb = rb;
+    out.cps = cps ? cps : kDefaultCps;
+    if (out.cps < 2) return bad("chunks_per_search must be >= 2");
+    for (size_t i = 0; i < n_patterns; ++i) {
+        if (!patterns[i]) return bad("null pattern");
+        std::string p = patterns[i];
+        if (p.size() != pattern_len) return bad("All patterns must have same length");  // :1503-1507
+        for (char c : p)
+            if (!is_mixed_base(c)) return bad("pattern must be a mixed base string");
+        out.patterns.push_back(p);
+    }
+    if (flags & 1u) {  // COF_F_ADD_REVCOMP: main.rs:253-259
+        for (size_t i = 0; i < n_patterns; ++i) {
+            std::string r = out.patterns[i];
+            for (char &c : r) c = complement_char(c);
+            std::reverse(r.begin(), r.end());
+            out.patterns.push_back(r);
+        }
+    }
+    for (size_t i = pattern_len; i > 0; --i) {  // main.rs:80-91
+        char c = out.patterns[0][i - 1];
+        if (c == 'N' || c == 'n') ++out.pam_len;
+        else break;
+    }
+    if (pattern_len > kMaxPatternLen)
+        return bad("pattern length above 32 is not supported by this build", kUnsupported);
+    bool myers = db > 0 || rb > 0;
+    if (!myers && mm >= pattern_len)
+        return bad("max_mismatches must be below the pattern length");
+    if (myers && (db > 8 || rb > 8 || mm + db + rb > 30))
+        return bad("bulge / edit limits above 8 bulges or 30 edits are not supported",
+                   kUnsupported);
+    return kOk;
+}
+
+}  // namespace cof

@@ -1,0 +1,153 @@
+/*
+ * cof.h -- C ABI of the B200 off-target search engine (libcof.so).
+ *
+ * This is the drop-in boundary for cas-offinder-rust's search path.  The
+ * Rust entry point it replaces is
+ *
+ *   pub fn search(devices: OclRunConfig, max_mismatches: u32,
+ *                 max_dna_bulges: u32, max_rna_bulges: u32,
+ *                 search_filter_ascii: &[u8], pattern_len: usize,
+ *                 patterns_ascii: &Vec<Vec<u8>>,
+ *                 recv: mpsc::Receiver<ChromChunkInfo>,
+ *                 dest: mpsc::SyncSender<Vec<Match>>)
+ *   (cas-offinder-lib/src/search.rs:1490-1500)
+ *
+ * together with the writer thread that turns its Match stream into the
+ * cas-offinder 2.5 / cas-offinder-bulge 8-column rows
+ * (cas-offinder-cli/src/main.rs:122-247).  The ChromChunkInfo channel becomes
+ * a genome handle that is filled once (chunk by chunk, or from a FASTA/.2bit
+ * path) and then stays resident in HBM across searches.
+ *
+ * Every function returns COF_OK (0) or a negative status; the message of the
+ * last failure on the calling thread is available from cof_last_error().  No
+ * call aborts the process.  One genome handle drives one GPU; calls on the
+ * same handle are serialised internally.
+ */
+#ifndef COF_H
+#define COF_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define COF_API __attribute__((visibility("default")))
+#else
+#define COF_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes.  The reference panics on these conditions
+ * (search.rs:1502-1507 asserts, :1617 and :1655 CUDA errors, loader
+ * CliError unwraps in main.rs:106-121). */
+#define COF_OK 0
+#define COF_E_BADINPUT (-1)    /* invalid request, pattern or genome file  */
+#define COF_E_OOM (-2)         /* device or host allocation failed         */
+#define COF_E_CUDA (-3)        /* CUDA runtime error                       */
+#define COF_E_IO (-4)          /* genome file could not be read            */
+#define COF_E_UNSUPPORTED (-5) /* valid input outside this build's limits  */
+#define COF_E_STATE (-6)       /* call order (e.g. add_chunk after upload) */
+#define COF_E_TIMEOUT (-7)     /* a bounded device wait gave up            */
+
+/* Request flags. */
+#define COF_F_ADD_REVCOMP 1u   /* patterns are user patterns; append their
+                                  reverse complements as main.rs:253-259 does */
+
+typedef struct cof_genome cof_genome;
+
+/* Creates an empty genome bound to CUDA device `device`.
+ * Replaces the Receiver<ChromChunkInfo> side of search.rs:1498. */
+COF_API int cof_genome_create(int device, cof_genome **out);
+
+/* Appends one chunk, in stream order.  Fields of ChromChunkInfo
+ * (cas-offinder-lib/src/chrom_chunk.rs:4-16): the record name, the bit4
+ * one-hot data (two nucleotides per byte, even index in the low nibble,
+ * ceil((chunk_end - chunk_start) / 2) bytes), and the nucleotide range
+ * [chunk_start, chunk_end) within the record; chunk_start == 0 starts a new
+ * record.  At most 65536 nucleotides per chunk. */
+COF_API int cof_genome_add_chunk(cof_genome *g, const char *chr_name,
+                                 const uint8_t *bit4, uint64_t chunk_start,
+                                 uint64_t chunk_end);
+
+/* Loads a genome path the way cas-offinder-cli/src/main.rs:106-121 does:
+ * a directory -> read_fasta_folder, first byte '>' -> read_fasta, otherwise
+ * read_2bit (cas-offinder-lib/src/read_fasta.rs:9-71, read_2bit.rs:33-118,
+ * read_fasta_folder.rs:8-23).  May be mixed with cof_genome_add_chunk. */
+COF_API int cof_genome_load(cof_genome *g, const char *path);
+
+/* Packs the chunk stream into HBM (bit4 stream + 2-bit/N-mask planes).
+ * Called implicitly by the first search; after it no chunk may be added. */
+COF_API int cof_genome_upload(cof_genome *g);
+
+COF_API uint64_t cof_genome_n_nucl(const cof_genome *g);
+COF_API uint64_t cof_genome_n_chunks(const cof_genome *g);
+COF_API void cof_genome_free(cof_genome *g);
+
+/* One search, with the arguments of search() (search.rs:1490-1500).
+ * patterns: patterns_ascii, all of length pattern_len; the first half are
+ * the forward patterns and the second half the reverse strand (as main.rs
+ * builds them), unless COF_F_ADD_REVCOMP is set, in which case they are the
+ * user patterns and the library appends the reverse complements.
+ * max_dna_bulges or max_rna_bulges > 0 selects the bulge (Myers) path
+ * exactly as search.rs:1513 does.
+ * chunks_per_search: 64 Knt chunks per search batch; 0 selects 16384, the
+ * batch search() uses with a GPU device (search.rs:22, :44-50). */
+typedef struct {
+    const char *search_filter;
+    size_t pattern_len;
+    const char *const *patterns;
+    size_t n_patterns;
+    uint32_t max_mismatches;
+    uint32_t max_dna_bulges;
+    uint32_t max_rna_bulges;
+    uint32_t flags;
+    uint32_t chunks_per_search;
+} cof_request;
+
+/* Output of one request: the writer's rows (main.rs:130-245) without the
+ * header line, '\n'-terminated, ordered by genome position then pattern
+ * (the reference's order is unspecified; compare sorted). */
+typedef struct {
+    char *text;
+    size_t text_len;
+    uint64_t n_rows;
+    double device_ms;      /* device time of this call's kernels + copies */
+} cof_result;
+
+/* The header line main.rs:131-135 writes before the rows. */
+#define COF_HEADER \
+    "#Bulge type\tcrRNA\tDNA\tChromosome\tPosition\tDirection\tMismatches\tBulge Size\n"
+
+/* search() followed by main.rs's writer, for one request. */
+COF_API int cof_search(cof_genome *g, const cof_request *req, cof_result *out);
+
+/* Many requests over one genome pass: guide sets of different lengths,
+ * PAMs and thresholds are scanned by one persistent launch per kernel
+ * stage.  outs[i] receives exactly what cof_search(reqs[i]) would return.
+ * No reference counterpart (the reference takes one filter per run,
+ * cli_utils.rs:97-108). */
+COF_API int cof_search_batch(cof_genome *g, const cof_request *reqs, size_t n_reqs,
+                             cof_result *outs);
+
+COF_API void cof_result_free(cof_result *r);
+
+/* Device timings and counters of the last search on `g`: ms5 = {scan,
+ * verify, format, device->host copy, total} milliseconds (CUDA events);
+ * counts5 = {PAM-passing windows, window x pattern comparisons, scan
+ * candidates, rows, kernel launches}.  Instrumentation for benchmarks; no
+ * reference counterpart. */
+COF_API int cof_genome_last_stats(const cof_genome *g, double *ms5, uint64_t *counts5);
+
+/* Message of the last failed call on this thread ("" if none). */
+COF_API const char *cof_last_error(void);
+
+/* ABI version of this header. */
+#define COF_ABI_VERSION 1
+COF_API int cof_abi_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

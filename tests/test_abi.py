@@ -1,0 +1,119 @@
+"""CPU tests of the C ABI: the library loads, exports every symbol that
+include/cof.h declares, validates requests, loads genomes on the host exactly
+like the oracle, and fails loudly (an error status, no fallback) when no GPU
+is usable."""
+import os
+import re
+import subprocess
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def _declared():
+    with open(os.path.join(ROOT, "include", "cof.h")) as f:
+        src = f.read()
+    return sorted(set(re.findall(r"COF_API\s+[\w\s\*]+?\b(cof_\w+)\s*\(", src)))
+
+
+def test_exports_every_declared_symbol(cof_mod):
+    lib = cof_mod.load_library()
+    names = _declared()
+    assert len(names) >= 13
+    for n in names:
+        assert hasattr(lib, n), n
+    assert set(names) == set(cof_mod.EXPORTS)
+    assert lib.cof_abi_version() == 1
+
+
+def test_nm_dynamic_symbols(cof_mod):
+    out = subprocess.run(["nm", "-D", "--defined-only", cof_mod.LIB_PATH], capture_output=True,
+                         text=True, check=True).stdout
+    exported = {l.split()[-1] for l in out.splitlines() if " T " in l}
+    assert set(_declared()) <= exported
+    # no C++ internals leak through the boundary
+    assert not [s for s in exported if s.startswith("_Z")]
+
+
+def test_host_loader_matches_oracle(cof_mod, oracle_mod, golden):
+    for name in ("upstream1000.fa", "upstream1000.2bit"):
+        path = os.path.join(golden, name)
+        g = cof_mod.Genome(path)
+        o = oracle_mod.OracleGenome(path)
+        assert g.n_chunks == o.n_chunks == 13
+        assert g.n_nucl == o.n_nucl == 12507
+
+
+def test_bad_requests_rejected(cof_mod, golden):
+    g = cof_mod.Genome(os.path.join(golden, "upstream1000.fa"))
+    with pytest.raises(cof_mod.CofError) as e:
+        g.search("NNNN", ["ACGTA"], 1)  # length mismatch
+    assert e.value.code == cof_mod.COF_E_BADINPUT
+    with pytest.raises(cof_mod.CofError) as e:
+        g.search("NNXN", ["ACGT"], 1)  # not a mixed-base filter
+    assert e.value.code == cof_mod.COF_E_BADINPUT
+    with pytest.raises(cof_mod.CofError) as e:
+        g.search("NNNN", ["ACGT"], 4)  # mm >= pattern length
+    assert e.value.code == cof_mod.COF_E_BADINPUT
+    with pytest.raises(cof_mod.CofError) as e:
+        g.search("N" * 40, ["A" * 40], 3)  # above the 32-cell word
+    assert e.value.code == cof_mod.COF_E_UNSUPPORTED
+
+
+def test_bad_genome_files(cof_mod, tmp_path):
+    p = tmp_path / "bad.fa"
+    p.write_text("ACGT\n>x\nACGT\n")  # sequence before the first header
+    g = cof_mod.Genome()
+    with pytest.raises(cof_mod.CofError) as e:
+        g.load(str(p))
+    assert e.value.code == cof_mod.COF_E_BADINPUT
+    p2 = tmp_path / "bad.2bit"
+    p2.write_bytes(b"\x00\x01\x02\x03junk")
+    with pytest.raises(cof_mod.CofError):
+        cof_mod.Genome(str(p2))
+    with pytest.raises(cof_mod.CofError) as e:
+        cof_mod.Genome(str(tmp_path / "missing.fa"))
+    assert e.value.code == cof_mod.COF_E_IO
+
+
+def test_chunk_order_enforced(cof_mod):
+    g = cof_mod.Genome()
+    g.add_chunk("a", b"\x44", 0, 2)
+    with pytest.raises(cof_mod.CofError):
+        g.add_chunk("a", b"\x44", 5, 7)  # search.rs:1396-1399
+
+
+def _gpu_usable():
+    try:
+        import torch
+        return torch.cuda.is_available()
+    except Exception:
+        return False
+
+
+@pytest.mark.skipif(_gpu_usable(), reason="checks the no-GPU failure path")
+def test_no_gpu_fails_loudly(cof_mod, golden):
+    g = cof_mod.Genome(os.path.join(golden, "upstream1000.fa"))
+    with pytest.raises(cof_mod.CofError) as e:
+        g.search("N" * 24, ["CCGTGGTTCAACATTTGCTTAGCA"], 3)
+    assert e.value.code in (cof_mod.COF_E_CUDA, cof_mod.COF_E_OOM)
+
+
+def test_cli_input_errors(cof_mod, tmp_path):
+    cli = os.path.join(os.path.dirname(cof_mod.LIB_PATH), "cof-offinder")
+    cases = {
+        "x.fa\nNNNN\nACGT\n": "Pattern line must have",
+        "x.fa\nNNNN\nACGT 1\nACG 1\n": "same length",
+        "x.fa\nNNNN\nACGT 1\nACGT 2\n": "all mismatches",
+        "x.fa\nNNNN 1\nACGT 1\n": "2nd line must be",
+        "x.fa\nNNNN\n": "at least 1 pattern",
+        "x.fa\nNNNN\nAXGT 1\n": "mixed base",
+    }
+    for text, msg in cases.items():
+        p = tmp_path / "in.txt"
+        p.write_text(text)
+        r = subprocess.run([cli, str(p), "G", "-"], capture_output=True, text=True)
+        assert r.returncode != 0 and msg in r.stderr, (text, r.stderr)
+    r = subprocess.run([cli, str(p), "X", "-"], capture_output=True, text=True)
+    assert r.returncode != 0 and "C|G|A" in r.stderr

@@ -1,0 +1,127 @@
+"""GPU parity tests: libcof.so (through the C ABI) against the oracle and the
+committed golden rows.  Bit-exact: sorted row sets must be identical."""
+import os
+import random
+import subprocess
+
+import pytest
+
+import randgen
+
+pytestmark = pytest.mark.gpu
+
+KAT_PATS = ["CCGTGGTTCAACATTTGCTTAGCA", "GATGTTGGTAAGTGGGATATGGCA"]
+
+
+def _rows(text):
+    return sorted(text.splitlines())
+
+
+def _golden_rows(golden, name):
+    with open(os.path.join(golden, name)) as f:
+        return f.read().splitlines()
+
+
+@pytest.mark.parametrize("cps", [0, 64, 2])
+def test_kat_popcount_117(cof_mod, golden, cps):
+    g = cof_mod.Genome(os.path.join(golden, "upstream1000.fa"))
+    text, n = g.search("N" * 24, KAT_PATS, 11, chunks_per_search=cps)
+    assert n == 117
+    assert _rows(text) == _golden_rows(golden, "kat_popcount_rows.txt")
+
+
+def test_kat_popcount_2bit(cof_mod, oracle_mod, golden):
+    path = os.path.join(golden, "upstream1000.2bit")
+    g = cof_mod.Genome(path)
+    text, n = g.search("N" * 24, KAT_PATS, 11)
+    o, _ = oracle_mod.OracleGenome(path).search("N" * 24, KAT_PATS, 11)
+    assert n == 117 and _rows(text) == _rows(o)
+
+
+def _both(cof_mod, oracle_mod, chunks):
+    g = cof_mod.Genome()
+    o = oracle_mod.OracleGenome()
+    for name, data, _nibs, s, e in chunks:
+        g.add_chunk(name, data, s, e)
+        o.add_chunk(name, data, s, e)
+    return g, o
+
+
+@pytest.mark.parametrize("seed", range(24))
+def test_random_popcount_parity(cof_mod, oracle_mod, seed):
+    case = randgen.random_case(seed)
+    g, o = _both(cof_mod, oracle_mod, case["chunks"])
+    text, n = g.search(case["filter"], case["patterns"], case["mm"],
+                       chunks_per_search=case["cps"])
+    ref, nref = o.search(case["filter"], case["patterns"], case["mm"],
+                         chunks_per_search=case["cps"])
+    assert _rows(text) == _rows(ref)
+    assert n == nref > 0
+
+
+def test_full_pattern_list_matches_add_revcomp(cof_mod, golden):
+    # search() takes fwd+rc as main.rs builds them; COF_F_ADD_REVCOMP builds them
+    import bruteforce
+    g = cof_mod.Genome(os.path.join(golden, "upstream1000.fa"))
+    a, _ = g.search("N" * 24, KAT_PATS, 11)
+    full = KAT_PATS + [bruteforce.revcomp(p) for p in KAT_PATS]
+    b, _ = g.search("N" * 24, full, 11, add_revcomp=False)
+    assert a == b
+
+
+def test_batched_equals_single(cof_mod, oracle_mod):
+    rng = random.Random(5)
+    _, records = randgen.random_genome(rng, 4, 3000, 9000)
+    cases = [randgen.REQUEST_SHAPES[i] for i in (0, 1, 2, 4)]
+    reqs = []
+    for filt, mk, mm in cases:
+        guides = ["".join(rng.choice("ACGT") for _ in range(25)) for _ in range(3)]
+        pats = [mk(x) for x in guides]
+        for p in pats:
+            randgen.plant_sites(rng, records, p, filt, 5, 2)
+        reqs.append(dict(search_filter=filt, patterns=pats, max_mismatches=mm))
+    chunks = randgen.chunk_records(rng, records, 500)
+    g, o = _both(cof_mod, oracle_mod, chunks)
+    batched = g.search_batch(reqs)
+    for r, (text, n) in zip(reqs, batched):
+        single, ns = g.search(**r)
+        ref, _ = o.search(r["search_filter"], r["patterns"], r["max_mismatches"])
+        assert text == single and n == ns
+        assert _rows(text) == _rows(ref)
+
+
+def test_planted_sites_found(cof_mod, oracle_mod, tmp_path):
+    import synth
+    cfg = synth.config_plain_small(seed=11, scale=0.05)
+    gen = cfg["genome"]
+    g = cof_mod.Genome()
+    gen.load_into(g)
+    text, n = g.search(cfg["filter"], cfg["patterns"], cfg["max_mismatches"])
+    rows = text.splitlines()
+    found = {(r.split("\t")[3], int(r.split("\t")[4]), r.split("\t")[5]) for r in rows}
+    for rec, pos, strand, _gi, _k, ln in cfg["truth"]:
+        # − strand rows report the position shifted by pam_len - 1 (main.rs:229-236)
+        want = pos + (2 if strand == "-" else 0)
+        assert (gen.names[rec], want, strand) in found
+    fa = tmp_path / "g.fa"
+    gen.write_fasta(str(fa))
+    ref, nref = oracle_mod.OracleGenome(str(fa)).search(cfg["filter"], cfg["patterns"],
+                                                         cfg["max_mismatches"])
+    assert _rows(text) == _rows(ref) and n == nref
+
+
+def test_cli_matches_oracle_cli(cof_mod, oracle_mod, golden, tmp_path):
+    cli = os.path.join(os.path.dirname(cof_mod.LIB_PATH), "cof-offinder")
+    ocli = os.path.join(os.path.dirname(oracle_mod.LIB_PATH), "cof_oracle")
+    inp = tmp_path / "in.txt"
+    inp.write_text(os.path.join(golden, "upstream1000.fa") + "\n" + "N" * 24 + "\n" +
+                   "".join(f"{p} 11\n" for p in KAT_PATS))
+    for dev in ("C", "G"):
+        out, oout = tmp_path / f"o{dev}.txt", tmp_path / f"r{dev}.txt"
+        subprocess.run([cli, str(inp), dev, str(out)], check=True, capture_output=True)
+        subprocess.run([ocli, str(inp), dev, str(oout)], check=True, capture_output=True)
+        a, b = out.read_text().splitlines(), oout.read_text().splitlines()
+        assert a[0] == b[0] and a[0].startswith("#Bulge type")
+        assert sorted(a[1:]) == sorted(b[1:]) and len(a) == 118
+        log = (tmp_path / f"o{dev}.txt.log").read_text()
+        assert "=== Cas-OFFinder Rust ===" in log and "Matches found: 117" in log
