@@ -163,8 +163,8 @@ class Genome:
                                        max_rna_bulges=max_rna_bulges, add_revcomp=add_revcomp,
                                        chunks_per_search=chunks_per_search)])[0]
 
-    def search_batch(self, requests):
-        """Many requests in one pass; returns [(rows_text, n_rows), ...]."""
+    def prepare(self, requests):
+        """Encodes requests once for repeated cof_search_batch calls."""
         keep = []
         reqs = (_Request * len(requests))()
         for i, r in enumerate(requests):
@@ -172,14 +172,29 @@ class Genome:
                                     r.get("max_dna_bulges", 0), r.get("max_rna_bulges", 0),
                                     r.get("add_revcomp", True), r.get("chunks_per_search", 0),
                                     keep)
-        outs = (_Result * len(requests))()
-        _check(_lib.cof_search_batch(self._h, reqs, len(requests), outs))
+        return reqs, keep
+
+    def run_prepared(self, prepared, as_text=True):
+        """One cof_search_batch call; returns [(rows, n_rows), ...] with rows
+        as str (as_text), bytes, or None (result buffers freed unread)."""
+        reqs, _keep = prepared
+        outs = (_Result * len(reqs))()
+        _check(_lib.cof_search_batch(self._h, reqs, len(reqs), outs))
         res = []
         for o in outs:
-            text = ctypes.string_at(o.text, o.text_len).decode("latin-1") if o.text_len else ""
-            res.append((text, o.n_rows))
+            if as_text is None:
+                data = o.text_len
+            else:
+                data = ctypes.string_at(o.text, o.text_len) if o.text_len else b""
+                if as_text:
+                    data = data.decode("latin-1")
+            res.append((data, o.n_rows))
             _lib.cof_result_free(ctypes.byref(o))
         return res
+
+    def search_batch(self, requests):
+        """Many requests in one pass; returns [(rows_text, n_rows), ...]."""
+        return self.run_prepared(self.prepare(requests))
 
     def last_stats(self):
         ms = (ctypes.c_double * 5)()

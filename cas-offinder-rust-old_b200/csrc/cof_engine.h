@@ -78,8 +78,11 @@ int make_request(const char *filter, size_t pattern_len, const char *const *patt
                  size_t n_patterns, uint32_t mm, uint32_t db, uint32_t rb, uint32_t flags,
                  uint32_t cps, Request &out, Error &err);
 
+// Rows of one request: a view into the engine's pinned host buffer, valid
+// until the next search on the same engine.
 struct Result {
-    std::string text;
+    const char *text = nullptr;
+    size_t text_len = 0;
     uint64_t n_rows = 0;
     double device_ms = 0;
 };

@@ -210,27 +210,29 @@ struct ScanParams {
     Counters *ctr;
 };
 
+// Compares the first n <= kQCap queued windows with every pattern of the
+// group, kCpt windows per lane.
 __device__ __forceinline__ void flush_queue(const uint4 *q, int n, const FastPattern *pt,
                                             uint32_t pbeg, uint32_t npat, uint32_t batch,
                                             const ScanParams &P, int lane) {
     uint32_t ch[kCpt], cl[kCpt], cs[kCpt], sl[kCpt];
 #pragma unroll
     for (int j = 0; j < kCpt; ++j) {
-        int idx = lane + 32 * j;
-        uint4 e = idx < n ? q[idx] : make_uint4(0xFFFFFFFFu, 0, 0, 0xFFFFFFFFu);
+        const int idx = lane + 32 * j;
+        const uint4 e = idx < n ? q[idx] : make_uint4(0xFFFFFFFFu, 0, 0, 0xFFFFFFFFu);
         sl[j] = e.x;
         ch[j] = e.y;
         cl[j] = e.z;
         cs[j] = e.w;
     }
     for (uint32_t p = 0; p < npat; ++p) {
-        FastPattern fp = pt[p];
+        const FastPattern fp = pt[p];
 #pragma unroll
         for (int j = 0; j < kCpt; ++j) {
-            uint32_t m = ((ch[j] ^ fp.h) | (cl[j] ^ fp.l) | cs[j]) & fp.care;
+            const uint32_t m = ((ch[j] ^ fp.h) | (cl[j] ^ fp.l) | cs[j]) & fp.care;
             if ((int)__popc(m) <= fp.k) {
                 if (lane + 32 * j < n) {
-                    uint32_t i = atomicAdd(&P.ctr->hits, 1u);
+                    const uint32_t i = atomicAdd(&P.ctr->hits, 1u);
                     if (i < P.hit_cap) P.hits[i] = Hit{sl[j], pbeg + p, batch, 0};
                     else P.ctr->overflow = 1;
                 }
@@ -315,10 +317,17 @@ scan_kernel(ScanParams P, uint64_t total_tiles_unused) {
             }
             qn += __popc(bal);
             if (qn >= kQCap) {
+                // full pass over kQCap windows; the (< 32) windows beyond it
+                // move to the front of the queue
                 __syncwarp();
-                flush_queue(q, qn, pt, sg.pat_begin, npat, qbatch, P, lane);
+                flush_queue(q, kQCap, pt, sg.pat_begin, npat, qbatch, P, lane);
+                const int rest = qn - kQCap;
+                uint4 e = make_uint4(0, 0, 0, 0);
+                if (lane < rest) e = q[kQCap + lane];
                 __syncwarp();
-                qn = 0;
+                if (lane < rest) q[lane] = e;
+                __syncwarp();
+                qn = rest;
             }
         }
     }
@@ -922,7 +931,8 @@ int Engine::search(const std::vector<Request> &reqs, std::vector<Result> &out, E
         uint64_t t1 = text_bytes;
         if (r1 < n_rows) CU(cudaMemcpy(&t1, d.offs.p + r1, 8, cudaMemcpyDeviceToHost));
         out[ri].n_rows = req_rows[ri];
-        if (t1 > t0) out[ri].text.assign(d.h_text + t0, d.h_text + t1);
+        out[ri].text = d.h_text ? d.h_text + t0 : nullptr;
+        out[ri].text_len = t1 - t0;
         r0 = r1;
         t0 = t1;
     }
