@@ -22,7 +22,7 @@ COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC,-fvisibility=hi
           "-I" + os.path.join(ROOT, "include")]
 HEADERS = [os.path.join(CSRC, "cof_engine.h"), os.path.join(ROOT, "include", "cof.h")]
 
-SOURCES = ["engine.cu", "loader.cpp", "cabi.cpp"]
+SOURCES = ["engine.cu", "loader.cpp", "cabi.cpp", "noalloc.cu"]
 
 
 def _stale(out, deps):

@@ -35,7 +35,7 @@ EXPORTS = (
     "cof_genome_create", "cof_genome_add_chunk", "cof_genome_load", "cof_genome_upload",
     "cof_genome_n_nucl", "cof_genome_n_chunks", "cof_genome_free", "cof_search",
     "cof_search_batch", "cof_result_free", "cof_genome_last_stats", "cof_last_error",
-    "cof_abi_version",
+    "cof_abi_version", "cof_search_seq_noalloc",
 )
 
 
@@ -97,6 +97,10 @@ def load_library(path=LIB_PATH):
     lib.cof_genome_last_stats.argtypes = [vp, c.POINTER(c.c_double), c.POINTER(c.c_uint64)]
     lib.cof_last_error.restype = c.c_char_p
     lib.cof_abi_version.restype = c.c_int
+    lib.cof_search_seq_noalloc.argtypes = [c.c_void_p, c.c_uint64, c.c_char_p,
+                                           c.POINTER(c.c_char_p), c.c_size_t, c.c_uint32,
+                                           c.c_void_p, c.c_uint32, c.POINTER(c.c_uint32),
+                                           c.c_void_p]
     _lib = lib
     return lib
 

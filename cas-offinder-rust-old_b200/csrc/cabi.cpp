@@ -72,6 +72,11 @@ int fill_result(const cof::Result &r, cof_result *out) {
 
 }  // namespace
 
+namespace cof {
+// Records a failure for cof_last_error() from code outside this file.
+int set_last_error(int code, const std::string &msg) { return fail(code, msg); }
+}  // namespace cof
+
 extern "C" {
 
 COF_API int cof_abi_version(void) { return COF_ABI_VERSION; }

@@ -93,6 +93,9 @@ struct StageTimes {
     uint64_t candidates = 0, pairs = 0, raw_hits = 0, rows = 0, kernel_launches = 0;
 };
 
+// Sets the message returned by cof_last_error() on this thread; returns code.
+int set_last_error(int code, const std::string &msg);
+
 class DeviceGenome;  // engine.cu
 
 // A genome bound to one GPU: host chunk stream + resident device copy.

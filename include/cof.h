@@ -140,6 +140,43 @@ COF_API void cof_result_free(cof_result *r);
  * reference counterpart. */
 COF_API int cof_genome_last_stats(const cof_genome *g, double *ms5, uint64_t *counts5);
 
+/* Popcount search over one sequence that already sits in device memory,
+ * without allocating any memory.  No counterpart in the reference.
+ *
+ * For callers that cannot call cudaMalloc: an application whose own pool
+ * allocator owns the device memory and only hands out pointers into it (an
+ * allocation from this library would bypass or exceed that pool), or a
+ * serving loop that must not allocate while requests are in flight because
+ * allocation can synchronise the whole device.  The caller passes the input
+ * and the output as device pointers; counters, pattern tables and the
+ * candidate list live in one fixed device array of 8 MiB that every GPU which
+ * loads libcof.so keeps until the process exits.
+ *
+ * d_bit4: one record of n_nucl nucleotides in the reference's bit4 one-hot
+ * encoding (two per byte, even index in the low nibble), 16-byte aligned,
+ * n_nucl < 2^31.  patterns: the full fwd + reverse list as search() takes
+ * it, 1..512 patterns of the filter's length (<= 32).  Rows are the writer's
+ * rows of cof_search for a genome made of this one record: every window start
+ * s with s + L <= n_nucl that passes the PAM filter and the mismatch
+ * recount.  Each row is three uint32 in d_rows: s (0-based, the scan
+ * orientation start), pattern index, mismatches; order unspecified.
+ * *n_rows receives the number of rows found; if it exceeds rows_cap only the
+ * first rows_cap are written and COF_E_UNSUPPORTED is returned.  Requests
+ * beyond the stated maximums are rejected with COF_E_UNSUPPORTED and a
+ * message in cof_last_error().  stream: a cudaStream_t (NULL = default).
+ *
+ * The first call on a device looks up the array's device address
+ * (cudaGetSymbolAddress) with that device current; make it before any
+ * stream capture.  All calls share the array and leave their data in it;
+ * each call clears its counters first.  Calls are serialised inside the
+ * library and wait for their stream before returning; work from two calls
+ * that overlapped on the GPU would race on the shared array. */
+COF_API int cof_search_seq_noalloc(const uint8_t *d_bit4, uint64_t n_nucl,
+                                   const char *search_filter, const char *const *patterns,
+                                   size_t n_patterns, uint32_t max_mismatches,
+                                   uint32_t *d_rows, uint32_t rows_cap, uint32_t *n_rows,
+                                   void *stream);
+
 /* Message of the last failed call on this thread ("" if none). */
 COF_API const char *cof_last_error(void);
 
