@@ -32,6 +32,11 @@ PKG = os.path.join(ROOT, "cas-offinder-rust-old_b200")
 ORACLE = os.path.join(ROOT, "oracle")
 sys.path.insert(0, PKG)
 
+# dram__bytes_read.sum + dram__bytes_write.sum of one scan_kernel launch,
+# from the ncu capture summarised in profiles/ (620 Mbp case, scaled x5 by
+# genome size to the 3.1 Gbp workload: the scan reads each plane word once)
+TRAFFIC = (350.28e6 + 16.16e6) * 5
+
 METRIC = "Gbp*guides/s scanned (3.1 Gbp x 100 guides, 20 nt + NRG, mm<=6, both strands)"
 UNIT = "Gbp*guides/s"
 
@@ -280,10 +285,13 @@ def main():
                 "h2d_bytes_per_step": 100 * 23 * 2 + 4096,
                 "d2h_bytes_per_step": text_bytes},
         "roofline": {"bound": "alu", "kernel": "scan_kernel",
-                     "achieved": achieved, "peak": peaks["pairs_per_s"], "unit": "pairs/s",
-                     "frac": achieved / peaks["pairs_per_s"], "traffic": None,
-                     "peak_kind": "measured live: scan inner loop, register-resident",
-                     "popc_per_s": peaks["popc_per_s"], "lop3_per_s": peaks["lop3_per_s"],
+                     "achieved": achieved, "peak": peaks["popc_per_s"], "unit": "pairs/s",
+                     "frac": achieved / peaks["popc_per_s"], "traffic": TRAFFIC,
+                     "peak_kind": "measured live: POPC results/s of this GPU (XU pipe); "
+                                  "the scan needs one POPC per window x pattern pair",
+                     "inner_loop_peak_pairs_per_s": peaks["pairs_per_s"],
+                     "frac_of_inner_loop": achieved / peaks["pairs_per_s"],
+                     "lop3_per_s": peaks["lop3_per_s"],
                      "hbm_gbs_achieved": plane_bytes / (scan_ms * 1e-3) / 1e9,
                      "hbm_peak_gbs": hbm, "hbm_peak_kind": hbm_kind},
         "stages_ms": {k: statistics.median(s[k] for s in stats)

@@ -75,6 +75,14 @@ struct PamCell {
 };
 
 constexpr int kMaxPamCells = 32;
+constexpr int kMaxCareClasses = 8;
+
+// Patterns of a group that compare the same window cells (single-base cells
+// of the pattern): windows are masked once per class.  Pattern indices are
+// relative to the group.
+struct CareClass {
+    uint32_t care, pat_begin, pat_end, pad;
+};
 
 // One strand of one request: the windows whose non-N filter cells all hold
 // a single base of the filter's set are scanned against the patterns
@@ -83,8 +91,10 @@ struct ScanGroup {
     uint32_t n_pam;
     uint32_t pat_begin, pat_end;
     uint32_t seg_begin, seg_end;  // scan segments of this group
-    uint32_t pad[3];
+    uint32_t n_class;
+    uint32_t pad[2];
     PamCell pam[kMaxPamCells];
+    CareClass cls[kMaxCareClasses];
 };
 
 // A contiguous range of window starts inside one batch.
@@ -97,7 +107,8 @@ struct ScanSeg {
     uint32_t pad;
 };
 
-// Scan-form pattern (window cells in bit positions 0..L-1).
+// Scan-form pattern (window cells in bit positions 0..L-1), code bits
+// already masked by the pattern's care cells.
 struct FastPattern {
     uint32_t h, l, care;
     int32_t k;  // max mismatches
@@ -211,37 +222,45 @@ struct ScanParams {
 };
 
 // Compares the first n <= kQCap queued windows with every pattern of the
-// group, kCpt windows per lane.
-__device__ __forceinline__ void flush_queue(const uint4 *q, int n, const FastPattern *pt,
-                                            uint32_t pbeg, uint32_t npat, uint32_t batch,
+// group, kCpt windows per lane.  Per care class the windows are masked once;
+// per pattern the lane keeps the minimum mismatch count over its windows and
+// only a pattern whose minimum passes takes the (rare) emitting branch.
+__device__ __noinline__ void flush_queue(const uint4 *q, int n, const FastPattern *pt,
+                                            const ScanGroup &G, uint32_t batch,
                                             const ScanParams &P, int lane) {
-    uint32_t ch[kCpt], cl[kCpt], cs[kCpt], sl[kCpt];
-#pragma unroll
-    for (int j = 0; j < kCpt; ++j) {
-        const int idx = lane + 32 * j;
-        const uint4 e = idx < n ? q[idx] : make_uint4(0xFFFFFFFFu, 0, 0, 0xFFFFFFFFu);
-        sl[j] = e.x;
-        ch[j] = e.y;
-        cl[j] = e.z;
-        cs[j] = e.w;
-    }
-    for (uint32_t p = 0; p < npat; ++p) {
-        const FastPattern fp = pt[p];
+    for (uint32_t c = 0; c < G.n_class; ++c) {
+        const CareClass K = G.cls[c];
+        uint32_t mh[kCpt], ml[kCpt], ms[kCpt];
 #pragma unroll
         for (int j = 0; j < kCpt; ++j) {
-            const uint32_t m = ((ch[j] ^ fp.h) | (cl[j] ^ fp.l) | cs[j]) & fp.care;
-            if ((int)__popc(m) <= fp.k) {
-                if (lane + 32 * j < n) {
-                    const uint32_t i = atomicAdd(&P.ctr->hits, 1u);
-                    if (i < P.hit_cap) P.hits[i] = Hit{sl[j], pbeg + p, batch, 0};
-                    else P.ctr->overflow = 1;
+            const int idx = lane + 32 * j;
+            const uint4 e = idx < n ? q[idx] : make_uint4(0, 0, 0, 0xFFFFFFFFu);
+            mh[j] = e.y & K.care;
+            ml[j] = e.z & K.care;
+            ms[j] = e.w & K.care;
+        }
+        for (uint32_t p = K.pat_begin; p < K.pat_end; ++p) {
+            const FastPattern fp = pt[p];
+            int mn = 64;
+#pragma unroll
+            for (int j = 0; j < kCpt; ++j)
+                mn = min(mn, (int)__popc((mh[j] ^ fp.h) | (ml[j] ^ fp.l) | ms[j]));
+            if (mn <= fp.k) {
+#pragma unroll
+                for (int j = 0; j < kCpt; ++j) {
+                    const int idx = lane + 32 * j;
+                    if (idx < n && (int)__popc((mh[j] ^ fp.h) | (ml[j] ^ fp.l) | ms[j]) <= fp.k) {
+                        const uint32_t i = atomicAdd(&P.ctr->hits, 1u);
+                        if (i < P.hit_cap) P.hits[i] = Hit{q[idx].x, G.pat_begin + p, batch, 0};
+                        else P.ctr->overflow = 1;
+                    }
                 }
             }
         }
     }
 }
 
-__global__ void __launch_bounds__(kScanWarps * 32)
+__global__ void __launch_bounds__(kScanWarps * 32, 3)
 scan_kernel(ScanParams P, uint64_t total_tiles_unused) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     uint4 *queues = reinterpret_cast<uint4 *>(smem_raw);
@@ -279,7 +298,7 @@ scan_kernel(ScanParams P, uint64_t total_tiles_unused) {
         if (sgm.batch != qbatch) {
             if (qn) {
                 __syncwarp();
-                flush_queue(q, qn, pt, sg.pat_begin, npat, qbatch, P, lane);
+                flush_queue(q, qn, pt, sg, qbatch, P, lane);
                 __syncwarp();
                 qn = 0;
             }
@@ -320,7 +339,7 @@ scan_kernel(ScanParams P, uint64_t total_tiles_unused) {
                 // full pass over kQCap windows; the (< 32) windows beyond it
                 // move to the front of the queue
                 __syncwarp();
-                flush_queue(q, kQCap, pt, sg.pat_begin, npat, qbatch, P, lane);
+                flush_queue(q, kQCap, pt, sg, qbatch, P, lane);
                 const int rest = qn - kQCap;
                 uint4 e = make_uint4(0, 0, 0, 0);
                 if (lane < rest) e = q[kQCap + lane];
@@ -333,7 +352,7 @@ scan_kernel(ScanParams P, uint64_t total_tiles_unused) {
     }
     if (qn) {
         __syncwarp();
-        flush_queue(q, qn, pt, sg.pat_begin, npat, qbatch, P, lane);
+        flush_queue(q, qn, pt, sg, qbatch, P, lane);
     }
     // candidate count (for the roofline's algorithmic work)
     for (int o = 16; o; o >>= 1) ncand += __shfl_down_sync(0xFFFFFFFFu, ncand, o);
@@ -743,16 +762,43 @@ int Engine::search(const std::vector<Request> &reqs, std::vector<Result> &out, E
         for (uint32_t strand = 0; strand < 2; ++strand) {
             const size_t pb = strand ? nfwd : 0, pe = strand ? np : nfwd;
             if (pb == pe) continue;
-            ScanGroup g{};
-            g.pat_begin = (uint32_t)fpats.size();
+            ScanGroup proto{};
             for (uint32_t c = 0; c < L; ++c) {
                 if (rd.fisn[strand][c]) continue;
-                if (g.n_pam == kMaxPamCells) break;
+                if (proto.n_pam == kMaxPamCells) break;
                 const uint8_t fs = rd.fset[strand][c];
                 PamCell pc{c, (fs & 4) ? ~0u : 0u, (fs & 2) ? ~0u : 0u, (fs & 8) ? ~0u : 0u,
                            (fs & 1) ? ~0u : 0u};
-                g.pam[g.n_pam++] = pc;
+                proto.pam[proto.n_pam++] = pc;
             }
+            // scan segments: one per batch, shared by this strand's groups
+            proto.seg_begin = (uint32_t)segs.size();
+            uint64_t tiles = 0;
+            for (size_t bi = 0; bi < batches.size(); ++bi) {
+                const BatchDev &b = batches[bi];
+                // legacy_match_start_min_nucl (search.rs:540-546): starts in the
+                // head chunk that the previous batch already emitted
+                const uint64_t c1 = hb[bi].has_head ? b.active_start : 0;
+                const uint64_t msmin = c1 > L - 1 ? c1 - (L - 1) : 0;
+                ScanSeg sgm{};
+                sgm.lo = b.base + msmin;
+                sgm.hi = b.base + b.valid;
+                if (sgm.hi <= sgm.lo) continue;
+                sgm.base = b.base;
+                sgm.w0 = sgm.lo / 32;
+                sgm.tile_begin = tiles;
+                sgm.batch = (uint32_t)bi;
+                tiles += (sgm.hi - sgm.w0 * 32 + 1023) / 1024;
+                segs.push_back(sgm);
+            }
+            proto.seg_end = (uint32_t)segs.size();
+            if (proto.seg_end - proto.seg_begin > (uint32_t)kMaxSegs) {
+                err = {kUnsupported, "too many search batches for one scan launch"};
+                return err.code;
+            }
+            if (proto.seg_end == proto.seg_begin) continue;
+            // compile the strand's patterns, ordered by care mask
+            std::vector<std::pair<FastPattern, ExactPattern>> comp;
             for (size_t p = pb; p < pe; ++p) {
                 FastPattern fp{0, 0, 0, (int32_t)r.max_mm};
                 ExactPattern ep{};
@@ -770,35 +816,36 @@ int Engine::search(const std::vector<Request> &reqs, std::vector<Result> &out, E
                         fp.l |= (cd & 1u) << c;
                     }
                 }
-                fpats.push_back(fp);
-                epats.push_back(ep);
+                comp.push_back({fp, ep});
+            }
+            std::stable_sort(comp.begin(), comp.end(),
+                             [](const std::pair<FastPattern, ExactPattern> &a,
+                                const std::pair<FastPattern, ExactPattern> &b) {
+                                 return a.first.care < b.first.care;
+                             });
+            // groups of at most kMaxCareClasses classes
+            ScanGroup g = proto;
+            g.pat_begin = (uint32_t)fpats.size();
+            g.n_class = 0;
+            for (size_t i = 0; i < comp.size(); ++i) {
+                const uint32_t care = comp[i].first.care;
+                const bool new_class = g.n_class == 0 || g.cls[g.n_class - 1].care != care;
+                if (new_class && g.n_class == (uint32_t)kMaxCareClasses) {
+                    g.pat_end = (uint32_t)fpats.size();
+                    groups.push_back(g);
+                    g = proto;
+                    g.pat_begin = (uint32_t)fpats.size();
+                    g.n_class = 0;
+                }
+                const uint32_t rel = (uint32_t)fpats.size() - g.pat_begin;
+                if (g.n_class == 0 || g.cls[g.n_class - 1].care != care)
+                    g.cls[g.n_class++] = CareClass{care, rel, rel, 0};
+                g.cls[g.n_class - 1].pat_end = rel + 1;
+                fpats.push_back(comp[i].first);
+                epats.push_back(comp[i].second);
             }
             g.pat_end = (uint32_t)fpats.size();
-            g.seg_begin = (uint32_t)segs.size();
-            uint64_t tiles = 0;
-            for (size_t bi = 0; bi < batches.size(); ++bi) {
-                const BatchDev &b = batches[bi];
-                // legacy_match_start_min_nucl (search.rs:540-546): starts in the
-                // head chunk that the previous batch already emitted
-                const uint64_t c1 = hb[bi].has_head ? b.active_start : 0;
-                const uint64_t msmin = c1 > L - 1 ? c1 - (L - 1) : 0;
-                ScanSeg s{};
-                s.lo = b.base + msmin;
-                s.hi = b.base + b.valid;
-                if (s.hi <= s.lo) continue;
-                s.base = b.base;
-                s.w0 = s.lo / 32;
-                s.tile_begin = tiles;
-                s.batch = (uint32_t)bi;
-                tiles += (s.hi - s.w0 * 32 + 1023) / 1024;
-                segs.push_back(s);
-            }
-            g.seg_end = (uint32_t)segs.size();
-            if (g.seg_end - g.seg_begin > (uint32_t)kMaxSegs) {
-                err = {kUnsupported, "too many search batches for one scan launch"};
-                return err.code;
-            }
-            if (g.seg_end > g.seg_begin) groups.push_back(g);
+            groups.push_back(g);
         }
     }
 

@@ -4,9 +4,10 @@
 //   popc : __popc results per second (8 independent chains per thread)
 //   lop3 : 3-input logic results per second (8 independent chains)
 //   pair : window x pattern comparisons per second of the scan's inner loop
-//          (((H^pH)|(L^pL)|S) & care, popc, compare with the threshold) on
-//          register-resident windows and shared-memory patterns, i.e. the
-//          scan with no memory traffic and no hits.
+//          (popc((H^pH)|(L^pL)|S) folded into a per-pattern minimum over 8
+//          windows, one threshold test per pattern) on register-resident,
+//          care-masked windows and shared-memory patterns, i.e. the scan with
+//          no memory traffic and no hits.
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -60,11 +61,10 @@ __global__ void pair_kernel(uint32_t seed, int iters, uint32_t *out) {
     for (int it = 0; it < iters; ++it) {
         for (int p = 0; p < kPats; ++p) {
             const uint4 q = pat[p];
+            int mn = 64;
 #pragma unroll
-            for (int j = 0; j < 8; ++j) {
-                const uint32_t m = ((h[j] ^ q.x) | (l[j] ^ q.y) | s[j]) & q.z;
-                if ((int)__popc(m) <= (int)q.w) hits += j + 1;  // q.w = -1: never
-            }
+            for (int j = 0; j < 8; ++j) mn = min(mn, (int)__popc((h[j] ^ q.x) | (l[j] ^ q.y) | s[j]));
+            if (mn <= (int)q.w) hits += mn + 1;  // q.w = -1: never
         }
     }
     if (hits) out[0] = hits;
