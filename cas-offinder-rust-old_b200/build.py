@@ -20,9 +20,10 @@ NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC,-fvisibility=hidden",
           "-I" + os.path.join(ROOT, "include")]
-HEADERS = [os.path.join(CSRC, "cof_engine.h"), os.path.join(ROOT, "include", "cof.h")]
+HEADERS = [os.path.join(CSRC, "cof_engine.h"), os.path.join(CSRC, "engine_dev.cuh"),
+           os.path.join(ROOT, "include", "cof.h")]
 
-SOURCES = ["engine.cu", "loader.cpp", "cabi.cpp", "noalloc.cu"]
+SOURCES = ["engine.cu", "bulge.cu", "loader.cpp", "cabi.cpp", "noalloc.cu"]
 
 
 def _stale(out, deps):

@@ -85,6 +85,7 @@ struct Result {
     size_t text_len = 0;
     uint64_t n_rows = 0;
     double device_ms = 0;
+    std::string owned;  // backing store when `text` does not point into the engine
 };
 
 // Per-stage device timings of the last search (milliseconds, CUDA events).
@@ -115,6 +116,8 @@ class Engine {
     int device() const { return device_; }
 
   private:
+    int run_popcount(const std::vector<Request> &reqs, std::vector<Result> &out, Error &err);
+    int run_bulge(const std::vector<Request> &reqs, std::vector<Result> &out, Error &err);
     int device_;
     HostGenome host_;
     DeviceGenome *dev_ = nullptr;

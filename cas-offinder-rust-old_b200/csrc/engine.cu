@@ -35,6 +35,7 @@
 #include <vector>
 
 #include "cof_engine.h"
+#include "engine_dev.cuh"
 
 namespace cof {
 
@@ -42,31 +43,9 @@ namespace cof {
 // error plumbing
 // ---------------------------------------------------------------------------
 
-#define CU(call)                                                                     \
-    do {                                                                             \
-        cudaError_t e_ = (call);                                                     \
-        if (e_ != cudaSuccess) {                                                     \
-            err = {e_ == cudaErrorMemoryAllocation ? kOom : kCuda,                   \
-                   std::string(#call) + ": " + cudaGetErrorString(e_)};              \
-            return err.code;                                                         \
-        }                                                                            \
-    } while (0)
-
 // ---------------------------------------------------------------------------
 // device structures
 // ---------------------------------------------------------------------------
-
-// One search batch of the reference (SearchChunkInfo, search.rs:57-90): the
-// chunks [first, first + nch) of the stream, starting at nucleotide `base`.
-struct BatchDev {
-    uint64_t base;         // global nucleotide index of the batch start
-    uint32_t valid;        // valid nucleotides (2 x tight-packed bytes)
-    uint32_t pad0;
-    uint32_t first;        // first chunk
-    uint32_t nch;          // chunks in the batch
-    uint32_t active_start; // Myers active start (search.rs:1087-1091)
-    uint32_t pad;
-};
 
 // PAM cell of a scan group: window cell index and allowed 2-bit codes as
 // full-word masks (all ones if the code is allowed).
@@ -125,40 +104,6 @@ struct RequestDev {
     uint8_t fset[2][kMaxPatternLen];  // filter bit4 per strand, scan orientation
     uint8_t fisn[2][kMaxPatternLen];  // filter char is N/n
 };
-
-struct Hit {
-    uint32_t s_local, pattern, batch, pad;
-};
-
-struct Row {
-    uint64_t s_global;   // window start
-    uint64_t clip;       // batch end (exclusive); cells at or past it read 0
-    uint64_t pos;        // chrom_idx (record coordinate)
-    uint32_t chunk;
-    uint32_t pattern;
-    uint32_t mm;
-    uint32_t pad;
-};
-
-struct Counters {
-    uint32_t hits;
-    uint32_t rows;
-    uint32_t overflow;
-    uint32_t pad;
-    unsigned long long candidates;
-    unsigned long long pairs;
-};
-
-__constant__ char c_b4str[16];
-
-__device__ __forceinline__ uint8_t nib(const uint8_t *__restrict__ g, uint64_t i) {
-    uint8_t b = __ldg(g + (i >> 1));
-    return (i & 1) ? (uint8_t)(b >> 4) : (uint8_t)(b & 0xF);
-}
-__device__ __forceinline__ uint8_t dcomp4(uint8_t v) {
-    return (uint8_t)(((v << 2) | (v >> 2)) & 0xF);
-}
-__device__ __forceinline__ bool single_base(uint8_t v) { return v && !(v & (v - 1)); }
 
 // ---------------------------------------------------------------------------
 // pack: bit4 stream -> H / L / S planes (one thread per 32 nt word)
@@ -366,15 +311,6 @@ scan_kernel(ScanParams P, uint64_t total_tiles_unused) {
 // verify: the reference's exact decision per candidate hit
 // ---------------------------------------------------------------------------
 
-struct GenomeDev {
-    const uint8_t *bit4;
-    const uint64_t *boff, *start, *end;
-    const uint32_t *name_idx;
-    const char *names;
-    const uint32_t *name_off;
-    uint64_t n_chunks;
-};
-
 __global__ void verify_kernel(GenomeDev G, const BatchDev *__restrict__ batches,
                               const ExactPattern *__restrict__ pats,
                               const RequestDev *__restrict__ reqs, const Hit *__restrict__ hits,
@@ -433,11 +369,6 @@ __global__ void verify_kernel(GenomeDev G, const BatchDev *__restrict__ batches,
 // format: row lengths, then row text (main.rs:198-242)
 // ---------------------------------------------------------------------------
 
-__device__ __forceinline__ uint32_t ndigits(uint64_t v) {
-    uint32_t d = 1;
-    while (v >= 10) { v /= 10; ++d; }
-    return d;
-}
 __device__ __forceinline__ uint64_t pos_out(const Row &w, const RequestDev &R, uint32_t strand) {
     uint64_t a = R.pam_len ? R.pam_len - 1 : 0;  // db == 0 on this path
     return strand ? w.pos + a : w.pos;
@@ -457,14 +388,6 @@ __global__ void row_len_kernel(GenomeDev G, const Row *__restrict__ rows,
         len[i] = 2 + P.L + 1 + P.L + 1 + name_len + 1 + ndigits(pos_out(w, R, P.strand)) + 3 +
                  ndigits(w.mm) + 3;
     }
-}
-
-__device__ __forceinline__ char *put_u64(char *o, uint64_t v) {
-    char t[20];
-    int k = 0;
-    do { t[k++] = (char)('0' + v % 10); v /= 10; } while (v);
-    while (k) *o++ = t[--k];
-    return o;
 }
 
 __global__ void row_write_kernel(GenomeDev G, const Row *__restrict__ rows,
@@ -491,8 +414,8 @@ __global__ void row_write_kernel(GenomeDev G, const Row *__restrict__ rows,
             if (g == 0xF) g = 0;
             uint8_t p = P.b4[sc];
             if (!fwd) { g = dcomp4(g); p = dcomp4(p); }
-            rna[c] = c_b4str[p];
-            char d = c_b4str[g];
+            rna[c] = b4char(p);
+            char d = b4char(g);
             if (g == 0) d = (p == 0xF) ? 'N' : 'n';
             else if (p == 0xF) {}
             else if (!(single_base(g) && (g & p))) d = (char)(d | 0x20);
@@ -520,68 +443,6 @@ __global__ void row_write_kernel(GenomeDev G, const Row *__restrict__ rows,
 // device genome + scratch
 // ---------------------------------------------------------------------------
 
-template <class T>
-struct DevBuf {
-    T *p = nullptr;
-    size_t cap = 0;
-    int ensure(size_t n, Error &err) {
-        if (n <= cap) return kOk;
-        if (p) cudaFree(p);
-        p = nullptr;
-        cap = 0;
-        size_t want = std::max<size_t>(n, 64);
-        CU(cudaMalloc((void **)&p, want * sizeof(T)));
-        cap = want;
-        return kOk;
-    }
-    void release() {
-        if (p) cudaFree(p);
-        p = nullptr;
-        cap = 0;
-    }
-};
-
-class DeviceGenome {
-  public:
-    int device = 0;
-    cudaStream_t stream = nullptr;
-    cudaEvent_t ev[8] = {};
-    int n_sm = 0;
-    DevBuf<uint8_t> bit4;
-    DevBuf<uint32_t> planes;
-    uint64_t n_words = 0;
-    DevBuf<uint64_t> boff, start, end;
-    DevBuf<uint32_t> name_idx, name_off;
-    DevBuf<char> names;
-    uint64_t n_chunks = 0;
-    // per-search scratch
-    DevBuf<unsigned char> tables;
-    DevBuf<Hit> hits;
-    DevBuf<Row> rows;
-    DevBuf<uint64_t> keys, keys2, offs;
-    DevBuf<uint32_t> vals, vals2, lens, req_rows;
-    DevBuf<Counters> ctr;
-    DevBuf<char> text;
-    DevBuf<unsigned char> cub_tmp;
-    char *h_text = nullptr;
-    size_t h_text_cap = 0;
-
-    ~DeviceGenome() {
-        bit4.release(); planes.release(); boff.release(); start.release(); end.release();
-        name_idx.release(); name_off.release(); names.release(); tables.release();
-        hits.release(); rows.release(); keys.release(); keys2.release(); offs.release();
-        vals.release(); vals2.release(); lens.release(); req_rows.release(); ctr.release();
-        text.release(); cub_tmp.release();
-        if (h_text) cudaFreeHost(h_text);
-        for (auto &e : ev)
-            if (e) cudaEventDestroy(e);
-        if (stream) cudaStreamDestroy(stream);
-    }
-    GenomeDev view() const {
-        return GenomeDev{bit4.p, boff.p, start.p, end.p, name_idx.p, names.p, name_off.p, n_chunks};
-    }
-};
-
 Engine::Engine(int device) : device_(device) {}
 Engine::~Engine() {
     if (dev_) {
@@ -598,7 +459,6 @@ int Engine::upload(Error &err) {
     CU(cudaStreamCreateWithFlags(&d->stream, cudaStreamNonBlocking));
     for (auto &e : d->ev) CU(cudaEventCreate(&e));
     CU(cudaDeviceGetAttribute(&d->n_sm, cudaDevAttrMultiProcessorCount, device_));
-    CU(cudaMemcpyToSymbol(c_b4str, bit4().b4str, 16));  // per device context
     const HostGenome &h = host_;
     const uint64_t n_bytes = h.data.size();
     const uint64_t n_nucl = 2 * n_bytes;
@@ -650,64 +510,11 @@ int Engine::upload(Error &err) {
 // host orchestration
 // ---------------------------------------------------------------------------
 
-namespace {
-
-struct HostBatch {
-    size_t first, last;
-    bool has_head;
-};
-
-// Send thread of search.rs:1531-1572.
-std::vector<HostBatch> make_batches(size_t n_chunks, uint32_t cps) {
-    std::vector<HostBatch> out;
-    size_t bfirst = 0, blen = 0;
-    bool head = false;
-    for (size_t k = 0; k < n_chunks; ++k) {
-        if (blen == 0) bfirst = k;
-        ++blen;
-        if (blen == cps) {
-            out.push_back({bfirst, k, head});
-            bfirst = k;
-            blen = 1;
-            head = true;
-        }
-    }
-    if (blen && !(head && blen == 1)) out.push_back({bfirst, bfirst + blen - 1, head});
-    return out;
-}
-
-// Packs plain-old-data tables into one upload buffer.
-struct TablePack {
-    std::vector<unsigned char> buf;
-    template <class T>
-    size_t add(const std::vector<T> &v) {
-        size_t o = (buf.size() + 255) & ~size_t(255);
-        buf.resize(o + std::max<size_t>(v.size(), 1) * sizeof(T));
-        if (!v.empty()) std::memcpy(buf.data() + o, v.data(), v.size() * sizeof(T));
-        return o;
-    }
-};
-
-uint32_t code2(uint8_t b4) {  // single base one-hot -> 2-bit code A0 C1 G2 T3
-    switch (b4) {
-        case 4: return 0;
-        case 2: return 1;
-        case 8: return 2;
-        default: return 3;
-    }
-}
-
-}  // namespace
-
 int Engine::search(const std::vector<Request> &reqs, std::vector<Result> &out, Error &err) {
     times_ = StageTimes();
     out.assign(reqs.size(), Result());
     if (reqs.empty()) return kOk;
     for (const Request &r : reqs) {
-        if (r.max_db || r.max_rb) {
-            err = {kUnsupported, "bulge search is not available in this build"};
-            return err.code;
-        }
         if (r.cps != reqs[0].cps) {
             err = {kBadInput, "batched requests must share chunks_per_search"};
             return err.code;
@@ -715,6 +522,50 @@ int Engine::search(const std::vector<Request> &reqs, std::vector<Result> &out, E
     }
     if (upload(err)) return err.code;
     CU(cudaSetDevice(device_));
+    DeviceGenome &d = *dev_;
+    CU(cudaEventRecord(d.ev[8], d.stream));
+    // search.rs:1513: any bulge selects the Myers path for that request
+    std::vector<size_t> pi, bi;
+    std::vector<Request> pr, br;
+    for (size_t i = 0; i < reqs.size(); ++i) {
+        if (reqs[i].max_db || reqs[i].max_rb) {
+            bi.push_back(i);
+            br.push_back(reqs[i]);
+        } else {
+            pi.push_back(i);
+            pr.push_back(reqs[i]);
+        }
+    }
+    if (!pr.empty()) {
+        std::vector<Result> po;
+        if (run_popcount(pr, po, err)) return err.code;
+        for (size_t k = 0; k < pi.size(); ++k) {
+            out[pi[k]] = po[k];
+            if (!br.empty()) {  // the bulge path reuses the pinned text buffer
+                out[pi[k]].owned.assign(po[k].text ? po[k].text : "", po[k].text_len);
+                out[pi[k]].text = out[pi[k]].owned.data();
+            }
+        }
+    }
+    if (!br.empty()) {
+        std::vector<Result> bo;
+        if (run_bulge(br, bo, err)) return err.code;
+        for (size_t k = 0; k < bi.size(); ++k) {
+            out[bi[k]] = std::move(bo[k]);
+            out[bi[k]].text = out[bi[k]].owned.data();
+        }
+    }
+    CU(cudaEventRecord(d.ev[9], d.stream));
+    CU(cudaEventSynchronize(d.ev[9]));
+    float ms = 0;
+    cudaEventElapsedTime(&ms, d.ev[8], d.ev[9]);
+    times_.total_ms = ms;
+    for (auto &r : out) r.device_ms = ms;
+    return kOk;
+}
+
+int Engine::run_popcount(const std::vector<Request> &reqs, std::vector<Result> &out, Error &err) {
+    out.assign(reqs.size(), Result());
     DeviceGenome &d = *dev_;
     const HostGenome &h = host_;
     const Bit4Tables &t = bit4();
@@ -992,9 +843,6 @@ int Engine::search(const std::vector<Request> &reqs, std::vector<Result> &out, E
     times_.format_ms = ms;
     cudaEventElapsedTime(&ms, d.ev[4], d.ev[5]);
     times_.d2h_ms = ms;
-    cudaEventElapsedTime(&ms, d.ev[0], d.ev[5]);
-    times_.total_ms = ms;
-    for (auto &r : out) r.device_ms = times_.total_ms;
     return kOk;
 }
 

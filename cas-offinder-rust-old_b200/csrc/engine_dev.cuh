@@ -1,0 +1,227 @@
+// engine_dev.cuh -- device-side definitions shared by the popcount path
+// (engine.cu) and the bulge path (bulge.cu): the resident genome, search
+// batches, small device helpers and scratch buffers.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "cof_engine.h"
+
+namespace cof {
+
+#define CU(call)                                                                     \
+    do {                                                                             \
+        cudaError_t e_ = (call);                                                     \
+        if (e_ != cudaSuccess) {                                                     \
+            err = {e_ == cudaErrorMemoryAllocation ? kOom : kCuda,                   \
+                   std::string(#call) + ": " + cudaGetErrorString(e_)};              \
+            return err.code;                                                         \
+        }                                                                            \
+    } while (0)
+
+// One search batch of the reference (SearchChunkInfo, search.rs:57-90): the
+// chunks [first, first + nch) of the stream, starting at nucleotide `base`.
+struct BatchDev {
+    uint64_t base;         // global nucleotide index of the batch start
+    uint32_t valid;        // valid nucleotides (2 x tight-packed bytes)
+    uint32_t pad0;
+    uint32_t first;        // first chunk
+    uint32_t nch;          // chunks in the batch
+    uint32_t active_start; // Myers active start (search.rs:1087-1091)
+    uint32_t pad;
+};
+
+// BIT4_TO_STR of bit4ops.rs:118 for one nibble: 0 -> NUL, T C Y A W M H G
+// K S B R D V N for 1..15 (one byte per nibble value, little endian).
+__device__ __forceinline__ char b4char(uint32_t v) {
+    constexpr unsigned long long lo = 0x484D574159435400ull;  // 7..0: H M W A Y C T NUL
+    constexpr unsigned long long hi = 0x4E56445242534B47ull;  // 15..8: N V D R B S K G
+    return (char)(((v & 8) ? hi : lo) >> ((v & 7) * 8));
+}
+
+// Popcount path records.
+struct Hit {
+    uint32_t s_local, pattern, batch, pad;
+};
+
+struct Row {
+    uint64_t s_global;   // window start
+    uint64_t clip;       // batch end (exclusive); cells at or past it read 0
+    uint64_t pos;        // chrom_idx (record coordinate)
+    uint32_t chunk;
+    uint32_t pattern;
+    uint32_t mm;
+    uint32_t pad;
+};
+
+struct Counters {
+    uint32_t hits;
+    uint32_t rows;
+    uint32_t overflow;
+    uint32_t pad;
+    unsigned long long candidates;
+    unsigned long long pairs;
+};
+
+// Bulge path records.
+// A Myers/PAM candidate: end position t (batch-local) of pattern p.
+struct MyersCand {
+    uint32_t t_local, batch, pattern, pad;
+};
+// One enumerated alignment that survived classify and convert.
+struct MyersRow {
+    uint64_t start;      // global nucleotide index of the alignment start
+    uint64_t pos;        // chrom_idx (record coordinate)
+    uint64_t ops[2];     // 2 bits per op, forward order: 0 M, 1 S, 2 DNA bulge, 3 RNA bulge
+    uint32_t chunk, pattern;
+    uint8_t n_ops, mm, db, rb;
+    uint32_t pad;
+};
+
+__device__ __forceinline__ uint8_t nib(const uint8_t *__restrict__ g, uint64_t i) {
+    uint8_t b = __ldg(g + (i >> 1));
+    return (i & 1) ? (uint8_t)(b >> 4) : (uint8_t)(b & 0xF);
+}
+__device__ __forceinline__ uint8_t dcomp4(uint8_t v) {
+    return (uint8_t)(((v << 2) | (v >> 2)) & 0xF);
+}
+__device__ __forceinline__ bool single_base(uint8_t v) { return v && !(v & (v - 1)); }
+
+struct GenomeDev {
+    const uint8_t *bit4;
+    const uint64_t *boff, *start, *end;
+    const uint32_t *name_idx;
+    const char *names;
+    const uint32_t *name_off;
+    uint64_t n_chunks;
+};
+
+__device__ __forceinline__ uint32_t ndigits(uint64_t v) {
+    uint32_t d = 1;
+    while (v >= 10) { v /= 10; ++d; }
+    return d;
+}
+__device__ __forceinline__ char *put_u64(char *o, uint64_t v) {
+    char t[20];
+    int k = 0;
+    do { t[k++] = (char)('0' + v % 10); v /= 10; } while (v);
+    while (k) *o++ = t[--k];
+    return o;
+}
+
+template <class T>
+struct DevBuf {
+    T *p = nullptr;
+    size_t cap = 0;
+    int ensure(size_t n, Error &err) {
+        if (n <= cap) return kOk;
+        if (p) cudaFree(p);
+        p = nullptr;
+        cap = 0;
+        size_t want = std::max<size_t>(n, 64);
+        CU(cudaMalloc((void **)&p, want * sizeof(T)));
+        cap = want;
+        return kOk;
+    }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        cap = 0;
+    }
+};
+
+class DeviceGenome {
+  public:
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev[10] = {};
+    int n_sm = 0;
+    DevBuf<uint8_t> bit4;
+    DevBuf<uint32_t> planes;
+    uint64_t n_words = 0;
+    DevBuf<uint64_t> boff, start, end;
+    DevBuf<uint32_t> name_idx, name_off;
+    DevBuf<char> names;
+    uint64_t n_chunks = 0;
+    // per-search scratch
+    DevBuf<unsigned char> tables;
+    DevBuf<Hit> hits;
+    DevBuf<Row> rows;
+    DevBuf<uint64_t> keys, keys2, offs;
+    DevBuf<uint32_t> vals, vals2, lens, req_rows;
+    DevBuf<Counters> ctr;
+    DevBuf<char> text;
+    DevBuf<unsigned char> cub_tmp;
+    DevBuf<MyersCand> mcand;
+    DevBuf<MyersRow> mrows;
+    char *h_text = nullptr;
+    size_t h_text_cap = 0;
+
+    ~DeviceGenome() {
+        bit4.release(); planes.release(); boff.release(); start.release(); end.release();
+        name_idx.release(); name_off.release(); names.release(); tables.release();
+        hits.release(); rows.release(); keys.release(); keys2.release(); offs.release();
+        vals.release(); vals2.release(); lens.release(); req_rows.release(); ctr.release();
+        text.release(); cub_tmp.release(); mcand.release(); mrows.release();
+        if (h_text) cudaFreeHost(h_text);
+        for (auto &e : ev)
+            if (e) cudaEventDestroy(e);
+        if (stream) cudaStreamDestroy(stream);
+    }
+    GenomeDev view() const {
+        return GenomeDev{bit4.p, boff.p, start.p, end.p, name_idx.p, names.p, name_off.p, n_chunks};
+    }
+};
+
+struct HostBatch {
+    size_t first, last;
+    bool has_head;
+};
+
+// Send thread of search.rs:1531-1572.
+inline std::vector<HostBatch> make_batches(size_t n_chunks, uint32_t cps) {
+    std::vector<HostBatch> out;
+    size_t bfirst = 0, blen = 0;
+    bool head = false;
+    for (size_t k = 0; k < n_chunks; ++k) {
+        if (blen == 0) bfirst = k;
+        ++blen;
+        if (blen == cps) {
+            out.push_back({bfirst, k, head});
+            bfirst = k;
+            blen = 1;
+            head = true;
+        }
+    }
+    if (blen && !(head && blen == 1)) out.push_back({bfirst, bfirst + blen - 1, head});
+    return out;
+}
+
+// Packs plain-old-data tables into one upload buffer.
+struct TablePack {
+    std::vector<unsigned char> buf;
+    template <class T>
+    size_t add(const std::vector<T> &v) {
+        size_t o = (buf.size() + 255) & ~size_t(255);
+        buf.resize(o + std::max<size_t>(v.size(), 1) * sizeof(T));
+        if (!v.empty()) std::memcpy(buf.data() + o, v.data(), v.size() * sizeof(T));
+        return o;
+    }
+};
+
+inline uint32_t code2(uint8_t b4) {  // single base one-hot -> 2-bit code A0 C1 G2 T3
+    switch (b4) {
+        case 4: return 0;
+        case 2: return 1;
+        case 8: return 2;
+        default: return 3;
+    }
+}
+
+
+}  // namespace cof

@@ -1,0 +1,92 @@
+"""GPU parity tests of the bulge (Myers + DP traceback) path against the oracle
+and the committed golden rows.  Bit-exact: sorted row sets must be equal."""
+import os
+import random
+
+import pytest
+
+import randgen
+
+pytestmark = pytest.mark.gpu
+
+
+def _rows(text):
+    return sorted(text.splitlines())
+
+
+def _both(cof_mod, oracle_mod, chunks):
+    g = cof_mod.Genome()
+    o = oracle_mod.OracleGenome()
+    for name, data, _nibs, s, e in chunks:
+        g.add_chunk(name, data, s, e)
+        o.add_chunk(name, data, s, e)
+    return g, o
+
+
+@pytest.mark.parametrize("cps", [0, 64, 3])
+def test_kat_bulge_rows(cof_mod, golden, cps):
+    # integration_bulge.rs:208-259 input; rows pinned by the oracle
+    g = cof_mod.Genome(os.path.join(golden, "upstream1000.fa"))
+    text, n = g.search("N" * 25 + "GG", ["CCGTGGTTCAACATTTGCTTAGCANNN"], 5, 1, 1,
+                       chunks_per_search=cps)
+    with open(os.path.join(golden, "kat_bulge_rows.txt")) as f:
+        want = f.read().splitlines()
+    assert _rows(text) == want and n == len(want)
+    for r in want:
+        c = r.split("\t")
+        assert len(c) == 8 and c[0] in ("X", "DNA", "RNA")
+
+
+@pytest.mark.parametrize("seed", range(20))
+def test_random_bulge_parity(cof_mod, oracle_mod, seed):
+    case = randgen.random_case(100 + seed, bulge=True)
+    g, o = _both(cof_mod, oracle_mod, case["chunks"])
+    text, n = g.search(case["filter"], case["patterns"], case["mm"], case["db"], case["rb"],
+                       chunks_per_search=case["cps"])
+    ref, nref = o.search(case["filter"], case["patterns"], case["mm"], case["db"], case["rb"],
+                         chunks_per_search=case["cps"])
+    assert _rows(text) == _rows(ref)
+    assert n == nref
+
+
+def test_bulge_shape_small(cof_mod, oracle_mod):
+    # the bulge benchmark shape (20 nt + NRG, mm <= 4, DNA/RNA bulges <= 2) on
+    # a 200 kb genome with planted bulged sites
+    import synth
+    cfg = synth.config_bulge(seed=9, scale=0.0004, n_guides=4, planted=3)
+    gen = cfg["genome"]
+    g = cof_mod.Genome()
+    o = oracle_mod.OracleGenome()
+    for name, data, s, e in gen.chunks():
+        g.add_chunk(name, data, s, e)
+        o.add_chunk(name, data, s, e)
+    args = (cfg["filter"], cfg["patterns"], 4, 2, 2)
+    text, n = g.search(*args)
+    ref, nref = o.search(*args)
+    assert n == nref > 1000
+    assert _rows(text) == _rows(ref)
+    st = g.last_stats()
+    assert st["candidates"] > 0 and st["rows"] == n
+
+
+def test_mixed_popcount_and_bulge_batch(cof_mod, oracle_mod):
+    rng = random.Random(77)
+    _, records = randgen.random_genome(rng, 3, 2000, 6000)
+    reqs = []
+    for k, (filt, mk, mm) in enumerate([randgen.REQUEST_SHAPES[i] for i in (0, 1, 2)]):
+        guides = ["".join(rng.choice("ACGT") for _ in range(25)) for _ in range(2)]
+        pats = [mk(x) for x in guides]
+        for p in pats:
+            randgen.plant_sites(rng, records, p, filt, 4, 2)
+        db, rb = [(0, 0), (1, 1), (2, 0)][k]
+        reqs.append(dict(search_filter=filt, patterns=pats, max_mismatches=min(mm, 3),
+                         max_dna_bulges=db, max_rna_bulges=rb))
+    chunks = randgen.chunk_records(rng, records, 700)
+    g, o = _both(cof_mod, oracle_mod, chunks)
+    batched = g.search_batch(reqs)
+    for r, (text, n) in zip(reqs, batched):
+        single, ns = g.search(**r)
+        ref, nref = o.search(r["search_filter"], r["patterns"], r["max_mismatches"],
+                             r["max_dna_bulges"], r["max_rna_bulges"])
+        assert _rows(text) == _rows(single) == _rows(ref)
+        assert n == ns == nref
