@@ -35,7 +35,8 @@ EXPORTS = (
     "cof_genome_create", "cof_genome_add_chunk", "cof_genome_load", "cof_genome_upload",
     "cof_genome_n_nucl", "cof_genome_n_chunks", "cof_genome_free", "cof_search",
     "cof_search_batch", "cof_result_free", "cof_genome_last_stats", "cof_last_error",
-    "cof_abi_version", "cof_search_seq_noalloc",
+    "cof_abi_version", "cof_search_seq_noalloc", "cof_server_create", "cof_server_submit",
+    "cof_server_wait", "cof_server_stats", "cof_server_free",
 )
 
 
@@ -68,6 +69,11 @@ class _Result(ctypes.Structure):
     ]
 
 
+class _ServerConfig(ctypes.Structure):
+    _fields_ = [("max_requests_per_pass", ctypes.c_uint32),
+                ("memory_budget_bytes", ctypes.c_uint64)]
+
+
 _lib = None
 
 
@@ -97,6 +103,13 @@ def load_library(path=LIB_PATH):
     lib.cof_genome_last_stats.argtypes = [vp, c.POINTER(c.c_double), c.POINTER(c.c_uint64)]
     lib.cof_last_error.restype = c.c_char_p
     lib.cof_abi_version.restype = c.c_int
+    lib.cof_server_create.argtypes = [vp, c.POINTER(_ServerConfig), c.POINTER(vp)]
+    lib.cof_server_submit.argtypes = [vp, c.POINTER(_Request), c.POINTER(c.c_uint64)]
+    lib.cof_server_wait.argtypes = [vp, c.c_uint64, c.c_int64, c.POINTER(_Result),
+                                    c.POINTER(c.c_double)]
+    lib.cof_server_stats.argtypes = [vp, c.POINTER(c.c_uint64)]
+    lib.cof_server_free.argtypes = [vp]
+    lib.cof_server_free.restype = None
     lib.cof_search_seq_noalloc.argtypes = [c.c_void_p, c.c_uint64, c.c_char_p,
                                            c.POINTER(c.c_char_p), c.c_size_t, c.c_uint32,
                                            c.c_void_p, c.c_uint32, c.POINTER(c.c_uint32),
@@ -238,3 +251,58 @@ def search(devices, max_mismatches, max_dna_bulges, max_rna_bulges, search_filte
     text, _ = genome.search(search_filter_ascii, patterns_ascii, max_mismatches, max_dna_bulges,
                             max_rna_bulges, add_revcomp=False)
     return text.splitlines()
+
+
+class Server:
+    """Continuous-batching request loop over a resident Genome
+    (cof_server_*).  max_requests_per_pass=1 is the plain loop."""
+
+    def __init__(self, genome, max_requests_per_pass=0, memory_budget_bytes=0):
+        self.genome = genome
+        cfg = _ServerConfig(max_requests_per_pass, memory_budget_bytes)
+        h = ctypes.c_void_p()
+        _check(_lib.cof_server_create(genome._h, ctypes.byref(cfg), ctypes.byref(h)))
+        self._h = h
+        self._keep = {}
+
+    def submit(self, search_filter, patterns, max_mismatches, max_dna_bulges=0,
+               max_rna_bulges=0, add_revcomp=True, chunks_per_search=0):
+        keep = []
+        r = _make_request(search_filter, patterns, max_mismatches, max_dna_bulges,
+                          max_rna_bulges, add_revcomp, chunks_per_search, keep)
+        t = ctypes.c_uint64()
+        _check(_lib.cof_server_submit(self._h, ctypes.byref(r), ctypes.byref(t)))
+        return t.value
+
+    def wait(self, ticket, timeout_ms=-1, as_text=True):
+        """Returns (rows, n_rows, latency_ms); rows as str, bytes or None."""
+        o = _Result()
+        lat = ctypes.c_double()
+        _check(_lib.cof_server_wait(self._h, ticket, timeout_ms, ctypes.byref(o),
+                                    ctypes.byref(lat)))
+        if as_text is None:
+            data = o.text_len
+        else:
+            data = ctypes.string_at(o.text, o.text_len) if o.text_len else b""
+            if as_text:
+                data = data.decode("latin-1")
+        n = o.n_rows
+        _lib.cof_result_free(ctypes.byref(o))
+        return data, n, lat.value
+
+    def stats(self):
+        s = (ctypes.c_uint64 * 4)()
+        _check(_lib.cof_server_stats(self._h, s))
+        return dict(passes=s[0], completed=s[1], queued=s[2], largest_pass=s[3])
+
+    def close(self):
+        if getattr(self, "_h", None):
+            _lib.cof_server_free(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+

@@ -75,6 +75,19 @@ int fill_result(const cof::Result &r, cof_result *out) {
 namespace cof {
 // Records a failure for cof_last_error() from code outside this file.
 int set_last_error(int code, const std::string &msg) { return fail(code, msg); }
+
+// Entry points of the request server (server.cpp) into a genome handle.
+int genome_search(cof_genome *g, const std::vector<Request> &reqs, std::vector<Result> &out,
+                  Error &err) {
+    std::lock_guard<std::mutex> lk(g->mu);
+    return g->engine.search(reqs, out, err);
+}
+uint64_t genome_nucl(const cof_genome *g) { return g->engine.host().n_nucl(); }
+int genome_free_device_bytes(cof_genome *g, uint64_t *free_bytes, Error &err) {
+    std::lock_guard<std::mutex> lk(g->mu);
+    if (g->engine.upload(err)) return err.code;
+    return g->engine.free_device_bytes(free_bytes, err);
+}
 }  // namespace cof
 
 extern "C" {

@@ -112,6 +112,7 @@ class Engine {
     bool uploaded() const { return dev_ != nullptr; }
     int upload(Error &err);
     int search(const std::vector<Request> &reqs, std::vector<Result> &out, Error &err);
+    int free_device_bytes(uint64_t *free_bytes, Error &err);
     const StageTimes &last_times() const { return times_; }
     int device() const { return device_; }
 

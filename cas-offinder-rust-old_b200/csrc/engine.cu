@@ -30,6 +30,7 @@
 
 #include <algorithm>
 #include <cstring>
+#include <map>
 #include <memory>
 #include <string>
 #include <vector>
@@ -313,6 +314,7 @@ scan_kernel(ScanParams P, uint64_t total_tiles_unused) {
 
 __global__ void verify_kernel(GenomeDev G, const BatchDev *__restrict__ batches,
                               const ExactPattern *__restrict__ pats,
+                              const uint32_t *__restrict__ fast2exact,
                               const RequestDev *__restrict__ reqs, const Hit *__restrict__ hits,
                               uint32_t n_hits, Row *__restrict__ rows, uint64_t *__restrict__ keys,
                               uint32_t *__restrict__ vals, Counters *ctr,
@@ -321,7 +323,8 @@ __global__ void verify_kernel(GenomeDev G, const BatchDev *__restrict__ batches,
          i += gridDim.x * blockDim.x) {
         const Hit h = hits[i];
         const BatchDev B = batches[h.batch];
-        const ExactPattern &P = pats[h.pattern];
+        const uint32_t pe = fast2exact[h.pattern];
+        const ExactPattern &P = pats[pe];
         const RequestDev &R = reqs[P.request];
         const uint32_t L = P.L;
         const uint64_t sg = B.base + h.s_local;
@@ -358,8 +361,8 @@ __global__ void verify_kernel(GenomeDev G, const BatchDev *__restrict__ batches,
         }
         if (!pam_ok || actual > R.max_mm) continue;
         const uint32_t r = atomicAdd(&ctr->rows, 1u);
-        rows[r] = Row{sg, B.base + B.valid, pos, k, h.pattern, actual, 0};
-        keys[r] = ((uint64_t)h.pattern << 34) | sg;
+        rows[r] = Row{sg, B.base + B.valid, pos, k, pe, actual, 0};
+        keys[r] = ((uint64_t)pe << 34) | sg;
         vals[r] = r;
         atomicAdd(&req_rows[P.request], 1u);
     }
@@ -510,6 +513,14 @@ int Engine::upload(Error &err) {
 // host orchestration
 // ---------------------------------------------------------------------------
 
+int Engine::free_device_bytes(uint64_t *free_bytes, Error &err) {
+    CU(cudaSetDevice(device_));
+    size_t f = 0, total = 0;
+    CU(cudaMemGetInfo(&f, &total));
+    *free_bytes = f;
+    return kOk;
+}
+
 int Engine::search(const std::vector<Request> &reqs, std::vector<Result> &out, Error &err) {
     times_ = StageTimes();
     out.assign(reqs.size(), Result());
@@ -591,6 +602,12 @@ int Engine::run_popcount(const std::vector<Request> &reqs, std::vector<Result> &
     std::vector<ScanGroup> groups;
     std::vector<ScanSeg> segs;
     std::vector<uint32_t> req_first_pat;
+    // Exact patterns are laid out request-major (the row sort key); scan
+    // groups gather the patterns of every request that shares a filter and a
+    // strand, so that one PAM sweep serves all of them.
+    std::vector<uint32_t> fast2exact;
+    std::map<std::pair<std::string, uint32_t>, std::vector<uint32_t>> by_filter;
+    std::vector<std::pair<std::string, uint32_t>> key_order;
     for (size_t ri = 0; ri < reqs.size(); ++ri) {
         const Request &r = reqs[ri];
         const uint32_t L = (uint32_t)r.filter.size();
@@ -610,99 +627,113 @@ int Engine::run_popcount(const std::vector<Request> &reqs, std::vector<Result> &
         rdev.push_back(rd);
         req_first_pat.push_back((uint32_t)epats.size());
         const size_t np = r.patterns.size(), nfwd = np / 2;
-        for (uint32_t strand = 0; strand < 2; ++strand) {
-            const size_t pb = strand ? nfwd : 0, pe = strand ? np : nfwd;
-            if (pb == pe) continue;
-            ScanGroup proto{};
-            for (uint32_t c = 0; c < L; ++c) {
-                if (rd.fisn[strand][c]) continue;
-                if (proto.n_pam == kMaxPamCells) break;
-                const uint8_t fs = rd.fset[strand][c];
-                PamCell pc{c, (fs & 4) ? ~0u : 0u, (fs & 2) ? ~0u : 0u, (fs & 8) ? ~0u : 0u,
-                           (fs & 1) ? ~0u : 0u};
-                proto.pam[proto.n_pam++] = pc;
-            }
-            // scan segments: one per batch, shared by this strand's groups
-            proto.seg_begin = (uint32_t)segs.size();
-            uint64_t tiles = 0;
-            for (size_t bi = 0; bi < batches.size(); ++bi) {
-                const BatchDev &b = batches[bi];
-                // legacy_match_start_min_nucl (search.rs:540-546): starts in the
-                // head chunk that the previous batch already emitted
-                const uint64_t c1 = hb[bi].has_head ? b.active_start : 0;
-                const uint64_t msmin = c1 > L - 1 ? c1 - (L - 1) : 0;
-                ScanSeg sgm{};
-                sgm.lo = b.base + msmin;
-                sgm.hi = b.base + b.valid;
-                if (sgm.hi <= sgm.lo) continue;
-                sgm.base = b.base;
-                sgm.w0 = sgm.lo / 32;
-                sgm.tile_begin = tiles;
-                sgm.batch = (uint32_t)bi;
-                tiles += (sgm.hi - sgm.w0 * 32 + 1023) / 1024;
-                segs.push_back(sgm);
-            }
-            proto.seg_end = (uint32_t)segs.size();
-            if (proto.seg_end - proto.seg_begin > (uint32_t)kMaxSegs) {
-                err = {kUnsupported, "too many search batches for one scan launch"};
-                return err.code;
-            }
-            if (proto.seg_end == proto.seg_begin) continue;
-            // compile the strand's patterns, ordered by care mask
-            std::vector<std::pair<FastPattern, ExactPattern>> comp;
-            for (size_t p = pb; p < pe; ++p) {
-                FastPattern fp{0, 0, 0, (int32_t)r.max_mm};
-                ExactPattern ep{};
-                ep.request = (uint32_t)ri;
-                ep.strand = strand;
-                ep.L = L;
-                ep.max_mm = r.max_mm;
-                for (uint32_t c = 0; c < L; ++c) {
-                    const uint8_t v = t.str2b4[1][(uint8_t)r.patterns[p][c]];
-                    ep.b4[c] = v;
-                    if (v && !(v & (v - 1))) {
-                        const uint32_t cd = code2(v);
-                        fp.care |= 1u << c;
-                        fp.h |= ((cd >> 1) & 1u) << c;
-                        fp.l |= (cd & 1u) << c;
-                    }
-                }
-                comp.push_back({fp, ep});
-            }
-            std::stable_sort(comp.begin(), comp.end(),
-                             [](const std::pair<FastPattern, ExactPattern> &a,
-                                const std::pair<FastPattern, ExactPattern> &b) {
-                                 return a.first.care < b.first.care;
-                             });
-            // groups of at most kMaxCareClasses classes
-            ScanGroup g = proto;
-            g.pat_begin = (uint32_t)fpats.size();
-            g.n_class = 0;
-            for (size_t i = 0; i < comp.size(); ++i) {
-                const uint32_t care = comp[i].first.care;
-                const bool new_class = g.n_class == 0 || g.cls[g.n_class - 1].care != care;
-                if (new_class && g.n_class == (uint32_t)kMaxCareClasses) {
-                    g.pat_end = (uint32_t)fpats.size();
-                    groups.push_back(g);
-                    g = proto;
-                    g.pat_begin = (uint32_t)fpats.size();
-                    g.n_class = 0;
-                }
-                const uint32_t rel = (uint32_t)fpats.size() - g.pat_begin;
-                if (g.n_class == 0 || g.cls[g.n_class - 1].care != care)
-                    g.cls[g.n_class++] = CareClass{care, rel, rel, 0};
-                g.cls[g.n_class - 1].pat_end = rel + 1;
-                fpats.push_back(comp[i].first);
-                epats.push_back(comp[i].second);
-            }
-            g.pat_end = (uint32_t)fpats.size();
-            groups.push_back(g);
+        for (size_t p = 0; p < np; ++p) {
+            const uint32_t strand = p >= nfwd;
+            ExactPattern ep{};
+            ep.request = (uint32_t)ri;
+            ep.strand = strand;
+            ep.L = L;
+            ep.max_mm = r.max_mm;
+            for (uint32_t c = 0; c < L; ++c) ep.b4[c] = t.str2b4[1][(uint8_t)r.patterns[p][c]];
+            // filters are compared case-insensitively for N, exactly otherwise
+            std::string key = r.filter;
+            for (char &ch : key) ch = (char)((ch >= 'a' && ch <= 'z') ? ch - 32 : ch);
+            auto k = std::make_pair(key, strand);
+            if (!by_filter.count(k)) key_order.push_back(k);
+            by_filter[k].push_back((uint32_t)epats.size());
+            epats.push_back(ep);
         }
+    }
+    for (const auto &key : key_order) {
+        const std::vector<uint32_t> &members = by_filter[key];
+        const uint32_t strand = key.second;
+        const RequestDev &rd = rdev[epats[members[0]].request];
+        const uint32_t L = rd.L;
+        ScanGroup proto{};
+        for (uint32_t c = 0; c < L; ++c) {
+            if (rd.fisn[strand][c]) continue;
+            if (proto.n_pam == kMaxPamCells) break;
+            const uint8_t fs = rd.fset[strand][c];
+            PamCell pc{c, (fs & 4) ? ~0u : 0u, (fs & 2) ? ~0u : 0u, (fs & 8) ? ~0u : 0u,
+                       (fs & 1) ? ~0u : 0u};
+            proto.pam[proto.n_pam++] = pc;
+        }
+        // scan segments: one per batch
+        proto.seg_begin = (uint32_t)segs.size();
+        uint64_t tiles = 0;
+        for (size_t bi = 0; bi < batches.size(); ++bi) {
+            const BatchDev &b = batches[bi];
+            // legacy_match_start_min_nucl (search.rs:540-546): starts in the
+            // head chunk that the previous batch already emitted
+            const uint64_t c1 = hb[bi].has_head ? b.active_start : 0;
+            const uint64_t msmin = c1 > L - 1 ? c1 - (L - 1) : 0;
+            ScanSeg sgm{};
+            sgm.lo = b.base + msmin;
+            sgm.hi = b.base + b.valid;
+            if (sgm.hi <= sgm.lo) continue;
+            sgm.base = b.base;
+            sgm.w0 = sgm.lo / 32;
+            sgm.tile_begin = tiles;
+            sgm.batch = (uint32_t)bi;
+            tiles += (sgm.hi - sgm.w0 * 32 + 1023) / 1024;
+            segs.push_back(sgm);
+        }
+        proto.seg_end = (uint32_t)segs.size();
+        if (proto.seg_end - proto.seg_begin > (uint32_t)kMaxSegs) {
+            err = {kUnsupported, "too many search batches for one scan launch"};
+            return err.code;
+        }
+        if (proto.seg_end == proto.seg_begin) continue;
+        // scan form of the members, ordered by care mask
+        std::vector<std::pair<FastPattern, uint32_t>> comp;
+        for (uint32_t e : members) {
+            const ExactPattern &ep = epats[e];
+            FastPattern fp{0, 0, 0, (int32_t)ep.max_mm};
+            for (uint32_t c = 0; c < L; ++c) {
+                const uint8_t v = ep.b4[c];
+                if (v && !(v & (v - 1))) {
+                    const uint32_t cd = code2(v);
+                    fp.care |= 1u << c;
+                    fp.h |= ((cd >> 1) & 1u) << c;
+                    fp.l |= (cd & 1u) << c;
+                }
+            }
+            comp.push_back({fp, e});
+        }
+        std::stable_sort(comp.begin(), comp.end(),
+                         [](const std::pair<FastPattern, uint32_t> &x,
+                            const std::pair<FastPattern, uint32_t> &y) {
+                             return x.first.care < y.first.care;
+                         });
+        // groups of at most kMaxCareClasses classes
+        ScanGroup g = proto;
+        g.pat_begin = (uint32_t)fpats.size();
+        g.n_class = 0;
+        for (size_t i = 0; i < comp.size(); ++i) {
+            const uint32_t care = comp[i].first.care;
+            const bool new_class = g.n_class == 0 || g.cls[g.n_class - 1].care != care;
+            if (new_class && g.n_class == (uint32_t)kMaxCareClasses) {
+                g.pat_end = (uint32_t)fpats.size();
+                groups.push_back(g);
+                g = proto;
+                g.pat_begin = (uint32_t)fpats.size();
+                g.n_class = 0;
+            }
+            const uint32_t rel = (uint32_t)fpats.size() - g.pat_begin;
+            if (g.n_class == 0 || g.cls[g.n_class - 1].care != care)
+                g.cls[g.n_class++] = CareClass{care, rel, rel, 0};
+            g.cls[g.n_class - 1].pat_end = rel + 1;
+            fpats.push_back(comp[i].first);
+            fast2exact.push_back(comp[i].second);
+        }
+        g.pat_end = (uint32_t)fpats.size();
+        groups.push_back(g);
     }
 
     TablePack tp;
     const size_t o_batch = tp.add(batches), o_rdev = tp.add(rdev), o_fp = tp.add(fpats),
-                 o_ep = tp.add(epats), o_grp = tp.add(groups), o_seg = tp.add(segs);
+                 o_ep = tp.add(epats), o_grp = tp.add(groups), o_seg = tp.add(segs),
+                 o_f2e = tp.add(fast2exact);
     if (d.tables.ensure(tp.buf.size(), err)) return err.code;
     cudaStream_t s = d.stream;
     CU(cudaEventRecord(d.ev[0], s));
@@ -764,6 +795,7 @@ int Engine::run_popcount(const std::vector<Request> &reqs, std::vector<Result> &
         unsigned vb = (unsigned)std::min<uint64_t>((n_hits + 255) / 256, (uint64_t)d.n_sm * 8);
         verify_kernel<<<vb, 256, 0, s>>>(d.view(), (const BatchDev *)tab(o_batch),
                                          (const ExactPattern *)tab(o_ep),
+                                         (const uint32_t *)tab(o_f2e),
                                          (const RequestDev *)tab(o_rdev), d.hits.p, n_hits,
                                          d.rows.p, d.keys.p, d.vals.p, d.ctr.p, d.req_rows.p);
         CU(cudaGetLastError());

@@ -133,6 +133,34 @@ COF_API int cof_search_batch(cof_genome *g, const cof_request *reqs, size_t n_re
 
 COF_API void cof_result_free(cof_result *r);
 
+/* Continuous-batching request server over a resident genome.  No reference
+ * counterpart.  A worker thread repeatedly admits queued requests in arrival
+ * order while their estimated device memory for candidate and row buffers
+ * fits memory_budget_bytes (0 = half of the device memory free after the
+ * genome upload) and, if max_requests_per_pass > 0, at most that many; runs
+ * them as one cof_search_batch pass; and completes their tickets.  Requests
+ * submitted while a pass runs join the next pass.  max_requests_per_pass = 1
+ * gives the plain one-request-per-pass loop.  Direct searches on the same
+ * genome are serialised with the server's passes. */
+typedef struct cof_server cof_server;
+typedef struct {
+    uint32_t max_requests_per_pass;
+    uint64_t memory_budget_bytes;
+} cof_server_config;
+
+COF_API int cof_server_create(cof_genome *g, const cof_server_config *cfg, cof_server **out);
+/* Queues a copy of *req; *ticket identifies it for cof_server_wait. */
+COF_API int cof_server_submit(cof_server *s, const cof_request *req, uint64_t *ticket);
+/* Waits up to timeout_ms (< 0: forever) for a ticket; COF_E_TIMEOUT if it is
+ * still pending.  On completion fills *out (free with cof_result_free) and
+ * *latency_ms (submit to completion, host clock) and forgets the ticket. */
+COF_API int cof_server_wait(cof_server *s, uint64_t ticket, int64_t timeout_ms, cof_result *out,
+                            double *latency_ms);
+/* stats4 = {passes, completed requests, queued requests, largest pass}. */
+COF_API int cof_server_stats(cof_server *s, uint64_t *stats4);
+/* Finishes the queued requests, stops the worker and frees the server. */
+COF_API void cof_server_free(cof_server *s);
+
 /* Device timings and counters of the last search on `g`: ms5 = {scan,
  * verify, format, device->host copy, total} milliseconds (CUDA events);
  * counts5 = {PAM-passing windows, window x pattern comparisons, scan
