@@ -52,6 +52,10 @@ def parse():
     ap.add_argument("--cpu-sample-s", type=float, default=15.0,
                     help="target seconds of CPU work for the CPU baseline")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--serving-requests", type=int, default=64)
+    ap.add_argument("--serving-rate", type=float, default=200.0, help="arrivals per second")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip the batched mixed-PAM and serving measurements")
     return ap.parse_args()
 
 
@@ -134,6 +138,98 @@ def make_workload(args, rank):
         rng = np.random.default_rng(1000 + rank)
         cfg["patterns"] = [synth.random_guide(rng, 20) + "NNN" for _ in range(args.guides)]
     return cfg
+
+
+def mixed_pam_requests(seed=3, n_each=50):
+    """Batched workload: 50 x (25 nt + NNGRRT) and 50 x (TTTN + 25 nt), mm <= 6."""
+    import numpy as np
+    import synth
+    rng = np.random.default_rng(seed)
+    a = [synth.random_guide(rng, 25) + "NNNNNN" for _ in range(n_each)]
+    b = ["NNNN" + synth.random_guide(rng, 25) for _ in range(n_each)]
+    return [dict(search_filter="N" * 25 + "NNGRRT", patterns=a, max_mismatches=6),
+            dict(search_filter="TTTN" + "N" * 25, patterns=b, max_mismatches=6)]
+
+
+def bench_mixed_pam(g, n_nt, steps):
+    """Both guide sets in one pass (cof_search_batch) vs one pass each."""
+    reqs = mixed_pam_requests()
+    both = g.prepare(reqs)
+    single = [g.prepare([r]) for r in reqs]
+    g.run_prepared(both, as_text=None)
+    for p in single:
+        g.run_prepared(p, as_text=None)
+    bat, plain = [], []
+    for _ in range(steps):
+        g.run_prepared(both, as_text=None)
+        st = g.last_stats()
+        bat.append(st["total_ms"])
+        t = 0.0
+        for p in single:
+            g.run_prepared(p, as_text=None)
+            t += g.last_stats()["total_ms"]
+        plain.append(t)
+    work = n_nt * 1e-9 * 100
+    b, p = statistics.median(bat), statistics.median(plain)
+    return {"workload": "50 x (25 nt + NNGRRT) + 50 x (TTTN + 25 nt), mm<=6, same genome",
+            "batched_value": work / (b * 1e-3), "plain_value": work / (p * 1e-3),
+            "unit": UNIT, "batched_ms": b, "plain_ms": p, "speedup": p / b}
+
+
+def serving_requests(n, seed=5):
+    """Request mix of the serving stream: guides log-uniform in 1..500,
+    guide length U{17..25}, PAM in {NRG, NNGRRT, TTTN, NNNRRT}, mm U{0..4},
+    no bulges (see DESIGN.md for why bulges and mm 5-6 are left out)."""
+    import numpy as np
+    import synth
+    rng = np.random.default_rng(seed)
+    pams = [("NRG", False), ("NNGRRT", False), ("TTTN", True), ("NNNRRT", False)]
+    out = []
+    for _ in range(n):
+        ng = int(round(np.exp(rng.uniform(0, np.log(500)))))
+        gl = int(rng.integers(17, 26))
+        pam, five = pams[int(rng.integers(0, 4))]
+        mm = int(rng.integers(0, 5))
+        guides = [synth.random_guide(rng, gl) for _ in range(ng)]
+        if five:
+            filt = pam + "N" * gl
+            pats = ["N" * len(pam) + x for x in guides]
+        else:
+            filt = "N" * gl + pam
+            pats = [x + "N" * len(pam) for x in guides]
+        out.append(dict(search_filter=filt, patterns=pats, max_mismatches=mm))
+    return out
+
+
+def bench_serving(cof, g, n_nt, n_req, rate, seed=7):
+    import numpy as np
+    reqs = serving_requests(n_req)
+    rng = np.random.default_rng(seed)
+    arrivals = np.cumsum(rng.exponential(1.0 / rate, size=n_req))
+    work = sum(n_nt * 1e-9 * len(r["patterns"]) for r in reqs)
+    res = {}
+    for mode, per_pass in (("plain", 1), ("batched", 0)):
+        srv = cof.Server(g, max_requests_per_pass=per_pass)
+        t0 = time.perf_counter()
+        tickets = []
+        for a, r in zip(arrivals, reqs):
+            dt = t0 + a - time.perf_counter()
+            if dt > 0:
+                time.sleep(dt)
+            tickets.append(srv.submit(**r))
+        lats = [srv.wait(t, as_text=None)[2] for t in tickets]
+        span = time.perf_counter() - t0
+        st = srv.stats()
+        srv.close()
+        lats.sort()
+        res[mode] = {"value": work / span, "unit": UNIT, "makespan_s": span,
+                     "p50_ms": lats[len(lats) // 2],
+                     "p99_ms": lats[min(len(lats) - 1, int(0.99 * len(lats)))],
+                     "passes": st["passes"], "largest_pass": st["largest_pass"]}
+    res["speedup"] = res["batched"]["value"] / res["plain"]["value"]
+    res["workload"] = (f"{n_req} requests, Poisson arrivals at {rate:g}/s, guides log-uniform "
+                       f"1..500 (17-25 nt), PAM NRG/NNGRRT/TTTN/NNNRRT, mm 0..4, no bulges")
+    return res
 
 
 def cpu_baseline(cfg, target_s, n_threads=0):
@@ -301,6 +397,9 @@ def main():
         "genome_upload_s": t_upload, "genome_generate_s": t_gen,
         "clocks": clk,
     }
+    if not args.no_extras and world == 1:
+        line["batched_mixed_pam"] = bench_mixed_pam(g, n_nt, max(3, args.steps // 2))
+        line["serving"] = bench_serving(cof, g, n_nt, args.serving_requests, args.serving_rate)
     if not args.no_cpu_baseline and world == 1:
         base, _ = cpu_baseline(cfg, args.cpu_sample_s)
         line["cpu_baseline"] = base

@@ -157,11 +157,15 @@ constexpr int kCpt = kQCap / 32;       // queued windows per lane in a flush
 constexpr int kSmemPatterns = 2048;    // patterns staged in shared memory
 constexpr int kMaxSegs = 64;
 
+constexpr uint32_t kSpanTiles = 64;    // 1024-start tiles per work item
+
 struct ScanParams {
     const uint32_t *H, *L, *S;
     const ScanGroup *groups;
     const ScanSeg *segs;
     const FastPattern *pats;
+    const uint64_t *item_begin;  // per group: first work item; [n_groups] = total
+    uint32_t n_groups;
     Hit *hits;
     uint32_t hit_cap;
     Counters *ctr;
@@ -206,105 +210,150 @@ __device__ __noinline__ void flush_queue(const uint4 *q, int n, const FastPatter
     }
 }
 
+// Persistent scan: CTAs pull work items -- a span of kSpanTiles tiles of one
+// scan group -- from a global counter, so groups of very different sizes
+// (few or many patterns, sparse or dense PAMs) share the GPU evenly.  A CTA
+// stages a group's patterns in shared memory when it switches groups; each
+// warp takes every kScanWarps-th tile of the span.
 __global__ void __launch_bounds__(kScanWarps * 32, 3)
-scan_kernel(ScanParams P, uint64_t total_tiles_unused) {
+scan_kernel(ScanParams P) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     uint4 *queues = reinterpret_cast<uint4 *>(smem_raw);
     FastPattern *spat = reinterpret_cast<FastPattern *>(queues + kScanWarps * kQSlots);
     __shared__ ScanGroup sg;
     __shared__ ScanSeg ssegs[kMaxSegs];
+    __shared__ unsigned long long s_item;
+    __shared__ uint32_t s_group;
 
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    if (threadIdx.x == 0) sg = P.groups[blockIdx.y];
-    __syncthreads();
-    const uint32_t nseg = sg.seg_end - sg.seg_begin;
-    for (uint32_t i = threadIdx.x; i < nseg; i += blockDim.x) ssegs[i] = P.segs[sg.seg_begin + i];
-    const uint32_t npat = sg.pat_end - sg.pat_begin;
-    const FastPattern *pt = P.pats + sg.pat_begin;
-    if (npat <= (uint32_t)kSmemPatterns) {
-        for (uint32_t i = threadIdx.x; i < npat; i += blockDim.x) spat[i] = pt[i];
-        pt = spat;
-    }
-    __syncthreads();
-    const uint64_t total_tiles = ssegs[nseg - 1].tile_begin +
-        ((ssegs[nseg - 1].hi - ssegs[nseg - 1].w0 * 32 + 1023) >> 10);
-
     uint4 *q = queues + warp * kQSlots;
     int qn = 0;
     uint32_t qbatch = 0xFFFFFFFFu;
     const uint32_t lt_mask = (1u << lane) - 1u;
-    unsigned long long ncand = 0;
+    unsigned long long ncand = 0, npairs = 0;
+    uint32_t cur_g = 0xFFFFFFFFu, nseg = 0, npat = 0;
+    uint64_t g_tiles = 0;
+    const FastPattern *pt = spat;
+    const uint64_t total_items = P.item_begin[P.n_groups];
 
-    const uint64_t gw = (uint64_t)blockIdx.x * kScanWarps + warp;
-    const uint64_t gstride = (uint64_t)gridDim.x * kScanWarps;
-    uint32_t sidx = 0;
-    for (uint64_t tile = gw; tile < total_tiles; tile += gstride) {
-        while (sidx + 1 < nseg && tile >= ssegs[sidx + 1].tile_begin) ++sidx;
-        const ScanSeg &sgm = ssegs[sidx];
-        if (sgm.batch != qbatch) {
-            if (qn) {
+    while (true) {
+        if (threadIdx.x == 0) {
+            const unsigned long long it = atomicAdd(&P.ctr->next_item, 1ull);
+            uint32_t lo = 0, hi = P.n_groups;
+            if (it < total_items) {
+                while (hi - lo > 1) {
+                    const uint32_t mid = (lo + hi) >> 1;
+                    if (P.item_begin[mid] <= it) lo = mid; else hi = mid;
+                }
+            }
+            s_item = it;
+            s_group = lo;
+        }
+        __syncthreads();
+        const uint64_t item = s_item;
+        const uint32_t g = s_group;
+        if (item >= total_items) break;
+        if (g != cur_g) {
+            if (qn) {  // the queue belongs to the previous group's patterns
                 __syncwarp();
                 flush_queue(q, qn, pt, sg, qbatch, P, lane);
                 __syncwarp();
                 qn = 0;
             }
-            qbatch = sgm.batch;
-        }
-        const uint64_t w = sgm.w0 + (tile - sgm.tile_begin) * 32 + lane;
-        const uint32_t h0 = __ldg(P.H + w), h1 = __ldg(P.H + w + 1);
-        const uint32_t l0 = __ldg(P.L + w), l1 = __ldg(P.L + w + 1);
-        const uint32_t s0 = __ldg(P.S + w), s1 = __ldg(P.S + w + 1);
-        // window starts 32w + k in [lo, hi)
-        const uint64_t p0 = w * 32;
-        uint32_t m = 0xFFFFFFFFu;
-        if (p0 < sgm.lo) m = (sgm.lo - p0 >= 32) ? 0u : (m << (uint32_t)(sgm.lo - p0));
-        if (p0 + 32 > sgm.hi) m = (sgm.hi <= p0) ? 0u : (m & (0xFFFFFFFFu >> (uint32_t)(32 - (sgm.hi - p0))));
-        for (uint32_t c = 0; c < sg.n_pam && m; ++c) {
-            const PamCell pc = sg.pam[c];
-            const uint32_t h = __funnelshift_r(h0, h1, pc.cell);
-            const uint32_t l = __funnelshift_r(l0, l1, pc.cell);
-            const uint32_t s = __funnelshift_r(s0, s1, pc.cell);
-            const uint32_t t0 = (l & pc.fc) | (~l & pc.fa);
-            const uint32_t t1 = (l & pc.ft) | (~l & pc.fg);
-            m &= ((h & t1) | (~h & t0)) & ~s;
-        }
-        ncand += __popc(m);
-        // drain PAM-passing starts into the warp queue, one per lane per step
-        while (__any_sync(0xFFFFFFFFu, m)) {
-            const bool has = m != 0;
-            const uint32_t bal = __ballot_sync(0xFFFFFFFFu, has);
-            if (has) {
-                const uint32_t k = __ffs(m) - 1;
-                m &= m - 1;
-                const int slot = qn + __popc(bal & lt_mask);
-                q[slot] = make_uint4((uint32_t)(p0 + k - sgm.base), __funnelshift_r(h0, h1, k),
-                                     __funnelshift_r(l0, l1, k), __funnelshift_r(s0, s1, k));
+            __syncthreads();
+            if (threadIdx.x == 0) sg = P.groups[g];
+            __syncthreads();
+            nseg = sg.seg_end - sg.seg_begin;
+            for (uint32_t i = threadIdx.x; i < nseg; i += blockDim.x) ssegs[i] = P.segs[sg.seg_begin + i];
+            npat = sg.pat_end - sg.pat_begin;
+            pt = P.pats + sg.pat_begin;
+            if (npat <= (uint32_t)kSmemPatterns) {
+                for (uint32_t i = threadIdx.x; i < npat; i += blockDim.x) spat[i] = pt[i];
+                pt = spat;
             }
-            qn += __popc(bal);
-            if (qn >= kQCap) {
-                // full pass over kQCap windows; the (< 32) windows beyond it
-                // move to the front of the queue
-                __syncwarp();
-                flush_queue(q, kQCap, pt, sg, qbatch, P, lane);
-                const int rest = qn - kQCap;
-                uint4 e = make_uint4(0, 0, 0, 0);
-                if (lane < rest) e = q[kQCap + lane];
-                __syncwarp();
-                if (lane < rest) q[lane] = e;
-                __syncwarp();
-                qn = rest;
+            __syncthreads();
+            g_tiles = ssegs[nseg - 1].tile_begin +
+                      ((ssegs[nseg - 1].hi - ssegs[nseg - 1].w0 * 32 + 1023) >> 10);
+            cur_g = g;
+            qbatch = 0xFFFFFFFFu;
+        }
+        const uint64_t t_begin = (item - P.item_begin[g]) * kSpanTiles;
+        const uint64_t t_end = min(t_begin + kSpanTiles, g_tiles);
+        uint32_t sidx = 0;
+        for (uint64_t tile = t_begin + warp; tile < t_end; tile += kScanWarps) {
+            while (sidx + 1 < nseg && tile >= ssegs[sidx + 1].tile_begin) ++sidx;
+            const ScanSeg &sgm = ssegs[sidx];
+            if (sgm.batch != qbatch) {
+                if (qn) {
+                    __syncwarp();
+                    flush_queue(q, qn, pt, sg, qbatch, P, lane);
+                    __syncwarp();
+                    qn = 0;
+                }
+                qbatch = sgm.batch;
+            }
+            const uint64_t w = sgm.w0 + (tile - sgm.tile_begin) * 32 + lane;
+            const uint32_t h0 = __ldg(P.H + w), h1 = __ldg(P.H + w + 1);
+            const uint32_t l0 = __ldg(P.L + w), l1 = __ldg(P.L + w + 1);
+            const uint32_t s0 = __ldg(P.S + w), s1 = __ldg(P.S + w + 1);
+            // window starts 32w + k in [lo, hi)
+            const uint64_t p0 = w * 32;
+            uint32_t m = 0xFFFFFFFFu;
+            if (p0 < sgm.lo) m = (sgm.lo - p0 >= 32) ? 0u : (m << (uint32_t)(sgm.lo - p0));
+            if (p0 + 32 > sgm.hi) m = (sgm.hi <= p0) ? 0u : (m & (0xFFFFFFFFu >> (uint32_t)(32 - (sgm.hi - p0))));
+            for (uint32_t c = 0; c < sg.n_pam && m; ++c) {
+                const PamCell pc = sg.pam[c];
+                const uint32_t h = __funnelshift_r(h0, h1, pc.cell);
+                const uint32_t l = __funnelshift_r(l0, l1, pc.cell);
+                const uint32_t s = __funnelshift_r(s0, s1, pc.cell);
+                const uint32_t t0 = (l & pc.fc) | (~l & pc.fa);
+                const uint32_t t1 = (l & pc.ft) | (~l & pc.fg);
+                m &= ((h & t1) | (~h & t0)) & ~s;
+            }
+            const uint32_t nm = __popc(m);
+            ncand += nm;
+            npairs += (unsigned long long)nm * npat;
+            // drain PAM-passing starts into the warp queue, one per lane per step
+            while (__any_sync(0xFFFFFFFFu, m)) {
+                const bool has = m != 0;
+                const uint32_t bal = __ballot_sync(0xFFFFFFFFu, has);
+                if (has) {
+                    const uint32_t k = __ffs(m) - 1;
+                    m &= m - 1;
+                    const int slot = qn + __popc(bal & lt_mask);
+                    q[slot] = make_uint4((uint32_t)(p0 + k - sgm.base), __funnelshift_r(h0, h1, k),
+                                         __funnelshift_r(l0, l1, k), __funnelshift_r(s0, s1, k));
+                }
+                qn += __popc(bal);
+                if (qn >= kQCap) {
+                    // full pass over kQCap windows; the (< 32) windows beyond it
+                    // move to the front of the queue
+                    __syncwarp();
+                    flush_queue(q, kQCap, pt, sg, qbatch, P, lane);
+                    const int rest = qn - kQCap;
+                    uint4 e = make_uint4(0, 0, 0, 0);
+                    if (lane < rest) e = q[kQCap + lane];
+                    __syncwarp();
+                    if (lane < rest) q[lane] = e;
+                    __syncwarp();
+                    qn = rest;
+                }
             }
         }
+        __syncthreads();  // s_item / s_group are rewritten by the next fetch
     }
     if (qn) {
         __syncwarp();
         flush_queue(q, qn, pt, sg, qbatch, P, lane);
     }
-    // candidate count (for the roofline's algorithmic work)
-    for (int o = 16; o; o >>= 1) ncand += __shfl_down_sync(0xFFFFFFFFu, ncand, o);
+    // candidate and pair counts (the roofline's algorithmic work)
+    for (int o = 16; o; o >>= 1) {
+        ncand += __shfl_down_sync(0xFFFFFFFFu, ncand, o);
+        npairs += __shfl_down_sync(0xFFFFFFFFu, npairs, o);
+    }
     if (lane == 0 && ncand) {
         atomicAdd(&P.ctr->candidates, ncand);
-        atomicAdd(&P.ctr->pairs, ncand * (unsigned long long)npat);
+        atomicAdd(&P.ctr->pairs, npairs);
     }
 }
 
@@ -731,9 +780,16 @@ int Engine::run_popcount(const std::vector<Request> &reqs, std::vector<Result> &
     }
 
     TablePack tp;
+    // work items: spans of kSpanTiles tiles per group
+    std::vector<uint64_t> item_begin{0};
+    for (const ScanGroup &g : groups) {
+        const ScanSeg &last = segs[g.seg_end - 1];
+        const uint64_t tiles = last.tile_begin + (last.hi - last.w0 * 32 + 1023) / 1024;
+        item_begin.push_back(item_begin.back() + (tiles + kSpanTiles - 1) / kSpanTiles);
+    }
     const size_t o_batch = tp.add(batches), o_rdev = tp.add(rdev), o_fp = tp.add(fpats),
                  o_ep = tp.add(epats), o_grp = tp.add(groups), o_seg = tp.add(segs),
-                 o_f2e = tp.add(fast2exact);
+                 o_f2e = tp.add(fast2exact), o_items = tp.add(item_begin);
     if (d.tables.ensure(tp.buf.size(), err)) return err.code;
     cudaStream_t s = d.stream;
     CU(cudaEventRecord(d.ev[0], s));
@@ -753,6 +809,8 @@ int Engine::run_popcount(const std::vector<Request> &reqs, std::vector<Result> &
             sp.groups = (const ScanGroup *)tab(o_grp);
             sp.segs = (const ScanSeg *)tab(o_seg);
             sp.pats = (const FastPattern *)tab(o_fp);
+            sp.item_begin = (const uint64_t *)tab(o_items);
+            sp.n_groups = (uint32_t)groups.size();
             sp.hits = d.hits.p;
             sp.hit_cap = (uint32_t)std::min<size_t>(d.hits.cap, 0xFFFFFFF0u);
             sp.ctr = d.ctr.p;
@@ -761,9 +819,10 @@ int Engine::run_popcount(const std::vector<Request> &reqs, std::vector<Result> &
             int occ = 0;
             CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, scan_kernel, kScanWarps * 32, smem));
             occ = std::max(occ, 1);
-            unsigned gx = (unsigned)std::max<int>(1, (d.n_sm * occ) / (int)groups.size());
+            const uint64_t n_items = item_begin.back();
+            const unsigned gx = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>(n_items, (uint64_t)d.n_sm * occ));
             CU(cudaEventRecord(d.ev[1], s));
-            scan_kernel<<<dim3(gx, (unsigned)groups.size()), kScanWarps * 32, smem, s>>>(sp, 0);
+            scan_kernel<<<gx, kScanWarps * 32, smem, s>>>(sp);
             CU(cudaGetLastError());
             CU(cudaEventRecord(d.ev[2], s));
             ++times_.kernel_launches;

@@ -66,6 +66,7 @@ struct Counters {
     uint32_t pad;
     unsigned long long candidates;
     unsigned long long pairs;
+    unsigned long long next_item;  // work-item counter of the persistent scan
 };
 
 // Bulge path records.
