@@ -394,6 +394,7 @@ def main():
                       for k in ("scan_ms", "verify_ms", "format_ms", "d2h_ms", "total_ms")},
         "rows_per_step": rows_per_step, "candidates_per_step": stats[-1]["candidates"],
         "pairs_per_step": pairs,
+        "scan_tile_shape": g.tuning()["last"],
         "genome_upload_s": t_upload, "genome_generate_s": t_gen,
         "clocks": clk,
     }

@@ -36,7 +36,7 @@ EXPORTS = (
     "cof_genome_n_nucl", "cof_genome_n_chunks", "cof_genome_free", "cof_search",
     "cof_search_batch", "cof_result_free", "cof_genome_last_stats", "cof_last_error",
     "cof_abi_version", "cof_search_seq_noalloc", "cof_server_create", "cof_server_submit",
-    "cof_server_wait", "cof_server_stats", "cof_server_free",
+    "cof_server_wait", "cof_server_stats", "cof_server_free", "cof_genome_tuning",
 )
 
 
@@ -103,6 +103,7 @@ def load_library(path=LIB_PATH):
     lib.cof_genome_last_stats.argtypes = [vp, c.POINTER(c.c_double), c.POINTER(c.c_uint64)]
     lib.cof_last_error.restype = c.c_char_p
     lib.cof_abi_version.restype = c.c_int
+    lib.cof_genome_tuning.argtypes = [vp, c.c_char_p, c.c_size_t]
     lib.cof_server_create.argtypes = [vp, c.POINTER(_ServerConfig), c.POINTER(vp)]
     lib.cof_server_submit.argtypes = [vp, c.POINTER(_Request), c.POINTER(c.c_uint64)]
     lib.cof_server_wait.argtypes = [vp, c.c_uint64, c.c_int64, c.POINTER(_Result),
@@ -220,6 +221,13 @@ class Genome:
         return dict(scan_ms=ms[0], verify_ms=ms[1], format_ms=ms[2], d2h_ms=ms[3],
                     total_ms=ms[4], candidates=cnt[0], pairs=cnt[1], raw_hits=cnt[2],
                     rows=cnt[3], kernel_launches=cnt[4])
+
+    def tuning(self):
+        """Autotuner state (dict)."""
+        import json
+        buf = ctypes.create_string_buffer(1 << 16)
+        _check(_lib.cof_genome_tuning(self._h, buf, len(buf)))
+        return json.loads(buf.value.decode())
 
     def close(self):
         if getattr(self, "_h", None):

@@ -1,4 +1,5 @@
 // cabi.cpp -- extern "C" entry points of libcof.so (declared in include/cof.h).
+#include <cstdio>
 #include <cstdlib>
 #include <cstring>
 #include <mutex>
@@ -200,6 +201,20 @@ COF_API int cof_genome_last_stats(const cof_genome *g, double *ms5, uint64_t *co
     counts5[3] = t.rows;
     counts5[4] = t.kernel_launches;
     return COF_OK;
+}
+
+// Autotuner state of a genome: JSON {"last": tile shape of the last scan,
+// "variant": its index, "cache": {shape key: variant index}}.  No reference
+// counterpart.
+COF_API int cof_genome_tuning(cof_genome *g, char *buf, size_t len) {
+    if (!g || !buf || !len) return fail(COF_E_BADINPUT, "null argument");
+    std::lock_guard<std::mutex> lk(g->mu);
+    const cof::StageTimes &t = g->engine.last_times();
+    std::string js = "{\"last\": \"" + t.scan_shape + "\", \"variant\": " +
+                     std::to_string(t.scan_variant) + ", \"cache\": " +
+                     g->engine.tuner().report() + "}";
+    std::snprintf(buf, len, "%s", js.c_str());
+    return js.size() < len ? COF_OK : fail(COF_E_BADINPUT, "buffer too small");
 }
 
 }  // extern "C"

@@ -6,6 +6,7 @@
 
 #include <cstddef>
 #include <cstdint>
+#include <map>
 #include <string>
 #include <vector>
 
@@ -92,6 +93,23 @@ struct Result {
 struct StageTimes {
     double scan_ms = 0, verify_ms = 0, format_ms = 0, d2h_ms = 0, total_ms = 0;
     uint64_t candidates = 0, pairs = 0, raw_hits = 0, rows = 0, kernel_launches = 0;
+    int scan_variant = -1;        // tile shape the scan ran with
+    std::string scan_shape;
+};
+
+// Scan tile-shape choices per request shape.  Enabled unless COF_AUTOTUNE=0;
+// if COF_TUNE_CACHE names a file, choices are read from and appended to it.
+class Tuner {
+  public:
+    bool enabled() const;
+    bool lookup(const std::string &key, int &variant);
+    void store(const std::string &key, int variant);
+    std::string report() const;  // JSON object key -> variant index
+
+  private:
+    void load();
+    std::map<std::string, int> cache_;
+    bool loaded_ = false;
 };
 
 // Sets the message returned by cof_last_error() on this thread; returns code.
@@ -114,6 +132,7 @@ class Engine {
     int search(const std::vector<Request> &reqs, std::vector<Result> &out, Error &err);
     int free_device_bytes(uint64_t *free_bytes, Error &err);
     const StageTimes &last_times() const { return times_; }
+    Tuner &tuner() { return tuner_; }
     int device() const { return device_; }
 
   private:
@@ -123,6 +142,7 @@ class Engine {
     HostGenome host_;
     DeviceGenome *dev_ = nullptr;
     StageTimes times_;
+    Tuner tuner_;
 };
 
 }  // namespace cof

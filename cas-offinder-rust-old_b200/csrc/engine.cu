@@ -29,6 +29,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <memory>
@@ -150,14 +151,13 @@ __global__ void pack_planes_kernel(const uint4 *__restrict__ bit4, uint64_t n_wo
 // scan: PAM prefilter + warp-queue compaction + popcount compare
 // ---------------------------------------------------------------------------
 
-constexpr int kScanWarps = 8;
-constexpr int kQCap = 256;             // flush threshold per warp queue
-constexpr int kQSlots = kQCap + 32;    // one drain step adds at most 32
-constexpr int kCpt = kQCap / 32;       // queued windows per lane in a flush
+// Tile shape of the scan (chosen per request shape by the autotuner):
+//   CPT   queued windows per lane in a flush (the queue flushes at 32 x CPT)
+//   WARPS warps per CTA
+//   MINB  CTAs per SM the register allocation is bounded for
 constexpr int kSmemPatterns = 2048;    // patterns staged in shared memory
 constexpr int kMaxSegs = 64;
 
-constexpr uint32_t kSpanTiles = 64;    // 1024-start tiles per work item
 
 struct ScanParams {
     const uint32_t *H, *L, *S;
@@ -166,15 +166,17 @@ struct ScanParams {
     const FastPattern *pats;
     const uint64_t *item_begin;  // per group: first work item; [n_groups] = total
     uint32_t n_groups;
+    uint32_t span_tiles;         // 1024-start tiles per work item
     Hit *hits;
     uint32_t hit_cap;
     Counters *ctr;
 };
 
-// Compares the first n <= kQCap queued windows with every pattern of the
-// group, kCpt windows per lane.  Per care class the windows are masked once;
+// Compares the first n <= 32 x CPT queued windows with every pattern of the
+// group, CPT windows per lane.  Per care class the windows are masked once;
 // per pattern the lane keeps the minimum mismatch count over its windows and
 // only a pattern whose minimum passes takes the (rare) emitting branch.
+template <int kCpt>
 __device__ __noinline__ void flush_queue(const uint4 *q, int n, const FastPattern *pt,
                                             const ScanGroup &G, uint32_t batch,
                                             const ScanParams &P, int lane) {
@@ -215,8 +217,11 @@ __device__ __noinline__ void flush_queue(const uint4 *q, int n, const FastPatter
 // (few or many patterns, sparse or dense PAMs) share the GPU evenly.  A CTA
 // stages a group's patterns in shared memory when it switches groups; each
 // warp takes every kScanWarps-th tile of the span.
-__global__ void __launch_bounds__(kScanWarps * 32, 3)
+template <int kCpt, int kScanWarps, int kMinBlocks>
+__global__ void __launch_bounds__(kScanWarps * 32, kMinBlocks)
 scan_kernel(ScanParams P) {
+    constexpr int kQCap = 32 * kCpt;     // flush threshold per warp queue
+    constexpr int kQSlots = kQCap + 32;  // one drain step adds at most 32
     extern __shared__ __align__(16) unsigned char smem_raw[];
     uint4 *queues = reinterpret_cast<uint4 *>(smem_raw);
     FastPattern *spat = reinterpret_cast<FastPattern *>(queues + kScanWarps * kQSlots);
@@ -256,7 +261,7 @@ scan_kernel(ScanParams P) {
         if (g != cur_g) {
             if (qn) {  // the queue belongs to the previous group's patterns
                 __syncwarp();
-                flush_queue(q, qn, pt, sg, qbatch, P, lane);
+                flush_queue<kCpt>(q, qn, pt, sg, qbatch, P, lane);
                 __syncwarp();
                 qn = 0;
             }
@@ -277,8 +282,8 @@ scan_kernel(ScanParams P) {
             cur_g = g;
             qbatch = 0xFFFFFFFFu;
         }
-        const uint64_t t_begin = (item - P.item_begin[g]) * kSpanTiles;
-        const uint64_t t_end = min(t_begin + kSpanTiles, g_tiles);
+        const uint64_t t_begin = (item - P.item_begin[g]) * P.span_tiles;
+        const uint64_t t_end = min(t_begin + P.span_tiles, g_tiles);
         uint32_t sidx = 0;
         for (uint64_t tile = t_begin + warp; tile < t_end; tile += kScanWarps) {
             while (sidx + 1 < nseg && tile >= ssegs[sidx + 1].tile_begin) ++sidx;
@@ -286,7 +291,7 @@ scan_kernel(ScanParams P) {
             if (sgm.batch != qbatch) {
                 if (qn) {
                     __syncwarp();
-                    flush_queue(q, qn, pt, sg, qbatch, P, lane);
+                    flush_queue<kCpt>(q, qn, pt, sg, qbatch, P, lane);
                     __syncwarp();
                     qn = 0;
                 }
@@ -329,7 +334,7 @@ scan_kernel(ScanParams P) {
                     // full pass over kQCap windows; the (< 32) windows beyond it
                     // move to the front of the queue
                     __syncwarp();
-                    flush_queue(q, kQCap, pt, sg, qbatch, P, lane);
+                    flush_queue<kCpt>(q, kQCap, pt, sg, qbatch, P, lane);
                     const int rest = qn - kQCap;
                     uint4 e = make_uint4(0, 0, 0, 0);
                     if (lane < rest) e = q[kQCap + lane];
@@ -344,7 +349,7 @@ scan_kernel(ScanParams P) {
     }
     if (qn) {
         __syncwarp();
-        flush_queue(q, qn, pt, sg, qbatch, P, lane);
+        flush_queue<kCpt>(q, qn, pt, sg, qbatch, P, lane);
     }
     // candidate and pair counts (the roofline's algorithmic work)
     for (int o = 16; o; o >>= 1) {
@@ -356,6 +361,27 @@ scan_kernel(ScanParams P) {
         atomicAdd(&P.ctr->pairs, npairs);
     }
 }
+
+struct ScanVariant {
+    int cpt, warps, min_blocks;
+    uint32_t span_tiles;
+    void (*kernel)(ScanParams);
+    size_t smem() const {
+        return (size_t)warps * (32 * cpt + 32) * sizeof(uint4) + kSmemPatterns * sizeof(FastPattern);
+    }
+};
+
+template <int C, int W, int B>
+constexpr ScanVariant variant(uint32_t span) {
+    return ScanVariant{C, W, B, span, scan_kernel<C, W, B>};
+}
+
+// Candidate tile shapes; the autotuner times them on a sample of the genome.
+const ScanVariant kScanVariants[] = {
+    variant<8, 8, 3>(64),  variant<4, 8, 4>(64),  variant<16, 8, 2>(64),
+    variant<8, 4, 6>(32),  variant<16, 4, 4>(32), variant<4, 16, 2>(128),
+};
+constexpr int kNumScanVariants = sizeof(kScanVariants) / sizeof(kScanVariants[0]);
 
 // ---------------------------------------------------------------------------
 // verify: the reference's exact decision per candidate hit
@@ -780,16 +806,42 @@ int Engine::run_popcount(const std::vector<Request> &reqs, std::vector<Result> &
     }
 
     TablePack tp;
-    // work items: spans of kSpanTiles tiles per group
-    std::vector<uint64_t> item_begin{0};
+    // work items: spans of span_tiles tiles per group (a table per span in
+    // use).  The autotuner's sample is the first tune_tiles tiles of every
+    // group, sized so that the sample alone fills every SM.
+    uint64_t full_tiles = 0;
     for (const ScanGroup &g : groups) {
         const ScanSeg &last = segs[g.seg_end - 1];
-        const uint64_t tiles = last.tile_begin + (last.hi - last.w0 * 32 + 1023) / 1024;
-        item_begin.push_back(item_begin.back() + (tiles + kSpanTiles - 1) / kSpanTiles);
+        full_tiles += last.tile_begin + (last.hi - last.w0 * 32 + 1023) / 1024;
     }
+    // ~16 work items of 64 tiles per resident CTA, so that the sample runs in
+    // steady state rather than in its tail
+    const uint64_t tune_tiles =
+        std::max<uint64_t>(256, (uint64_t)16 * 64 * 3 * d.n_sm / std::max<size_t>(groups.size(), 1));
+    auto make_items = [&](uint32_t span, uint64_t cap_tiles) {
+        std::vector<uint64_t> ib{0};
+        for (const ScanGroup &g : groups) {
+            const ScanSeg &last = segs[g.seg_end - 1];
+            const uint64_t tiles = std::min<uint64_t>(
+                last.tile_begin + (last.hi - last.w0 * 32 + 1023) / 1024, cap_tiles);
+            ib.push_back(ib.back() + (tiles + span - 1) / span);
+        }
+        return ib;
+    };
+    std::map<uint32_t, size_t> o_items, o_sample;
+    std::map<uint32_t, uint64_t> n_items, n_sample;
     const size_t o_batch = tp.add(batches), o_rdev = tp.add(rdev), o_fp = tp.add(fpats),
                  o_ep = tp.add(epats), o_grp = tp.add(groups), o_seg = tp.add(segs),
-                 o_f2e = tp.add(fast2exact), o_items = tp.add(item_begin);
+                 o_f2e = tp.add(fast2exact);
+    for (const ScanVariant &v : kScanVariants) {
+        if (o_items.count(v.span_tiles)) continue;
+        auto full = make_items(v.span_tiles, ~0ull);
+        auto samp = make_items(v.span_tiles, tune_tiles);
+        n_items[v.span_tiles] = full.back();
+        n_sample[v.span_tiles] = samp.back();
+        o_items[v.span_tiles] = tp.add(full);
+        o_sample[v.span_tiles] = tp.add(samp);
+    }
     if (d.tables.ensure(tp.buf.size(), err)) return err.code;
     cudaStream_t s = d.stream;
     CU(cudaEventRecord(d.ev[0], s));
@@ -798,34 +850,93 @@ int Engine::run_popcount(const std::vector<Request> &reqs, std::vector<Result> &
     if (d.ctr.ensure(1, err) || d.req_rows.ensure(reqs.size(), err)) return err.code;
     if (d.hits.cap == 0 && d.hits.ensure(1u << 22, err)) return err.code;
 
+    ScanParams sp{};
+    sp.H = d.planes.p;
+    sp.L = d.planes.p + d.n_words;
+    sp.S = d.planes.p + 2 * d.n_words;
+    sp.groups = (const ScanGroup *)tab(o_grp);
+    sp.segs = (const ScanSeg *)tab(o_seg);
+    sp.pats = (const FastPattern *)tab(o_fp);
+    sp.n_groups = (uint32_t)groups.size();
+    sp.hits = d.hits.p;
+    sp.ctr = d.ctr.p;
+    // launches variant v over the full work list or over the tuning sample
+    auto launch = [&](const ScanVariant &v, bool sample) -> int {
+        const size_t smem = v.smem();
+        CU(cudaFuncSetAttribute(v.kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        int occ = 0;
+        CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, v.kernel, v.warps * 32, smem));
+        occ = std::max(occ, 1);
+        sp.span_tiles = v.span_tiles;
+        sp.item_begin = (const uint64_t *)tab(sample ? o_sample[v.span_tiles] : o_items[v.span_tiles]);
+        sp.hit_cap = (uint32_t)std::min<size_t>(d.hits.cap, 0xFFFFFFF0u);
+        const uint64_t items = sample ? n_sample[v.span_tiles] : n_items[v.span_tiles];
+        const unsigned gx = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>(items, (uint64_t)d.n_sm * occ));
+        CU(cudaMemsetAsync(d.ctr.p, 0, sizeof(Counters), s));
+        v.kernel<<<gx, v.warps * 32, smem, s>>>(sp);
+        CU(cudaGetLastError());
+        ++times_.kernel_launches;
+        return kOk;
+    };
+
     Counters hc{};
     if (!groups.empty()) {
+        // autotuner: the fastest tile shape for this request shape, timed on
+        // the first kTuneTiles tiles of every group; cached per shape
+        uint32_t tot_pat = 0, max_l = 0, n_pam = 0, max_mm = 0;
+        for (const ScanGroup &g : groups) {
+            tot_pat += g.pat_end - g.pat_begin;
+            n_pam += g.n_pam;
+        }
+        for (const RequestDev &r : rdev) {
+            max_l = std::max(max_l, r.L);
+            max_mm = std::max(max_mm, r.max_mm);
+        }
+        // shape key: patterns per group (power-of-4 bucket), groups (bucket),
+        // PAM cells per group, longest pattern, largest threshold
+        const uint32_t per_group = tot_pat / (uint32_t)groups.size();
+        uint32_t bucket = 1;
+        while (bucket < per_group) bucket <<= 2;
+        const uint32_t gbucket = groups.size() <= 2 ? (uint32_t)groups.size()
+                                 : groups.size() <= 8 ? 8u : 64u;
+        const std::string key = "pat" + std::to_string(bucket) + "-grp" + std::to_string(gbucket) +
+                                "-pam" + std::to_string(n_pam / groups.size()) + "-L" +
+                                std::to_string(max_l) + "-mm" + std::to_string(max_mm);
+        // tuning pays off only when the search is much larger than its sample
+        const bool worth = full_tiles >= 8 * tune_tiles * groups.size();
+        int vi = 0;
+        const char *force = std::getenv("COF_SCAN_VARIANT");  // testing: pin a shape
+        if (force && *force) {
+            vi = std::max(0, std::min(kNumScanVariants - 1, std::atoi(force)));
+        } else if (!tuner_.lookup(key, vi) && tuner_.enabled() && worth) {
+            if (launch(kScanVariants[0], true)) return err.code;  // warm-up
+            float t[kNumScanVariants];
+            for (int k = 0; k < kNumScanVariants; ++k) t[k] = 1e30f;
+            for (int rep = 0; rep < 2; ++rep) {  // interleaved repeats, best of two
+                for (int k = 0; k < kNumScanVariants; ++k) {
+                    CU(cudaEventRecord(d.ev[1], s));
+                    if (launch(kScanVariants[k], true)) return err.code;
+                    CU(cudaEventRecord(d.ev[2], s));
+                    CU(cudaEventSynchronize(d.ev[2]));
+                    float ms = 0;
+                    cudaEventElapsedTime(&ms, d.ev[1], d.ev[2]);
+                    t[k] = std::min(t[k], ms);
+                }
+            }
+            // the default shape wins unless another is clearly faster
+            for (int k = 1; k < kNumScanVariants; ++k)
+                if (t[k] < 0.97f * t[vi]) vi = k;
+            tuner_.store(key, vi);
+        }
+        const ScanVariant &v = kScanVariants[vi];
+        times_.scan_variant = vi;
+        times_.scan_shape = "cpt" + std::to_string(v.cpt) + "-warps" + std::to_string(v.warps) +
+                            "-minb" + std::to_string(v.min_blocks) + "-span" +
+                            std::to_string(v.span_tiles);
         for (int attempt = 0; attempt < 2; ++attempt) {
-            CU(cudaMemsetAsync(d.ctr.p, 0, sizeof(Counters), s));
-            ScanParams sp;
-            sp.H = d.planes.p;
-            sp.L = d.planes.p + d.n_words;
-            sp.S = d.planes.p + 2 * d.n_words;
-            sp.groups = (const ScanGroup *)tab(o_grp);
-            sp.segs = (const ScanSeg *)tab(o_seg);
-            sp.pats = (const FastPattern *)tab(o_fp);
-            sp.item_begin = (const uint64_t *)tab(o_items);
-            sp.n_groups = (uint32_t)groups.size();
-            sp.hits = d.hits.p;
-            sp.hit_cap = (uint32_t)std::min<size_t>(d.hits.cap, 0xFFFFFFF0u);
-            sp.ctr = d.ctr.p;
-            const size_t smem = kScanWarps * kQSlots * sizeof(uint4) + kSmemPatterns * sizeof(FastPattern);
-            CU(cudaFuncSetAttribute(scan_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-            int occ = 0;
-            CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, scan_kernel, kScanWarps * 32, smem));
-            occ = std::max(occ, 1);
-            const uint64_t n_items = item_begin.back();
-            const unsigned gx = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>(n_items, (uint64_t)d.n_sm * occ));
             CU(cudaEventRecord(d.ev[1], s));
-            scan_kernel<<<gx, kScanWarps * 32, smem, s>>>(sp);
-            CU(cudaGetLastError());
+            if (launch(v, false)) return err.code;
             CU(cudaEventRecord(d.ev[2], s));
-            ++times_.kernel_launches;
             CU(cudaMemcpyAsync(&hc, d.ctr.p, sizeof(Counters), cudaMemcpyDeviceToHost, s));
             CU(cudaStreamSynchronize(s));
             if (!hc.overflow && hc.hits <= d.hits.cap) break;

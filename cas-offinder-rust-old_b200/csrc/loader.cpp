@@ -13,6 +13,7 @@
 #include <algorithm>
 #include <cerrno>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 
 #include "cof_engine.h"
@@ -317,6 +318,51 @@ int load_genome_path(HostGenome &g, const std::string &path, Error &err) {
         return err.code;
     }
     return buf[0] == '>' ? parse_fasta(g, buf, err) : parse_2bit(g, buf, err);
+}
+
+bool Tuner::enabled() const {
+    const char *e = std::getenv("COF_AUTOTUNE");
+    return !(e && std::strcmp(e, "0") == 0);
+}
+
+void Tuner::load() {
+    if (loaded_) return;
+    loaded_ = true;
+    const char *path = std::getenv("COF_TUNE_CACHE");
+    if (!path) return;
+    FILE *f = std::fopen(path, "r");
+    if (!f) return;
+    char key[256];
+    int v;
+    while (std::fscanf(f, "%255s %d", key, &v) == 2) cache_[key] = v;
+    std::fclose(f);
+}
+
+bool Tuner::lookup(const std::string &key, int &variant) {
+    load();
+    auto it = cache_.find(key);
+    if (it == cache_.end()) return false;
+    variant = it->second;
+    return true;
+}
+
+void Tuner::store(const std::string &key, int variant) {
+    cache_[key] = variant;
+    const char *path = std::getenv("COF_TUNE_CACHE");
+    if (!path) return;
+    if (FILE *f = std::fopen(path, "a")) {
+        std::fprintf(f, "%s %d\n", key.c_str(), variant);
+        std::fclose(f);
+    }
+}
+
+std::string Tuner::report() const {
+    std::string out = "{";
+    for (const auto &kv : cache_) {
+        if (out.size() > 1) out += ", ";
+        out += "\"" + kv.first + "\": " + std::to_string(kv.second);
+    }
+    return out + "}";
 }
 
 int make_request(const char *filter, size_t pattern_len, const char *const *patterns,

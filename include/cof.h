@@ -205,6 +205,14 @@ COF_API int cof_search_seq_noalloc(const uint8_t *d_bit4, uint64_t n_nucl,
                                    uint32_t *d_rows, uint32_t rows_cap, uint32_t *n_rows,
                                    void *stream);
 
+/* Autotuner state as JSON: {"last": tile shape of the last scan, "variant":
+ * its index, "cache": {request-shape key: variant index}}.  The scan's tile
+ * shape is chosen per request shape by timing the candidate shapes on a
+ * sample of the genome at the first search of that shape (COF_AUTOTUNE=0
+ * turns this off; COF_TUNE_CACHE=<file> persists the choices).  No reference
+ * counterpart. */
+COF_API int cof_genome_tuning(cof_genome *g, char *buf, size_t len);
+
 /* Message of the last failed call on this thread ("" if none). */
 COF_API const char *cof_last_error(void);
 

@@ -125,3 +125,26 @@ def test_cli_matches_oracle_cli(cof_mod, oracle_mod, golden, tmp_path):
         assert sorted(a[1:]) == sorted(b[1:]) and len(a) == 118
         log = (tmp_path / f"o{dev}.txt.log").read_text()
         assert "=== Cas-OFFinder Rust ===" in log and "Matches found: 117" in log
+
+
+@pytest.mark.parametrize("variant", range(6))
+def test_every_scan_tile_shape(cof_mod, oracle_mod, golden, variant, monkeypatch):
+    # the autotuner may pick any tile shape; all must give the same rows
+    monkeypatch.setenv("COF_SCAN_VARIANT", str(variant))
+    g = cof_mod.Genome(os.path.join(golden, "upstream1000.fa"))
+    text, n = g.search("N" * 24, KAT_PATS, 11)
+    assert n == 117 and _rows(text) == _golden_rows(golden, "kat_popcount_rows.txt")
+    case = randgen.random_case(variant + 40)
+    g2, o = _both(cof_mod, oracle_mod, case["chunks"])
+    text, _ = g2.search(case["filter"], case["patterns"], case["mm"], chunks_per_search=case["cps"])
+    ref, _ = o.search(case["filter"], case["patterns"], case["mm"], chunks_per_search=case["cps"])
+    assert _rows(text) == _rows(ref)
+    assert g2.tuning()["variant"] == variant
+
+
+def test_autotuner_records_choice(cof_mod, golden, monkeypatch):
+    monkeypatch.delenv("COF_SCAN_VARIANT", raising=False)
+    g = cof_mod.Genome(os.path.join(golden, "upstream1000.fa"))
+    g.search("N" * 24, KAT_PATS, 11)
+    t = g.tuning()
+    assert t["last"].startswith("cpt") and 0 <= t["variant"] < 6
