@@ -176,8 +176,8 @@ def bench_mixed_pam(g, n_nt, steps):
             "unit": UNIT, "batched_ms": b, "plain_ms": p, "speedup": p / b}
 
 
-def serving_requests(n, seed=5):
-    """Request mix of the serving stream: guides log-uniform in 1..500,
+def serving_requests(n, seed=5, max_guides=500, max_mm=4):
+    """Request mix of the serving stream: guides log-uniform in 1..max_guides,
     guide length U{17..25}, PAM in {NRG, NNGRRT, TTTN, NNNRRT}, mm U{0..4},
     no bulges (see DESIGN.md for why bulges and mm 5-6 are left out)."""
     import numpy as np
@@ -186,10 +186,10 @@ def serving_requests(n, seed=5):
     pams = [("NRG", False), ("NNGRRT", False), ("TTTN", True), ("NNNRRT", False)]
     out = []
     for _ in range(n):
-        ng = int(round(np.exp(rng.uniform(0, np.log(500)))))
+        ng = int(round(np.exp(rng.uniform(0, np.log(max_guides)))))
         gl = int(rng.integers(17, 26))
         pam, five = pams[int(rng.integers(0, 4))]
-        mm = int(rng.integers(0, 5))
+        mm = int(rng.integers(0, max_mm + 1))
         guides = [synth.random_guide(rng, gl) for _ in range(ng)]
         if five:
             filt = pam + "N" * gl
@@ -201,13 +201,17 @@ def serving_requests(n, seed=5):
     return out
 
 
-def bench_serving(cof, g, n_nt, n_req, rate, seed=7):
+def bench_serving(cof, g, n_nt, n_req, rate, seed=7, max_guides=500, max_mm=4):
     import numpy as np
-    reqs = serving_requests(n_req)
+    reqs = serving_requests(n_req, max_guides=max_guides, max_mm=max_mm)
     rng = np.random.default_rng(seed)
     arrivals = np.cumsum(rng.exponential(1.0 / rate, size=n_req))
     work = sum(n_nt * 1e-9 * len(r["patterns"]) for r in reqs)
     res = {}
+    # both modes run the default scan tile shape: first-time autotuning of a
+    # new request shape would otherwise be charged to whichever mode meets it
+    prev = os.environ.get("COF_AUTOTUNE")
+    os.environ["COF_AUTOTUNE"] = "0"
     for mode, per_pass in (("plain", 1), ("batched", 0)):
         srv = cof.Server(g, max_requests_per_pass=per_pass)
         t0 = time.perf_counter()
@@ -226,9 +230,14 @@ def bench_serving(cof, g, n_nt, n_req, rate, seed=7):
                      "p50_ms": lats[len(lats) // 2],
                      "p99_ms": lats[min(len(lats) - 1, int(0.99 * len(lats)))],
                      "passes": st["passes"], "largest_pass": st["largest_pass"]}
+    if prev is None:
+        os.environ.pop("COF_AUTOTUNE", None)
+    else:
+        os.environ["COF_AUTOTUNE"] = prev
     res["speedup"] = res["batched"]["value"] / res["plain"]["value"]
     res["workload"] = (f"{n_req} requests, Poisson arrivals at {rate:g}/s, guides log-uniform "
-                       f"1..500 (17-25 nt), PAM NRG/NNGRRT/TTTN/NNNRRT, mm 0..4, no bulges")
+                       f"1..{max_guides} (17-25 nt), PAM NRG/NNGRRT/TTTN/NNNRRT, mm 0..{max_mm}, "
+                       f"no bulges")
     return res
 
 
@@ -401,6 +410,8 @@ def main():
     if not args.no_extras and world == 1:
         line["batched_mixed_pam"] = bench_mixed_pam(g, n_nt, max(3, args.steps // 2))
         line["serving"] = bench_serving(cof, g, n_nt, args.serving_requests, args.serving_rate)
+        line["serving_small_requests"] = bench_serving(cof, g, n_nt, 4 * args.serving_requests,
+                                                       2000.0, seed=8, max_guides=4, max_mm=3)
     if not args.no_cpu_baseline and world == 1:
         base, _ = cpu_baseline(cfg, args.cpu_sample_s)
         line["cpu_baseline"] = base
