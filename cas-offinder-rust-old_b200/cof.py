@@ -27,6 +27,7 @@ COF_E_UNSUPPORTED = -5
 COF_E_STATE = -6
 COF_E_TIMEOUT = -7
 COF_F_ADD_REVCOMP = 1
+COF_F_RAW_MATCHES = 2
 
 HEADER = "#Bulge type\tcrRNA\tDNA\tChromosome\tPosition\tDirection\tMismatches\tBulge Size\n"
 
@@ -124,7 +125,7 @@ def _check(rc):
         raise CofError(rc, _lib.cof_last_error().decode(errors="replace"))
 
 
-def _make_request(filt, patterns, mm, db, rb, add_revcomp, cps, keep):
+def _make_request(filt, patterns, mm, db, rb, add_revcomp, cps, keep, raw=False):
     fb = filt.encode() if isinstance(filt, str) else bytes(filt)
     pb = [p.encode() if isinstance(p, str) else bytes(p) for p in patterns]
     arr = (ctypes.c_char_p * len(pb))(*pb)
@@ -137,7 +138,7 @@ def _make_request(filt, patterns, mm, db, rb, add_revcomp, cps, keep):
     r.max_mismatches = mm
     r.max_dna_bulges = db
     r.max_rna_bulges = rb
-    r.flags = COF_F_ADD_REVCOMP if add_revcomp else 0
+    r.flags = (COF_F_ADD_REVCOMP if add_revcomp else 0) | (COF_F_RAW_MATCHES if raw else 0)
     r.chunks_per_search = cps
     return r
 
@@ -173,13 +174,14 @@ class Genome:
         return _lib.cof_genome_n_chunks(self._h)
 
     def search(self, search_filter, patterns, max_mismatches, max_dna_bulges=0,
-               max_rna_bulges=0, add_revcomp=True, chunks_per_search=0):
-        """Returns (rows_text, n_rows) for one request."""
+               max_rna_bulges=0, add_revcomp=True, chunks_per_search=0, raw=False):
+        """Returns (rows_text, n_rows) for one request (raw=True: search()'s
+        Match lines, COF_F_RAW_MATCHES)."""
         return self.search_batch([dict(search_filter=search_filter, patterns=patterns,
                                        max_mismatches=max_mismatches,
                                        max_dna_bulges=max_dna_bulges,
                                        max_rna_bulges=max_rna_bulges, add_revcomp=add_revcomp,
-                                       chunks_per_search=chunks_per_search)])[0]
+                                       chunks_per_search=chunks_per_search, raw=raw)])[0]
 
     def prepare(self, requests):
         """Encodes requests once for repeated cof_search_batch calls."""
@@ -189,7 +191,7 @@ class Genome:
             reqs[i] = _make_request(r["search_filter"], r["patterns"], r["max_mismatches"],
                                     r.get("max_dna_bulges", 0), r.get("max_rna_bulges", 0),
                                     r.get("add_revcomp", True), r.get("chunks_per_search", 0),
-                                    keep)
+                                    keep, r.get("raw", False))
         return reqs, keep
 
     def run_prepared(self, prepared, as_text=True):

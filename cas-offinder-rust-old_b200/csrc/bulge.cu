@@ -55,7 +55,8 @@ struct MyersPattern {
 };
 
 struct MyersReqDev {
-    uint32_t L, mm, db, rb, E, W, pam_len, pad;
+    uint32_t L, mm, db, rb, E, W, pam_len, raw;  // raw: Match lines, not rows
+    uint32_t first_pattern, pad[3];
 };
 
 struct MyersTile {
@@ -337,6 +338,12 @@ __global__ void mrow_len_kernel(GenomeDev G, const MyersRow *__restrict__ rows,
         const uint32_t ni = G.name_idx[w.chunk];
         const uint32_t name_len = G.name_off[ni + 1] - G.name_off[ni];
         const uint32_t size = w.db + w.rb;
+        if (R.raw) {  // name pos pidx dir mm db rb rna dna
+            len[i] = name_len + 1 + ndigits(w.pos) + 1 + ndigits(w.pattern - R.first_pattern) + 3 +
+                     ndigits(w.mm) + 1 + ndigits(w.db) + 1 + ndigits(w.rb) + 1 + w.n_ops + 1 +
+                     w.n_ops + 1;
+            continue;
+        }
         const uint32_t tlen = size == 0 ? 1 : 3;
         len[i] = tlen + 1 + w.n_ops + 1 + w.n_ops + 1 + name_len + 1 +
                  ndigits(mpos_out(w, R, P.strand)) + 3 + ndigits(w.mm) + 1 + ndigits(size) + 1;
@@ -355,14 +362,30 @@ __global__ void mrow_write_kernel(GenomeDev G, const MyersRow *__restrict__ rows
         const bool fwd = P.strand == 0;
         char *o = text + off[i];
         const uint32_t size = w.db + w.rb;
-        if (size == 0) {
+        const uint32_t ni = G.name_idx[w.chunk];
+        if (R.raw) {  // search()'s Match: name, chrom_idx, pattern, strand, mm, db, rb
+            for (uint32_t c = G.name_off[ni]; c < G.name_off[ni + 1]; ++c) *o++ = G.names[c];
+            *o++ = '\t';
+            o = put_u64(o, w.pos);
+            *o++ = '\t';
+            o = put_u64(o, w.pattern - R.first_pattern);
+            *o++ = '\t';
+            *o++ = fwd ? '+' : '-';
+            *o++ = '\t';
+            o = put_u64(o, w.mm);
+            *o++ = '\t';
+            o = put_u64(o, w.db);
+            *o++ = '\t';
+            o = put_u64(o, w.rb);
+            *o++ = '\t';
+        } else if (size == 0) {
             *o++ = 'X';
         } else if (w.db > 0) {
             *o++ = 'D'; *o++ = 'N'; *o++ = 'A';
         } else {
             *o++ = 'R'; *o++ = 'N'; *o++ = 'A';
         }
-        *o++ = '\t';
+        if (!R.raw) *o++ = '\t';
         const uint32_t no = w.n_ops;
         char *rna = o;
         char *dna = o + no + 1;
@@ -395,8 +418,11 @@ __global__ void mrow_write_kernel(GenomeDev G, const MyersRow *__restrict__ rows
         o += no;
         *o++ = '\t';
         o += no;
+        if (R.raw) {
+            *o++ = '\n';
+            continue;
+        }
         *o++ = '\t';
-        const uint32_t ni = G.name_idx[w.chunk];
         for (uint32_t c = G.name_off[ni]; c < G.name_off[ni + 1]; ++c) *o++ = G.names[c];
         *o++ = '\t';
         o = put_u64(o, mpos_out(w, R, P.strand));
@@ -470,7 +496,8 @@ int Engine::run_bulge(const std::vector<Request> &reqs, std::vector<Result> &out
         const Request &r = reqs[ri];
         const uint32_t L = (uint32_t)r.filter.size();
         MyersReqDev rd{L, r.max_mm, r.max_db, r.max_rb, r.max_mm + r.max_db + r.max_rb,
-                       L + r.max_db, (uint32_t)r.pam_len, 0};
+                       L + r.max_db, (uint32_t)r.pam_len, r.raw ? 1u : 0u,
+                       (uint32_t)pats.size(), {0, 0, 0}};
         if (rd.W > (uint32_t)kMaxCells) {
             err = {kUnsupported, "pattern length + max_dna_bulges above 40"};
             return err.code;

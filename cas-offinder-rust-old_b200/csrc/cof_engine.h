@@ -73,6 +73,7 @@ struct Request {
     uint32_t max_mm = 0, max_db = 0, max_rb = 0;
     uint32_t cps = kDefaultCps;
     uint64_t pam_len = 0;               // main.rs:80-91
+    bool raw = false;                   // search()'s raw Match stream, not rows
 };
 // Validates a cof_request-like description and builds a Request.
 int make_request(const char *filter, size_t pattern_len, const char *const *patterns,
@@ -138,6 +139,7 @@ class Engine {
   private:
     int run_popcount(const std::vector<Request> &reqs, std::vector<Result> &out, Error &err);
     int run_bulge(const std::vector<Request> &reqs, std::vector<Result> &out, Error &err);
+    int run_raw(const Request &req, Result &out, Error &err);
     int device_;
     HostGenome host_;
     DeviceGenome *dev_ = nullptr;

@@ -614,6 +614,12 @@ int Engine::search(const std::vector<Request> &reqs, std::vector<Result> &out, E
     std::vector<size_t> pi, bi;
     std::vector<Request> pr, br;
     for (size_t i = 0; i < reqs.size(); ++i) {
+        if (reqs[i].raw && !reqs[i].max_db && !reqs[i].max_rb) {
+            // search()'s raw stream: every window, no PAM prefilter
+            if (run_raw(reqs[i], out[i], err)) return err.code;
+            if (out[i].text) out[i].text = out[i].owned.data();
+            continue;
+        }
         if (reqs[i].max_db || reqs[i].max_rb) {
             bi.push_back(i);
             br.push_back(reqs[i]);

@@ -392,6 +392,7 @@ int make_request(const char *filter, size_t pattern_len, const char *const *patt
             if (!is_mixed_base(c)) return bad("pattern must be a mixed base string");
         out.patterns.push_back(p);
     }
+    out.raw = (flags & 2u) != 0;  // COF_F_RAW_MATCHES
     if (flags & 1u) {  // COF_F_ADD_REVCOMP: main.rs:253-259
         for (size_t i = 0; i < n_patterns; ++i) {
             std::string r = out.patterns[i];

@@ -54,6 +54,16 @@ extern "C" {
 /* Request flags. */
 #define COF_F_ADD_REVCOMP 1u   /* patterns are user patterns; append their
                                   reverse complements as main.rs:253-259 does */
+#define COF_F_RAW_MATCHES 2u   /* return search()'s raw Match stream instead of
+                                  the writer's rows: one line per Match
+                                  (chrom_chunk.rs:19-29),
+                                  name \t chrom_idx \t pattern_idx \t +|- \t
+                                  mismatches \t dna_bulge_size \t
+                                  rna_bulge_size \t rna_seq \t dna_seq \n;
+                                  the popcount path's raw stream has no PAM
+                                  filter (the writer applies it), its
+                                  mismatches are max(kernel count, 0) and its
+                                  dna_seq keeps NUL bytes for N and padding */
 
 typedef struct cof_genome cof_genome;
 

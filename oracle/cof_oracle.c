@@ -552,6 +552,7 @@ typedef struct {
     const char *filter;
     uint32_t mm, db, rb;
     uint64_t pam_len;      /* main.rs:80-91 */
+    int raw;               /* emit raw Match lines */
 } creq;
 
 static void creq_free(creq *c) {
@@ -568,6 +569,7 @@ static int creq_init(creq *c, const orc_request *r, char *err, size_t errlen) {
     c->n_pat = 2 * r->n_patterns;
     c->filter = r->filter;
     c->mm = r->max_mismatches; c->db = r->max_dna_bulges; c->rb = r->max_rna_bulges;
+    c->raw = r->raw_matches;
     if (c->L == 0) { set_err(err, errlen, "empty filter"); return -1; }
     for (size_t i = 0; i < r->n_patterns; i++) {
         if (strlen(r->patterns[i]) != c->L) {
@@ -742,6 +744,24 @@ static void convert_and_write_popcount(const bview *v, const creq *c, const uint
             rna[i] = B4STR[get_bit4(c->pat_bit4[m->pattern], i)];
         }
         if (!fwd) { revcomp_inplace(dna, L); revcomp_inplace(rna, L); }
+        if (c->raw) {
+            sb_put(out, v->g->names[v->g->name_idx[k]], strlen(v->g->names[v->g->name_idx[k]]));
+            sb_putc(out, '\t');
+            sb_putu(out, pos);
+            sb_putc(out, '\t');
+            sb_putu(out, m->pattern);
+            sb_putc(out, '\t');
+            sb_putc(out, fwd ? '+' : '-');
+            sb_putc(out, '\t');
+            sb_putu(out, (uint64_t)m->mm);
+            sb_put(out, "\t0\t0\t", 5);
+            sb_put(out, rna, L);
+            sb_putc(out, '\t');
+            sb_put(out, dna, L);
+            sb_putc(out, '\n');
+            (*n_rows)++;
+            continue;
+        }
         /* writer post-filter, main.rs:172-197 */
         int pam_ok = 1;
         uint32_t actual = 0;
@@ -987,6 +1007,29 @@ static void emit_alignment(void *vctx, const uint8_t *ops_rev, size_t nops, size
     int fwd = x->p < x->c->n_pat / 2;
     if (!fwd) { revcomp_inplace(x->ta, na); revcomp_inplace(x->pa, na); }
     sbuf *o = x->out;
+    if (x->c->raw) {
+        const char *nm = v->g->names[v->g->name_idx[k]];
+        sb_put(o, nm, strlen(nm));
+        sb_putc(o, '\t');
+        sb_putu(o, pos);
+        sb_putc(o, '\t');
+        sb_putu(o, x->p);
+        sb_putc(o, '\t');
+        sb_putc(o, fwd ? '+' : '-');
+        sb_putc(o, '\t');
+        sb_putu(o, mm);
+        sb_putc(o, '\t');
+        sb_putu(o, db);
+        sb_putc(o, '\t');
+        sb_putu(o, rb);
+        sb_putc(o, '\t');
+        sb_put(o, x->pa, na);
+        sb_putc(o, '\t');
+        sb_put(o, x->ta, na);
+        sb_putc(o, '\n');
+        (*x->n_rows)++;
+        return;
+    }
     uint32_t tot = db + rb;
     if (tot == 0) sb_put(o, "X\t", 2);
     else if (db > 0) sb_put(o, "DNA\t", 4);

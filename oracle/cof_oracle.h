@@ -87,7 +87,17 @@ typedef struct {
     uint32_t max_rna_bulges;
     uint32_t chunks_per_search;  /* 0 -> 16384 */
     int n_threads;               /* 0 -> hardware threads */
+    int raw_matches;             /* 1: emit search()'s Match stream instead of
+                                    the writer's rows (see below) */
 } orc_request;
+
+/* Raw Match lines (raw_matches = 1), one per element of the Vec<Match>
+ * batches search() sends (chrom_chunk.rs:19-29; built at search.rs:1474-1484
+ * and :1361-1371):
+ *   chr_name \t chrom_idx \t pattern_idx \t +|- \t mismatches \t
+ *   dna_bulge_size \t rna_bulge_size \t rna_seq \t dna_seq \n
+ * The popcount path's dna_seq may contain NUL bytes (N and padding decode to
+ * 0 on the masked batch buffer); its mismatches are max(kernel count, 0). */
 
 int orc_search(const orc_genome *g, const orc_request *req, char **rows,
                size_t *rows_len, uint64_t *n_rows, char *err, size_t errlen);

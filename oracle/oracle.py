@@ -25,6 +25,7 @@ class _Req(ctypes.Structure):
         ("max_rna_bulges", ctypes.c_uint32),
         ("chunks_per_search", ctypes.c_uint32),
         ("n_threads", ctypes.c_int),
+        ("raw_matches", ctypes.c_int),
     ]
 
 
@@ -76,7 +77,7 @@ class OracleError(RuntimeError):
     pass
 
 
-def _req(filt, patterns, mm, db, rb, cps, threads, keep):
+def _req(filt, patterns, mm, db, rb, cps, threads, keep, raw=False):
     fb = filt.encode() if isinstance(filt, str) else filt
     pb = [p.encode() if isinstance(p, str) else p for p in patterns]
     arr = (ctypes.c_char_p * len(pb))(*pb)
@@ -90,6 +91,7 @@ def _req(filt, patterns, mm, db, rb, cps, threads, keep):
     r.max_rna_bulges = rb
     r.chunks_per_search = cps
     r.n_threads = threads
+    r.raw_matches = 1 if raw else 0
     return r
 
 
@@ -136,11 +138,12 @@ class OracleGenome:
         return lib().orc_n_batches(self._h, cps)
 
     def search(self, search_filter, patterns, max_mismatches, max_dna_bulges=0,
-               max_rna_bulges=0, chunks_per_search=0, n_threads=0):
-        """Rows of main.rs's writer for user patterns (rc appended)."""
+               max_rna_bulges=0, chunks_per_search=0, n_threads=0, raw=False):
+        """Rows of main.rs's writer for user patterns (rc appended), or with
+        raw=True the raw Match lines of search()."""
         keep = []
         r = _req(search_filter, patterns, max_mismatches, max_dna_bulges, max_rna_bulges,
-                 chunks_per_search, n_threads, keep)
+                 chunks_per_search, n_threads, keep, raw)
         out = ctypes.c_void_p()
         n = ctypes.c_size_t()
         nr = ctypes.c_uint64()

@@ -88,7 +88,7 @@ def _tail(name, pos, fwd, db, mm, size, pam_len):
     return f"\t{name}\t{pos}\t{'+' if fwd else '-'}\t{mm}\t{size}"
 
 
-def search(chunks, filt, user_patterns, mm, db=0, rb=0, cps=16384):
+def search(chunks, filt, user_patterns, mm, db=0, rb=0, cps=16384, raw=False):
     """chunks: list of (name, nibble list, chunk_start, chunk_end).
     Returns the sorted list of output rows."""
     pats = list(user_patterns) + [revcomp(p) for p in user_patterns]
@@ -105,13 +105,14 @@ def search(chunks, filt, user_patterns, mm, db=0, rb=0, cps=16384):
         nch = last - first + 1
         meta = [chunks[k] for k in range(first, last + 1)]
         if db == 0 and rb == 0:
-            rows += _popcount_batch(buf, offs, meta, nch, head, filt, pats, mm, L, pam_len)
+            rows += _popcount_batch(buf, offs, meta, nch, head, filt, pats, mm, L, pam_len, raw)
         else:
-            rows += _myers_batch(buf, offs, meta, nch, head, filt, pats, mm, db, rb, L, pam_len)
+            rows += _myers_batch(buf, offs, meta, nch, head, filt, pats, mm, db, rb, L, pam_len,
+                                 raw)
     return sorted(rows)
 
 
-def _popcount_batch(buf, offs, meta, nch, head, filt, pats, mm, L, pam_len):
+def _popcount_batch(buf, offs, meta, nch, head, filt, pats, mm, L, pam_len, raw=False):
     out = []
     gm = [0 if v == 0xF else v for v in buf]  # mask_genome_n_to_zero_inplace
     msmin = max(offs[1] * 2 - (L - 1), 0) if head else 0
@@ -137,6 +138,10 @@ def _popcount_batch(buf, offs, meta, nch, head, filt, pats, mm, L, pam_len):
             if not fwd:
                 dna = list(revcomp("".join(dna)))
                 rna = list(revcomp("".join(rna)))
+            if raw:  # search()'s Match, before the writer
+                out.append(f"{name}\t{pos}\t{p}\t{'+' if fwd else '-'}\t{max(L - matches, 0)}"
+                           f"\t0\t0\t" + "".join(rna) + "\t" + "".join(dna))
+                continue
             ok, actual = True, 0
             for i in range(L):
                 if filt[i] not in "Nn" and not cmp_chars(dna[i], filt[i]):
@@ -173,9 +178,8 @@ def _loose(p, t):
     return (p & t) != 0
 
 
-def _myers_batch(buf, offs, meta, nch, head, filt, pats, mm, db, rb, L, pam_len):
+def _myers_batch(buf, offs, meta, nch, head, filt, pats, mm, db, rb, L, pam_len, raw=False):
     out = []
-    total = len(buf) - (1 if False else 0)
     total = offs[-1] * 2
     active = offs[1] * 2 if head else 0
     W = L + db
@@ -291,6 +295,10 @@ def _myers_batch(buf, offs, meta, nch, head, filt, pats, mm, db, rb, L, pam_len)
                 rna_s, dna_s = "".join(pa), "".join(ta)
                 if not fwd:
                     rna_s, dna_s = revcomp(rna_s), revcomp(dna_s)
+                if raw:
+                    out.append(f"{name}\t{pos}\t{p}\t{'+' if fwd else '-'}\t{m_}\t{d_}\t{r_}\t"
+                               + rna_s + "\t" + dna_s)
+                    continue
                 typ = "X" if d_ + r_ == 0 else ("DNA" if d_ > 0 else "RNA")
                 out.append(typ + "\t" + rna_s + "\t" + dna_s +
                            _tail(name, pos, fwd, d_, m_, d_ + r_, pam_len))

@@ -148,3 +148,33 @@ def test_autotuner_records_choice(cof_mod, golden, monkeypatch):
     g.search("N" * 24, KAT_PATS, 11)
     t = g.tuning()
     assert t["last"].startswith("cpt") and 0 <= t["variant"] < 6
+
+
+@pytest.mark.parametrize("seed", range(8))
+def test_raw_matches_parity(cof_mod, oracle_mod, seed):
+    # COF_F_RAW_MATCHES: search()'s Match stream before the writer
+    case = randgen.random_case(seed)
+    g, o = _both(cof_mod, oracle_mod, case["chunks"])
+    text, n = g.search(case["filter"], case["patterns"], case["mm"],
+                       chunks_per_search=case["cps"], raw=True)
+    ref, nref = o.search(case["filter"], case["patterns"], case["mm"],
+                         chunks_per_search=case["cps"], raw=True)
+    assert sorted(text.split("\n")[:-1]) == sorted(ref.split("\n")[:-1])
+    assert n == nref > 0
+
+
+def test_raw_matches_bulge_parity(cof_mod, oracle_mod):
+    case = randgen.random_case(105, bulge=True)
+    g, o = _both(cof_mod, oracle_mod, case["chunks"])
+    args = (case["filter"], case["patterns"], case["mm"], case["db"], case["rb"])
+    text, n = g.search(*args, chunks_per_search=case["cps"], raw=True)
+    ref, nref = o.search(*args, chunks_per_search=case["cps"], raw=True)
+    assert sorted(text.split("\n")[:-1]) == sorted(ref.split("\n")[:-1]) and n == nref
+
+
+def test_raw_kat_has_unfiltered_windows(cof_mod, golden):
+    # with a PAM in the filter the raw stream holds windows the writer drops
+    g = cof_mod.Genome(os.path.join(golden, "upstream1000.fa"))
+    raw, nraw = g.search("N" * 21 + "GG", ["CCGTGGTTCAACATTTGCTTNNN"], 6, raw=True)
+    rows, nrows = g.search("N" * 21 + "GG", ["CCGTGGTTCAACATTTGCTTNNN"], 6)
+    assert nraw > nrows

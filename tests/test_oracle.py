@@ -129,3 +129,15 @@ def test_bruteforce_fasta_chunking(oracle_mod, tmp_path):
     bf = bruteforce.chunks_from_fasta_text(text)
     got = [(n, s, e) for n, _d, s, e in g.chunks()]
     assert got == [(n, s, e) for n, _nb, s, e in bf]
+
+
+@pytest.mark.parametrize("seed", [0, 1, 2, 3, 104, 105])
+def test_oracle_raw_matches_vs_bruteforce(oracle_mod, seed):
+    case = randgen.random_case(seed, bulge=seed >= 100)
+    g = _oracle_from_chunks(oracle_mod, case["chunks"])
+    text, _ = g.search(case["filter"], case["patterns"], case["mm"], case["db"], case["rb"],
+                       chunks_per_search=case["cps"], raw=True)
+    bf = bruteforce.search([(n, nb, s, e) for n, _d, nb, s, e in case["chunks"]],
+                           case["filter"], case["patterns"], case["mm"], case["db"], case["rb"],
+                           cps=case["cps"], raw=True)
+    assert sorted(text.split("\n")[:-1]) == bf and len(bf) > 0
