@@ -15,6 +15,18 @@ def build():
     subprocess.run(["make", "-s", "-C", _HERE], check=True)
 
 
+REFERENCE_SRC = "/root/reference/cas-offinder-lib/src"
+
+
+def build_reference_kernels():
+    """Builds _ref/ (the reference's kernel.cu / kernel_myers.cu for sm_100a
+    and the launcher ref_gpu.cu) when the reference tree is present; a
+    machine without it keeps the files built where it was."""
+    if os.path.exists(os.path.join(REFERENCE_SRC, "kernel.cu")):
+        subprocess.run(["make", "-s", "-j8", "-C", _HERE, "ref", "REF=" + REFERENCE_SRC],
+                       check=True)
+
+
 class _Req(ctypes.Structure):
     _fields_ = [
         ("filter", ctypes.c_char_p),

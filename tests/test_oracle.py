@@ -141,3 +141,16 @@ def test_oracle_raw_matches_vs_bruteforce(oracle_mod, seed):
                            case["filter"], case["patterns"], case["mm"], case["db"], case["rb"],
                            cps=case["cps"], raw=True)
     assert sorted(text.split("\n")[:-1]) == bf and len(bf) > 0
+
+
+def test_reference_kernel_launcher_loads():
+    # oracle/_ref/: the reference's kernels for sm_100a and their launcher
+    import ref_gpu
+    if not ref_gpu.available():
+        pytest.skip("oracle/_ref not built (needs the reference tree)")
+    lib = ref_gpu.lib()
+    for sym in ("refgpu_open", "refgpu_n_batches", "refgpu_batch", "refgpu_close",
+                "refgpu_popcount_count", "refgpu_popcount_run", "refgpu_myers_run"):
+        assert hasattr(lib, sym)
+    assert os.path.exists(ref_gpu.popcount_cubin(23))
+    assert os.path.exists(ref_gpu.myers_cubin(23, 3, 4, 2, 2))
