@@ -52,6 +52,10 @@ def parse():
     ap.add_argument("--cpu-sample-s", type=float, default=15.0,
                     help="target seconds of CPU work for the CPU baseline")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--ref-step-s", type=float, default=4.0,
+                    help="seconds of CPU work per step of --impl reference")
+    ap.add_argument("--no-ref-gpu", action="store_true",
+                    help="--impl reference: skip timing the reference's own GPU kernel")
     ap.add_argument("--serving-requests", type=int, default=64)
     ap.add_argument("--serving-rate", type=float, default=200.0, help="arrivals per second")
     ap.add_argument("--no-extras", action="store_true",
@@ -241,58 +245,122 @@ def bench_serving(cof, g, n_nt, n_req, rate, seed=7, max_guides=500, max_mm=4):
     return res
 
 
-def cpu_baseline(cfg, target_s, n_threads=0):
+class CpuSample:
     """The reference CPU path (C restatement, oracle/) over a leading slice of
-    the same genome, all host threads, CPU batch size (64 chunks)."""
-    sys.path.insert(0, ORACLE)
-    import oracle
-    oracle.build()
-    cores = n_threads or os.cpu_count()
-    chunks = list(cfg["genome"].chunks())
+    the workload's genome: all host threads, CPU batch size (64 chunks).  The
+    slice is calibrated once to about `target_s` seconds of work."""
 
-    def run(n_chunks):
-        o = oracle.OracleGenome()
-        nt = 0
-        for name, data, s, e in chunks[:n_chunks]:
+    def __init__(self, cfg, target_s, n_threads=0):
+        sys.path.insert(0, ORACLE)
+        import oracle
+        oracle.build()
+        self.oracle = oracle
+        self.cfg = cfg
+        self.n_threads = n_threads
+        self.cores = n_threads or os.cpu_count()
+        self.chunks = list(cfg["genome"].chunks())
+        t, nt = self._time(self._genome(min(len(self.chunks), 64)))  # one 4 Mnt batch
+        per_nt = t / max(nt, 1)
+        want = int(target_s / max(per_nt, 1e-12))
+        self.n_chunks = max(64, min(len(self.chunks), want // 65520 // 64 * 64))
+        self.genome = self._genome(self.n_chunks)
+        self.nt = self.genome.n_nucl
+
+    def _genome(self, n_chunks):
+        o = self.oracle.OracleGenome()
+        for name, data, s, e in self.chunks[:n_chunks]:
             o.add_chunk(name, data, s, e)
-            nt += e - s
-        t0 = time.perf_counter()
-        o.search(cfg["filter"], cfg["patterns"], cfg["max_mismatches"], chunks_per_search=64,
-                 n_threads=n_threads)
-        return time.perf_counter() - t0, nt
+        return o
 
-    t, nt = run(min(len(chunks), 64))  # calibration: one 4 Mnt batch
-    per_nt = t / max(nt, 1)
-    want = int(target_s / max(per_nt, 1e-12))
-    n_chunks = max(64, min(len(chunks), want // 65520 // 64 * 64))
-    t, nt = run(n_chunks)
-    rate = nt * 1e-9 * len(cfg["patterns"]) / t
-    return dict(value=rate, unit=UNIT, cores=cores, kind="port",
-                sample=f"first {nt / 1e6:.1f} Mbp of the genome x {len(cfg['patterns'])} "
-                       f"guides, oracle/ C restatement of search_compute_cpu + writer, "
-                       f"{cores} threads, {t:.1f} s"), t
+    def _time(self, o):
+        c = self.cfg
+        t0 = time.perf_counter()
+        o.search(c["filter"], c["patterns"], c["max_mismatches"], chunks_per_search=64,
+                 n_threads=self.n_threads)
+        return time.perf_counter() - t0, o.n_nucl
+
+    def run(self):
+        """One timed pass over the slice; returns (Gbp*guides/s, seconds)."""
+        t, nt = self._time(self.genome)
+        return nt * 1e-9 * len(self.cfg["patterns"]) / t, t
+
+    def describe(self, value, t):
+        return dict(value=value, unit=UNIT, cores=self.cores, kind="port",
+                    sample=f"first {self.nt / 1e6:.1f} Mbp of the genome x "
+                           f"{len(self.cfg['patterns'])} guides, oracle/ C restatement of "
+                           f"search_compute_cpu + writer, {self.cores} threads, {t:.1f} s")
+
+
+def cpu_baseline(cfg, target_s, n_threads=0):
+    smp = CpuSample(cfg, target_s, n_threads)
+    v, t = smp.run()
+    return smp.describe(v, t), t
+
+
+def reference_gpu_kernel(cfg):
+    """The reference's own find_matches kernel (oracle/_ref, built from the
+    reference sources for sm_100a) launched as search.rs launches it, on this
+    workload: device time of its launches and of its whole device loop."""
+    sys.path.insert(0, ORACLE)
+    try:
+        import ref_gpu
+    except ImportError as e:
+        return {"unavailable": f"oracle/ref_gpu.py: {e}"}
+    if not ref_gpu.available():
+        return {"unavailable": "oracle/_ref not built (the reference tree was absent)"}
+    import synth
+    chunks = list(cfg["genome"].chunks())
+    pats = cfg["patterns"] + [synth.revcomp(p) for p in cfg["patterns"]]
+    ref = ref_gpu.RefGpu(chunks, 0)
+    try:
+        counts = ref.popcount_counts(pats, cfg["max_mismatches"])
+        runs = [ref.popcount(pats, cfg["max_mismatches"], counts, keep=False)[1]
+                for _ in range(3)]
+    finally:
+        ref.close()
+    best = min(runs[1:], key=lambda t: t["kernel_ms"])
+    units = cfg["genome"].n_nucl * 1e-9 * len(cfg["patterns"])
+    return {"kernel": "find_matches (kernel.cu), 1 Gnt batches, grid (n/128, patterns)",
+            "kernel_ms": best["kernel_ms"], "launches": best["launches"],
+            "kernel_value": units / (best["kernel_ms"] * 1e-3),
+            "device_loop_ms": best["wall_ms"],
+            "device_loop_value": units / (best["wall_ms"] * 1e-3), "unit": UNIT,
+            "kernel_records": sum(counts),
+            "note": "device loop = pack + N mask + H2D + kernel + D2H per batch, "
+                    "before the reference's CPU writer; best of 2 after 1 warm-up"}
 
 
 def run_reference(args, rank, world):
+    """The reference arm: the reference's CPU search path on the host cores
+    (oracle/ C restatement; Rust cannot be built here), each step one pass
+    over a fixed slice of the workload calibrated to --ref-step-s seconds.
+    Under torchrun only rank 0 runs."""
     if rank != 0:
         return
     cfg = make_workload(args, 0)
-    gbp_guides = None
-    vals = []
+    smp = CpuSample(cfg, args.ref_step_s)
+    vals, times = [], []
     for i in range(args.warmup + args.steps):
-        base, t = cpu_baseline(cfg, args.cpu_sample_s / 2)
+        v, t = smp.run()
         if i >= args.warmup:
-            vals.append(base["value"])
+            vals.append(v)
+            times.append(t)
     v = statistics.median(vals)
-    base["value"] = v
+    base = smp.describe(v, statistics.median(times))
     line = {"metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
-            "impl": "reference",
+            "warmup": args.warmup, "ms_per_step": statistics.median(times) * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
+            "data": "synthetic", "impl": "reference",
             "config": {"workload": cfg["name"], "genome_nt": cfg["genome"].n_nucl,
-                       "guides": len(cfg["patterns"])},
+                       "guides": len(cfg["patterns"]),
+                       "sample_nt": smp.nt, "chunks_per_search": 64},
             "cpu_baseline": base,
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    if not args.no_ref_gpu:
+        try:
+            line["reference_gpu_kernel"] = reference_gpu_kernel(cfg)
+        except Exception as e:  # the CPU line above stands on its own
+            line["reference_gpu_kernel"] = {"unavailable": f"{type(e).__name__}: {e}"}
     print(json.dumps(line), flush=True)
 
 
