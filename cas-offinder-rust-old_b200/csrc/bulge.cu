@@ -27,6 +27,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstdlib>
 #include <cstring>
 #include <memory>
 #include <string>
@@ -320,6 +321,556 @@ traceback_kernel(GenomeDev G, const BatchDev *__restrict__ batches,
     }
 }
 
+// ---- warp-per-candidate traceback ------------------------------------------
+//
+// Same rows as traceback_kernel, with the work laid out for a GPU.  One warp
+// takes one candidate from a dynamic queue, so that a few candidates with
+// thousands of alignments cannot serialise a whole warp or leave SMs idle.
+//
+// 1. Budget DP, as a wavefront (lane = pattern row i, step s = i + j, the
+//    upper row's values arrive by shuffle).  F[bd][br](i, j) = fewest
+//    mismatches on any alignment of pattern cells [0, i) ending at text cell
+//    j that uses at most bd DNA and br RNA bulges.  It obeys exactly the move
+//    rules of the enumeration: a diagonal step is barred under a pattern N
+//    on a mismatch and where classify's filter test fails; the bulge steps
+//    have their N-neighbour rules; a node over a padding cell is dead.
+//    Values clamp at mm + 1 ("infeasible").  All (db + 1)(rb + 1) budgets
+//    of a cell are bytes of four registers and are updated together with
+//    SIMD byte min / max.
+// 2. Enumeration with exact pruning.  A node (i, j) with m mismatches and
+//    d, r bulges so far is kept iff m + F[db - d][rb - r](i, j) <= mm.  So
+//    every kept node lies on at least one emitted alignment: the cost bound
+//    and the caps of the reference's walk are both implied, and nothing else
+//    is cut.  The warp pops up to 32 nodes of a shared-memory stack, expands
+//    them in parallel and pushes the children, writing leaves (i = 0) as
+//    rows after classify's filter (already enforced) and the record-end
+//    drop.
+constexpr int kTbWarps = 4;                  // warps per block
+constexpr int kTbCap = 160;                  // stack slots per warp
+constexpr int kTbMargin = 2 * kMaxCells;     // slots a one-node-at-a-time walk can add
+constexpr int kTbMaxBudgets = 16;            // (db + 1) * (rb + 1) bytes per cell
+constexpr uint32_t kTbBudget = 96;           // iterations on one tree before handing it on
+constexpr uint32_t kTbQueue = 1u << 21;      // subtrees per hand-on queue
+constexpr int kTbMaxPasses = 24;             // the last pass finishes every tree
+
+struct TbNode {
+    uint64_t ops;     // walk-back order, 2 bits per op, depths 0..31
+    uint32_t ops_hi;  // depths 32..39
+    uint32_t st;      // i | j << 6 | m << 12 | d << 18 | r << 22 | depth << 26
+};
+
+// one unit of enumeration work: a candidate's root, or a subtree handed on
+// by a warp that spent its iteration budget (cand == ~0u: an empty slot)
+struct TbItem {
+    uint32_t cand, pad;
+    TbNode node;
+};
+
+// walk-back ops (2 bits per step, n_ops steps, steps 32.. in hi) into
+// alignment order: reverse all 64 two-bit groups of the 128-bit value, then
+// drop the 64 - n_ops unused groups
+__device__ __forceinline__ void ops_forward(uint64_t lo, uint64_t hi, uint32_t n_ops,
+                                            uint64_t &o0, uint64_t &o1) {
+    const uint64_t k5 = 0x5555555555555555ull;
+    uint64_t rl = __brevll(hi), rh = __brevll(lo);
+    rl = ((rl >> 1) & k5) | ((rl & k5) << 1);
+    rh = ((rh >> 1) & k5) | ((rh & k5) << 1);
+    const uint32_t sh = 2 * (64 - n_ops);  // 48..126
+    if (sh >= 64) {
+        o0 = rh >> (sh - 64);
+        o1 = 0;
+    } else {
+        o0 = (rl >> sh) | (rh << (64 - sh));
+        o1 = rh >> sh;
+    }
+}
+
+__device__ __forceinline__ uint32_t tb_st(uint32_t i, uint32_t j, uint32_t m, uint32_t d,
+                                          uint32_t r, uint32_t dep) {
+    return i | (j << 6) | (m << 12) | (d << 18) | (r << 22) | (dep << 26);
+}
+
+// classify's filter test of a match / substitution cell
+__device__ __forceinline__ bool filt_ok(uint8_t fl, uint8_t g) {
+    return fl == 0xF ? g != 0 : (g != 0 && g != 0xF && (g & fl));
+}
+
+// the 16 budget bytes moved s (1..15) places up: byte b takes byte b - s,
+// zeros shifted in (selects, not a dynamically indexed array, so the
+// vectors stay in registers)
+__device__ __forceinline__ void shl_bytes(const uint32_t (&a)[4], uint32_t s, uint32_t (&o)[4]) {
+    const int ws = (int)(s >> 2);
+    const uint32_t b = 8 * (s & 3);
+    auto pick = [&](int k) -> uint32_t {
+        return k == 0 ? a[0] : k == 1 ? a[1] : k == 2 ? a[2] : k == 3 ? a[3] : 0u;
+    };
+#pragma unroll
+    for (int w = 0; w < 4; ++w) {
+        const uint32_t hi = pick(w - ws), lo = pick(w - ws - 1);
+        o[w] = b ? __funnelshift_l(lo, hi, b) : hi;
+    }
+}
+
+// shared-memory bytes one warp needs for tables of tbl_words words
+__host__ __device__ constexpr size_t tb_warp_bytes(uint32_t tbl_words) {
+    return (kTbCap * sizeof(TbNode) + (size_t)tbl_words * 4 + 64 + 3 * 48 + 15) & ~(size_t)15;
+}
+
+__global__ void __launch_bounds__(kTbWarps * 32)
+traceback_warp_kernel(GenomeDev G, const BatchDev *__restrict__ batches,
+                      const MyersPattern *__restrict__ pats, const MyersReqDev *__restrict__ reqs,
+                      const MyersCand *__restrict__ cand, uint32_t n_cand,
+                      const TbItem *__restrict__ items, uint32_t n_items, TbItem *spill,
+                      uint32_t spill_cap, uint32_t iter_budget, uint32_t tbl_words,
+                      MyersRow *rows, uint32_t row_cap, uint64_t *keys, uint32_t *vals,
+                      Counters *ctr, uint32_t *req_rows) {
+    extern __shared__ __align__(16) unsigned char tb_smem[];
+    const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    unsigned char *wbase = tb_smem + warp * tb_warp_bytes(tbl_words);
+    TbNode *stk = reinterpret_cast<TbNode *>(wbase);
+    uint32_t *tbl = reinterpret_cast<uint32_t *>(wbase + kTbCap * sizeof(TbNode));
+    uint8_t *stext = wbase + kTbCap * sizeof(TbNode) + (size_t)tbl_words * 4;
+    uint8_t *spb = stext + 64, *sisn = spb + 48, *seff = sisn + 48;
+    const unsigned full = 0xFFFFFFFFu;
+
+    const uint32_t n_work = items ? n_items : n_cand;
+    for (;;) {
+        uint32_t wi = 0;
+        if (lane == 0) wi = (uint32_t)min(atomicAdd(&ctr->next_item, 1ull), (unsigned long long)n_work);
+        wi = __shfl_sync(full, wi, 0);
+        if (wi >= n_work) break;
+        __syncwarp();  // the previous item's readers are done
+        uint32_t ci = wi;
+        TbNode start_node{0, 0, 0};
+        if (items) {
+            const TbItem it = items[wi];
+            if (it.cand == ~0u) continue;
+            ci = it.cand;
+            start_node = it.node;
+        }
+        const MyersCand c = cand[ci];
+        const BatchDev B = batches[c.batch];
+        const MyersPattern &P = pats[c.pattern];
+        const MyersReqDev R = reqs[P.request];
+        const uint32_t L = P.L, t = c.t_local;
+        const uint32_t n = min(R.W, t + 1);  // text cells of the window
+        const uint32_t cols = n + 1;
+        const uint32_t nb = (R.db + 1) * (R.rb + 1), nbw = (nb + 3) >> 2;
+        const uint32_t cl = min(R.mm + 1, 127u);
+        for (uint32_t k = lane; k < n; k += 32) stext[k] = nib(G.bit4, B.base + t + 1 - n + k);
+        for (uint32_t k = lane; k < L; k += 32) {
+            spb[k] = P.b4[k];
+            sisn[k] = P.isn[k];
+            seff[k] = P.eff[k];
+        }
+        for (uint32_t k = lane; k < cols * nbw; k += 32) tbl[k] = 0;  // row 0
+        __syncwarp();
+
+        // -- 1. budget DP wavefront
+        const uint32_t i = lane + 1;
+        const bool row_on = i <= L;
+        uint8_t pbi = 0, effi = 0;
+        bool isn1 = false, rna_ok = false, dna_ok = false;
+        if (row_on) {
+            pbi = spb[i - 1];
+            effi = seff[i - 1];
+            isn1 = sisn[i - 1];
+            const bool isn0 = i < L && sisn[i];
+            const bool isn2 = i >= 2 && sisn[i - 2];
+            rna_ok = R.rb > 0 && !isn1 && !isn0 && !isn2;
+            dna_ok = R.db > 0 && i < L && !(isn1 && isn0);
+        }
+        uint32_t inv_r[4], inv_d[4];  // 0x7F in the bytes a move cannot reach
+#pragma unroll
+        for (int w = 0; w < 4; ++w) {
+            inv_r[w] = inv_d[w] = 0;
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const uint32_t b = 4 * w + q;
+                if (b >= nb || b % (R.rb + 1) == 0) inv_r[w] |= 0x7Fu << (8 * q);
+                if (b >= nb || b < R.rb + 1) inv_d[w] |= 0x7Fu << (8 * q);
+            }
+        }
+        const uint32_t clv = cl * 0x01010101u;
+        uint32_t left[4] = {0, 0, 0, 0}, upc[4] = {0, 0, 0, 0}, upp[4] = {0, 0, 0, 0};
+        for (uint32_t s = 0; s < L + n; ++s) {
+#pragma unroll
+            for (int w = 0; w < 4; ++w) {
+                uint32_t u = __shfl_up_sync(full, left[w], 1);
+                if (lane == 0) u = 0;  // row 0: F = 0
+                upp[w] = upc[w];
+                upc[w] = u;
+            }
+            const int j = (int)s - (int)lane;
+            if (row_on && j >= 0 && j <= (int)n) {
+                uint32_t dg[4], rn[4], dn[4];
+#pragma unroll
+                for (int w = 0; w < 4; ++w) dg[w] = rn[w] = dn[w] = 0x7F7F7F7Fu;
+                const uint8_t tx = j ? stext[j - 1] : 0;
+                if (j >= 1) {
+                    const uint32_t mc = loose(pbi, tx) ? 0u : 1u;
+                    if (!(mc && isn1) && filt_ok(effi, tx)) {
+#pragma unroll
+                        for (int w = 0; w < 4; ++w) dg[w] = upp[w] + mc * 0x01010101u;
+                    }
+                }
+                if (rna_ok) {
+                    shl_bytes(upc, 1, rn);
+#pragma unroll
+                    for (int w = 0; w < 4; ++w) rn[w] = __vmaxu4(rn[w], inv_r[w]);
+                }
+                if (dna_ok && j >= 1) {
+                    shl_bytes(left, R.rb + 1, dn);
+#pragma unroll
+                    for (int w = 0; w < 4; ++w) dn[w] = __vmaxu4(dn[w], inv_d[w]);
+                }
+                const bool dead = j >= 1 && tx == 0;
+                uint32_t *cell = tbl + (i * cols + (uint32_t)j) * nbw;
+#pragma unroll
+                for (int w = 0; w < 4; ++w) {
+                    const uint32_t v =
+                        dead ? clv : __vminu4(__vminu4(__vminu4(dg[w], rn[w]), dn[w]), clv);
+                    left[w] = v;
+                    if ((uint32_t)w < nbw) cell[w] = v;
+                }
+            }
+        }
+        __syncwarp();
+        auto F = [&](uint32_t ii, uint32_t jj, uint32_t b) -> uint32_t {
+            return (tbl[(ii * cols + jj) * nbw + (b >> 2)] >> (8 * (b & 3))) & 0xFFu;
+        };
+        if (!items) {
+            if (F(L, n, nb - 1) > R.mm) continue;  // no alignment within the caps
+            start_node = TbNode{0, 0, tb_st(L, n, 0, 0, 0, 0)};
+        }
+        // every leaf starts in [t + 1 - n, t + 1]: one chunk lookup serves
+        // them all unless that range crosses a chunk boundary
+        auto chunk_of = [&](uint64_t start) {
+            const uint64_t gbyte = start >> 1;
+            uint32_t lo = B.first, hi = B.first + B.nch;
+            while (hi - lo > 1) {
+                const uint32_t mid = (lo + hi) >> 1;
+                if (G.boff[mid] <= gbyte) lo = mid; else hi = mid;
+            }
+            return lo;
+        };
+        const uint32_t k_lo = chunk_of(B.base + t + 1 - n), k_hi = chunk_of(B.base + t + 1);
+
+        // -- 2. enumeration
+        uint32_t size = 1;
+        if (lane == 0) stk[0] = start_node;
+        __syncwarp();
+        const uint32_t rb1 = R.rb + 1;
+        uint32_t iters = 0;
+        bool may_spill = iter_budget != 0 && spill != nullptr;
+        while (size > 0) {
+            if (may_spill && iters >= iter_budget) {
+                // hand the rest of this tree to other warps
+                uint32_t sb = 0;
+                if (lane == 0) sb = atomicAdd(&ctr->hits, size);
+                sb = __shfl_sync(full, sb, 0);
+                if ((uint64_t)sb + size <= spill_cap) {
+                    for (uint32_t q = lane; q < size; q += 32) spill[sb + q] = TbItem{ci, 0, stk[q]};
+                    __syncwarp();
+                    break;
+                }
+                for (uint32_t q = sb + lane; q < spill_cap && q < sb + size; q += 32) spill[q].cand = ~0u;
+                may_spill = false;  // queue full: finish the tree here
+            }
+            ++iters;
+            // pop k nodes; with size + 2k <= cap - margin the stack cannot
+            // overflow, and below that a one-node walk adds <= margin slots
+            const int room = kTbCap - kTbMargin - (int)size;
+            const uint32_t k = room >= 2 ? min(min(32u, size), (uint32_t)room / 2) : 1u;
+            const bool have = lane < k;
+            TbNode nd{0, 0, 0};
+            if (have) nd = stk[size - 1 - lane];
+            size -= k;
+            __syncwarp();
+            // up to three children (diagonal, RNA, DNA) and two leaves
+            // (diagonal or RNA step into row 0), in named slots
+            struct Kid { uint32_t st, op; bool on; };
+            struct Leaf { uint64_t start, pos; uint32_t chunk, m, d, r, op; bool on; };
+            Kid ka{0, 0, false}, kb{0, 0, false}, kc{0, 0, false};
+            Leaf la{0, 0, 0, 0, 0, 0, 0, false}, lb{0, 0, 0, 0, 0, 0, 0, false};
+            uint32_t dep = 0;
+            if (have) {
+                const uint32_t st = nd.st;
+                const uint32_t ni = st & 63, nj = (st >> 6) & 63, m = (st >> 12) & 63;
+                const uint32_t d = (st >> 18) & 15, r = (st >> 22) & 15;
+                dep = st >> 26;
+                // convert_matches_myers: owning chunk and record-end drop
+                auto leaf = [&](Leaf &o, uint32_t jf, uint32_t lm, uint32_t ld, uint32_t lr,
+                                uint32_t op) {
+                    const uint64_t start = B.base + t + 1 - (n - jf);
+                    const uint32_t lo = k_lo == k_hi ? k_lo : chunk_of(start);
+                    const uint64_t pos = G.start[lo] + (start - 2 * G.boff[lo]);
+                    const bool end_chrom = (lo == B.first + B.nch - 1) || G.start[lo + 1] == 0;
+                    if (end_chrom && pos + (uint64_t)L + ld - lr > G.end[lo]) return;
+                    o = Leaf{start, pos, lo, lm, ld, lr, op, true};
+                };
+                // diagonal: match / substitution
+                if (nj >= 1) {
+                    const uint8_t tx = stext[nj - 1];
+                    const uint32_t mc = loose(spb[ni - 1], tx) ? 0u : 1u;
+                    if (!(mc && sisn[ni - 1]) && filt_ok(seff[ni - 1], tx) && m + mc <= R.mm) {
+                        if (ni == 1)
+                            leaf(la, nj - 1, m + mc, d, r, mc);
+                        else if (m + mc + F(ni - 1, nj - 1, (R.db - d) * rb1 + (R.rb - r)) <= R.mm)
+                            ka = Kid{tb_st(ni - 1, nj - 1, m + mc, d, r, dep + 1), mc, true};
+                    }
+                }
+                // RNA bulge: pattern cell skipped
+                if (r < R.rb) {
+                    const bool isn0 = ni < L && sisn[ni], isn2 = ni >= 2 && sisn[ni - 2];
+                    if (!sisn[ni - 1] && !isn0 && !isn2) {
+                        if (ni == 1)
+                            leaf(lb, nj, m, d, r + 1, 3);
+                        else if (m + F(ni - 1, nj, (R.db - d) * rb1 + (R.rb - r - 1)) <= R.mm)
+                            kb = Kid{tb_st(ni - 1, nj, m, d, r + 1, dep + 1), 3, true};
+                    }
+                }
+                // DNA bulge: text cell skipped
+                if (d < R.db && nj >= 1 && ni < L && !(sisn[ni - 1] && sisn[ni])) {
+                    if (m + F(ni, nj - 1, (R.db - d - 1) * rb1 + (R.rb - r)) <= R.mm)
+                        kc = Kid{tb_st(ni, nj - 1, m, d + 1, r, dep + 1), 2, true};
+                }
+            }
+            auto ops_with = [&](uint32_t op, uint64_t &o, uint32_t &oh) {
+                o = nd.ops;
+                oh = nd.ops_hi;
+                if (dep < 32) o |= (uint64_t)op << (2 * dep);
+                else oh |= op << (2 * (dep - 32));
+            };
+            const uint32_t nc = (uint32_t)ka.on + kb.on + kc.on;
+            const uint32_t ne = (uint32_t)la.on + lb.on;
+            // push the children
+            uint32_t incl = nc;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const uint32_t y = __shfl_up_sync(full, incl, o);
+                if ((int)lane >= o) incl += y;
+            }
+            const uint32_t tot = __shfl_sync(full, incl, 31);
+            uint32_t at = size + incl - nc;
+            auto push = [&](const Kid &k2) {
+                if (!k2.on) return;
+                TbNode o;
+                ops_with(k2.op, o.ops, o.ops_hi);
+                o.st = k2.st;
+                stk[at++] = o;
+            };
+            push(ka);
+            push(kb);
+            push(kc);
+            size += tot;
+            // write the rows, one counter update per warp
+            uint32_t einc = ne;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const uint32_t y = __shfl_up_sync(full, einc, o);
+                if ((int)lane >= o) einc += y;
+            }
+            const uint32_t etot = __shfl_sync(full, einc, 31);
+            if (etot) {
+                uint32_t base = 0;
+                if (lane == 0) {
+                    base = atomicAdd(&ctr->rows, etot);
+                    atomicAdd(&req_rows[P.request], etot);
+                }
+                base = __shfl_sync(full, base, 0);
+                uint32_t rr = base + einc - ne;
+                auto put = [&](const Leaf &l2) {
+                    if (!l2.on) return;
+                    if (rr < row_cap) {
+                        uint64_t o, oh32;
+                        uint32_t oh;
+                        ops_with(l2.op, o, oh);
+                        oh32 = oh;
+                        const uint32_t n_ops = dep + 1;
+                        MyersRow w;
+                        w.start = l2.start;
+                        w.pos = l2.pos;
+                        ops_forward(o, oh32, n_ops, w.ops[0], w.ops[1]);
+                        w.chunk = l2.chunk;
+                        w.pattern = c.pattern;
+                        w.n_ops = (uint8_t)n_ops;
+                        w.mm = (uint8_t)l2.m;
+                        w.db = (uint8_t)l2.d;
+                        w.rb = (uint8_t)l2.r;
+                        w.pad = 0;
+                        rows[rr] = w;
+                        keys[rr] = ((uint64_t)c.pattern << 34) | l2.start;
+                        vals[rr] = rr;
+                    } else {
+                        ctr->overflow = 1;
+                    }
+                    ++rr;
+                };
+                put(la);
+                put(lb);
+            }
+            __syncwarp();
+        }
+    }
+}
+
+// Exact pre-test of the warp traceback, one thread per candidate: the
+// root value F[db][rb](L, n) of the budget DP, computed row by row (pattern
+// cell i) with the previous row kept in shared memory, interleaved by
+// thread so that a warp's accesses hit 32 different banks.  Every
+// alignment path crosses every row, and fewer bulges never need fewer
+// mismatches, so the root value is at least the smallest full-budget value
+// of any row: a row whose minimum exceeds mm ends the test early.  A
+// candidate whose root value exceeds mm has no alignment within the caps
+// (most of the ones the Myers bound lets through), so only the others are
+// passed on.  NBW = budget words per cell ((db + 1)(rb + 1) <= 4 * NBW).
+constexpr int kBfThreads = 128;
+
+// byte shift of an NBW-word budget vector; s < 4 needs no word moves
+template <int NBW>
+__device__ __forceinline__ void shl_budget(const uint32_t (&a)[NBW], uint32_t s,
+                                           uint32_t (&o)[NBW]) {
+    if (s < 4) {
+        const uint32_t b = 8 * s;
+        o[0] = a[0] << b;
+#pragma unroll
+        for (int w = 1; w < NBW; ++w) o[w] = __funnelshift_l(a[w - 1], a[w], b);
+        return;
+    }
+    uint32_t x[4] = {0, 0, 0, 0}, y[4];
+#pragma unroll
+    for (int w = 0; w < NBW; ++w) x[w] = a[w];
+    shl_bytes(x, s, y);
+#pragma unroll
+    for (int w = 0; w < NBW; ++w) o[w] = y[w];
+}
+
+template <int NBW>
+__global__ void __launch_bounds__(kBfThreads)
+budget_filter_kernel(GenomeDev G, const BatchDev *__restrict__ batches,
+                     const MyersPattern *__restrict__ pats, const MyersReqDev *__restrict__ reqs,
+                     const MyersCand *__restrict__ cand, uint32_t n_cand,
+                     MyersCand *__restrict__ out, uint32_t *n_out) {
+    extern __shared__ uint32_t bf_row[];  // [cell * NBW + w][thread], cells 0..n
+    const uint32_t tid = threadIdx.x;
+    auto Rw = [&](uint32_t j, int w) -> uint32_t & {
+        return bf_row[(j * NBW + w) * kBfThreads + tid];
+    };
+    for (uint32_t base = blockIdx.x * kBfThreads; base < n_cand; base += gridDim.x * kBfThreads) {
+        const uint32_t ci = base + tid;
+        bool keep = false;
+        MyersCand c{0, 0, 0, 0};
+        if (ci < n_cand) {
+            c = cand[ci];
+            const BatchDev B = batches[c.batch];
+            const MyersPattern &P = pats[c.pattern];
+            const MyersReqDev R = reqs[P.request];
+            const uint32_t L = P.L, t = c.t_local;
+            const uint32_t n = min(R.W, t + 1);
+            const uint32_t nb = (R.db + 1) * (R.rb + 1), rb1 = R.rb + 1;
+            const uint32_t cl = min(R.mm + 1, 127u), clv = cl * 0x01010101u;
+            const uint32_t fb = nb - 1, fw = fb >> 2, fs = 8 * (fb & 3);  // full budget byte
+            uint32_t inv_r[NBW], inv_d[NBW];
+#pragma unroll
+            for (int w = 0; w < NBW; ++w) {
+                inv_r[w] = inv_d[w] = 0;
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    const uint32_t b = 4 * w + q;
+                    if (b >= nb || b % rb1 == 0) inv_r[w] |= 0x7Fu << (8 * q);
+                    if (b >= nb || b < rb1) inv_d[w] |= 0x7Fu << (8 * q);
+                }
+            }
+            // the window's n text cells, cell k in bits 4k of (t2:t1:t0)
+            const uint64_t tbase = B.base + t + 1 - n;
+            uint64_t tw0 = 0, tw1 = 0, tw2 = 0;
+            for (uint32_t k = 0; k < n; ++k) {
+                const uint64_t x = (uint64_t)nib(G.bit4, tbase + k) << (4 * (k & 15));
+                if (k < 16) tw0 |= x; else if (k < 32) tw1 |= x; else tw2 |= x;
+            }
+            for (uint32_t j = 0; j <= n; ++j) {
+#pragma unroll
+                for (int w = 0; w < NBW; ++w) Rw(j, w) = 0;  // row 0
+            }
+            keep = true;
+            for (uint32_t i = 1; i <= L && keep; ++i) {
+                const uint8_t pb = P.b4[i - 1], ef = P.eff[i - 1];
+                const bool isn1 = P.isn[i - 1], isn0 = i < L && P.isn[i],
+                           isn2 = i >= 2 && P.isn[i - 2];
+                const bool rna_ok = R.rb > 0 && !isn1 && !isn0 && !isn2;
+                const bool dna_ok = R.db > 0 && i < L && !(isn1 && isn0);
+                uint32_t dsrc[NBW], left[NBW];
+                // column 0: only an RNA bulge from the cell above
+#pragma unroll
+                for (int w = 0; w < NBW; ++w) dsrc[w] = Rw(0, w);
+                if (rna_ok) {
+                    shl_budget<NBW>(dsrc, 1, left);
+#pragma unroll
+                    for (int w = 0; w < NBW; ++w) left[w] = __vminu4(__vmaxu4(left[w], inv_r[w]), clv);
+                } else {
+#pragma unroll
+                    for (int w = 0; w < NBW; ++w) left[w] = clv;
+                }
+                uint32_t row_min = (left[fw] >> fs) & 0xFFu;
+#pragma unroll
+                for (int w = 0; w < NBW; ++w) Rw(0, w) = left[w];
+                uint64_t a0 = tw0, a1 = tw1, a2 = tw2;  // text shift register
+                for (uint32_t j = 1; j <= n; ++j) {
+                    const uint8_t tx = (uint8_t)(a0 & 0xF);
+                    a0 = (a0 >> 4) | (a1 << 60);
+                    a1 = (a1 >> 4) | (a2 << 60);
+                    a2 >>= 4;
+                    uint32_t up[NBW], v[NBW];
+#pragma unroll
+                    for (int w = 0; w < NBW; ++w) up[w] = Rw(j, w);
+                    if (tx == 0) {  // a node over a padding cell is dead
+#pragma unroll
+                        for (int w = 0; w < NBW; ++w) v[w] = clv;
+                    } else {
+#pragma unroll
+                        for (int w = 0; w < NBW; ++w) v[w] = clv;
+                        const uint32_t mc = loose(pb, tx) ? 0u : 1u;
+                        if (!(mc && isn1) && filt_ok(ef, tx)) {
+#pragma unroll
+                            for (int w = 0; w < NBW; ++w) v[w] = __vminu4(v[w], dsrc[w] + mc * 0x01010101u);
+                        }
+                        if (rna_ok) {
+                            uint32_t x[NBW];
+                            shl_budget<NBW>(up, 1, x);
+#pragma unroll
+                            for (int w = 0; w < NBW; ++w) v[w] = __vminu4(v[w], __vmaxu4(x[w], inv_r[w]));
+                        }
+                        if (dna_ok) {
+                            uint32_t x[NBW];
+                            shl_budget<NBW>(left, rb1, x);
+#pragma unroll
+                            for (int w = 0; w < NBW; ++w) v[w] = __vminu4(v[w], __vmaxu4(x[w], inv_d[w]));
+                        }
+                    }
+#pragma unroll
+                    for (int w = 0; w < NBW; ++w) {
+                        Rw(j, w) = v[w];
+                        dsrc[w] = up[w];
+                        left[w] = v[w];
+                    }
+                    row_min = min(row_min, (v[fw] >> fs) & 0xFFu);
+                }
+                if (row_min > R.mm) keep = false;
+            }
+            if (keep) keep = ((Rw(n, (int)fw) >> fs) & 0xFFu) <= R.mm;
+        }
+        // warp-aggregated compaction of the survivors
+        const unsigned full = 0xFFFFFFFFu;
+        const unsigned m = __ballot_sync(full, keep);
+        const uint32_t lane = tid & 31;
+        uint32_t o = 0;
+        if (lane == 0 && m) o = atomicAdd(n_out, (uint32_t)__popc(m));
+        o = __shfl_sync(full, o, 0);
+        if (keep) out[o + __popc(m & ((1u << lane) - 1u))] = c;
+    }
+}
+
 __device__ __forceinline__ uint64_t mpos_out(const MyersRow &w, const MyersReqDev &R,
                                              uint32_t strand) {
     if (!strand) return w.pos;
@@ -589,17 +1140,107 @@ int Engine::run_bulge(const std::vector<Request> &reqs, std::vector<Result> &out
         d.vals2.ensure(row_cap, err) || d.lens.ensure(row_cap + 1, err) ||
         d.offs.ensure(row_cap + 1, err))
         return err.code;
-    uint32_t chunk = std::max<uint32_t>(1, std::min<uint32_t>(n_cand, 1u << 21));
+    // warp-per-candidate traceback when every request's bulge budgets fit
+    // the 16 bytes of a table cell; COF_BULGE_WARP=0 selects the
+    // thread-per-candidate kernel
+    bool warp_tb = true;
+    uint32_t tbl_words = 0;
+    for (const MyersReqDev &rd : rdev) {
+        const uint32_t nb = (rd.db + 1) * (rd.rb + 1);
+        if (nb > (uint32_t)kTbMaxBudgets) warp_tb = false;
+        tbl_words = std::max(tbl_words, (rd.L + 1) * (rd.W + 1) * ((nb + 3) / 4));
+    }
+    if (const char *e = std::getenv("COF_BULGE_WARP"))
+        if (e[0] == '0') warp_tb = false;
+    if (warp_tb && d.tb_items.ensure(2 * (size_t)kTbQueue * sizeof(TbItem), err)) return err.code;
+    const size_t tb_smem = (size_t)kTbWarps * tb_warp_bytes(tbl_words);
+    int tb_blocks_per_sm = 1;
+    if (warp_tb) {
+        CU(cudaFuncSetAttribute(traceback_warp_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)tb_smem));
+        CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&tb_blocks_per_sm, traceback_warp_kernel,
+                                                         kTbWarps * 32, tb_smem));
+        tb_blocks_per_sm = std::max(1, tb_blocks_per_sm);
+    }
+    // exact pre-test: only candidates with an alignment within the caps go
+    // on to the warp traceback
+    const MyersCand *cands = d.mcand.p;
+    uint32_t n_work = n_cand;
+    if (warp_tb && n_cand) {
+        uint32_t wmax = 0, nbw = 1;
+        for (const MyersReqDev &rd : rdev) {
+            wmax = std::max(wmax, rd.W);
+            nbw = std::max(nbw, ((rd.db + 1) * (rd.rb + 1) + 3) / 4);
+        }
+        const size_t bf_smem = (size_t)(wmax + 1) * nbw * kBfThreads * 4;
+        if (d.mcand2.ensure(n_cand, err)) return err.code;
+        auto kfn = nbw == 1 ? budget_filter_kernel<1>
+                 : nbw == 2 ? budget_filter_kernel<2>
+                 : nbw == 3 ? budget_filter_kernel<3> : budget_filter_kernel<4>;
+        CU(cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bf_smem));
+        int bf_per_sm = 1;
+        CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bf_per_sm, kfn, kBfThreads, bf_smem));
+        CU(cudaMemsetAsync(&d.ctr.p->rows, 0, 4, s));
+        CU(cudaEventRecord(d.ev[3], s));
+        const unsigned bg = (unsigned)std::max<uint64_t>(
+            1, std::min<uint64_t>((n_cand + kBfThreads - 1) / kBfThreads,
+                                  (uint64_t)d.n_sm * std::max(1, bf_per_sm)));
+        kfn<<<bg, kBfThreads, bf_smem, s>>>(d.view(), dB, dP, dR, d.mcand.p, n_cand, d.mcand2.p,
+                                           &d.ctr.p->rows);
+        CU(cudaGetLastError());
+        CU(cudaEventRecord(d.ev[4], s));
+        ++times_.kernel_launches;
+        CU(cudaMemcpyAsync(&n_work, &d.ctr.p->rows, 4, cudaMemcpyDeviceToHost, s));
+        CU(cudaStreamSynchronize(s));
+        cudaEventElapsedTime(&ms, d.ev[3], d.ev[4]);
+        times_.verify_ms += ms;
+        cands = d.mcand2.p;
+    }
+    uint32_t chunk = std::max<uint32_t>(1, std::min<uint32_t>(n_work, 1u << 21));
     uint32_t c0 = 0;
-    while (c0 < n_cand) {
-        const uint32_t cn = std::min(chunk, n_cand - c0);
+    while (c0 < n_work) {
+        const uint32_t cn = std::min(chunk, n_work - c0);
         CU(cudaMemsetAsync(d.ctr.p, 0, sizeof(Counters), s));
         CU(cudaMemsetAsync(d.req_rows.p, 0, reqs.size() * 4, s));
         CU(cudaEventRecord(d.ev[3], s));
-        const unsigned tb = (unsigned)std::min<uint64_t>((cn + 127) / 128, (uint64_t)d.n_sm * 32);
-        traceback_kernel<<<tb, 128, 0, s>>>(d.view(), dB, dP, dR, d.mcand.p + c0, cn, d.mrows.p,
-                                            (uint32_t)row_cap, d.keys.p, d.vals.p, d.ctr.p,
-                                            d.req_rows.p);
+        if (warp_tb) {
+            // pass 0 walks every candidate; a warp that spends kTbBudget
+            // iterations on one tree hands its remaining stack on, and the
+            // next pass spreads those subtrees over all warps
+            const unsigned grid = (unsigned)((uint64_t)d.n_sm * tb_blocks_per_sm);
+            TbItem *q[2] = {reinterpret_cast<TbItem *>(d.tb_items.p),
+                            reinterpret_cast<TbItem *>(d.tb_items.p) + kTbQueue};
+            const TbItem *in = nullptr;
+            uint32_t n_in = 0;
+            for (int pass = 0;; ++pass) {
+                const bool last = pass >= kTbMaxPasses;
+                CU(cudaMemsetAsync(&d.ctr.p->next_item, 0, sizeof(unsigned long long), s));
+                CU(cudaMemsetAsync(&d.ctr.p->hits, 0, sizeof(uint32_t), s));
+                const uint64_t work = in ? n_in : cn;
+                const unsigned tb = (unsigned)std::max<uint64_t>(
+                    1, std::min<uint64_t>((work + kTbWarps - 1) / kTbWarps, grid));
+                TbItem *out_q = q[pass & 1];
+                traceback_warp_kernel<<<tb, kTbWarps * 32, tb_smem, s>>>(
+                    d.view(), dB, dP, dR, cands + c0, cn, in, n_in, last ? nullptr : out_q,
+                    kTbQueue, kTbBudget, tbl_words, d.mrows.p, (uint32_t)row_cap, d.keys.p,
+                    d.vals.p, d.ctr.p, d.req_rows.p);
+                CU(cudaGetLastError());
+                ++times_.kernel_launches;
+                if (last) break;
+                uint32_t n_spill = 0;
+                CU(cudaMemcpyAsync(&n_spill, &d.ctr.p->hits, 4, cudaMemcpyDeviceToHost, s));
+                CU(cudaStreamSynchronize(s));
+                if (n_spill == 0) break;
+                in = out_q;
+                n_in = std::min<uint32_t>(n_spill, kTbQueue);
+            }
+            --times_.kernel_launches;  // counted once more below
+        } else {
+            const unsigned tb = (unsigned)std::min<uint64_t>((cn + 127) / 128, (uint64_t)d.n_sm * 32);
+            traceback_kernel<<<tb, 128, 0, s>>>(d.view(), dB, dP, dR, cands + c0, cn, d.mrows.p,
+                                                (uint32_t)row_cap, d.keys.p, d.vals.p, d.ctr.p,
+                                                d.req_rows.p);
+        }
         CU(cudaGetLastError());
         CU(cudaEventRecord(d.ev[4], s));
         ++times_.kernel_launches;

@@ -90,3 +90,30 @@ def test_mixed_popcount_and_bulge_batch(cof_mod, oracle_mod):
                              r["max_dna_bulges"], r["max_rna_bulges"])
         assert _rows(text) == _rows(single) == _rows(ref)
         assert n == ns == nref
+
+
+@pytest.mark.parametrize("n_guides,planted", [(4, 5), (20, 30)])
+def test_warp_traceback_equals_thread_traceback(cof_mod, oracle_mod, monkeypatch, n_guides,
+                                                planted):
+    # planted sites with up to 4 mismatches and 2 bulges: candidates with
+    # hundreds of alignments next to ones with none.  The warp-per-candidate
+    # traceback must give the rows of the thread-per-candidate kernel (and of
+    # the oracle, on the smaller case).
+    import synth
+    cfg = synth.config_bulge(seed=4, scale=0.0004, n_guides=n_guides, planted=planted)
+    g = cof_mod.Genome()
+    cfg["genome"].load_into(g)
+    args = (cfg["filter"], cfg["patterns"], cfg["max_mismatches"], cfg["max_dna_bulges"],
+            cfg["max_rna_bulges"])
+    monkeypatch.delenv("COF_BULGE_WARP", raising=False)
+    text, n = g.search(*args)
+    monkeypatch.setenv("COF_BULGE_WARP", "0")
+    text0, n0 = g.search(*args)
+    assert n == n0 > 0
+    assert sorted(text.splitlines()) == sorted(text0.splitlines())
+    if n_guides == 4:
+        o = oracle_mod.OracleGenome()
+        for name, data, s, e in cfg["genome"].chunks():
+            o.add_chunk(name, data, s, e)
+        ref, nref = o.search(*args)
+        assert nref == n and sorted(ref.splitlines()) == sorted(text.splitlines())
