@@ -57,7 +57,13 @@ struct MyersPattern {
 
 struct MyersReqDev {
     uint32_t L, mm, db, rb, E, W, pam_len, raw;  // raw: Match lines, not rows
-    uint32_t first_pattern, pad[3];
+    uint32_t first_pattern, T, nbits, pad;       // T = mm + 1 thresholds per budget
+    // bit sets of the budget DP cells (bit b * T + v: "F[b] <= v"):
+    uint64_t m_valid[2];  // the (db + 1)(rb + 1) * T bits in use
+    uint64_t m_sub[2];    // valid bits with v >= 1 (targets of a +1 shift)
+    uint64_t m_rna[2];    // budgets with br >= 1 (targets of an RNA step)
+    uint64_t m_dna[2];    // budgets with bd >= 1 (targets of a DNA step)
+    uint64_t m_full[2];   // the full budget (db, rb)
 };
 
 struct MyersTile {
@@ -323,32 +329,39 @@ traceback_kernel(GenomeDev G, const BatchDev *__restrict__ batches,
 
 // ---- warp-per-candidate traceback ------------------------------------------
 //
-// Same rows as traceback_kernel, with the work laid out for a GPU.  One warp
-// takes one candidate from a dynamic queue, so that a few candidates with
-// thousands of alignments cannot serialise a whole warp or leave SMs idle.
+// Same rows as traceback_kernel, with the work laid out for a GPU.
 //
-// 1. Budget DP, as a wavefront (lane = pattern row i, step s = i + j, the
-//    upper row's values arrive by shuffle).  F[bd][br](i, j) = fewest
-//    mismatches on any alignment of pattern cells [0, i) ending at text cell
-//    j that uses at most bd DNA and br RNA bulges.  It obeys exactly the move
-//    rules of the enumeration: a diagonal step is barred under a pattern N
-//    on a mismatch and where classify's filter test fails; the bulge steps
-//    have their N-neighbour rules; a node over a padding cell is dead.
-//    Values clamp at mm + 1 ("infeasible").  All (db + 1)(rb + 1) budgets
-//    of a cell are bytes of four registers and are updated together with
-//    SIMD byte min / max.
-// 2. Enumeration with exact pruning.  A node (i, j) with m mismatches and
-//    d, r bulges so far is kept iff m + F[db - d][rb - r](i, j) <= mm.  So
-//    every kept node lies on at least one emitted alignment: the cost bound
-//    and the caps of the reference's walk are both implied, and nothing else
-//    is cut.  The warp pops up to 32 nodes of a shared-memory stack, expands
-//    them in parallel and pushes the children, writing leaves (i = 0) as
-//    rows after classify's filter (already enforced) and the record-end
-//    drop.
+// Budget DP.  F[bd][br](i, j) = fewest mismatches on any alignment of
+// pattern cells [0, i) ending at text cell j that uses at most bd DNA and
+// br RNA bulges.  It obeys exactly the move rules of the enumeration: a
+// diagonal step is barred under a pattern N on a mismatch and where
+// classify's filter test fails; the bulge steps have their N-neighbour
+// rules; a node over a padding cell is dead.  Only "F <= v" for
+// v = 0..mm matters, so a cell is stored as a bit set over (budget, v):
+// bit b * T + v (T = mm + 1, b = bd * (rb + 1) + br) is set iff
+// F[b] <= v.  Then min is OR, a mismatch (+1) is a shift by one bit within
+// each budget group, a bulge step (smaller budget) is a shift by whole
+// groups, and values above mm are simply absent.  One or two 64-bit words
+// per cell (NW) hold (db + 1)(rb + 1)(mm + 1) <= 128 bits.
+//
+// traceback_warp_kernel: one warp takes one candidate (or a handed-on
+// subtree) from a dynamic queue, computes the table as a wavefront (lane =
+// pattern row i, step s = i + j, the upper row arrives by shuffle) into
+// shared memory, then enumerates with exact pruning: a node (i, j) with m
+// mismatches and d, r bulges so far is kept iff bit
+// ((db - d)(rb + 1) + rb - r) * T + mm - m of its cell is set, so every
+// kept node lies on at least one emitted alignment (the reference's cost
+// bound and caps are both implied, nothing else is cut).  The warp pops up
+// to 32 nodes of a shared-memory stack, expands them in parallel and pushes
+// the children; leaves (i = 0) are written as rows after the record-end
+// drop (classify's filter test is already part of the moves).  A warp that
+// spends kTbBudget iterations on one tree hands its remaining stack to a
+// global queue, which the next pass spreads over all warps, so a candidate
+// with thousands of alignments cannot serialise the launch.
 constexpr int kTbWarps = 4;                  // warps per block
 constexpr int kTbCap = 160;                  // stack slots per warp
 constexpr int kTbMargin = 2 * kMaxCells;     // slots a one-node-at-a-time walk can add
-constexpr int kTbMaxBudgets = 16;            // (db + 1) * (rb + 1) bytes per cell
+constexpr uint32_t kTbMaxBits = 128;         // budget bits per cell (NW <= 2)
 constexpr uint32_t kTbBudget = 96;           // iterations on one tree before handing it on
 constexpr uint32_t kTbQueue = 1u << 21;      // subtrees per hand-on queue
 constexpr int kTbMaxPasses = 24;             // the last pass finishes every tree
@@ -395,27 +408,60 @@ __device__ __forceinline__ bool filt_ok(uint8_t fl, uint8_t g) {
     return fl == 0xF ? g != 0 : (g != 0 && g != 0xF && (g & fl));
 }
 
-// the 16 budget bytes moved s (1..15) places up: byte b takes byte b - s,
-// zeros shifted in (selects, not a dynamically indexed array, so the
-// vectors stay in registers)
-__device__ __forceinline__ void shl_bytes(const uint32_t (&a)[4], uint32_t s, uint32_t (&o)[4]) {
-    const int ws = (int)(s >> 2);
-    const uint32_t b = 8 * (s & 3);
-    auto pick = [&](int k) -> uint32_t {
-        return k == 0 ? a[0] : k == 1 ? a[1] : k == 2 ? a[2] : k == 3 ? a[3] : 0u;
-    };
-#pragma unroll
-    for (int w = 0; w < 4; ++w) {
-        const uint32_t hi = pick(w - ws), lo = pick(w - ws - 1);
-        o[w] = b ? __funnelshift_l(lo, hi, b) : hi;
+// NW-word bit set shifted toward higher bits by s (1..127), zeros in
+template <int NW>
+__device__ __forceinline__ void bshl(const uint64_t (&a)[NW], uint32_t s, uint64_t (&o)[NW]) {
+    if (NW == 1) {
+        o[0] = s < 64 ? a[0] << s : 0;
+    } else if (s >= 64) {
+        o[NW - 1] = a[0] << (s - 64);
+        o[0] = 0;
+    } else {
+        o[NW - 1] = (a[NW - 1] << s) | (a[0] >> (64 - s));
+        o[0] = a[0] << s;
     }
 }
 
-// shared-memory bytes one warp needs for tables of tbl_words words
-__host__ __device__ constexpr size_t tb_warp_bytes(uint32_t tbl_words) {
-    return (kTbCap * sizeof(TbNode) + (size_t)tbl_words * 4 + 64 + 3 * 48 + 15) & ~(size_t)15;
+// one cell of the budget DP from its three neighbours: diagonal (i-1, j-1),
+// up (i-1, j) and left (i, j-1)
+template <int NW>
+__device__ __forceinline__ void budget_cell(const uint64_t (&dg)[NW], const uint64_t (&up)[NW],
+                                            const uint64_t (&lf)[NW], bool diag_ok, uint32_t mc,
+                                            bool rna_ok, bool dna_ok, uint32_t T, uint32_t dsh,
+                                            const MyersReqDev &R, uint64_t (&v)[NW]) {
+#pragma unroll
+    for (int w = 0; w < NW; ++w) v[w] = 0;
+    if (diag_ok) {
+        if (mc) {
+            uint64_t x[NW];
+            bshl<NW>(dg, 1, x);
+#pragma unroll
+            for (int w = 0; w < NW; ++w) v[w] = x[w] & R.m_sub[w];
+        } else {
+#pragma unroll
+            for (int w = 0; w < NW; ++w) v[w] = dg[w];
+        }
+    }
+    if (rna_ok) {
+        uint64_t x[NW];
+        bshl<NW>(up, T, x);
+#pragma unroll
+        for (int w = 0; w < NW; ++w) v[w] |= x[w] & R.m_rna[w];
+    }
+    if (dna_ok) {
+        uint64_t x[NW];
+        bshl<NW>(lf, dsh, x);
+#pragma unroll
+        for (int w = 0; w < NW; ++w) v[w] |= x[w] & R.m_dna[w];
+    }
 }
 
+// shared-memory bytes one warp needs for tables of tbl_words 64-bit words
+__host__ __device__ constexpr size_t tb_warp_bytes(uint32_t tbl_words) {
+    return (kTbCap * sizeof(TbNode) + (size_t)tbl_words * 8 + 64 + 3 * 48 + 15) & ~(size_t)15;
+}
+
+template <int NW>
 __global__ void __launch_bounds__(kTbWarps * 32)
 traceback_warp_kernel(GenomeDev G, const BatchDev *__restrict__ batches,
                       const MyersPattern *__restrict__ pats, const MyersReqDev *__restrict__ reqs,
@@ -428,8 +474,8 @@ traceback_warp_kernel(GenomeDev G, const BatchDev *__restrict__ batches,
     const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     unsigned char *wbase = tb_smem + warp * tb_warp_bytes(tbl_words);
     TbNode *stk = reinterpret_cast<TbNode *>(wbase);
-    uint32_t *tbl = reinterpret_cast<uint32_t *>(wbase + kTbCap * sizeof(TbNode));
-    uint8_t *stext = wbase + kTbCap * sizeof(TbNode) + (size_t)tbl_words * 4;
+    uint64_t *tbl = reinterpret_cast<uint64_t *>(wbase + kTbCap * sizeof(TbNode));
+    uint8_t *stext = wbase + kTbCap * sizeof(TbNode) + (size_t)tbl_words * 8;
     uint8_t *spb = stext + 64, *sisn = spb + 48, *seff = sisn + 48;
     const unsigned full = 0xFFFFFFFFu;
 
@@ -451,19 +497,24 @@ traceback_warp_kernel(GenomeDev G, const BatchDev *__restrict__ batches,
         const MyersCand c = cand[ci];
         const BatchDev B = batches[c.batch];
         const MyersPattern &P = pats[c.pattern];
-        const MyersReqDev R = reqs[P.request];
-        const uint32_t L = P.L, t = c.t_local;
+        const MyersReqDev &R = reqs[P.request];
+        const uint32_t L = P.L, t = c.t_local, mm = R.mm, T = R.T;
         const uint32_t n = min(R.W, t + 1);  // text cells of the window
         const uint32_t cols = n + 1;
-        const uint32_t nb = (R.db + 1) * (R.rb + 1), nbw = (nb + 3) >> 2;
-        const uint32_t cl = min(R.mm + 1, 127u);
+        const uint32_t rb1 = R.rb + 1, dsh = T * rb1;
         for (uint32_t k = lane; k < n; k += 32) stext[k] = nib(G.bit4, B.base + t + 1 - n + k);
         for (uint32_t k = lane; k < L; k += 32) {
             spb[k] = P.b4[k];
             sisn[k] = P.isn[k];
             seff[k] = P.eff[k];
         }
-        for (uint32_t k = lane; k < cols * nbw; k += 32) tbl[k] = 0;  // row 0
+        uint64_t valid[NW];
+#pragma unroll
+        for (int w = 0; w < NW; ++w) valid[w] = R.m_valid[w];
+        for (uint32_t k = lane; k < cols; k += 32) {  // row 0: F = 0 for every budget
+#pragma unroll
+            for (int w = 0; w < NW; ++w) tbl[k * NW + w] = valid[w];
+        }
         __syncwarp();
 
         // -- 1. budget DP wavefront
@@ -480,67 +531,47 @@ traceback_warp_kernel(GenomeDev G, const BatchDev *__restrict__ batches,
             rna_ok = R.rb > 0 && !isn1 && !isn0 && !isn2;
             dna_ok = R.db > 0 && i < L && !(isn1 && isn0);
         }
-        uint32_t inv_r[4], inv_d[4];  // 0x7F in the bytes a move cannot reach
+        uint64_t left[NW], upc[NW], upp[NW];
 #pragma unroll
-        for (int w = 0; w < 4; ++w) {
-            inv_r[w] = inv_d[w] = 0;
-#pragma unroll
-            for (int q = 0; q < 4; ++q) {
-                const uint32_t b = 4 * w + q;
-                if (b >= nb || b % (R.rb + 1) == 0) inv_r[w] |= 0x7Fu << (8 * q);
-                if (b >= nb || b < R.rb + 1) inv_d[w] |= 0x7Fu << (8 * q);
-            }
-        }
-        const uint32_t clv = cl * 0x01010101u;
-        uint32_t left[4] = {0, 0, 0, 0}, upc[4] = {0, 0, 0, 0}, upp[4] = {0, 0, 0, 0};
+        for (int w = 0; w < NW; ++w) left[w] = upc[w] = upp[w] = 0;
         for (uint32_t s = 0; s < L + n; ++s) {
 #pragma unroll
-            for (int w = 0; w < 4; ++w) {
-                uint32_t u = __shfl_up_sync(full, left[w], 1);
-                if (lane == 0) u = 0;  // row 0: F = 0
+            for (int w = 0; w < NW; ++w) {
+                uint64_t u = __shfl_up_sync(full, left[w], 1);
+                if (lane == 0) u = valid[w];  // row 0
                 upp[w] = upc[w];
                 upc[w] = u;
             }
             const int j = (int)s - (int)lane;
             if (row_on && j >= 0 && j <= (int)n) {
-                uint32_t dg[4], rn[4], dn[4];
-#pragma unroll
-                for (int w = 0; w < 4; ++w) dg[w] = rn[w] = dn[w] = 0x7F7F7F7Fu;
+                uint64_t v[NW];
                 const uint8_t tx = j ? stext[j - 1] : 0;
-                if (j >= 1) {
+                if (j == 0) {
+                    budget_cell<NW>(upp, upc, left, false, 0, rna_ok, false, T, dsh, R, v);
+                } else if (tx == 0) {  // a node over a padding cell is dead
+#pragma unroll
+                    for (int w = 0; w < NW; ++w) v[w] = 0;
+                } else {
                     const uint32_t mc = loose(pbi, tx) ? 0u : 1u;
-                    if (!(mc && isn1) && filt_ok(effi, tx)) {
-#pragma unroll
-                        for (int w = 0; w < 4; ++w) dg[w] = upp[w] + mc * 0x01010101u;
-                    }
+                    const bool dok = !(mc && isn1) && filt_ok(effi, tx);
+                    budget_cell<NW>(upp, upc, left, dok, mc, rna_ok, dna_ok, T, dsh, R, v);
                 }
-                if (rna_ok) {
-                    shl_bytes(upc, 1, rn);
+                uint64_t *cell = tbl + (i * cols + (uint32_t)j) * NW;
 #pragma unroll
-                    for (int w = 0; w < 4; ++w) rn[w] = __vmaxu4(rn[w], inv_r[w]);
-                }
-                if (dna_ok && j >= 1) {
-                    shl_bytes(left, R.rb + 1, dn);
-#pragma unroll
-                    for (int w = 0; w < 4; ++w) dn[w] = __vmaxu4(dn[w], inv_d[w]);
-                }
-                const bool dead = j >= 1 && tx == 0;
-                uint32_t *cell = tbl + (i * cols + (uint32_t)j) * nbw;
-#pragma unroll
-                for (int w = 0; w < 4; ++w) {
-                    const uint32_t v =
-                        dead ? clv : __vminu4(__vminu4(__vminu4(dg[w], rn[w]), dn[w]), clv);
-                    left[w] = v;
-                    if ((uint32_t)w < nbw) cell[w] = v;
+                for (int w = 0; w < NW; ++w) {
+                    left[w] = v[w];
+                    cell[w] = v[w];
                 }
             }
         }
         __syncwarp();
-        auto F = [&](uint32_t ii, uint32_t jj, uint32_t b) -> uint32_t {
-            return (tbl[(ii * cols + jj) * nbw + (b >> 2)] >> (8 * (b & 3))) & 0xFFu;
+        // F[b](ii, jj) <= mm - m ?
+        auto feas = [&](uint32_t ii, uint32_t jj, uint32_t b, uint32_t m) -> bool {
+            const uint32_t bit = b * T + (mm - m);
+            return (tbl[(ii * cols + jj) * NW + (bit >> 6)] >> (bit & 63)) & 1u;
         };
         if (!items) {
-            if (F(L, n, nb - 1) > R.mm) continue;  // no alignment within the caps
+            if (!feas(L, n, R.db * rb1 + R.rb, 0)) continue;  // no alignment within the caps
             start_node = TbNode{0, 0, tb_st(L, n, 0, 0, 0, 0)};
         }
         // every leaf starts in [t + 1 - n, t + 1]: one chunk lookup serves
@@ -560,7 +591,6 @@ traceback_warp_kernel(GenomeDev G, const BatchDev *__restrict__ batches,
         uint32_t size = 1;
         if (lane == 0) stk[0] = start_node;
         __syncwarp();
-        const uint32_t rb1 = R.rb + 1;
         uint32_t iters = 0;
         bool may_spill = iter_budget != 0 && spill != nullptr;
         while (size > 0) {
@@ -613,10 +643,10 @@ traceback_warp_kernel(GenomeDev G, const BatchDev *__restrict__ batches,
                 if (nj >= 1) {
                     const uint8_t tx = stext[nj - 1];
                     const uint32_t mc = loose(spb[ni - 1], tx) ? 0u : 1u;
-                    if (!(mc && sisn[ni - 1]) && filt_ok(seff[ni - 1], tx) && m + mc <= R.mm) {
+                    if (!(mc && sisn[ni - 1]) && filt_ok(seff[ni - 1], tx) && m + mc <= mm) {
                         if (ni == 1)
                             leaf(la, nj - 1, m + mc, d, r, mc);
-                        else if (m + mc + F(ni - 1, nj - 1, (R.db - d) * rb1 + (R.rb - r)) <= R.mm)
+                        else if (feas(ni - 1, nj - 1, (R.db - d) * rb1 + (R.rb - r), m + mc))
                             ka = Kid{tb_st(ni - 1, nj - 1, m + mc, d, r, dep + 1), mc, true};
                     }
                 }
@@ -626,13 +656,13 @@ traceback_warp_kernel(GenomeDev G, const BatchDev *__restrict__ batches,
                     if (!sisn[ni - 1] && !isn0 && !isn2) {
                         if (ni == 1)
                             leaf(lb, nj, m, d, r + 1, 3);
-                        else if (m + F(ni - 1, nj, (R.db - d) * rb1 + (R.rb - r - 1)) <= R.mm)
+                        else if (feas(ni - 1, nj, (R.db - d) * rb1 + (R.rb - r - 1), m))
                             kb = Kid{tb_st(ni - 1, nj, m, d, r + 1, dep + 1), 3, true};
                     }
                 }
                 // DNA bulge: text cell skipped
                 if (d < R.db && nj >= 1 && ni < L && !(sisn[ni - 1] && sisn[ni])) {
-                    if (m + F(ni, nj - 1, (R.db - d - 1) * rb1 + (R.rb - r)) <= R.mm)
+                    if (feas(ni, nj - 1, (R.db - d - 1) * rb1 + (R.rb - r), m))
                         kc = Kid{tb_st(ni, nj - 1, m, d + 1, r, dep + 1), 2, true};
                 }
             }
@@ -716,46 +746,26 @@ traceback_warp_kernel(GenomeDev G, const BatchDev *__restrict__ batches,
 }
 
 // Exact pre-test of the warp traceback, one thread per candidate: the
-// root value F[db][rb](L, n) of the budget DP, computed row by row (pattern
-// cell i) with the previous row kept in shared memory, interleaved by
-// thread so that a warp's accesses hit 32 different banks.  Every
-// alignment path crosses every row, and fewer bulges never need fewer
-// mismatches, so the root value is at least the smallest full-budget value
-// of any row: a row whose minimum exceeds mm ends the test early.  A
-// candidate whose root value exceeds mm has no alignment within the caps
-// (most of the ones the Myers bound lets through), so only the others are
-// passed on.  NBW = budget words per cell ((db + 1)(rb + 1) <= 4 * NBW).
+// budget DP row by row (pattern cell i) with the previous row kept in
+// shared memory, interleaved by thread so that a warp's accesses hit
+// different banks, and only the root cell's full-budget bit at mm tested.
+// Every alignment path crosses every row, and a smaller budget never needs
+// fewer mismatches, so the root can only be feasible if some cell of every
+// row has a full-budget bit at mm: a row without one ends the test early.
+// Most candidates the Myers bound lets through fail here; only the others
+// are passed on.
 constexpr int kBfThreads = 128;
 
-// byte shift of an NBW-word budget vector; s < 4 needs no word moves
-template <int NBW>
-__device__ __forceinline__ void shl_budget(const uint32_t (&a)[NBW], uint32_t s,
-                                           uint32_t (&o)[NBW]) {
-    if (s < 4) {
-        const uint32_t b = 8 * s;
-        o[0] = a[0] << b;
-#pragma unroll
-        for (int w = 1; w < NBW; ++w) o[w] = __funnelshift_l(a[w - 1], a[w], b);
-        return;
-    }
-    uint32_t x[4] = {0, 0, 0, 0}, y[4];
-#pragma unroll
-    for (int w = 0; w < NBW; ++w) x[w] = a[w];
-    shl_bytes(x, s, y);
-#pragma unroll
-    for (int w = 0; w < NBW; ++w) o[w] = y[w];
-}
-
-template <int NBW>
+template <int NW>
 __global__ void __launch_bounds__(kBfThreads)
 budget_filter_kernel(GenomeDev G, const BatchDev *__restrict__ batches,
                      const MyersPattern *__restrict__ pats, const MyersReqDev *__restrict__ reqs,
                      const MyersCand *__restrict__ cand, uint32_t n_cand,
                      MyersCand *__restrict__ out, uint32_t *n_out) {
-    extern __shared__ uint32_t bf_row[];  // [cell * NBW + w][thread], cells 0..n
+    extern __shared__ uint64_t bf_row[];  // [cell * NW + w][thread], cells 0..n
     const uint32_t tid = threadIdx.x;
-    auto Rw = [&](uint32_t j, int w) -> uint32_t & {
-        return bf_row[(j * NBW + w) * kBfThreads + tid];
+    auto Rw = [&](uint32_t j, int w) -> uint64_t & {
+        return bf_row[(j * NW + w) * kBfThreads + tid];
     };
     for (uint32_t base = blockIdx.x * kBfThreads; base < n_cand; base += gridDim.x * kBfThreads) {
         const uint32_t ci = base + tid;
@@ -765,22 +775,16 @@ budget_filter_kernel(GenomeDev G, const BatchDev *__restrict__ batches,
             c = cand[ci];
             const BatchDev B = batches[c.batch];
             const MyersPattern &P = pats[c.pattern];
-            const MyersReqDev R = reqs[P.request];
-            const uint32_t L = P.L, t = c.t_local;
+            const MyersReqDev &R = reqs[P.request];
+            const uint32_t L = P.L, t = c.t_local, T = R.T;
             const uint32_t n = min(R.W, t + 1);
-            const uint32_t nb = (R.db + 1) * (R.rb + 1), rb1 = R.rb + 1;
-            const uint32_t cl = min(R.mm + 1, 127u), clv = cl * 0x01010101u;
-            const uint32_t fb = nb - 1, fw = fb >> 2, fs = 8 * (fb & 3);  // full budget byte
-            uint32_t inv_r[NBW], inv_d[NBW];
+            const uint32_t dsh = T * (R.rb + 1);
+            const uint32_t top = ((R.db + 1) * (R.rb + 1) - 1) * T + R.mm;  // root bit
+            uint64_t fullg[NW], valid[NW];
 #pragma unroll
-            for (int w = 0; w < NBW; ++w) {
-                inv_r[w] = inv_d[w] = 0;
-#pragma unroll
-                for (int q = 0; q < 4; ++q) {
-                    const uint32_t b = 4 * w + q;
-                    if (b >= nb || b % rb1 == 0) inv_r[w] |= 0x7Fu << (8 * q);
-                    if (b >= nb || b < rb1) inv_d[w] |= 0x7Fu << (8 * q);
-                }
+            for (int w = 0; w < NW; ++w) {
+                fullg[w] = R.m_full[w];
+                valid[w] = R.m_valid[w];
             }
             // the window's n text cells, cell k in bits 4k of (t2:t1:t0)
             const uint64_t tbase = B.base + t + 1 - n;
@@ -791,7 +795,7 @@ budget_filter_kernel(GenomeDev G, const BatchDev *__restrict__ batches,
             }
             for (uint32_t j = 0; j <= n; ++j) {
 #pragma unroll
-                for (int w = 0; w < NBW; ++w) Rw(j, w) = 0;  // row 0
+                for (int w = 0; w < NW; ++w) Rw(j, w) = valid[w];  // row 0
             }
             keep = true;
             for (uint32_t i = 1; i <= L && keep; ++i) {
@@ -800,65 +804,44 @@ budget_filter_kernel(GenomeDev G, const BatchDev *__restrict__ batches,
                            isn2 = i >= 2 && P.isn[i - 2];
                 const bool rna_ok = R.rb > 0 && !isn1 && !isn0 && !isn2;
                 const bool dna_ok = R.db > 0 && i < L && !(isn1 && isn0);
-                uint32_t dsrc[NBW], left[NBW];
+                uint64_t dsrc[NW], left[NW], v[NW], up[NW];
                 // column 0: only an RNA bulge from the cell above
 #pragma unroll
-                for (int w = 0; w < NBW; ++w) dsrc[w] = Rw(0, w);
-                if (rna_ok) {
-                    shl_budget<NBW>(dsrc, 1, left);
+                for (int w = 0; w < NW; ++w) dsrc[w] = Rw(0, w);
+                budget_cell<NW>(dsrc, dsrc, dsrc, false, 0, rna_ok, false, T, dsh, R, left);
+                uint64_t row_or = 0;
 #pragma unroll
-                    for (int w = 0; w < NBW; ++w) left[w] = __vminu4(__vmaxu4(left[w], inv_r[w]), clv);
-                } else {
-#pragma unroll
-                    for (int w = 0; w < NBW; ++w) left[w] = clv;
+                for (int w = 0; w < NW; ++w) {
+                    Rw(0, w) = left[w];
+                    row_or |= left[w] & fullg[w];
                 }
-                uint32_t row_min = (left[fw] >> fs) & 0xFFu;
-#pragma unroll
-                for (int w = 0; w < NBW; ++w) Rw(0, w) = left[w];
                 uint64_t a0 = tw0, a1 = tw1, a2 = tw2;  // text shift register
                 for (uint32_t j = 1; j <= n; ++j) {
                     const uint8_t tx = (uint8_t)(a0 & 0xF);
                     a0 = (a0 >> 4) | (a1 << 60);
                     a1 = (a1 >> 4) | (a2 << 60);
                     a2 >>= 4;
-                    uint32_t up[NBW], v[NBW];
 #pragma unroll
-                    for (int w = 0; w < NBW; ++w) up[w] = Rw(j, w);
+                    for (int w = 0; w < NW; ++w) up[w] = Rw(j, w);
                     if (tx == 0) {  // a node over a padding cell is dead
 #pragma unroll
-                        for (int w = 0; w < NBW; ++w) v[w] = clv;
+                        for (int w = 0; w < NW; ++w) v[w] = 0;
                     } else {
-#pragma unroll
-                        for (int w = 0; w < NBW; ++w) v[w] = clv;
                         const uint32_t mc = loose(pb, tx) ? 0u : 1u;
-                        if (!(mc && isn1) && filt_ok(ef, tx)) {
-#pragma unroll
-                            for (int w = 0; w < NBW; ++w) v[w] = __vminu4(v[w], dsrc[w] + mc * 0x01010101u);
-                        }
-                        if (rna_ok) {
-                            uint32_t x[NBW];
-                            shl_budget<NBW>(up, 1, x);
-#pragma unroll
-                            for (int w = 0; w < NBW; ++w) v[w] = __vminu4(v[w], __vmaxu4(x[w], inv_r[w]));
-                        }
-                        if (dna_ok) {
-                            uint32_t x[NBW];
-                            shl_budget<NBW>(left, rb1, x);
-#pragma unroll
-                            for (int w = 0; w < NBW; ++w) v[w] = __vminu4(v[w], __vmaxu4(x[w], inv_d[w]));
-                        }
+                        const bool dok = !(mc && isn1) && filt_ok(ef, tx);
+                        budget_cell<NW>(dsrc, up, left, dok, mc, rna_ok, dna_ok, T, dsh, R, v);
                     }
 #pragma unroll
-                    for (int w = 0; w < NBW; ++w) {
+                    for (int w = 0; w < NW; ++w) {
                         Rw(j, w) = v[w];
                         dsrc[w] = up[w];
                         left[w] = v[w];
+                        row_or |= v[w] & fullg[w];
                     }
-                    row_min = min(row_min, (v[fw] >> fs) & 0xFFu);
                 }
-                if (row_min > R.mm) keep = false;
+                if (!row_or) keep = false;
             }
-            if (keep) keep = ((Rw(n, (int)fw) >> fs) & 0xFFu) <= R.mm;
+            if (keep) keep = (Rw(n, (int)(top >> 6)) >> (top & 63)) & 1u;
         }
         // warp-aggregated compaction of the survivors
         const unsigned full = 0xFFFFFFFFu;
@@ -1046,9 +1029,34 @@ int Engine::run_bulge(const std::vector<Request> &reqs, std::vector<Result> &out
     for (size_t ri = 0; ri < reqs.size(); ++ri) {
         const Request &r = reqs[ri];
         const uint32_t L = (uint32_t)r.filter.size();
-        MyersReqDev rd{L, r.max_mm, r.max_db, r.max_rb, r.max_mm + r.max_db + r.max_rb,
-                       L + r.max_db, (uint32_t)r.pam_len, r.raw ? 1u : 0u,
-                       (uint32_t)pats.size(), {0, 0, 0}};
+        MyersReqDev rd;
+        std::memset(&rd, 0, sizeof rd);
+        rd.L = L;
+        rd.mm = r.max_mm;
+        rd.db = r.max_db;
+        rd.rb = r.max_rb;
+        rd.E = r.max_mm + r.max_db + r.max_rb;
+        rd.W = L + r.max_db;
+        rd.pam_len = (uint32_t)r.pam_len;
+        rd.raw = r.raw ? 1u : 0u;
+        rd.first_pattern = (uint32_t)pats.size();
+        // budget DP bit sets: bit b * T + v, b = bd * (rb + 1) + br
+        rd.T = rd.mm + 1;
+        const uint32_t nbud = (rd.db + 1) * (rd.rb + 1);
+        rd.nbits = nbud * rd.T;
+        auto setb = [](uint64_t(&m)[2], uint32_t bit) {
+            if (bit < 128) m[bit >> 6] |= 1ull << (bit & 63);
+        };
+        for (uint32_t b = 0; b < nbud; ++b) {
+            for (uint32_t v = 0; v < rd.T; ++v) {
+                const uint32_t bit = b * rd.T + v;
+                setb(rd.m_valid, bit);
+                if (v >= 1) setb(rd.m_sub, bit);
+                if (b % (rd.rb + 1) >= 1) setb(rd.m_rna, bit);
+                if (b / (rd.rb + 1) >= 1) setb(rd.m_dna, bit);
+                if (b == nbud - 1) setb(rd.m_full, bit);
+            }
+        }
         if (rd.W > (uint32_t)kMaxCells) {
             err = {kUnsupported, "pattern length + max_dna_bulges above 40"};
             return err.code;
@@ -1140,26 +1148,28 @@ int Engine::run_bulge(const std::vector<Request> &reqs, std::vector<Result> &out
         d.vals2.ensure(row_cap, err) || d.lens.ensure(row_cap + 1, err) ||
         d.offs.ensure(row_cap + 1, err))
         return err.code;
-    // warp-per-candidate traceback when every request's bulge budgets fit
-    // the 16 bytes of a table cell; COF_BULGE_WARP=0 selects the
+    // warp-per-candidate traceback when every request's budget bit set
+    // fits 128 bits ((db + 1)(rb + 1)(mm + 1)); COF_BULGE_WARP=0 selects the
     // thread-per-candidate kernel
     bool warp_tb = true;
-    uint32_t tbl_words = 0;
+    uint32_t nw = 1, wmax = 0;
     for (const MyersReqDev &rd : rdev) {
-        const uint32_t nb = (rd.db + 1) * (rd.rb + 1);
-        if (nb > (uint32_t)kTbMaxBudgets) warp_tb = false;
-        tbl_words = std::max(tbl_words, (rd.L + 1) * (rd.W + 1) * ((nb + 3) / 4));
+        if (rd.nbits > kTbMaxBits) warp_tb = false;
+        nw = std::max(nw, (rd.nbits + 63) / 64);
+        wmax = std::max(wmax, rd.W);
     }
+    uint32_t tbl_words = 0;  // 64-bit words of one warp's table
+    for (const MyersReqDev &rd : rdev) tbl_words = std::max(tbl_words, (rd.L + 1) * (rd.W + 1) * nw);
     if (const char *e = std::getenv("COF_BULGE_WARP"))
         if (e[0] == '0') warp_tb = false;
     if (warp_tb && d.tb_items.ensure(2 * (size_t)kTbQueue * sizeof(TbItem), err)) return err.code;
     const size_t tb_smem = (size_t)kTbWarps * tb_warp_bytes(tbl_words);
+    auto tb_fn = nw == 1 ? traceback_warp_kernel<1> : traceback_warp_kernel<2>;
     int tb_blocks_per_sm = 1;
     if (warp_tb) {
-        CU(cudaFuncSetAttribute(traceback_warp_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)tb_smem));
-        CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&tb_blocks_per_sm, traceback_warp_kernel,
-                                                         kTbWarps * 32, tb_smem));
+        CU(cudaFuncSetAttribute(tb_fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tb_smem));
+        CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&tb_blocks_per_sm, tb_fn, kTbWarps * 32,
+                                                         tb_smem));
         tb_blocks_per_sm = std::max(1, tb_blocks_per_sm);
     }
     // exact pre-test: only candidates with an alignment within the caps go
@@ -1167,16 +1177,9 @@ int Engine::run_bulge(const std::vector<Request> &reqs, std::vector<Result> &out
     const MyersCand *cands = d.mcand.p;
     uint32_t n_work = n_cand;
     if (warp_tb && n_cand) {
-        uint32_t wmax = 0, nbw = 1;
-        for (const MyersReqDev &rd : rdev) {
-            wmax = std::max(wmax, rd.W);
-            nbw = std::max(nbw, ((rd.db + 1) * (rd.rb + 1) + 3) / 4);
-        }
-        const size_t bf_smem = (size_t)(wmax + 1) * nbw * kBfThreads * 4;
+        const size_t bf_smem = (size_t)(wmax + 1) * nw * kBfThreads * 8;
         if (d.mcand2.ensure(n_cand, err)) return err.code;
-        auto kfn = nbw == 1 ? budget_filter_kernel<1>
-                 : nbw == 2 ? budget_filter_kernel<2>
-                 : nbw == 3 ? budget_filter_kernel<3> : budget_filter_kernel<4>;
+        auto kfn = nw == 1 ? budget_filter_kernel<1> : budget_filter_kernel<2>;
         CU(cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bf_smem));
         int bf_per_sm = 1;
         CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bf_per_sm, kfn, kBfThreads, bf_smem));
@@ -1220,7 +1223,7 @@ int Engine::run_bulge(const std::vector<Request> &reqs, std::vector<Result> &out
                 const unsigned tb = (unsigned)std::max<uint64_t>(
                     1, std::min<uint64_t>((work + kTbWarps - 1) / kTbWarps, grid));
                 TbItem *out_q = q[pass & 1];
-                traceback_warp_kernel<<<tb, kTbWarps * 32, tb_smem, s>>>(
+                tb_fn<<<tb, kTbWarps * 32, tb_smem, s>>>(
                     d.view(), dB, dP, dR, cands + c0, cn, in, n_in, last ? nullptr : out_q,
                     kTbQueue, kTbBudget, tbl_words, d.mrows.p, (uint32_t)row_cap, d.keys.p,
                     d.vals.p, d.ctr.p, d.req_rows.p);
