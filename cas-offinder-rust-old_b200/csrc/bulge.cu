@@ -27,6 +27,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <array>
 #include <cstdlib>
 #include <cstring>
 #include <memory>
@@ -998,6 +999,21 @@ void build_eq16(const std::string &p, uint32_t eq16[16]) {
     }
 }
 
+// Grows a device byte buffer to hold `need` bytes, keeping its first `used`
+// bytes (capacity at least doubles, so appends stay amortised).
+int grow_keep(DevBuf<char> &b, size_t need, size_t used, cudaStream_t s, Error &err) {
+    if (need <= b.cap) return kOk;
+    const size_t cap = std::max(need, 2 * b.cap);
+    char *p = nullptr;
+    CU(cudaMalloc((void **)&p, cap));
+    if (used) CU(cudaMemcpyAsync(p, b.p, used, cudaMemcpyDeviceToDevice, s));
+    CU(cudaStreamSynchronize(s));
+    if (b.p) cudaFree(b.p);
+    b.p = p;
+    b.cap = cap;
+    return kOk;
+}
+
 }  // namespace
 
 int Engine::run_bulge(const std::vector<Request> &reqs, std::vector<Result> &out, Error &err) {
@@ -1140,8 +1156,11 @@ int Engine::run_bulge(const std::vector<Request> &reqs, std::vector<Result> &out
 
     // stage 2: traceback over candidate chunks; each chunk's rows are sorted
     // (pattern, start), formatted and appended to the requests' texts
-    std::vector<std::string> texts(reqs.size());
+    // every chunk's rows go to one device text arena; segs = (arena offset,
+    // bytes, request) per chunk and request
     std::vector<uint64_t> nrows(reqs.size(), 0);
+    std::vector<std::array<uint64_t, 3>> segs;
+    uint64_t arena = 0;
     const size_t row_cap = 1u << 24;
     if (d.mrows.ensure(row_cap, err) || d.keys.ensure(row_cap, err) ||
         d.keys2.ensure(row_cap, err) || d.vals.ensure(row_cap, err) ||
@@ -1282,21 +1301,12 @@ int Engine::run_bulge(const std::vector<Request> &reqs, std::vector<Result> &out
             uint64_t bytes = 0;
             CU(cudaMemcpyAsync(&bytes, d.offs.p + nr, 8, cudaMemcpyDeviceToHost, s));
             CU(cudaStreamSynchronize(s));
-            if (d.text.ensure(bytes + 1, err)) return err.code;
+            if (grow_keep(d.text, arena + bytes + 1, arena, s, err)) return err.code;
             mrow_write_kernel<<<fb, 256, 0, s>>>(d.view(), d.mrows.p, d.vals2.p, nr, dP, dR,
-                                                 d.offs.p, d.text.p);
+                                                 d.offs.p, d.text.p + arena);
             CU(cudaGetLastError());
-            times_.kernel_launches += 4;
-            if (bytes > d.h_text_cap) {
-                if (d.h_text) cudaFreeHost(d.h_text);
-                d.h_text = nullptr;
-                d.h_text_cap = 0;
-                CU(cudaMallocHost((void **)&d.h_text, bytes));
-                d.h_text_cap = bytes;
-            }
             CU(cudaEventRecord(d.ev[6], s));
-            CU(cudaMemcpyAsync(d.h_text, d.text.p, bytes, cudaMemcpyDeviceToHost, s));
-            CU(cudaEventRecord(d.ev[7], s));
+            times_.kernel_launches += 4;
             // request boundaries inside this chunk's sorted rows
             std::vector<uint64_t> bound(reqs.size() + 1, bytes);
             uint64_t r0 = 0;
@@ -1309,19 +1319,49 @@ int Engine::run_bulge(const std::vector<Request> &reqs, std::vector<Result> &out
             CU(cudaStreamSynchronize(s));
             cudaEventElapsedTime(&ms, d.ev[5], d.ev[6]);
             times_.format_ms += ms;
-            cudaEventElapsedTime(&ms, d.ev[6], d.ev[7]);
-            times_.d2h_ms += ms;
             for (size_t ri = 0; ri < reqs.size(); ++ri) {
-                texts[ri].append(d.h_text + bound[ri], d.h_text + bound[ri + 1]);
+                if (bound[ri + 1] > bound[ri])
+                    segs.push_back({arena + bound[ri], bound[ri + 1] - bound[ri], (uint64_t)ri});
                 nrows[ri] += rq[ri];
             }
+            arena += bytes;
         }
         c0 += cn;
     }
+    // one copy to the host: request-major (gathered on the device when rows
+    // of several requests interleave across chunks), into the pinned buffer
+    std::vector<uint64_t> req_off(reqs.size() + 1, 0);
+    for (const auto &sg : segs) req_off[sg[2] + 1] += sg[1];
+    for (size_t ri = 0; ri < reqs.size(); ++ri) req_off[ri + 1] += req_off[ri];
+    const char *src = d.text.p;
+    bool ordered = true;
+    for (size_t k = 1; k < segs.size(); ++k) ordered = ordered && segs[k][2] >= segs[k - 1][2];
+    if (!ordered) {
+        if (d.text2.ensure(arena + 1, err)) return err.code;
+        std::vector<uint64_t> at(req_off.begin(), req_off.end() - 1);
+        for (const auto &sg : segs) {
+            CU(cudaMemcpyAsync(d.text2.p + at[sg[2]], d.text.p + sg[0], sg[1],
+                               cudaMemcpyDeviceToDevice, s));
+            at[sg[2]] += sg[1];
+        }
+        src = d.text2.p;
+    }
+    if (arena > d.h_text_cap) {
+        if (d.h_text) cudaFreeHost(d.h_text);
+        d.h_text = nullptr;
+        d.h_text_cap = 0;
+        CU(cudaMallocHost((void **)&d.h_text, arena));
+        d.h_text_cap = arena;
+    }
+    CU(cudaEventRecord(d.ev[6], s));
+    if (arena) CU(cudaMemcpyAsync(d.h_text, src, arena, cudaMemcpyDeviceToHost, s));
+    CU(cudaEventRecord(d.ev[7], s));
+    CU(cudaStreamSynchronize(s));
+    cudaEventElapsedTime(&ms, d.ev[6], d.ev[7]);
+    times_.d2h_ms += ms;
     for (size_t ri = 0; ri < reqs.size(); ++ri) {
-        out[ri].owned = std::move(texts[ri]);
-        out[ri].text = out[ri].owned.data();
-        out[ri].text_len = out[ri].owned.size();
+        out[ri].text = d.h_text ? d.h_text + req_off[ri] : nullptr;
+        out[ri].text_len = req_off[ri + 1] - req_off[ri];
         out[ri].n_rows = nrows[ri];
     }
     return kOk;

@@ -78,10 +78,20 @@ namespace cof {
 int set_last_error(int code, const std::string &msg) { return fail(code, msg); }
 
 // Entry points of the request server (server.cpp) into a genome handle.
+// Results may point into the engine's pinned buffer, which the next search
+// on this genome overwrites, so they become owned before the lock is let go.
 int genome_search(cof_genome *g, const std::vector<Request> &reqs, std::vector<Result> &out,
                   Error &err) {
     std::lock_guard<std::mutex> lk(g->mu);
-    return g->engine.search(reqs, out, err);
+    const int rc = g->engine.search(reqs, out, err);
+    if (rc) return rc;
+    for (Result &r : out) {
+        if (r.text && r.text != r.owned.data()) {
+            r.owned.assign(r.text, r.text_len);
+            r.text = r.owned.data();
+        }
+    }
+    return rc;
 }
 uint64_t genome_nucl(const cof_genome *g) { return g->engine.host().n_nucl(); }
 int genome_free_device_bytes(cof_genome *g, uint64_t *free_bytes, Error &err) {

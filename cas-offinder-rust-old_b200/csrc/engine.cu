@@ -642,10 +642,7 @@ int Engine::search(const std::vector<Request> &reqs, std::vector<Result> &out, E
     if (!br.empty()) {
         std::vector<Result> bo;
         if (run_bulge(br, bo, err)) return err.code;
-        for (size_t k = 0; k < bi.size(); ++k) {
-            out[bi[k]] = std::move(bo[k]);
-            out[bi[k]].text = out[bi[k]].owned.data();
-        }
+        for (size_t k = 0; k < bi.size(); ++k) out[bi[k]] = std::move(bo[k]);  // views
     }
     CU(cudaEventRecord(d.ev[9], d.stream));
     CU(cudaEventSynchronize(d.ev[9]));

@@ -118,7 +118,7 @@ struct cof_server {
                 if (rc) {
                     d.err = err.msg;
                 } else {
-                    d.text.assign(res[i].text ? res[i].text : "", res[i].text_len);
+                    d.text = std::move(res[i].owned);  // owned by genome_search
                     d.n_rows = res[i].n_rows;
                     d.device_ms = res[i].device_ms;
                 }
