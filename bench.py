@@ -59,7 +59,12 @@ def parse():
     ap.add_argument("--serving-requests", type=int, default=64)
     ap.add_argument("--serving-rate", type=float, default=200.0, help="arrivals per second")
     ap.add_argument("--no-extras", action="store_true",
-                    help="skip the batched mixed-PAM and serving measurements")
+                    help="skip the batched mixed-PAM, serving and bulge measurements")
+    ap.add_argument("--only-bulge", action="store_true",
+                    help="run only the bulge-path measurement (10 Mbp x 20 guides, mm<=4, "
+                         "DNA/RNA bulges<=2) and print it")
+    ap.add_argument("--bulge-scale", type=float, default=0.02,
+                    help="bulge genome factor (1.0 = 500 Mbp; ~720 k rows per Mbp)")
     return ap.parse_args()
 
 
@@ -245,6 +250,44 @@ def bench_serving(cof, g, n_nt, n_req, rate, seed=7, max_guides=500, max_mm=4):
     return res
 
 
+def bench_bulge(cof, device, steps, scale):
+    """The bulge (Myers + DP traceback) path: a 500 Mbp-generator genome
+    scaled to `scale`, 20 guides of 20 nt + NRG, mm<=4, DNA and RNA bulges
+    <= 2.  value = Gbp*guides / device time (Myers filter + budget pre-test +
+    traceback + format); e2e = the same over the C-ABI call with the rows
+    copied into a host buffer."""
+    import synth
+    cfg = synth.config_bulge(seed=4, scale=scale)
+    g = cof.Genome(device=device)
+    cfg["genome"].load_into(g)
+    g.upload()
+    prep = g.prepare([dict(search_filter=cfg["filter"], patterns=cfg["patterns"],
+                           max_mismatches=cfg["max_mismatches"],
+                           max_dna_bulges=cfg["max_dna_bulges"],
+                           max_rna_bulges=cfg["max_rna_bulges"])])
+    g.run_prepared(prep, as_text=None)  # warm-up: buffers, pinned memory
+    dev, wall, stats = [], [], []
+    for _ in range(steps):
+        t0 = time.perf_counter()
+        (nbytes, rows), = g.run_prepared(prep, as_text=None)
+        wall.append(time.perf_counter() - t0)
+        st = g.last_stats()
+        stats.append(st)
+        dev.append(st["scan_ms"] + st["verify_ms"] + st["format_ms"])
+    g.close()
+    units = cfg["genome"].n_nucl * 1e-9 * len(cfg["patterns"])
+    d, w = statistics.median(dev), statistics.median(wall)
+    return {"workload": f"{cfg['genome'].n_nucl / 1e6:.0f} Mbp x 20 guides (20 nt + NRG), "
+                        f"mm<=4, DNA/RNA bulges<=2",
+            "value": units / (d * 1e-3), "unit": UNIT, "device_ms": d,
+            "e2e": {"value": units / w, "unit": UNIT, "ms_per_step": w * 1e3,
+                    "d2h_bytes_per_step": nbytes},
+            "stages_ms": {k: statistics.median(s[k] for s in stats)
+                          for k in ("scan_ms", "verify_ms", "format_ms", "d2h_ms", "total_ms")},
+            "rows_per_step": rows, "candidates_per_step": stats[-1]["candidates"],
+            "gpu_launches_per_step": stats[-1]["kernel_launches"], "steps": steps}
+
+
 class CpuSample:
     """The reference CPU path (C restatement, oracle/) over a leading slice of
     the workload's genome: all host threads, CPU batch size (64 chunks).  The
@@ -387,6 +430,13 @@ def main():
     if dist:
         dist.barrier()
     import cof
+    if args.only_bulge:
+        if rank == 0:
+            print(json.dumps({"bulge": bench_bulge(cof, local, max(1, args.steps),
+                                                   args.bulge_scale)}), flush=True)
+        if dist:
+            dist.destroy_process_group()
+        return
 
     t0 = time.perf_counter()
     cfg = make_workload(args, rank)
@@ -480,6 +530,7 @@ def main():
         line["serving"] = bench_serving(cof, g, n_nt, args.serving_requests, args.serving_rate)
         line["serving_small_requests"] = bench_serving(cof, g, n_nt, 4 * args.serving_requests,
                                                        2000.0, seed=8, max_guides=4, max_mm=3)
+        line["bulge"] = bench_bulge(cof, local, 3, args.bulge_scale)
     if not args.no_cpu_baseline and world == 1:
         base, _ = cpu_baseline(cfg, args.cpu_sample_s)
         line["cpu_baseline"] = base

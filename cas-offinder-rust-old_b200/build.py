@@ -23,7 +23,8 @@ COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC,-fvisibility=hi
 HEADERS = [os.path.join(CSRC, "cof_engine.h"), os.path.join(CSRC, "engine_dev.cuh"),
            os.path.join(ROOT, "include", "cof.h")]
 
-SOURCES = ["engine.cu", "bulge.cu", "raw.cu", "loader.cpp", "cabi.cpp", "server.cpp", "noalloc.cu"]
+SOURCES = ["engine.cu", "bulge.cu", "raw.cu", "loader.cpp", "cabi.cpp", "server.cpp", "noalloc.cu",
+           "hostpool.cpp"]
 
 
 def _stale(out, deps):

@@ -1021,7 +1021,8 @@ int Engine::run_bulge(const std::vector<Request> &reqs, std::vector<Result> &out
     const HostGenome &h = host_;
     const Bit4Tables &t = bit4();
     cudaStream_t s = d.stream;
-    out.assign(reqs.size(), Result());
+    out.clear();
+    out.resize(reqs.size());
 
     const auto hb = make_batches(h.n_chunks(), reqs[0].cps);
     std::vector<BatchDev> batches;
@@ -1328,42 +1329,32 @@ int Engine::run_bulge(const std::vector<Request> &reqs, std::vector<Result> &out
         }
         c0 += cn;
     }
-    // one copy to the host: request-major (gathered on the device when rows
-    // of several requests interleave across chunks), into the pinned buffer
-    std::vector<uint64_t> req_off(reqs.size() + 1, 0);
-    for (const auto &sg : segs) req_off[sg[2] + 1] += sg[1];
-    for (size_t ri = 0; ri < reqs.size(); ++ri) req_off[ri + 1] += req_off[ri];
-    const char *src = d.text.p;
-    bool ordered = true;
-    for (size_t k = 1; k < segs.size(); ++k) ordered = ordered && segs[k][2] >= segs[k - 1][2];
-    if (!ordered) {
-        if (d.text2.ensure(arena + 1, err)) return err.code;
-        std::vector<uint64_t> at(req_off.begin(), req_off.end() - 1);
-        for (const auto &sg : segs) {
-            CU(cudaMemcpyAsync(d.text2.p + at[sg[2]], d.text.p + sg[0], sg[1],
-                               cudaMemcpyDeviceToDevice, s));
-            at[sg[2]] += sg[1];
+    // each request's rows go from the arena straight into its own
+    // page-locked result buffer, segment by segment in chunk order
+    std::vector<uint64_t> req_len(reqs.size(), 0), at(reqs.size(), 0);
+    for (const auto &sg : segs) req_len[sg[2]] += sg[1];
+    for (size_t ri = 0; ri < reqs.size(); ++ri) {
+        char *buf = PinnedPool::get().acquire(req_len[ri] + 1);
+        if (!buf) {
+            err = {kOom, "out of page-locked host memory for result text"};
+            return err.code;
         }
-        src = d.text2.p;
-    }
-    if (arena > d.h_text_cap) {
-        if (d.h_text) cudaFreeHost(d.h_text);
-        d.h_text = nullptr;
-        d.h_text_cap = 0;
-        CU(cudaMallocHost((void **)&d.h_text, arena));
-        d.h_text_cap = arena;
+        out[ri].pooled.p = buf;
+        out[ri].text = buf;
+        out[ri].text_len = req_len[ri];
+        out[ri].n_rows = nrows[ri];
     }
     CU(cudaEventRecord(d.ev[6], s));
-    if (arena) CU(cudaMemcpyAsync(d.h_text, src, arena, cudaMemcpyDeviceToHost, s));
+    for (const auto &sg : segs) {
+        CU(cudaMemcpyAsync(out[sg[2]].pooled.p + at[sg[2]], d.text.p + sg[0], sg[1],
+                           cudaMemcpyDeviceToHost, s));
+        at[sg[2]] += sg[1];
+    }
     CU(cudaEventRecord(d.ev[7], s));
     CU(cudaStreamSynchronize(s));
     cudaEventElapsedTime(&ms, d.ev[6], d.ev[7]);
     times_.d2h_ms += ms;
-    for (size_t ri = 0; ri < reqs.size(); ++ri) {
-        out[ri].text = d.h_text ? d.h_text + req_off[ri] : nullptr;
-        out[ri].text_len = req_off[ri + 1] - req_off[ri];
-        out[ri].n_rows = nrows[ri];
-    }
+    for (Result &r : out) r.pooled.p[r.text_len] = 0;
     return kOk;
 }
 

@@ -60,11 +60,18 @@ void parallel_copy(char *dst, const char *src, size_t n) {
     for (auto &x : th) x.join();
 }
 
-int fill_result(const cof::Result &r, cof_result *out) {
-    out->text = (char *)std::malloc(r.text_len + 1);
-    if (!out->text) return fail(COF_E_OOM, "out of host memory for result text");
-    if (r.text_len) parallel_copy(out->text, r.text, r.text_len);
-    out->text[r.text_len] = 0;
+// Hands a result to the caller: a page-locked pool buffer changes owner as
+// it is (cof_result_free returns it to the pool); anything else is copied
+// into malloc'd memory.
+int fill_result(cof::Result &r, cof_result *out) {
+    if (r.pooled.p && r.text == r.pooled.p) {
+        out->text = r.pooled.take();
+    } else {
+        out->text = (char *)std::malloc(r.text_len + 1);
+        if (!out->text) return fail(COF_E_OOM, "out of host memory for result text");
+        if (r.text_len) parallel_copy(out->text, r.text, r.text_len);
+        out->text[r.text_len] = 0;
+    }
     out->text_len = r.text_len;
     out->n_rows = r.n_rows;
     out->device_ms = r.device_ms;
@@ -78,15 +85,16 @@ namespace cof {
 int set_last_error(int code, const std::string &msg) { return fail(code, msg); }
 
 // Entry points of the request server (server.cpp) into a genome handle.
-// Results may point into the engine's pinned buffer, which the next search
-// on this genome overwrites, so they become owned before the lock is let go.
+// A result that is neither pooled nor owned points into an engine buffer
+// that the next search on this genome overwrites, so it becomes owned
+// before the lock is let go.
 int genome_search(cof_genome *g, const std::vector<Request> &reqs, std::vector<Result> &out,
                   Error &err) {
     std::lock_guard<std::mutex> lk(g->mu);
     const int rc = g->engine.search(reqs, out, err);
     if (rc) return rc;
     for (Result &r : out) {
-        if (r.text && r.text != r.owned.data()) {
+        if (r.text && r.text != r.owned.data() && r.text != r.pooled.p) {
             r.owned.assign(r.text, r.text_len);
             r.text = r.owned.data();
         }
@@ -187,7 +195,7 @@ COF_API int cof_search(cof_genome *g, const cof_request *req, cof_result *out) {
 
 COF_API void cof_result_free(cof_result *r) {
     if (!r) return;
-    std::free(r->text);
+    if (!cof::PinnedPool::get().release(r->text)) std::free(r->text);
     r->text = nullptr;
     r->text_len = 0;
     r->n_rows = 0;

@@ -7,7 +7,9 @@
 #include <cstddef>
 #include <cstdint>
 #include <map>
+#include <mutex>
 #include <string>
+#include <unordered_map>
 #include <vector>
 
 namespace cof {
@@ -80,14 +82,63 @@ int make_request(const char *filter, size_t pattern_len, const char *const *patt
                  size_t n_patterns, uint32_t mm, uint32_t db, uint32_t rb, uint32_t flags,
                  uint32_t cps, Request &out, Error &err);
 
-// Rows of one request: a view into the engine's pinned host buffer, valid
-// until the next search on the same engine.
+// Page-locked host buffers for result text.  The device copies each
+// request's rows straight into one of them, and that buffer becomes the
+// caller's cof_result.text; cof_result_free hands it back.  Freed buffers
+// are kept (up to kKeepBytes) and reused, so a steady stream of searches
+// neither pins nor first-touches new host pages.
+class PinnedPool {
+  public:
+    static constexpr size_t kKeepBytes = size_t(4) << 30;
+    static PinnedPool &get();
+    char *acquire(size_t bytes);  // nullptr when page-locked memory runs out
+    bool release(char *p);        // false when p did not come from the pool
+
+  private:
+    std::mutex mu_;
+    std::unordered_map<char *, size_t> live_;
+    std::multimap<size_t, char *> free_;
+    size_t free_bytes_ = 0;
+};
+
+// A pool buffer owned by one result (move-only; returned to the pool when
+// dropped unless taken).
+struct PooledText {
+    char *p = nullptr;
+    PooledText() = default;
+    PooledText(const PooledText &) = delete;
+    PooledText &operator=(const PooledText &) = delete;
+    PooledText(PooledText &&o) noexcept : p(o.p) { o.p = nullptr; }
+    PooledText &operator=(PooledText &&o) noexcept {
+        if (this != &o) {
+            reset();
+            p = o.p;
+            o.p = nullptr;
+        }
+        return *this;
+    }
+    ~PooledText() { reset(); }
+    void reset() {
+        if (p) PinnedPool::get().release(p);
+        p = nullptr;
+    }
+    char *take() {
+        char *q = p;
+        p = nullptr;
+        return q;
+    }
+};
+
+// Rows of one request.  `text` points into `pooled` (NUL-terminated, the
+// usual case), into `owned`, or -- for the views the engine hands between
+// its own stages -- into an engine buffer valid until its next search.
 struct Result {
     const char *text = nullptr;
     size_t text_len = 0;
     uint64_t n_rows = 0;
     double device_ms = 0;
-    std::string owned;  // backing store when `text` does not point into the engine
+    std::string owned;
+    PooledText pooled;
 };
 
 // Per-stage device timings of the last search (milliseconds, CUDA events).

@@ -598,7 +598,8 @@ int Engine::free_device_bytes(uint64_t *free_bytes, Error &err) {
 
 int Engine::search(const std::vector<Request> &reqs, std::vector<Result> &out, Error &err) {
     times_ = StageTimes();
-    out.assign(reqs.size(), Result());
+    out.clear();
+    out.resize(reqs.size());
     if (reqs.empty()) return kOk;
     for (const Request &r : reqs) {
         if (r.cps != reqs[0].cps) {
@@ -631,13 +632,7 @@ int Engine::search(const std::vector<Request> &reqs, std::vector<Result> &out, E
     if (!pr.empty()) {
         std::vector<Result> po;
         if (run_popcount(pr, po, err)) return err.code;
-        for (size_t k = 0; k < pi.size(); ++k) {
-            out[pi[k]] = po[k];
-            if (!br.empty()) {  // the bulge path reuses the pinned text buffer
-                out[pi[k]].owned.assign(po[k].text ? po[k].text : "", po[k].text_len);
-                out[pi[k]].text = out[pi[k]].owned.data();
-            }
-        }
+        for (size_t k = 0; k < pi.size(); ++k) out[pi[k]] = std::move(po[k]);
     }
     if (!br.empty()) {
         std::vector<Result> bo;
@@ -654,7 +649,8 @@ int Engine::search(const std::vector<Request> &reqs, std::vector<Result> &out, E
 }
 
 int Engine::run_popcount(const std::vector<Request> &reqs, std::vector<Result> &out, Error &err) {
-    out.assign(reqs.size(), Result());
+    out.clear();
+    out.resize(reqs.size());
     DeviceGenome &d = *dev_;
     const HostGenome &h = host_;
     const Bit4Tables &t = bit4();
@@ -1015,30 +1011,30 @@ int Engine::run_popcount(const std::vector<Request> &reqs, std::vector<Result> &
         CU(cudaGetLastError());
         times_.kernel_launches += 4;
     }
+    // each request's rows (sorted request-major) go straight from the
+    // device into its own page-locked result buffer
     CU(cudaEventRecord(d.ev[4], s));
-    if (text_bytes > d.h_text_cap) {
-        if (d.h_text) cudaFreeHost(d.h_text);
-        d.h_text = nullptr;
-        d.h_text_cap = 0;
-        CU(cudaMallocHost((void **)&d.h_text, text_bytes));
-        d.h_text_cap = text_bytes;
-    }
-    if (text_bytes) CU(cudaMemcpyAsync(d.h_text, d.text.p, text_bytes, cudaMemcpyDeviceToHost, s));
-    CU(cudaEventRecord(d.ev[5], s));
-    CU(cudaStreamSynchronize(s));
-
-    // split the text per request (rows are sorted request-major)
     uint64_t r0 = 0, t0 = 0;
     for (size_t ri = 0; ri < reqs.size(); ++ri) {
         const uint64_t r1 = r0 + req_rows[ri];
         uint64_t t1 = text_bytes;
         if (r1 < n_rows) CU(cudaMemcpy(&t1, d.offs.p + r1, 8, cudaMemcpyDeviceToHost));
+        char *buf = PinnedPool::get().acquire(t1 - t0 + 1);
+        if (!buf) {
+            err = {kOom, "out of page-locked host memory for result text"};
+            return err.code;
+        }
+        out[ri].pooled.p = buf;
+        if (t1 > t0) CU(cudaMemcpyAsync(buf, d.text.p + t0, t1 - t0, cudaMemcpyDeviceToHost, s));
         out[ri].n_rows = req_rows[ri];
-        out[ri].text = d.h_text ? d.h_text + t0 : nullptr;
+        out[ri].text = buf;
         out[ri].text_len = t1 - t0;
         r0 = r1;
         t0 = t1;
     }
+    CU(cudaEventRecord(d.ev[5], s));
+    CU(cudaStreamSynchronize(s));
+    for (Result &r : out) r.pooled.p[r.text_len] = 0;
     float ms;
     cudaEventElapsedTime(&ms, d.ev[1], d.ev[2]);
     times_.scan_ms = ms;

@@ -1,0 +1,63 @@
+// hostpool.cpp -- the page-locked result-buffer pool (PinnedPool in
+// cof_engine.h).  Buffers are portable pinned allocations, usable from every
+// device's stream, rounded up to 2 MiB so that nearby sizes reuse each other.
+#include <cuda_runtime.h>
+
+#include "cof_engine.h"
+
+namespace cof {
+
+PinnedPool &PinnedPool::get() {
+    static PinnedPool pool;  // process lifetime; buffers are released at exit
+    return pool;
+}
+
+char *PinnedPool::acquire(size_t bytes) {
+    const size_t want = ((bytes + 1) + (size_t(2) << 20) - 1) & ~((size_t(2) << 20) - 1);
+    std::lock_guard<std::mutex> lk(mu_);
+    // best fit among the kept buffers, at most twice the size asked for
+    auto it = free_.lower_bound(want);
+    if (it != free_.end() && it->first <= 2 * want) {
+        char *p = it->second;
+        const size_t n = it->first;
+        free_.erase(it);
+        free_bytes_ -= n;
+        live_[p] = n;
+        return p;
+    }
+    char *p = nullptr;
+    if (cudaHostAlloc((void **)&p, want, cudaHostAllocPortable) != cudaSuccess) {
+        cudaGetLastError();  // clear the recorded error of the failed call
+        // drop what is kept and try once more
+        for (auto &kv : free_) cudaFreeHost(kv.second);
+        free_.clear();
+        free_bytes_ = 0;
+        if (cudaHostAlloc((void **)&p, want, cudaHostAllocPortable) != cudaSuccess) {
+            cudaGetLastError();
+            return nullptr;
+        }
+    }
+    live_[p] = want;
+    return p;
+}
+
+bool PinnedPool::release(char *p) {
+    if (!p) return false;
+    std::lock_guard<std::mutex> lk(mu_);
+    auto it = live_.find(p);
+    if (it == live_.end()) return false;
+    const size_t n = it->second;
+    live_.erase(it);
+    free_.emplace(n, p);
+    free_bytes_ += n;
+    while (free_bytes_ > kKeepBytes && !free_.empty()) {  // keep the newest sizes
+        auto victim = free_.begin();
+        if (victim->second == p && free_.size() > 1) ++victim;
+        free_bytes_ -= victim->first;
+        cudaFreeHost(victim->second);
+        free_.erase(victim);
+    }
+    return true;
+}
+
+}  // namespace cof

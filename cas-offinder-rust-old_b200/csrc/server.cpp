@@ -50,7 +50,9 @@ struct Pending {
 struct Done {
     int status = COF_OK;
     std::string err;
-    std::string text;
+    cof::PooledText pooled;  // the rows, when the engine delivered them pooled
+    std::string text;        // the rows otherwise
+    size_t text_len = 0;
     uint64_t n_rows = 0;
     double device_ms = 0;
     double latency_ms = 0;
@@ -118,7 +120,11 @@ struct cof_server {
                 if (rc) {
                     d.err = err.msg;
                 } else {
-                    d.text = std::move(res[i].owned);  // owned by genome_search
+                    if (res[i].pooled.p && res[i].text == res[i].pooled.p)
+                        d.pooled = std::move(res[i].pooled);
+                    else
+                        d.text.assign(res[i].text ? res[i].text : "", res[i].text_len);
+                    d.text_len = res[i].text_len;
                     d.n_rows = res[i].n_rows;
                     d.device_ms = res[i].device_ms;
                 }
@@ -198,11 +204,15 @@ COF_API int cof_server_wait(cof_server *s, uint64_t ticket, int64_t timeout_ms, 
     lk.unlock();
     if (latency_ms) *latency_ms = d.latency_ms;
     if (d.status) return cof::set_last_error(d.status, d.err);
-    out->text = (char *)std::malloc(d.text.size() + 1);
-    if (!out->text) return cof::set_last_error(COF_E_OOM, "out of host memory");
-    std::memcpy(out->text, d.text.data(), d.text.size());
-    out->text[d.text.size()] = 0;
-    out->text_len = d.text.size();
+    if (d.pooled.p) {  // handed over as it is; cof_result_free returns it
+        out->text = d.pooled.take();
+    } else {
+        out->text = (char *)std::malloc(d.text.size() + 1);
+        if (!out->text) return cof::set_last_error(COF_E_OOM, "out of host memory");
+        std::memcpy(out->text, d.text.data(), d.text.size());
+        out->text[d.text.size()] = 0;
+    }
+    out->text_len = d.text_len;
     out->n_rows = d.n_rows;
     out->device_ms = d.device_ms;
     return COF_OK;
