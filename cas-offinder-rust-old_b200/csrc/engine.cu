@@ -176,10 +176,29 @@ struct ScanParams {
 // group, CPT windows per lane.  Per care class the windows are masked once;
 // per pattern the lane keeps the minimum mismatch count over its windows and
 // only a pattern whose minimum passes takes the (rare) emitting branch.
-template <int kCpt>
-__device__ __noinline__ void flush_queue(const uint4 *q, int n, const FastPattern *pt,
-                                            const ScanGroup &G, uint32_t batch,
-                                            const ScanParams &P, int lane) {
+// One pattern from shared memory (ld.shared.v4: the caller knows the
+// table is staged there; a generic load would have to resolve the window).
+__device__ __forceinline__ FastPattern lds_pattern(uint32_t saddr) {
+    FastPattern f;
+    uint32_t k;
+    asm("ld.shared.v4.u32 {%0, %1, %2, %3}, [%4];"
+        : "=r"(f.h), "=r"(f.l), "=r"(f.care), "=r"(k)
+        : "r"(saddr));
+    f.k = (int32_t)k;
+    return f;
+}
+
+// Compares the queued windows (32 * kCpt at most, kCpt per lane) with every
+// pattern of the group and appends the hits.  kSmem: the pattern table is in
+// shared memory (all but the largest groups).
+template <int kCpt, int kPair, bool kSmem>
+__device__ __forceinline__ void flush_body(const uint4 *q, int n, const FastPattern *pt,
+                                           const ScanGroup &G, uint32_t batch,
+                                           const ScanParams &P, int lane) {
+    const uint32_t pt_s = kSmem ? (uint32_t)__cvta_generic_to_shared(pt) : 0u;
+    auto load = [&](uint32_t p) -> FastPattern {
+        return kSmem ? lds_pattern(pt_s + p * (uint32_t)sizeof(FastPattern)) : pt[p];
+    };
     for (uint32_t c = 0; c < G.n_class; ++c) {
         const CareClass K = G.cls[c];
         uint32_t mh[kCpt], ml[kCpt], ms[kCpt];
@@ -191,25 +210,57 @@ __device__ __noinline__ void flush_queue(const uint4 *q, int n, const FastPatter
             ml[j] = e.z & K.care;
             ms[j] = e.w & K.care;
         }
-        for (uint32_t p = K.pat_begin; p < K.pat_end; ++p) {
-            const FastPattern fp = pt[p];
-            int mn = 64;
+        auto emit = [&](uint32_t p, const FastPattern &fp) {
 #pragma unroll
-            for (int j = 0; j < kCpt; ++j)
-                mn = min(mn, (int)__popc((mh[j] ^ fp.h) | (ml[j] ^ fp.l) | ms[j]));
-            if (mn <= fp.k) {
-#pragma unroll
-                for (int j = 0; j < kCpt; ++j) {
-                    const int idx = lane + 32 * j;
-                    if (idx < n && (int)__popc((mh[j] ^ fp.h) | (ml[j] ^ fp.l) | ms[j]) <= fp.k) {
-                        const uint32_t i = atomicAdd(&P.ctr->hits, 1u);
-                        if (i < P.hit_cap) P.hits[i] = Hit{q[idx].x, G.pat_begin + p, batch, 0};
-                        else P.ctr->overflow = 1;
-                    }
+            for (int j = 0; j < kCpt; ++j) {
+                const int idx = lane + 32 * j;
+                if (idx < n && (int)__popc((mh[j] ^ fp.h) | (ml[j] ^ fp.l) | ms[j]) <= fp.k) {
+                    const uint32_t i = atomicAdd(&P.ctr->hits, 1u);
+                    if (i < P.hit_cap) P.hits[i] = Hit{q[idx].x, G.pat_begin + p, batch, 0};
+                    else P.ctr->overflow = 1;
                 }
             }
+        };
+        uint32_t p = K.pat_begin;
+        if (kPair == 2) {  // two independent min chains per iteration
+            for (; p + 1 < K.pat_end; p += 2) {
+                const FastPattern f0 = load(p), f1 = load(p + 1);
+                int m0 = 64, m1 = 64;
+#pragma unroll
+                for (int j = 0; j < kCpt; ++j) {
+                    m0 = min(m0, (int)__popc((mh[j] ^ f0.h) | (ml[j] ^ f0.l) | ms[j]));
+                    m1 = min(m1, (int)__popc((mh[j] ^ f1.h) | (ml[j] ^ f1.l) | ms[j]));
+                }
+                if (m0 <= f0.k) emit(p, f0);
+                if (m1 <= f1.k) emit(p + 1, f1);
+            }
+        }
+        for (; p < K.pat_end; ++p) {
+            const FastPattern f0 = load(p);
+            int m0 = 64;
+#pragma unroll
+            for (int j = 0; j < kCpt; ++j)
+                m0 = min(m0, (int)__popc((mh[j] ^ f0.h) | (ml[j] ^ f0.l) | ms[j]));
+            if (m0 <= f0.k) emit(p, f0);
         }
     }
+}
+
+// One call target for both table locations keeps the caller's register
+// use around the (rare) call as low as with a single variant.
+template <int kCpt, int kPair>
+__device__ __noinline__ void flush_queue(const uint4 *q, int n, const FastPattern *pt,
+                                            bool smem, const ScanGroup &G, uint32_t batch,
+                                            const ScanParams &P, int lane) {
+    if (smem) flush_body<kCpt, kPair, true>(q, n, pt, G, batch, P, lane);
+    else flush_body<kCpt, kPair, false>(q, n, pt, G, batch, P, lane);
+}
+
+template <int kCpt, int kPair>
+__device__ __forceinline__ void flush(const uint4 *q, int n, const FastPattern *pt,
+                                      const FastPattern *spat, const ScanGroup &G,
+                                      uint32_t batch, const ScanParams &P, int lane) {
+    flush_queue<kCpt, kPair>(q, n, pt, pt == spat, G, batch, P, lane);
 }
 
 // Persistent scan: CTAs pull work items -- a span of kSpanTiles tiles of one
@@ -217,7 +268,7 @@ __device__ __noinline__ void flush_queue(const uint4 *q, int n, const FastPatter
 // (few or many patterns, sparse or dense PAMs) share the GPU evenly.  A CTA
 // stages a group's patterns in shared memory when it switches groups; each
 // warp takes every kScanWarps-th tile of the span.
-template <int kCpt, int kScanWarps, int kMinBlocks>
+template <int kCpt, int kScanWarps, int kMinBlocks, int kPair>
 __global__ void __launch_bounds__(kScanWarps * 32, kMinBlocks)
 scan_kernel(ScanParams P) {
     constexpr int kQCap = 32 * kCpt;     // flush threshold per warp queue
@@ -261,7 +312,7 @@ scan_kernel(ScanParams P) {
         if (g != cur_g) {
             if (qn) {  // the queue belongs to the previous group's patterns
                 __syncwarp();
-                flush_queue<kCpt>(q, qn, pt, sg, qbatch, P, lane);
+                flush<kCpt, kPair>(q, qn, pt, spat, sg, qbatch, P, lane);
                 __syncwarp();
                 qn = 0;
             }
@@ -291,7 +342,7 @@ scan_kernel(ScanParams P) {
             if (sgm.batch != qbatch) {
                 if (qn) {
                     __syncwarp();
-                    flush_queue<kCpt>(q, qn, pt, sg, qbatch, P, lane);
+                    flush<kCpt, kPair>(q, qn, pt, spat, sg, qbatch, P, lane);
                     __syncwarp();
                     qn = 0;
                 }
@@ -334,7 +385,7 @@ scan_kernel(ScanParams P) {
                     // full pass over kQCap windows; the (< 32) windows beyond it
                     // move to the front of the queue
                     __syncwarp();
-                    flush_queue<kCpt>(q, kQCap, pt, sg, qbatch, P, lane);
+                    flush<kCpt, kPair>(q, kQCap, pt, spat, sg, qbatch, P, lane);
                     const int rest = qn - kQCap;
                     uint4 e = make_uint4(0, 0, 0, 0);
                     if (lane < rest) e = q[kQCap + lane];
@@ -349,7 +400,7 @@ scan_kernel(ScanParams P) {
     }
     if (qn) {
         __syncwarp();
-        flush_queue<kCpt>(q, qn, pt, sg, qbatch, P, lane);
+        flush<kCpt, kPair>(q, qn, pt, spat, sg, qbatch, P, lane);
     }
     // candidate and pair counts (the roofline's algorithmic work)
     for (int o = 16; o; o >>= 1) {
@@ -363,7 +414,7 @@ scan_kernel(ScanParams P) {
 }
 
 struct ScanVariant {
-    int cpt, warps, min_blocks;
+    int cpt, warps, min_blocks, pair;
     uint32_t span_tiles;
     void (*kernel)(ScanParams);
     size_t smem() const {
@@ -371,15 +422,19 @@ struct ScanVariant {
     }
 };
 
-template <int C, int W, int B>
+template <int C, int W, int B, int Q = 1>
 constexpr ScanVariant variant(uint32_t span) {
-    return ScanVariant{C, W, B, span, scan_kernel<C, W, B>};
+    return ScanVariant{C, W, B, Q, span, scan_kernel<C, W, B, Q>};
 }
 
-// Candidate tile shapes; the autotuner times them on a sample of the genome.
+// Candidate tile shapes (windows per lane x warps x min blocks per SM, and
+// patterns per comparison step); the autotuner times them on a sample of the
+// genome.  Two patterns per step need registers that only the shapes with
+// fewer blocks per SM have.
 const ScanVariant kScanVariants[] = {
-    variant<8, 8, 3>(64),  variant<4, 8, 4>(64),  variant<16, 8, 2>(64),
-    variant<8, 4, 6>(32),  variant<16, 4, 4>(32), variant<4, 16, 2>(128),
+    variant<8, 8, 3>(64),     variant<4, 8, 4>(64),     variant<16, 8, 2>(64),
+    variant<8, 4, 6>(32),     variant<16, 4, 4>(32),    variant<4, 16, 2>(128),
+    variant<8, 8, 2, 2>(64),  variant<16, 8, 2, 2>(64), variant<8, 4, 4, 2>(32),
 };
 constexpr int kNumScanVariants = sizeof(kScanVariants) / sizeof(kScanVariants[0]);
 
@@ -929,7 +984,7 @@ int Engine::run_popcount(const std::vector<Request> &reqs, std::vector<Result> &
         }
         const ScanVariant &v = kScanVariants[vi];
         times_.scan_variant = vi;
-        times_.scan_shape = "cpt" + std::to_string(v.cpt) + "-warps" + std::to_string(v.warps) +
+        times_.scan_shape = std::string(v.pair == 2 ? "pp2-" : "") + "cpt" + std::to_string(v.cpt) + "-warps" + std::to_string(v.warps) +
                             "-minb" + std::to_string(v.min_blocks) + "-span" +
                             std::to_string(v.span_tiles);
         for (int attempt = 0; attempt < 2; ++attempt) {

@@ -127,7 +127,7 @@ def test_cli_matches_oracle_cli(cof_mod, oracle_mod, golden, tmp_path):
         assert "=== Cas-OFFinder Rust ===" in log and "Matches found: 117" in log
 
 
-@pytest.mark.parametrize("variant", range(6))
+@pytest.mark.parametrize("variant", range(9))
 def test_every_scan_tile_shape(cof_mod, oracle_mod, golden, variant, monkeypatch):
     # the autotuner may pick any tile shape; all must give the same rows
     monkeypatch.setenv("COF_SCAN_VARIANT", str(variant))
@@ -147,7 +147,7 @@ def test_autotuner_records_choice(cof_mod, golden, monkeypatch):
     g = cof_mod.Genome(os.path.join(golden, "upstream1000.fa"))
     g.search("N" * 24, KAT_PATS, 11)
     t = g.tuning()
-    assert t["last"].startswith("cpt") and 0 <= t["variant"] < 6
+    assert "cpt" in t["last"] and 0 <= t["variant"] < 9
 
 
 @pytest.mark.parametrize("seed", range(8))
