@@ -138,14 +138,33 @@ def hbm_peak():
         return 6650.0, "fallback"
 
 
+def rank_patterns(patterns, rank):
+    """Weak scaling: rank 0 searches the workload's own guides; every other
+    rank brings its own seeded guide set of the same size and shape
+    (20 nt + NNN)."""
+    if rank == 0:
+        return list(patterns)
+    import numpy as np
+    import synth
+    rng = np.random.default_rng(1000 + rank)
+    return [synth.random_guide(rng, 20) + "NNN" for _ in range(len(patterns))]
+
+
+def max_over_ranks(dist, values, device):
+    """Per-rank measurements reduced to the slowest rank's (MAX all-reduce):
+    the job is done when the last rank is."""
+    if dist is None:
+        return [float(v) for v in values]
+    import torch
+    t = torch.tensor([float(v) for v in values], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return t.tolist()
+
+
 def make_workload(args, rank):
     import synth
     cfg = synth.config_full_genome(seed=2, scale=args.scale, n_guides=args.guides)
-    if rank:
-        # weak scaling: every rank brings its own guide set
-        import numpy as np
-        rng = np.random.default_rng(1000 + rank)
-        cfg["patterns"] = [synth.random_guide(rng, 20) + "NNN" for _ in range(args.guides)]
+    cfg["patterns"] = rank_patterns(cfg["patterns"], rank)
     return cfg
 
 
@@ -480,10 +499,7 @@ def main():
     dev_ms = sum(s["scan_ms"] + s["verify_ms"] + s["format_ms"] for s in stats)
     scan_ms = sum(s["scan_ms"] for s in stats) / len(stats)
     e2e_s = sum(wall)
-    if dist:
-        t = torch.tensor([dev_ms, e2e_s], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        dev_ms, e2e_s = t.tolist()
+    dev_ms, e2e_s = max_over_ranks(dist, [dev_ms, e2e_s], "cuda")
     gbp_guides = n_nt * 1e-9 * len(cfg["patterns"])
     value = world * gbp_guides * args.steps / (dev_ms * 1e-3)
     e2e = world * gbp_guides * args.steps / e2e_s
