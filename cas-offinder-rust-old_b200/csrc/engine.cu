@@ -59,15 +59,18 @@ constexpr int kMaxPamCells = 32;
 constexpr int kMaxCareClasses = 8;
 
 // Patterns of a group that compare the same window cells (single-base cells
-// of the pattern): windows are masked once per class.  Pattern indices are
-// relative to the group.
+// of the pattern) from the same place in the window: windows are masked
+// once per class.  Pattern indices are relative to the group; `off` is where
+// the patterns' first cell sits in the 32-cell window (32 - L for groups
+// anchored at the PAM's end, 0 for groups anchored at the window start).
 struct CareClass {
-    uint32_t care, pat_begin, pat_end, pad;
+    uint32_t care, pat_begin, pat_end, off;
 };
 
-// One strand of one request: the windows whose non-N filter cells all hold
-// a single base of the filter's set are scanned against the patterns
-// [pat_begin, pat_end).
+// One strand of every request whose filter has the same non-N cells at the
+// same place relative to its anchor (the PAM: e.g. every NRG request, of any
+// guide length): the windows whose non-N filter cells all hold a single base
+// of the filter's set are scanned against the patterns [pat_begin, pat_end).
 struct ScanGroup {
     uint32_t n_pam;
     uint32_t pat_begin, pat_end;
@@ -78,10 +81,12 @@ struct ScanGroup {
     CareClass cls[kMaxCareClasses];
 };
 
-// A contiguous range of window starts inside one batch.
+// A contiguous range of window starts inside one batch.  Window starts are
+// global nucleotide indices + 32 (the planes begin with one padding word),
+// so that windows anchored at a PAM near position 0 can start before it.
 struct ScanSeg {
-    uint64_t lo, hi;        // global nucleotide range [lo, hi) of starts
-    uint64_t base;          // batch base
+    uint64_t lo, hi;        // range [lo, hi) of shifted window starts
+    uint64_t base;          // batch base + 32: window start - base = start in the batch
     uint64_t w0;            // first plane word (lo / 32)
     uint64_t tile_begin;    // prefix count of 1024-start tiles
     uint32_t batch;
@@ -216,7 +221,7 @@ __device__ __forceinline__ void flush_body(const uint4 *q, int n, const FastPatt
                 const int idx = lane + 32 * j;
                 if (idx < n && (int)__popc((mh[j] ^ fp.h) | (ml[j] ^ fp.l) | ms[j]) <= fp.k) {
                     const uint32_t i = atomicAdd(&P.ctr->hits, 1u);
-                    if (i < P.hit_cap) P.hits[i] = Hit{q[idx].x, G.pat_begin + p, batch, 0};
+                    if (i < P.hit_cap) P.hits[i] = Hit{q[idx].x + K.off, G.pat_begin + p, batch, 0};
                     else P.ctr->overflow = 1;
                 }
             }
@@ -457,6 +462,11 @@ __global__ void verify_kernel(GenomeDev G, const BatchDev *__restrict__ batches,
         const ExactPattern &P = pats[pe];
         const RequestDev &R = reqs[P.request];
         const uint32_t L = P.L;
+        // a scan group's windows cover the starts of all its pattern lengths:
+        // keep this length's own range (legacy_match_start_min_nucl,
+        // search.rs:540-546, up to the batch's valid cells)
+        const uint32_t msmin = B.active_start > L - 1 ? B.active_start - (L - 1) : 0;
+        if (h.s_local < msmin || h.s_local >= B.valid) continue;
         const uint64_t sg = B.base + h.s_local;
         // search_chunk_cpu count on the N-masked batch buffer (zero past the
         // batch's valid bytes)
@@ -601,13 +611,19 @@ int Engine::upload(Error &err) {
     if (d->bit4.ensure(d->n_words * 16 + 64, err)) return err.code;
     CU(cudaMemsetAsync(d->bit4.p, 0, d->n_words * 16 + 64, d->stream));
     if (n_bytes) CU(cudaMemcpyAsync(d->bit4.p, h.data.data(), n_bytes, cudaMemcpyHostToDevice, d->stream));
-    if (d->planes.ensure(3 * d->n_words, err)) return err.code;
+    // each plane starts with one padding word (32 non-single cells before
+    // position 0) for windows anchored at a PAM near the genome start
+    const uint64_t pw = d->n_words + 1;
+    if (d->planes.ensure(3 * pw, err)) return err.code;
+    CU(cudaMemsetAsync(d->planes.p, 0, 4, d->stream));
+    CU(cudaMemsetAsync(d->planes.p + pw, 0, 4, d->stream));
+    CU(cudaMemsetAsync(d->planes.p + 2 * pw, 0xFF, 4, d->stream));
     {
         int threads = 256;
         uint64_t blocks = std::min<uint64_t>((d->n_words + threads - 1) / threads, 65535ull * 16);
         pack_planes_kernel<<<(unsigned)std::max<uint64_t>(blocks, 1), threads, 0, d->stream>>>(
-            reinterpret_cast<const uint4 *>(d->bit4.p), d->n_words, d->planes.p,
-            d->planes.p + d->n_words, d->planes.p + 2 * d->n_words);
+            reinterpret_cast<const uint4 *>(d->bit4.p), d->n_words, d->planes.p + 1,
+            d->planes.p + pw + 1, d->planes.p + 2 * pw + 1);
         CU(cudaGetLastError());
     }
     const size_t nc = h.n_chunks();
@@ -731,12 +747,16 @@ int Engine::run_popcount(const std::vector<Request> &reqs, std::vector<Result> &
     std::vector<ScanGroup> groups;
     std::vector<ScanSeg> segs;
     std::vector<uint32_t> req_first_pat;
-    // Exact patterns are laid out request-major (the row sort key); scan
-    // groups gather the patterns of every request that shares a filter and a
-    // strand, so that one PAM sweep serves all of them.
+    // Exact patterns are laid out request-major (the row sort key).  Scan
+    // groups gather, per strand, the patterns of every request whose filter
+    // has the same non-N cells at the same place relative to its anchor --
+    // the window end when the PAM ends the pattern (3' PAMs), else the
+    // window start -- so that one PAM sweep serves requests of different
+    // guide lengths and mismatch limits.
     std::vector<uint32_t> fast2exact;
-    std::map<std::pair<std::string, uint32_t>, std::vector<uint32_t>> by_filter;
-    std::vector<std::pair<std::string, uint32_t>> key_order;
+    std::map<std::string, std::vector<uint32_t>> by_key;
+    std::vector<std::string> key_order;
+    std::vector<uint32_t> ep_off;  // window offset of each exact pattern's first cell
     for (size_t ri = 0; ri < reqs.size(); ++ri) {
         const Request &r = reqs[ri];
         const uint32_t L = (uint32_t)r.filter.size();
@@ -755,6 +775,22 @@ int Engine::run_popcount(const std::vector<Request> &reqs, std::vector<Result> &
         }
         rdev.push_back(rd);
         req_first_pat.push_back((uint32_t)epats.size());
+        std::string key[2];
+        uint32_t off[2];
+        for (uint32_t st = 0; st < 2; ++st) {
+            int first = -1, last = -1;
+            for (uint32_t c = 0; c < L; ++c) {
+                if (rd.fisn[st][c]) continue;
+                if (first < 0) first = (int)c;
+                last = (int)c;
+            }
+            const bool end_anchor = last == (int)L - 1 && first > 0;
+            off[st] = end_anchor ? kMaxPatternLen - L : 0;
+            key[st] = std::string(end_anchor ? "E" : "S") + (st ? "-" : "+");
+            for (uint32_t c = 0; c < L; ++c)
+                if (!rd.fisn[st][c])
+                    key[st] += std::to_string(c + off[st]) + ":" + std::to_string(rd.fset[st][c]) + ",";
+        }
         const size_t np = r.patterns.size(), nfwd = np / 2;
         for (size_t p = 0; p < np; ++p) {
             const uint32_t strand = p >= nfwd;
@@ -764,30 +800,34 @@ int Engine::run_popcount(const std::vector<Request> &reqs, std::vector<Result> &
             ep.L = L;
             ep.max_mm = r.max_mm;
             for (uint32_t c = 0; c < L; ++c) ep.b4[c] = t.str2b4[1][(uint8_t)r.patterns[p][c]];
-            // filters are compared case-insensitively for N, exactly otherwise
-            std::string key = r.filter;
-            for (char &ch : key) ch = (char)((ch >= 'a' && ch <= 'z') ? ch - 32 : ch);
-            auto k = std::make_pair(key, strand);
-            if (!by_filter.count(k)) key_order.push_back(k);
-            by_filter[k].push_back((uint32_t)epats.size());
+            if (!by_key.count(key[strand])) key_order.push_back(key[strand]);
+            by_key[key[strand]].push_back((uint32_t)epats.size());
             epats.push_back(ep);
+            ep_off.push_back(off[strand]);
         }
     }
     for (const auto &key : key_order) {
-        const std::vector<uint32_t> &members = by_filter[key];
-        const uint32_t strand = key.second;
-        const RequestDev &rd = rdev[epats[members[0]].request];
-        const uint32_t L = rd.L;
+        const std::vector<uint32_t> &members = by_key[key];
+        const ExactPattern &e0 = epats[members[0]];
+        const uint32_t strand = e0.strand;
+        const RequestDev &rd = rdev[e0.request];
+        const uint32_t off0 = ep_off[members[0]];
         ScanGroup proto{};
-        for (uint32_t c = 0; c < L; ++c) {
+        for (uint32_t c = 0; c < rd.L; ++c) {  // the same cells for every member
             if (rd.fisn[strand][c]) continue;
             if (proto.n_pam == kMaxPamCells) break;
             const uint8_t fs = rd.fset[strand][c];
-            PamCell pc{c, (fs & 4) ? ~0u : 0u, (fs & 2) ? ~0u : 0u, (fs & 8) ? ~0u : 0u,
+            PamCell pc{c + off0, (fs & 4) ? ~0u : 0u, (fs & 2) ? ~0u : 0u, (fs & 8) ? ~0u : 0u,
                        (fs & 1) ? ~0u : 0u};
             proto.pam[proto.n_pam++] = pc;
         }
-        // scan segments: one per batch
+        // the members' pattern lengths (with their window offsets)
+        std::vector<std::pair<uint32_t, uint32_t>> lens;
+        for (uint32_t e : members) lens.push_back({epats[e].L, ep_off[e]});
+        std::sort(lens.begin(), lens.end());
+        lens.erase(std::unique(lens.begin(), lens.end()), lens.end());
+        // scan segments: one per batch, the union of the members' window
+        // ranges; verify re-applies each length's own head-overlap threshold
         proto.seg_begin = (uint32_t)segs.size();
         uint64_t tiles = 0;
         for (size_t bi = 0; bi < batches.size(); ++bi) {
@@ -795,12 +835,19 @@ int Engine::run_popcount(const std::vector<Request> &reqs, std::vector<Result> &
             // legacy_match_start_min_nucl (search.rs:540-546): starts in the
             // head chunk that the previous batch already emitted
             const uint64_t c1 = hb[bi].has_head ? b.active_start : 0;
-            const uint64_t msmin = c1 > L - 1 ? c1 - (L - 1) : 0;
+            uint64_t lo = ~0ull, hi = 0;
+            for (const auto &lo_ : lens) {
+                const uint32_t L = lo_.first, o = lo_.second;
+                const uint64_t msmin = c1 > L - 1 ? c1 - (L - 1) : 0;
+                if (msmin >= b.valid) continue;
+                lo = std::min<uint64_t>(lo, b.base + msmin + kMaxPatternLen - o);
+                hi = std::max<uint64_t>(hi, b.base + b.valid + kMaxPatternLen - o);
+            }
+            if (hi <= lo) continue;
             ScanSeg sgm{};
-            sgm.lo = b.base + msmin;
-            sgm.hi = b.base + b.valid;
-            if (sgm.hi <= sgm.lo) continue;
-            sgm.base = b.base;
+            sgm.lo = lo;
+            sgm.hi = hi;
+            sgm.base = b.base + kMaxPatternLen;
             sgm.w0 = sgm.lo / 32;
             sgm.tile_begin = tiles;
             sgm.batch = (uint32_t)bi;
@@ -813,34 +860,39 @@ int Engine::run_popcount(const std::vector<Request> &reqs, std::vector<Result> &
             return err.code;
         }
         if (proto.seg_end == proto.seg_begin) continue;
-        // scan form of the members, ordered by care mask
-        std::vector<std::pair<FastPattern, uint32_t>> comp;
+        // scan form of the members (window cells from their offset), ordered
+        // by care mask and offset
+        struct Comp {
+            FastPattern fp;
+            uint32_t off, exact;
+        };
+        std::vector<Comp> comp;
         for (uint32_t e : members) {
             const ExactPattern &ep = epats[e];
+            const uint32_t o = ep_off[e];
             FastPattern fp{0, 0, 0, (int32_t)ep.max_mm};
-            for (uint32_t c = 0; c < L; ++c) {
+            for (uint32_t c = 0; c < ep.L; ++c) {
                 const uint8_t v = ep.b4[c];
                 if (v && !(v & (v - 1))) {
                     const uint32_t cd = code2(v);
-                    fp.care |= 1u << c;
-                    fp.h |= ((cd >> 1) & 1u) << c;
-                    fp.l |= (cd & 1u) << c;
+                    fp.care |= 1u << (c + o);
+                    fp.h |= ((cd >> 1) & 1u) << (c + o);
+                    fp.l |= (cd & 1u) << (c + o);
                 }
             }
-            comp.push_back({fp, e});
+            comp.push_back({fp, o, e});
         }
-        std::stable_sort(comp.begin(), comp.end(),
-                         [](const std::pair<FastPattern, uint32_t> &x,
-                            const std::pair<FastPattern, uint32_t> &y) {
-                             return x.first.care < y.first.care;
-                         });
+        std::stable_sort(comp.begin(), comp.end(), [](const Comp &x, const Comp &y) {
+            return x.fp.care != y.fp.care ? x.fp.care < y.fp.care : x.off < y.off;
+        });
         // groups of at most kMaxCareClasses classes
         ScanGroup g = proto;
         g.pat_begin = (uint32_t)fpats.size();
         g.n_class = 0;
         for (size_t i = 0; i < comp.size(); ++i) {
-            const uint32_t care = comp[i].first.care;
-            const bool new_class = g.n_class == 0 || g.cls[g.n_class - 1].care != care;
+            const uint32_t care = comp[i].fp.care, o = comp[i].off;
+            const bool new_class = g.n_class == 0 || g.cls[g.n_class - 1].care != care ||
+                                   g.cls[g.n_class - 1].off != o;
             if (new_class && g.n_class == (uint32_t)kMaxCareClasses) {
                 g.pat_end = (uint32_t)fpats.size();
                 groups.push_back(g);
@@ -849,11 +901,11 @@ int Engine::run_popcount(const std::vector<Request> &reqs, std::vector<Result> &
                 g.n_class = 0;
             }
             const uint32_t rel = (uint32_t)fpats.size() - g.pat_begin;
-            if (g.n_class == 0 || g.cls[g.n_class - 1].care != care)
-                g.cls[g.n_class++] = CareClass{care, rel, rel, 0};
+            if (g.n_class == 0 || g.cls[g.n_class - 1].care != care || g.cls[g.n_class - 1].off != o)
+                g.cls[g.n_class++] = CareClass{care, rel, rel, o};
             g.cls[g.n_class - 1].pat_end = rel + 1;
-            fpats.push_back(comp[i].first);
-            fast2exact.push_back(comp[i].second);
+            fpats.push_back(comp[i].fp);
+            fast2exact.push_back(comp[i].exact);
         }
         g.pat_end = (uint32_t)fpats.size();
         groups.push_back(g);
@@ -905,9 +957,9 @@ int Engine::run_popcount(const std::vector<Request> &reqs, std::vector<Result> &
     if (d.hits.cap == 0 && d.hits.ensure(1u << 22, err)) return err.code;
 
     ScanParams sp{};
-    sp.H = d.planes.p;
-    sp.L = d.planes.p + d.n_words;
-    sp.S = d.planes.p + 2 * d.n_words;
+    sp.H = d.planes.p;  // word w holds shifted window starts [32 w, 32 w + 32)
+    sp.L = d.planes.p + (d.n_words + 1);
+    sp.S = d.planes.p + 2 * (d.n_words + 1);
     sp.groups = (const ScanGroup *)tab(o_grp);
     sp.segs = (const ScanSeg *)tab(o_seg);
     sp.pats = (const FastPattern *)tab(o_fp);

@@ -178,3 +178,36 @@ def test_raw_kat_has_unfiltered_windows(cof_mod, golden):
     raw, nraw = g.search("N" * 21 + "GG", ["CCGTGGTTCAACATTTGCTTNNN"], 6, raw=True)
     rows, nrows = g.search("N" * 21 + "GG", ["CCGTGGTTCAACATTTGCTTNNN"], 6)
     assert nraw > nrows
+
+
+@pytest.mark.parametrize("cps", [0, 3])
+def test_shared_pam_groups_of_mixed_lengths(cof_mod, oracle_mod, cps):
+    # requests with one PAM but different guide lengths and mismatch limits
+    # share a scan group (windows anchored at the PAM); each result must
+    # equal the request alone and the oracle, also across batch boundaries
+    rng = random.Random(77)
+    _, records = randgen.random_genome(rng, 3, 4000, 9000)
+    reqs = []
+    for gl, mm in ((17, 2), (20, 4), (25, 3), (29, 5)):  # 3' NRG
+        guides = ["".join(rng.choice("ACGT") for _ in range(gl)) for _ in range(2)]
+        pats = [x + "NNN" for x in guides]
+        for p in pats:
+            randgen.plant_sites(rng, records, p, "N" * gl + "NRG", 4, 2)
+        reqs.append(dict(search_filter="N" * gl + "NRG", patterns=pats, max_mismatches=mm))
+    for gl, mm in ((18, 3), (23, 4)):  # 5' TTTN
+        guides = ["".join(rng.choice("ACGT") for _ in range(gl)) for _ in range(2)]
+        pats = ["NNNN" + x for x in guides]
+        for p in pats:
+            randgen.plant_sites(rng, records, p, "TTTN" + "N" * gl, 4, 2)
+        reqs.append(dict(search_filter="TTTN" + "N" * gl, patterns=pats, max_mismatches=mm))
+    chunks = randgen.chunk_records(rng, records, 700)
+    g, o = _both(cof_mod, oracle_mod, chunks)
+    for r in reqs:
+        r["chunks_per_search"] = cps
+    batched = g.search_batch(reqs)
+    for r, (text, n) in zip(reqs, batched):
+        single, ns = g.search(**r)
+        ref, nref = o.search(r["search_filter"], r["patterns"], r["max_mismatches"],
+                             chunks_per_search=cps)
+        assert text == single and n == ns
+        assert _rows(text) == _rows(ref) and n == nref > 0
