@@ -150,6 +150,129 @@ __global__ void myers_filter_kernel(const uint8_t *__restrict__ bit4,
     }
 }
 
+// ---- Myers filter with the PAM test precomputed per tile --------------------
+//
+// check_pam_quick depends on the pattern only through its PAM form: the
+// filter bit4 of its N cells from the first N cell on (pam_off) and the
+// alignment spans it tries (L + bd - br for every bd <= db, br <= rb when the
+// PAM leads the pattern, L otherwise).  All patterns of one request strand
+// share a form.  A block takes a few consecutive tiles and first computes,
+// for every form, Q(y) = "the PAM cells starting at batch cell y are all
+// good" and from it pam_ok(t) = OR over spans of Q(t + 1 - span + pam_off)
+// for the tile's end positions t, into shared memory.  Then every
+// (tile, pattern) thread runs the streaming Myers sweep and tests one bit
+// per position instead of the reference's per-position cell loads.
+constexpr uint32_t kMfThreads = 256;
+constexpr uint32_t kMfMaxTiles = 32;           // tiles per block
+constexpr uint32_t kMfMaxForms = 8;            // PAM forms per launch
+constexpr uint32_t kMfQWords = kTile / 32 + 2; // Q bits: 1024 ends + <= 16 span shifts
+
+struct PamForm {
+    uint32_t pam_off, pam_n, span_lo, span_hi;  // spans span_lo..span_hi
+    uint8_t f[kMaxCells];                        // filter bit4 of the PAM cells
+};
+
+__global__ void __launch_bounds__(kMfThreads)
+myers_tile_kernel(const uint8_t *__restrict__ bit4, const BatchDev *__restrict__ batches,
+                  const MyersTile *__restrict__ tiles, uint64_t n_tiles,
+                  const MyersPattern *__restrict__ pats, uint32_t n_pat,
+                  const PamForm *__restrict__ forms, uint32_t n_forms, uint32_t tpb,
+                  MyersCand *cand, uint32_t cap, Counters *ctr) {
+    extern __shared__ uint32_t mf_smem[];
+    uint32_t *q_bits = mf_smem;                            // [tpb][n_forms][kMfQWords]
+    uint32_t *ok_bits = q_bits + tpb * n_forms * kMfQWords; // [tpb][n_forms][32]
+    uint32_t *seq = ok_bits + tpb * n_forms * 32;          // [n_pat][16] when staged
+    const bool staged = n_pat <= (uint32_t)kSmemMyers;
+    if (staged)
+        for (uint32_t i = threadIdx.x; i < n_pat * 16; i += blockDim.x) seq[i] = pats[i / 16].eq16[i % 16];
+    for (uint64_t tb = blockIdx.x; tb * tpb < n_tiles; tb += gridDim.x) {
+        const uint64_t tile0 = tb * tpb;
+        const uint32_t nt = (uint32_t)(n_tiles - tile0 < tpb ? n_tiles - tile0 : tpb);
+        __syncthreads();  // the previous tile block's readers are done
+        // Q words: bit i of word w is Q(y0 + 32 w + i), y0 = t0 + 1 - span_hi + pam_off
+        for (uint32_t i = threadIdx.x; i < nt * n_forms * kMfQWords; i += blockDim.x) {
+            const uint32_t tl = i / (n_forms * kMfQWords), fi = (i / kMfQWords) % n_forms,
+                           w = i % kMfQWords;
+            const MyersTile T = tiles[tile0 + tl];
+            const BatchDev B = batches[T.batch];
+            const PamForm &F = forms[fi];
+            const int64_t y0 = (int64_t)(T.t0 - B.base) + 1 - (int64_t)F.span_hi + F.pam_off;
+            uint32_t bits = 0;
+            for (uint32_t b = 0; b < 32; ++b) {
+                const int64_t y = y0 + 32 * (int64_t)w + b;
+                if (y < (int64_t)F.pam_off) continue;  // alignment start before the batch
+                bool ok = true;
+                for (uint32_t k = 0; k < F.pam_n && ok; ++k) {
+                    const uint64_t gp = (uint64_t)y + k;
+                    if (gp >= B.valid) { ok = false; break; }
+                    const uint8_t g = nib(bit4, B.base + gp), f = F.f[k];
+                    ok = f == 0xF ? g != 0 : (g != 0 && g != 0xF && (g & f));
+                }
+                bits |= (uint32_t)ok << b;
+            }
+            q_bits[i] = bits;
+        }
+        __syncthreads();
+        // pam_ok words: end position t0 + 32 w + j, OR over the span shifts
+        for (uint32_t i = threadIdx.x; i < nt * n_forms * 32; i += blockDim.x) {
+            const uint32_t tf = i / 32, w = i % 32;
+            const PamForm &F = forms[tf % n_forms];
+            const uint32_t *Q = q_bits + tf * kMfQWords;
+            uint32_t v = 0;
+            for (uint32_t d = 0; d <= F.span_hi - F.span_lo; ++d) {
+                // bits 32 w + j + (span_hi - span) of Q, span = span_hi - d
+                const uint32_t s = 32 * w + d;
+                v |= __funnelshift_r(Q[s >> 5], Q[(s >> 5) + 1], s & 31);
+            }
+            ok_bits[i] = v;
+        }
+        __syncthreads();
+        // streaming Myers per (tile, pattern)
+        for (uint32_t i = threadIdx.x; i < nt * n_pat; i += blockDim.x) {
+            const uint32_t tl = i / n_pat, p = i % n_pat;
+            const MyersTile T = tiles[tile0 + tl];
+            const BatchDev B = batches[T.batch];
+            const MyersPattern &P = pats[p];
+            const uint32_t *eq = staged ? seq + 16 * p : P.eq16;
+            const uint32_t *okw = ok_bits + (tl * n_forms + P.pad) * 32;
+            const uint32_t L = P.L;
+            const uint32_t mask = L == 32 ? 0xFFFFFFFFu : ((1u << L) - 1u);
+            const uint32_t sh = L - 1;
+            uint32_t vp = mask, vn = 0;
+            int score = (int)L;
+            const uint64_t ws = T.t0 >= kWarm ? ((T.t0 - kWarm) & ~15ull) : 0;
+            unsigned long long word = 0;
+            uint32_t okb = 0;
+            for (uint64_t q = ws; q < T.t1; ++q) {
+                if ((q & 15) == 0 || q == ws)
+                    word = __ldg(reinterpret_cast<const unsigned long long *>(bit4 + ((q >> 1) & ~7ull)));
+                const uint32_t b = (uint32_t)(word >> ((q & 15) * 4)) & 0xF;
+                const uint32_t x = eq[b] | vn;
+                const uint32_t d0 = (((x & vp) + vp) ^ vp) | x;
+                const uint32_t hn = vp & d0;
+                const uint32_t hp = vn | ~(vp | d0);
+                const uint32_t xs = hp << 1;
+                vn = xs & d0;
+                vp = ((hn << 1) | ~(xs | d0)) & mask;
+                vn &= mask;
+                score += (int)((hp >> sh) & 1u) - (int)((hn >> sh) & 1u);
+                if (q >= T.t0) {
+                    const uint32_t r = (uint32_t)(q - T.t0);
+                    if ((r & 31) == 0) okb = okw[r >> 5];
+                    if (((okb >> (r & 31)) & 1u) && score <= (int)P.E) {
+                        const uint32_t tlc = (uint32_t)(q - B.base);
+                        if (tlc + 1 >= L) {
+                            const uint32_t c = atomicAdd(&ctr->hits, 1u);
+                            if (c < cap) cand[c] = MyersCand{tlc, T.batch, p, 0};
+                            else ctr->overflow = 1;
+                        }
+                    }
+                }
+            }
+        }
+    }
+}
+
 __device__ __forceinline__ bool loose(uint8_t p, uint8_t t) {  // cmp_loose_bit4
     if (t == 0) return false;
     if (p == 0xF) return true;
@@ -1043,6 +1166,7 @@ int Engine::run_bulge(const std::vector<Request> &reqs, std::vector<Result> &out
     }
     std::vector<MyersReqDev> rdev;
     std::vector<MyersPattern> pats;
+    std::vector<PamForm> forms;
     for (size_t ri = 0; ri < reqs.size(); ++ri) {
         const Request &r = reqs[ri];
         const uint32_t L = (uint32_t)r.filter.size();
@@ -1106,6 +1230,20 @@ int Engine::run_bulge(const std::vector<Request> &reqs, std::vector<Result> &out
             mp.pam_off = ps;
             for (uint32_t c = ps; c < L; ++c)
                 if (mp.isn[c]) mp.pamf[mp.pam_n++] = mp.eff[c];
+            // its PAM form: cells, and the spans check_pam_quick tries
+            // (search.rs:703-755; L + bd - br, or L alone when the PAM
+            // does not lead the pattern)
+            PamForm pf;
+            std::memset(&pf, 0, sizeof pf);
+            pf.pam_off = ps;
+            pf.pam_n = mp.pam_n;
+            std::memcpy(pf.f, mp.pamf, sizeof pf.f);
+            pf.span_lo = ps == 0 ? (uint32_t)std::max<int>(1, (int)L - (int)r.max_rb) : L;
+            pf.span_hi = ps == 0 ? L + r.max_db : L;
+            uint32_t fi = 0;
+            while (fi < forms.size() && std::memcmp(&forms[fi], &pf, sizeof pf) != 0) ++fi;
+            if (fi == forms.size()) forms.push_back(pf);
+            mp.pad = fi;
             pats.push_back(mp);
         }
     }
@@ -1113,7 +1251,7 @@ int Engine::run_bulge(const std::vector<Request> &reqs, std::vector<Result> &out
 
     TablePack tp;
     const size_t o_b = tp.add(batches), o_t = tp.add(tiles), o_p = tp.add(pats),
-                 o_r = tp.add(rdev);
+                 o_r = tp.add(rdev), o_f = tp.add(forms);
     if (d.tables.ensure(tp.buf.size(), err)) return err.code;
     CU(cudaEventRecord(d.ev[0], s));
     CU(cudaMemcpyAsync(d.tables.p, tp.buf.data(), tp.buf.size(), cudaMemcpyHostToDevice, s));
@@ -1130,13 +1268,33 @@ int Engine::run_bulge(const std::vector<Request> &reqs, std::vector<Result> &out
     for (int attempt = 0; attempt < 2; ++attempt) {
         CU(cudaMemsetAsync(d.ctr.p, 0, sizeof(Counters), s));
         CU(cudaEventRecord(d.ev[1], s));
-        const uint64_t items = (uint64_t)tiles.size() * n_pat;
-        const unsigned blocks =
-            (unsigned)std::max<uint64_t>(1, std::min<uint64_t>((items + 127) / 128, (uint64_t)d.n_sm * 16));
-        myers_filter_kernel<<<blocks, 128, 0, s>>>(d.bit4.p, dB, (const MyersTile *)tab(o_t),
-                                                   tiles.size(), dP, n_pat, dR, d.mcand.p,
-                                                   (uint32_t)std::min<size_t>(d.mcand.cap, 0xFFFFFFF0u),
-                                                   d.ctr.p);
+        const uint32_t cap = (uint32_t)std::min<size_t>(d.mcand.cap, 0xFFFFFFF0u);
+        if (forms.size() <= kMfMaxForms) {
+            // PAM test per tile in shared memory; enough tiles per block
+            // that its (tile, pattern) items fill the block
+            const uint32_t tpb = std::min<uint32_t>(
+                kMfMaxTiles, std::max<uint32_t>(1, (kMfThreads + n_pat - 1) / n_pat));
+            const size_t smem = (size_t)tpb * forms.size() * (kMfQWords + 32) * 4 +
+                                (n_pat <= (uint32_t)kSmemMyers ? (size_t)n_pat * 64 : 0);
+            CU(cudaFuncSetAttribute(myers_tile_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)smem));
+            int per_sm = 1;
+            CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, myers_tile_kernel, kMfThreads,
+                                                             smem));
+            const uint64_t tblocks = (tiles.size() + tpb - 1) / tpb;
+            const unsigned blocks = (unsigned)std::max<uint64_t>(
+                1, std::min<uint64_t>(tblocks, (uint64_t)d.n_sm * std::max(1, per_sm)));
+            myers_tile_kernel<<<blocks, kMfThreads, smem, s>>>(
+                d.bit4.p, dB, (const MyersTile *)tab(o_t), tiles.size(), dP, n_pat,
+                (const PamForm *)tab(o_f), (uint32_t)forms.size(), tpb, d.mcand.p, cap, d.ctr.p);
+        } else {
+            const uint64_t items = (uint64_t)tiles.size() * n_pat;
+            const unsigned blocks = (unsigned)std::max<uint64_t>(
+                1, std::min<uint64_t>((items + 127) / 128, (uint64_t)d.n_sm * 16));
+            myers_filter_kernel<<<blocks, 128, 0, s>>>(d.bit4.p, dB, (const MyersTile *)tab(o_t),
+                                                       tiles.size(), dP, n_pat, dR, d.mcand.p, cap,
+                                                       d.ctr.p);
+        }
         CU(cudaGetLastError());
         CU(cudaEventRecord(d.ev[2], s));
         ++times_.kernel_launches;
