@@ -1008,89 +1008,97 @@ __global__ void mrow_len_kernel(GenomeDev G, const MyersRow *__restrict__ rows,
     }
 }
 
-__global__ void mrow_write_kernel(GenomeDev G, const MyersRow *__restrict__ rows,
-                                  const uint32_t *__restrict__ order, uint32_t n,
-                                  const MyersPattern *__restrict__ pats,
-                                  const MyersReqDev *__restrict__ reqs,
-                                  const uint64_t *__restrict__ off, char *__restrict__ text) {
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        const MyersRow w = rows[order[i]];
-        const MyersPattern &P = pats[w.pattern];
-        const MyersReqDev R = reqs[P.request];
-        const bool fwd = P.strand == 0;
-        char *o = text + off[i];
-        const uint32_t size = w.db + w.rb;
-        const uint32_t ni = G.name_idx[w.chunk];
-        if (R.raw) {  // search()'s Match: name, chrom_idx, pattern, strand, mm, db, rb
+constexpr uint32_t kRowStage = 4096;  // staged text bytes per warp
+
+__global__ void __launch_bounds__(256)
+mrow_write_kernel(GenomeDev G, const MyersRow *__restrict__ rows,
+                  const uint32_t *__restrict__ order, uint32_t n,
+                  const MyersPattern *__restrict__ pats, const MyersReqDev *__restrict__ reqs,
+                  const uint64_t *__restrict__ off, char *__restrict__ text) {
+    __shared__ __align__(16) char stage_all[8][kRowStage];
+    char *stage = stage_all[threadIdx.x >> 5];
+    const uint64_t gw = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+    const uint64_t nw = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+    for (uint64_t i0 = gw * 32; i0 < n; i0 += nw * 32) {
+        warp_rows_staged((uint32_t)i0, n, off, text, stage, kRowStage, [&](uint32_t i, char *o) {
+            const MyersRow w = rows[order[i]];
+            const MyersPattern &P = pats[w.pattern];
+            const MyersReqDev R = reqs[P.request];
+            const bool fwd = P.strand == 0;
+            const uint32_t size = w.db + w.rb;
+            const uint32_t ni = G.name_idx[w.chunk];
+            if (R.raw) {  // search()'s Match: name, chrom_idx, pattern, strand, mm, db, rb
+                for (uint32_t c = G.name_off[ni]; c < G.name_off[ni + 1]; ++c) *o++ = G.names[c];
+                *o++ = '\t';
+                o = put_u64(o, w.pos);
+                *o++ = '\t';
+                o = put_u64(o, w.pattern - R.first_pattern);
+                *o++ = '\t';
+                *o++ = fwd ? '+' : '-';
+                *o++ = '\t';
+                o = put_u64(o, w.mm);
+                *o++ = '\t';
+                o = put_u64(o, w.db);
+                *o++ = '\t';
+                o = put_u64(o, w.rb);
+                *o++ = '\t';
+            } else if (size == 0) {
+                *o++ = 'X';
+            } else if (w.db > 0) {
+                *o++ = 'D'; *o++ = 'N'; *o++ = 'A';
+            } else {
+                *o++ = 'R'; *o++ = 'N'; *o++ = 'A';
+            }
+            if (!R.raw) *o++ = '\t';
+            const uint32_t no = w.n_ops;
+            char *rna = o;
+            char *dna = o + no + 1;
+            // aligned strings in alignment order (traceback.rs:267-298), then
+            // reverse-complemented for reverse-strand patterns
+            uint32_t pi = 0;
+            uint64_t gi = w.start;
+            for (uint32_t k = 0; k < no; ++k) {
+                const uint32_t op = (uint32_t)((k < 32 ? w.ops[0] >> (2 * k) : w.ops[1] >> (2 * (k - 32))) & 3);
+                uint8_t pv = 0, gv = 0;
+                bool pgap = false, ggap = false;
+                if (op <= 1) {
+                    pv = P.b4[pi++];
+                    gv = nib(G.bit4, gi++);
+                } else if (op == 2) {
+                    pgap = true;
+                    gv = nib(G.bit4, gi++);
+                } else {
+                    pv = P.b4[pi++];
+                    ggap = true;
+                }
+                const uint32_t at = fwd ? k : no - 1 - k;
+                if (!fwd) {
+                    pv = dcomp4(pv);
+                    gv = dcomp4(gv);
+                }
+                rna[at] = pgap ? '-' : b4char(pv);
+                dna[at] = ggap ? '-' : b4char(gv);
+            }
+            o += no;
+            *o++ = '\t';
+            o += no;
+            if (R.raw) {
+                *o++ = '\n';
+                return;
+            }
+            *o++ = '\t';
             for (uint32_t c = G.name_off[ni]; c < G.name_off[ni + 1]; ++c) *o++ = G.names[c];
             *o++ = '\t';
-            o = put_u64(o, w.pos);
-            *o++ = '\t';
-            o = put_u64(o, w.pattern - R.first_pattern);
+            o = put_u64(o, mpos_out(w, R, P.strand));
             *o++ = '\t';
             *o++ = fwd ? '+' : '-';
             *o++ = '\t';
             o = put_u64(o, w.mm);
             *o++ = '\t';
-            o = put_u64(o, w.db);
-            *o++ = '\t';
-            o = put_u64(o, w.rb);
-            *o++ = '\t';
-        } else if (size == 0) {
-            *o++ = 'X';
-        } else if (w.db > 0) {
-            *o++ = 'D'; *o++ = 'N'; *o++ = 'A';
-        } else {
-            *o++ = 'R'; *o++ = 'N'; *o++ = 'A';
-        }
-        if (!R.raw) *o++ = '\t';
-        const uint32_t no = w.n_ops;
-        char *rna = o;
-        char *dna = o + no + 1;
-        // aligned strings in alignment order (traceback.rs:267-298), then
-        // reverse-complemented for reverse-strand patterns
-        uint32_t pi = 0;
-        uint64_t gi = w.start;
-        for (uint32_t k = 0; k < no; ++k) {
-            const uint32_t op = (uint32_t)((k < 32 ? w.ops[0] >> (2 * k) : w.ops[1] >> (2 * (k - 32))) & 3);
-            uint8_t pv = 0, gv = 0;
-            bool pgap = false, ggap = false;
-            if (op <= 1) {
-                pv = P.b4[pi++];
-                gv = nib(G.bit4, gi++);
-            } else if (op == 2) {
-                pgap = true;
-                gv = nib(G.bit4, gi++);
-            } else {
-                pv = P.b4[pi++];
-                ggap = true;
-            }
-            const uint32_t at = fwd ? k : no - 1 - k;
-            if (!fwd) {
-                pv = dcomp4(pv);
-                gv = dcomp4(gv);
-            }
-            rna[at] = pgap ? '-' : b4char(pv);
-            dna[at] = ggap ? '-' : b4char(gv);
-        }
-        o += no;
-        *o++ = '\t';
-        o += no;
-        if (R.raw) {
+            o = put_u64(o, size);
             *o++ = '\n';
-            continue;
-        }
-        *o++ = '\t';
-        for (uint32_t c = G.name_off[ni]; c < G.name_off[ni + 1]; ++c) *o++ = G.names[c];
-        *o++ = '\t';
-        o = put_u64(o, mpos_out(w, R, P.strand));
-        *o++ = '\t';
-        *o++ = fwd ? '+' : '-';
-        *o++ = '\t';
-        o = put_u64(o, w.mm);
-        *o++ = '\t';
-        o = put_u64(o, size);
-        *o++ = '\n';
+
+        });
     }
 }
 

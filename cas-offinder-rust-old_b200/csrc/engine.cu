@@ -533,52 +533,60 @@ __global__ void row_len_kernel(GenomeDev G, const Row *__restrict__ rows,
     }
 }
 
-__global__ void row_write_kernel(GenomeDev G, const Row *__restrict__ rows,
-                                 const uint32_t *__restrict__ order, uint32_t n,
-                                 const ExactPattern *__restrict__ pats,
-                                 const RequestDev *__restrict__ reqs,
-                                 const uint64_t *__restrict__ off, char *__restrict__ text) {
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        const Row w = rows[order[i]];
-        const ExactPattern &P = pats[w.pattern];
-        const RequestDev &R = reqs[P.request];
-        const uint32_t L = P.L;
-        const bool fwd = P.strand == 0;
-        char *o = text + off[i];
-        *o++ = 'X';
-        *o++ = '\t';
-        char *rna = o;
-        char *dna = o + L + 1;
-        for (uint32_t c = 0; c < L; ++c) {
-            // output orientation: reverse strand strings are reverse complemented
-            const uint32_t sc = fwd ? c : L - 1 - c;
-            const uint64_t gi = w.s_global + sc;
-            uint8_t g = gi < w.clip ? nib(G.bit4, gi) : 0;
-            if (g == 0xF) g = 0;
-            uint8_t p = P.b4[sc];
-            if (!fwd) { g = dcomp4(g); p = dcomp4(p); }
-            rna[c] = b4char(p);
-            char d = b4char(g);
-            if (g == 0) d = (p == 0xF) ? 'N' : 'n';
-            else if (p == 0xF) {}
-            else if (!(single_base(g) && (g & p))) d = (char)(d | 0x20);
-            dna[c] = d;
-        }
-        o += L;
-        *o++ = '\t';
-        o += L;
-        *o++ = '\t';
-        const uint32_t ni = G.name_idx[w.chunk];
-        for (uint32_t c = G.name_off[ni]; c < G.name_off[ni + 1]; ++c) *o++ = G.names[c];
-        *o++ = '\t';
-        o = put_u64(o, pos_out(w, R, P.strand));
-        *o++ = '\t';
-        *o++ = fwd ? '+' : '-';
-        *o++ = '\t';
-        o = put_u64(o, w.mm);
-        *o++ = '\t';
-        *o++ = '0';
-        *o++ = '\n';
+constexpr uint32_t kRowStage = 4096;  // staged text bytes per warp
+
+__global__ void __launch_bounds__(256)
+row_write_kernel(GenomeDev G, const Row *__restrict__ rows, const uint32_t *__restrict__ order,
+                 uint32_t n, const ExactPattern *__restrict__ pats,
+                 const RequestDev *__restrict__ reqs, const uint64_t *__restrict__ off,
+                 char *__restrict__ text) {
+    __shared__ __align__(16) char stage_all[8][kRowStage];
+    char *stage = stage_all[threadIdx.x >> 5];
+    const uint64_t gw = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+    const uint64_t nw = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+    for (uint64_t i0 = gw * 32; i0 < n; i0 += nw * 32) {
+        warp_rows_staged((uint32_t)i0, n, off, text, stage, kRowStage, [&](uint32_t i, char *o) {
+            const Row w = rows[order[i]];
+            const ExactPattern &P = pats[w.pattern];
+            const RequestDev &R = reqs[P.request];
+            const uint32_t L = P.L;
+            const bool fwd = P.strand == 0;
+            *o++ = 'X';
+            *o++ = '\t';
+            char *rna = o;
+            char *dna = o + L + 1;
+            for (uint32_t c = 0; c < L; ++c) {
+                // output orientation: reverse strand strings are reverse complemented
+                const uint32_t sc = fwd ? c : L - 1 - c;
+                const uint64_t gi = w.s_global + sc;
+                uint8_t g = gi < w.clip ? nib(G.bit4, gi) : 0;
+                if (g == 0xF) g = 0;
+                uint8_t p = P.b4[sc];
+                if (!fwd) { g = dcomp4(g); p = dcomp4(p); }
+                rna[c] = b4char(p);
+                char d = b4char(g);
+                if (g == 0) d = (p == 0xF) ? 'N' : 'n';
+                else if (p == 0xF) {}
+                else if (!(single_base(g) && (g & p))) d = (char)(d | 0x20);
+                dna[c] = d;
+            }
+            o += L;
+            *o++ = '\t';
+            o += L;
+            *o++ = '\t';
+            const uint32_t ni = G.name_idx[w.chunk];
+            for (uint32_t c = G.name_off[ni]; c < G.name_off[ni + 1]; ++c) *o++ = G.names[c];
+            *o++ = '\t';
+            o = put_u64(o, pos_out(w, R, P.strand));
+            *o++ = '\t';
+            *o++ = fwd ? '+' : '-';
+            *o++ = '\t';
+            o = put_u64(o, w.mm);
+            *o++ = '\t';
+            *o++ = '0';
+            *o++ = '\n';
+
+        });
     }
 }
 

@@ -226,5 +226,40 @@ inline uint32_t code2(uint8_t b4) {  // single base one-hot -> 2-bit code A0 C1 
     }
 }
 
+// Row text through shared memory: a warp formats its 32 consecutive rows
+// (one per lane) into `stage`, whose bytes line up with the output modulo 4,
+// then stores the warp's contiguous output range with aligned, coalesced
+// 4-byte stores (single bytes at the two ragged ends).  Without the stage
+// every byte store of a warp would touch 32 scattered lines.  A range longer
+// than `cap` bytes (very long record names) is written directly.
+// `row(i, dst)` formats row i at dst; `off` holds each row's output offset
+// (n + 1 entries).
+template <class RowFn>
+__device__ __forceinline__ void warp_rows_staged(uint32_t i0, uint32_t n,
+                                                 const uint64_t *__restrict__ off,
+                                                 char *__restrict__ text, char *stage,
+                                                 uint32_t cap, RowFn row) {
+    const uint32_t lane = threadIdx.x & 31;
+    const uint32_t i = i0 + lane;
+    const uint64_t start = off[i0], end = off[min(i0 + 32, n)];
+    const uint64_t base = start & ~3ull;  // stage byte k <-> output byte base + k
+    if (end - base > cap) {
+        if (i < n) row(i, text + off[i]);
+        return;
+    }
+    if (i < n) row(i, stage + (off[i] - base));
+    __syncwarp();
+    const uint64_t a0 = (start + 3) & ~3ull, a1 = end & ~3ull;
+    if (a0 >= a1) {  // no whole aligned word: bytes only
+        for (uint64_t g = start + lane; g < end; g += 32) text[g] = stage[g - base];
+    } else {
+        if (start + lane < a0) text[start + lane] = stage[start + lane - base];
+        if (a1 + lane < end) text[a1 + lane] = stage[a1 + lane - base];
+        const uint32_t *sw = reinterpret_cast<const uint32_t *>(stage + (a0 - base));
+        uint32_t *gw = reinterpret_cast<uint32_t *>(text + a0);
+        for (uint64_t w = lane; w < (a1 - a0) / 4; w += 32) gw[w] = sw[w];
+    }
+    __syncwarp();
+}
 
 }  // namespace cof
