@@ -486,7 +486,7 @@ constexpr int kTbWarps = 4;                  // warps per block
 constexpr int kTbCap = 160;                  // stack slots per warp
 constexpr int kTbMargin = 2 * kMaxCells;     // slots a one-node-at-a-time walk can add
 constexpr uint32_t kTbMaxBits = 128;         // budget bits per cell (NW <= 2)
-constexpr uint32_t kTbBudget = 96;           // iterations on one tree before handing it on
+constexpr uint32_t kTbBudget = 384;          // iterations on one tree before handing it on
 constexpr uint32_t kTbQueue = 1u << 21;      // subtrees per hand-on queue
 constexpr int kTbMaxPasses = 24;             // the last pass finishes every tree
 
@@ -1349,6 +1349,8 @@ int Engine::run_bulge(const std::vector<Request> &reqs, std::vector<Result> &out
     if (const char *e = std::getenv("COF_BULGE_WARP"))
         if (e[0] == '0') warp_tb = false;
     if (warp_tb && d.tb_items.ensure(2 * (size_t)kTbQueue * sizeof(TbItem), err)) return err.code;
+    uint32_t tb_budget = kTbBudget;  // COF_TB_BUDGET: iterations before a tree is handed on
+    if (const char *e = std::getenv("COF_TB_BUDGET")) tb_budget = (uint32_t)std::max(1, std::atoi(e));
     const size_t tb_smem = (size_t)kTbWarps * tb_warp_bytes(tbl_words);
     auto tb_fn = nw == 1 ? traceback_warp_kernel<1> : traceback_warp_kernel<2>;
     int tb_blocks_per_sm = 1;
@@ -1411,7 +1413,7 @@ int Engine::run_bulge(const std::vector<Request> &reqs, std::vector<Result> &out
                 TbItem *out_q = q[pass & 1];
                 tb_fn<<<tb, kTbWarps * 32, tb_smem, s>>>(
                     d.view(), dB, dP, dR, cands + c0, cn, in, n_in, last ? nullptr : out_q,
-                    kTbQueue, kTbBudget, tbl_words, d.mrows.p, (uint32_t)row_cap, d.keys.p,
+                    kTbQueue, tb_budget, tbl_words, d.mrows.p, (uint32_t)row_cap, d.keys.p,
                     d.vals.p, d.ctr.p, d.req_rows.p);
                 CU(cudaGetLastError());
                 ++times_.kernel_launches;
