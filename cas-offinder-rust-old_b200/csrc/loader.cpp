@@ -8,13 +8,18 @@
 //   read_fasta_folder cas-offinder-lib/src/read_fasta_folder.rs:8-23
 //   path dispatch     cas-offinder-cli/src/main.rs:106-121
 #include <dirent.h>
+#include <fcntl.h>
+#include <sys/mman.h>
 #include <sys/stat.h>
+#include <unistd.h>
 
 #include <algorithm>
 #include <cerrno>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <thread>
+#include <vector>
 
 #include "cof_engine.h"
 
@@ -122,26 +127,37 @@ int slurp(const std::string &path, std::vector<char> &buf, Error &err) {
 // read_fasta.rs:9-71 over an in-memory file.  Lines end at '\n' with one
 // preceding '\r' dropped (BufRead::lines).  Genome characters use the mixed
 // base map (N -> 0xF, IUPAC -> union, anything else -> 0).
-int parse_fasta(HostGenome &g, const std::vector<char> &buf, Error &err) {
-    const Bit4Tables &t = bit4();
-    const uint8_t *m = t.str2b4[1];
-    const char *p = buf.data(), *e = p + buf.size();
+//
+// Two passes.  A sequential scan of the line ends decides the chunks exactly
+// as read_fasta.rs does (a record's lines fill a chunk until the next line
+// would take it past 65536 nt) and records, for each chunk, its record,
+// range and the file span of its lines.  Then every host thread converts a
+// share of the chunks straight into the genome's byte array, at offsets known
+// from the chunk sizes.
+int parse_fasta(HostGenome &g, const char *buf, size_t n, Error &err) {
+    struct Span {
+        uint32_t name;
+        uint64_t cs, ce;
+        const char *fb, *fe;  // the chunk's lines: file bytes [fb, fe)
+    };
+    std::vector<Span> spans;
+    const char *p = buf, *e = buf + n;
     bool started = false, have_name = false;
     uint32_t name = 0;
     uint64_t cs = 0, ce = 0;
-    std::vector<uint8_t> &cur = g.cur;
-    cur.assign(kChunkBytes, 0);
+    const char *fb = p;
     while (p < e) {
         const char *nl = (const char *)std::memchr(p, '\n', (size_t)(e - p));
         const char *le = nl ? nl : e;
+        const char *next = nl ? nl + 1 : e;
         size_t len = (size_t)(le - p);
         if (nl && len && p[len - 1] == '\r') --len;
         if (len >= 1 && p[0] == '>') {
-            if (ce != cs && g.add_chunk(name, cs, ce, cur.data(), err)) return err.code;
+            if (ce != cs) spans.push_back({name, cs, ce, fb, p});
             name = g.add_name(p + 1, len - 1);
             have_name = len > 1;
             cs = ce = 0;
-            std::fill(cur.begin(), cur.end(), 0);
+            fb = next;
             started = true;
         } else {
             if (!started) {
@@ -153,31 +169,110 @@ int parse_fasta(HostGenome &g, const std::vector<char> &buf, Error &err) {
                 return err.code;
             }
             if (len + (size_t)(ce - cs) > kChunkSize) {
-                if (g.add_chunk(name, cs, ce, cur.data(), err)) return err.code;
+                spans.push_back({name, cs, ce, fb, p});
                 cs = ce;
-                std::fill(cur.begin(), cur.end(), 0);
+                fb = p;
             }
             if (len > kChunkSize) {
                 err = {kBadInput, "line in fasta too long"};
                 return err.code;
             }
-            size_t o = (size_t)(ce - cs);
-            const uint8_t *s = (const uint8_t *)p;
-            size_t i = 0;
-            if (o & 1) {
-                if (len) cur[o >> 1] |= (uint8_t)(m[s[0]] << 4);
-                i = 1;
-            }
-            for (; i + 1 < len; i += 2)
-                cur[(o + i) >> 1] = (uint8_t)(m[s[i]] | (m[s[i + 1]] << 4));
-            if (i < len) cur[(o + i) >> 1] |= m[s[i]];
             ce += len;
         }
-        p = nl ? nl + 1 : e;
+        p = next;
     }
-    if (ce > cs && g.add_chunk(name, cs, ce, cur.data(), err)) return err.code;
+    if (ce > cs) spans.push_back({name, cs, ce, fb, e});
+
+    // chunk table, then the bytes of every chunk in parallel
+    const size_t k0 = g.start.size();
+    uint64_t total = g.data.size();
+    for (const Span &sp : spans) {
+        if (!g.start.empty() && sp.cs != 0 && g.end.back() != sp.cs) {
+            err = {kBadInput, "search expects chromosome chunks to arrive in order"};
+            return err.code;
+        }
+        g.name_idx.push_back(sp.name);
+        g.start.push_back(sp.cs);
+        g.end.push_back(sp.ce);
+        total += (sp.ce - sp.cs + 1) / 2;
+        g.boff.push_back(total);
+    }
+    g.data.resize(total, 0);
+    const uint8_t *m = bit4().str2b4[1];
+    auto convert = [&](size_t a, size_t b) {
+        for (size_t k = a; k < b; ++k) {
+            const Span &sp = spans[k];
+            uint8_t *out = g.data.data() + g.boff[k0 + k];
+            uint64_t o = 0;
+            for (const char *q = sp.fb; q < sp.fe;) {
+                const char *nl = (const char *)std::memchr(q, '\n', (size_t)(sp.fe - q));
+                const char *le = nl ? nl : sp.fe;
+                size_t len = (size_t)(le - q);
+                if (nl && len && q[len - 1] == '\r') --len;
+                const uint8_t *s = (const uint8_t *)q;
+                size_t i = 0;
+                if ((o & 1) && len) {
+                    out[o >> 1] |= (uint8_t)(m[s[0]] << 4);
+                    i = 1;
+                }
+                for (; i + 1 < len; i += 2)
+                    out[(o + i) >> 1] = (uint8_t)(m[s[i]] | (m[s[i + 1]] << 4));
+                if (i < len) out[(o + i) >> 1] |= m[s[i]];
+                o += len;
+                q = nl ? nl + 1 : sp.fe;
+            }
+        }
+    };
+    const size_t nsp = spans.size();
+    const unsigned nt = std::max(1u, std::min(std::thread::hardware_concurrency(), 32u));
+    if (nt == 1 || nsp < 64) {
+        convert(0, nsp);
+    } else {
+        std::vector<std::thread> th;
+        for (unsigned t = 0; t < nt; ++t) {
+            const size_t a = nsp * t / nt, b = nsp * (t + 1) / nt;
+            if (a < b) th.emplace_back(convert, a, b);
+        }
+        for (auto &x : th) x.join();
+    }
     return kOk;
 }
+
+// A read-only view of a whole file (mmap; read into memory where mapping
+// fails).
+struct FileView {
+    const char *p = nullptr;
+    size_t n = 0;
+    void *map = nullptr;
+    std::vector<char> copy;
+    ~FileView() {
+        if (map) ::munmap(map, n);
+    }
+    int open(const std::string &path, Error &err) {
+        const int fd = ::open(path.c_str(), O_RDONLY);
+        if (fd < 0) {
+            err = {kIo, "cannot open " + path + ": " + std::strerror(errno)};
+            return err.code;
+        }
+        struct stat st;
+        if (::fstat(fd, &st) == 0 && st.st_size > 0) {
+            n = (size_t)st.st_size;
+            void *m = ::mmap(nullptr, n, PROT_READ, MAP_PRIVATE, fd, 0);
+            if (m != MAP_FAILED) {
+                map = m;
+                p = (const char *)m;
+                ::madvise(m, n, MADV_SEQUENTIAL);
+            }
+        }
+        ::close(fd);
+        if (p) return kOk;
+        n = 0;
+        if (int rc = slurp(path, copy, err)) return rc;
+        p = copy.data();
+        n = copy.size();
+        return kOk;
+    }
+};
 
 uint32_t rd32(const std::vector<char> &b, size_t &o, bool &ok) {
     if (o + 4 > b.size()) {
@@ -305,19 +400,23 @@ int load_genome_path(HostGenome &g, const std::string &path, Error &err) {
             struct stat fs;
             if (::stat(p.c_str(), &fs) || !S_ISREG(fs.st_mode)) continue;
             if (p.size() >= 3 && p.compare(p.size() - 3, 3, ".fa") == 0) {
-                if ((rc = slurp(p, buf, err))) break;
-                if ((rc = parse_fasta(g, buf, err))) break;
+                FileView fv;
+                if ((rc = fv.open(p, err))) break;
+                if ((rc = parse_fasta(g, fv.p, fv.n, err))) break;
             }
         }
         ::closedir(d);
         return rc;
     }
-    if (int rc = slurp(path, buf, err)) return rc;
-    if (buf.empty()) {
+    FileView fv;
+    if (int rc = fv.open(path, err)) return rc;
+    if (fv.n == 0) {
         err = {kIo, "cannot read " + path};
         return err.code;
     }
-    return buf[0] == '>' ? parse_fasta(g, buf, err) : parse_2bit(g, buf, err);
+    if (fv.p[0] == '>') return parse_fasta(g, fv.p, fv.n, err);
+    buf.assign(fv.p, fv.p + fv.n);
+    return parse_2bit(g, buf, err);
 }
 
 bool Tuner::enabled() const {

@@ -211,3 +211,21 @@ def test_shared_pam_groups_of_mixed_lengths(cof_mod, oracle_mod, cps):
                              chunks_per_search=cps)
         assert text == single and n == ns
         assert _rows(text) == _rows(ref) and n == nref > 0
+
+
+def test_fasta_loader_matches_chunks(cof_mod, tmp_path):
+    # the parallel FASTA reader yields the chunks read_fasta.rs would: same
+    # chunk table and the same rows as the genome added chunk by chunk
+    import synth
+    cfg = synth.config_plain_small(seed=13, scale=0.05)
+    gen = cfg["genome"]
+    fa = tmp_path / "g.fa"
+    gen.write_fasta(str(fa))
+    a = cof_mod.Genome(str(fa))
+    b = cof_mod.Genome()
+    gen.load_into(b)
+    assert a.n_nucl == b.n_nucl == gen.n_nucl
+    args = (cfg["filter"], cfg["patterns"], cfg["max_mismatches"])
+    ta, na = a.search(*args, chunks_per_search=3)
+    tb, nb = b.search(*args, chunks_per_search=3)
+    assert ta == tb and na == nb > 0
