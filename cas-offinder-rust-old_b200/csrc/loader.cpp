@@ -274,7 +274,16 @@ struct FileView {
     }
 };
 
-uint32_t rd32(const std::vector<char> &b, size_t &o, bool &ok) {
+// A byte range of a file (the .2bit reader's view of it).
+struct FileBytes {
+    const char *p;
+    size_t n;
+    size_t size() const { return n; }
+    const char *data() const { return p; }
+    char operator[](size_t i) const { return p[i]; }
+};
+
+uint32_t rd32(const FileBytes &b, size_t &o, bool &ok) {
     if (o + 4 > b.size()) {
         ok = false;
         return 0;
@@ -287,7 +296,7 @@ uint32_t rd32(const std::vector<char> &b, size_t &o, bool &ok) {
 
 // read_2bit.rs:33-118.  Sequences are taken one after the other in index
 // order (the stored offsets are skipped, as the reference does).
-int parse_2bit(HostGenome &g, const std::vector<char> &b, Error &err) {
+int parse_2bit(HostGenome &g, const FileBytes &b, Error &err) {
     bool ok = true;
     size_t o = 0;
     auto trunc = [&]() {
@@ -321,13 +330,25 @@ int parse_2bit(HostGenome &g, const std::vector<char> &b, Error &err) {
         for (int j = 0; j < 4; ++j) v |= (uint16_t)((1u << ((i >> ((3 - j) * 2)) & 3)) << (4 * j));
         b2b4[i] = v;
     }
-    std::vector<uint8_t> &cur = g.cur;
-    cur.assign(kChunkBytes, 0);
+    // Pass 1 (sequential): record headers, N blocks, and one entry per
+    // 65536-nt chunk with its packed bytes and the N-block index the
+    // reference's loop (read_2bit.rs) has when it reaches the chunk -- the
+    // loop keeps that index across chunks and steps back by one each time,
+    // so it is replayed here without touching any bases.
+    struct Piece {
+        uint32_t rec;
+        uint64_t pos, rs;
+        size_t raw;   // file offset of the chunk's packed bases
+        int64_t bmi;  // N-block index at the chunk's start
+    };
+    std::vector<std::vector<std::pair<uint32_t, uint32_t>>> nblocks(cnt);
+    std::vector<Piece> pieces;
     for (uint32_t s = 0; s < cnt; ++s) {
         uint32_t chrlen = rd32(b, o, ok);
         uint32_t nbc = rd32(b, o, ok);
         if (!ok) return trunc();
-        std::vector<std::pair<uint32_t, uint32_t>> nb(nbc);
+        auto &nb = nblocks[s];
+        nb.resize(nbc);
         for (uint32_t i = 0; i < nbc; ++i) nb[i].first = rd32(b, o, ok);
         for (uint32_t i = 0; i < nbc; ++i) nb[i].second = rd32(b, o, ok);
         if (!ok) return trunc();
@@ -340,37 +361,74 @@ int parse_2bit(HostGenome &g, const std::vector<char> &b, Error &err) {
         size_t pos = 0;
         int64_t bmi = 0;
         while (pos < chrlen) {
-            size_t rs = std::min<size_t>(chrlen - pos, kChunkSize);
-            size_t nbytes = (rs + 3) / 4;
+            const size_t rs = std::min<size_t>(chrlen - pos, kChunkSize);
+            const size_t nbytes = (rs + 3) / 4;
             if (o + nbytes > b.size()) return trunc();
-            const uint8_t *raw = (const uint8_t *)b.data() + o;
+            bmi = std::max<int64_t>(bmi - 1, 0);
+            pieces.push_back({s, pos, rs, o, bmi});
+            while (bmi < (int64_t)nbc && (int64_t)nb[bmi].first - (int64_t)pos <= (int64_t)rs) ++bmi;
             o += nbytes;
+            pos += rs;
+        }
+    }
+    // chunk table
+    const size_t k0 = g.start.size();
+    uint64_t total = g.data.size();
+    for (const Piece &pc : pieces) {
+        if (!g.start.empty() && pc.pos != 0 && g.end.back() != pc.pos) {
+            err = {kBadInput, "search expects chromosome chunks to arrive in order"};
+            return err.code;
+        }
+        g.name_idx.push_back(names[pc.rec]);
+        g.start.push_back(pc.pos);
+        g.end.push_back(pc.pos + pc.rs);
+        total += (pc.rs + 1) / 2;
+        g.boff.push_back(total);
+    }
+    g.data.resize(total, 0);
+    // Pass 2 (all host threads): bases, padding and N runs per chunk
+    auto convert = [&](size_t a, size_t z) {
+        std::vector<uint8_t> cur(kChunkBytes);
+        for (size_t k = a; k < z; ++k) {
+            const Piece &pc = pieces[k];
+            const auto &nb = nblocks[pc.rec];
+            const size_t rs = pc.rs, nbytes = (rs + 3) / 4;
+            const uint8_t *raw = (const uint8_t *)b.data() + pc.raw;
             std::fill(cur.begin(), cur.end(), 0);
             for (size_t i = 0; i < nbytes; ++i) {
                 uint16_t v = b2b4[raw[i]];
                 cur[2 * i] = (uint8_t)v;
                 cur[2 * i + 1] = (uint8_t)(v >> 8);
             }
-            auto setn = [&](size_t a, size_t z, uint8_t v) {  // memsetbit4
-                for (size_t i = a; i < z; ++i) {
+            auto setn = [&](size_t lo, size_t hi, uint8_t v) {  // memsetbit4
+                for (size_t i = lo; i < hi; ++i) {
                     if (i & 1) cur[i >> 1] = (uint8_t)((cur[i >> 1] & 0x0F) | (v << 4));
                     else cur[i >> 1] = (uint8_t)((cur[i >> 1] & 0xF0) | v);
                 }
             };
             if (rs % 4) setn(rs, nbytes * 4, 0);
-            bmi = std::max<int64_t>(bmi - 1, 0);
-            while (bmi < (int64_t)nbc) {
-                int64_t bs = (int64_t)nb[bmi].first - (int64_t)pos;
-                int64_t be = (int64_t)(uint32_t)(nb[bmi].first + nb[bmi].second) - (int64_t)pos;
+            for (int64_t bmi = pc.bmi; bmi < (int64_t)nb.size(); ++bmi) {
+                int64_t bs = (int64_t)nb[bmi].first - (int64_t)pc.pos;
+                int64_t be = (int64_t)(uint32_t)(nb[bmi].first + nb[bmi].second) - (int64_t)pc.pos;
                 if (bs > (int64_t)rs) break;
-                int64_t a = std::max<int64_t>(bs, 0);
-                int64_t z = std::min<int64_t>(std::max<int64_t>(be, 0), (int64_t)rs);
-                if (a < z) setn((size_t)a, (size_t)z, 0xF);
-                ++bmi;
+                int64_t lo = std::max<int64_t>(bs, 0);
+                int64_t hi = std::min<int64_t>(std::max<int64_t>(be, 0), (int64_t)rs);
+                if (lo < hi) setn((size_t)lo, (size_t)hi, 0xF);
             }
-            if (g.add_chunk(names[s], pos, pos + rs, cur.data(), err)) return err.code;
-            pos += rs;
+            std::memcpy(g.data.data() + g.boff[k0 + k], cur.data(), (rs + 1) / 2);
         }
+    };
+    const size_t np = pieces.size();
+    const unsigned nt = std::max(1u, std::min(std::thread::hardware_concurrency(), 32u));
+    if (nt == 1 || np < 64) {
+        convert(0, np);
+    } else {
+        std::vector<std::thread> th;
+        for (unsigned t = 0; t < nt; ++t) {
+            const size_t lo = np * t / nt, hi = np * (t + 1) / nt;
+            if (lo < hi) th.emplace_back(convert, lo, hi);
+        }
+        for (auto &x : th) x.join();
     }
     return kOk;
 }
@@ -415,8 +473,7 @@ int load_genome_path(HostGenome &g, const std::string &path, Error &err) {
         return err.code;
     }
     if (fv.p[0] == '>') return parse_fasta(g, fv.p, fv.n, err);
-    buf.assign(fv.p, fv.p + fv.n);
-    return parse_2bit(g, buf, err);
+    return parse_2bit(g, FileBytes{fv.p, fv.n}, err);
 }
 
 bool Tuner::enabled() const {

@@ -229,3 +229,32 @@ def test_fasta_loader_matches_chunks(cof_mod, tmp_path):
     ta, na = a.search(*args, chunks_per_search=3)
     tb, nb = b.search(*args, chunks_per_search=3)
     assert ta == tb and na == nb > 0
+
+
+def test_2bit_loader_matches_fasta(cof_mod, oracle_mod, tmp_path):
+    # records of odd lengths, N runs crossing 64 Knt chunk boundaries and
+    # several runs per chunk; an all-N pattern in raw mode lists every window
+    # with its cells, so equal raw streams mean equal genomes
+    import twobit
+    rng = random.Random(21)
+    recs = []
+    for r, n in enumerate((70001, 140003, 3)):
+        seq = [rng.choice("ACGTacgt") for _ in range(n)]
+        for a, b in ((65530, 65541), (100, 130), (131060, 131090)):
+            for i in range(a, min(b, n)):
+                seq[i] = "N"
+        recs.append((f"chr{r}", "".join(seq)))
+    fa, tb = tmp_path / "g.fa", tmp_path / "g.2bit"
+    with open(fa, "w") as f:
+        for name, seq in recs:
+            f.write(">" + name + "\n")
+            for i in range(0, len(seq), 61):
+                f.write(seq[i:i + 61].upper() + "\n")
+    twobit.write_2bit(str(tb), recs)
+    a, b = cof_mod.Genome(str(tb)), cof_mod.Genome(str(fa))
+    assert a.n_nucl == b.n_nucl == sum(len(s) for _, s in recs)
+    ra, na = a.search("N" * 8, ["N" * 8], 7, raw=True)
+    rb, nb = b.search("N" * 8, ["N" * 8], 7, raw=True)
+    ref, nref = oracle_mod.OracleGenome(str(tb)).search("N" * 8, ["N" * 8], 7, raw=True)
+    assert na == nb == nref > 0
+    assert sorted(ra.split("\n")) == sorted(ref.split("\n"))
