@@ -836,7 +836,7 @@ int Engine::run_popcount(const std::vector<Request> &reqs, std::vector<Result> &
         lens.erase(std::unique(lens.begin(), lens.end()), lens.end());
         // scan segments: one per batch, the union of the members' window
         // ranges; verify re-applies each length's own head-overlap threshold
-        proto.seg_begin = (uint32_t)segs.size();
+        std::vector<ScanSeg> kseg;
         uint64_t tiles = 0;
         for (size_t bi = 0; bi < batches.size(); ++bi) {
             const BatchDev &b = batches[bi];
@@ -860,14 +860,9 @@ int Engine::run_popcount(const std::vector<Request> &reqs, std::vector<Result> &
             sgm.tile_begin = tiles;
             sgm.batch = (uint32_t)bi;
             tiles += (sgm.hi - sgm.w0 * 32 + 1023) / 1024;
-            segs.push_back(sgm);
+            kseg.push_back(sgm);
         }
-        proto.seg_end = (uint32_t)segs.size();
-        if (proto.seg_end - proto.seg_begin > (uint32_t)kMaxSegs) {
-            err = {kUnsupported, "too many search batches for one scan launch"};
-            return err.code;
-        }
-        if (proto.seg_end == proto.seg_begin) continue;
+        if (kseg.empty()) continue;
         // scan form of the members (window cells from their offset), ordered
         // by care mask and offset
         struct Comp {
@@ -893,30 +888,44 @@ int Engine::run_popcount(const std::vector<Request> &reqs, std::vector<Result> &
         std::stable_sort(comp.begin(), comp.end(), [](const Comp &x, const Comp &y) {
             return x.fp.care != y.fp.care ? x.fp.care < y.fp.care : x.off < y.off;
         });
-        // groups of at most kMaxCareClasses classes
-        ScanGroup g = proto;
-        g.pat_begin = (uint32_t)fpats.size();
-        g.n_class = 0;
-        for (size_t i = 0; i < comp.size(); ++i) {
-            const uint32_t care = comp[i].fp.care, o = comp[i].off;
-            const bool new_class = g.n_class == 0 || g.cls[g.n_class - 1].care != care ||
-                                   g.cls[g.n_class - 1].off != o;
-            if (new_class && g.n_class == (uint32_t)kMaxCareClasses) {
-                g.pat_end = (uint32_t)fpats.size();
-                groups.push_back(g);
-                g = proto;
-                g.pat_begin = (uint32_t)fpats.size();
-                g.n_class = 0;
+        // a scan group stages at most kMaxSegs batch segments in shared
+        // memory: longer batch lists (small chunks_per_search on a large
+        // genome) split into groups with the same patterns, tiles counted
+        // from each group's first segment
+        for (size_t s0 = 0; s0 < kseg.size(); s0 += kMaxSegs) {
+            const size_t s1 = std::min(kseg.size(), s0 + (size_t)kMaxSegs);
+            proto.seg_begin = (uint32_t)segs.size();
+            for (size_t k = s0; k < s1; ++k) {
+                ScanSeg sgm = kseg[k];
+                sgm.tile_begin -= kseg[s0].tile_begin;
+                segs.push_back(sgm);
             }
-            const uint32_t rel = (uint32_t)fpats.size() - g.pat_begin;
-            if (g.n_class == 0 || g.cls[g.n_class - 1].care != care || g.cls[g.n_class - 1].off != o)
-                g.cls[g.n_class++] = CareClass{care, rel, rel, o};
-            g.cls[g.n_class - 1].pat_end = rel + 1;
-            fpats.push_back(comp[i].fp);
-            fast2exact.push_back(comp[i].exact);
+            proto.seg_end = (uint32_t)segs.size();
+            // groups of at most kMaxCareClasses classes
+            ScanGroup g = proto;
+            g.pat_begin = (uint32_t)fpats.size();
+            g.n_class = 0;
+            for (size_t i = 0; i < comp.size(); ++i) {
+                const uint32_t care = comp[i].fp.care, o = comp[i].off;
+                const bool new_class = g.n_class == 0 || g.cls[g.n_class - 1].care != care ||
+                                       g.cls[g.n_class - 1].off != o;
+                if (new_class && g.n_class == (uint32_t)kMaxCareClasses) {
+                    g.pat_end = (uint32_t)fpats.size();
+                    groups.push_back(g);
+                    g = proto;
+                    g.pat_begin = (uint32_t)fpats.size();
+                    g.n_class = 0;
+                }
+                const uint32_t rel = (uint32_t)fpats.size() - g.pat_begin;
+                if (g.n_class == 0 || g.cls[g.n_class - 1].care != care || g.cls[g.n_class - 1].off != o)
+                    g.cls[g.n_class++] = CareClass{care, rel, rel, o};
+                g.cls[g.n_class - 1].pat_end = rel + 1;
+                fpats.push_back(comp[i].fp);
+                fast2exact.push_back(comp[i].exact);
+            }
+            g.pat_end = (uint32_t)fpats.size();
+            groups.push_back(g);
         }
-        g.pat_end = (uint32_t)fpats.size();
-        groups.push_back(g);
     }
 
     TablePack tp;

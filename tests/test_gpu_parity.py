@@ -258,3 +258,19 @@ def test_2bit_loader_matches_fasta(cof_mod, oracle_mod, tmp_path):
     ref, nref = oracle_mod.OracleGenome(str(tb)).search("N" * 8, ["N" * 8], 7, raw=True)
     assert na == nb == nref > 0
     assert sorted(ra.split("\n")) == sorted(ref.split("\n"))
+
+
+def test_more_batches_than_one_scan_group_holds(cof_mod, oracle_mod):
+    # ~300 batches (2 chunks each): more batch segments than a scan group
+    # stages, as with chunks_per_search 64 (the CLI's C) on a large genome
+    rng = random.Random(31)
+    _, records = randgen.random_genome(rng, 3, 12000, 16000)
+    pats = ["".join(rng.choice("ACGT") for _ in range(20)) + "NNN" for _ in range(3)]
+    for p in pats:
+        randgen.plant_sites(rng, records, p, "N" * 21 + "RG", 10, 2)
+    chunks = randgen.chunk_records(rng, records, 160)
+    assert len(chunks) > 250
+    g, o = _both(cof_mod, oracle_mod, chunks)
+    text, n = g.search("N" * 21 + "RG", pats, 4, chunks_per_search=2)
+    ref, nref = o.search("N" * 21 + "RG", pats, 4, chunks_per_search=2)
+    assert _rows(text) == _rows(ref) and n == nref > 0
