@@ -60,7 +60,8 @@ def parse():
     ap.add_argument("--serving-requests", type=int, default=64)
     ap.add_argument("--serving-rate", type=float, default=200.0, help="arrivals per second")
     ap.add_argument("--no-extras", action="store_true",
-                    help="skip the batched mixed-PAM, serving and bulge measurements")
+                    help="skip the batched mixed-PAM, serving, bulge and whole-process CLI "
+                         "measurements")
     ap.add_argument("--only-bulge", action="store_true",
                     help="run only the bulge-path measurement (10 Mbp x 20 guides, mm<=4, "
                          "DNA/RNA bulges<=2) and print it")
@@ -354,6 +355,50 @@ class CpuSample:
                            f"search_compute_cpu + writer, {self.cores} threads, {t:.1f} s")
 
 
+def bench_cli(cfg, n_rows, runs=2):
+    """The command line tool as a fresh process, the way main.rs is run:
+    `cof-offinder input.txt G out.txt` reads the genome from a .2bit file,
+    uploads it, searches, and writes the rows and the .log summary.  The
+    .2bit file is written once beforehand (page cache warm for every run)."""
+    import shutil
+    import tempfile
+    import build as cof_build
+    d = tempfile.mkdtemp(prefix="cof_cli_")
+    try:
+        t0 = time.perf_counter()
+        path2 = os.path.join(d, "genome.2bit")
+        cfg["genome"].write_2bit(path2)
+        t_write = time.perf_counter() - t0
+        inp = os.path.join(d, "input.txt")
+        with open(inp, "w") as f:
+            f.write(path2 + "\n" + cfg["filter"] + "\n")
+            for p in cfg["patterns"]:
+                f.write(f"{p} {cfg['max_mismatches']}\n")
+        out = os.path.join(d, "out.txt")
+        secs = []
+        for _ in range(runs):
+            t1 = time.perf_counter()
+            r = subprocess.run([cof_build.CLI, inp, "G", out], capture_output=True, text=True,
+                               timeout=600)
+            secs.append(time.perf_counter() - t1)
+            if r.returncode:
+                raise RuntimeError("cof-offinder failed: " + r.stderr.strip())
+        rows = 0
+        with open(out, "rb") as f:
+            for line in f:
+                rows += not line.startswith(b"#")
+        return {"workload": "cof-offinder input.txt G out.txt, " + cfg["name"],
+                "seconds": min(secs), "runs_s": secs, "rows": rows,
+                "rows_match_c_abi": rows == n_rows,
+                "genome_2bit_bytes": os.path.getsize(path2),
+                "output_bytes": os.path.getsize(out),
+                "includes": "process start, CUDA context, .2bit read + convert, upload, "
+                            "search, output + .log written",
+                "genome_2bit_write_s": t_write}
+    finally:
+        shutil.rmtree(d, ignore_errors=True)
+
+
 def cpu_baseline(cfg, target_s, n_threads=0):
     smp = CpuSample(cfg, target_s, n_threads)
     v, t = smp.run()
@@ -548,6 +593,7 @@ def main():
         line["serving_small_requests"] = bench_serving(cof, g, n_nt, 4 * args.serving_requests,
                                                        2000.0, seed=8, max_guides=4, max_mm=3)
         line["bulge"] = bench_bulge(cof, local, 3, args.bulge_scale)
+        line["cli_whole_process"] = bench_cli(cfg, rows_per_step)
     if not args.no_cpu_baseline and world == 1:
         base, _ = cpu_baseline(cfg, args.cpu_sample_s)
         line["cpu_baseline"] = base

@@ -76,6 +76,42 @@ class SynthGenome:
                 for s in range(0, len(chars), line_len):
                     f.write(chars[s:s + line_len].tobytes() + b"\n")
 
+    def write_2bit(self, path):
+        """UCSC .2bit v0 (the format read_2bit.rs reads): bases packed 2 bits
+        each, T=0 C=1 A=2 G=3, first base in the high bits; N runs as N
+        blocks.  The synthetic records hold only A, C, G, T and N."""
+        import struct
+        to2 = np.zeros(16, dtype=np.uint8)
+        to2[[1, 2, 4, 8]] = [0, 1, 2, 3]
+        blocks = []
+        for rec in self.records:
+            d = np.flatnonzero(rec == 15)
+            if len(d):
+                br = np.flatnonzero(np.diff(d) != 1)
+                starts = d[np.concatenate(([0], br + 1))]
+                ends = d[np.concatenate((br, [len(d) - 1]))] + 1
+            else:
+                starts = ends = d
+            blocks.append((starts.astype("<u4"), (ends - starts).astype("<u4")))
+        off = 16 + sum(1 + len(n) + 4 for n in self.names)
+        with open(path, "wb") as f:
+            f.write(struct.pack("<IIII", 0x1A412743, 0, len(self.names), 0))
+            for name, rec, (st, sz) in zip(self.names, self.records, blocks):
+                f.write(bytes([len(name)]) + name.encode() + struct.pack("<I", off))
+                off += 16 + 8 * len(st) + (len(rec) + 3) // 4
+            for rec, (st, sz) in zip(self.records, blocks):
+                f.write(struct.pack("<II", len(rec), len(st)) + st.tobytes() + sz.tobytes() +
+                        struct.pack("<II", 0, 0))
+                c = to2[rec]
+                n4 = len(c) // 4 * 4
+                v = c[:n4].view(">u4")
+                packed = ((v >> 18) & 0xC0) | ((v >> 12) & 0x30) | ((v >> 6) & 0xC) | (v & 3)
+                f.write(packed.astype(np.uint8).tobytes())
+                if n4 < len(c):
+                    t = np.zeros(4, dtype=np.uint8)
+                    t[:len(c) - n4] = c[n4:]
+                    f.write(bytes([(t[0] << 6) | (t[1] << 4) | (t[2] << 2) | t[3]]))
+
     def site(self, rec, pos, length):
         return bytes(_CHARS[self.records[rec][pos:pos + length]]).decode()
 

@@ -154,3 +154,24 @@ def test_reference_kernel_launcher_loads():
         assert hasattr(lib, sym)
     assert os.path.exists(ref_gpu.popcount_cubin(23))
     assert os.path.exists(ref_gpu.myers_cubin(23, 3, 4, 2, 2))
+
+
+def test_synth_2bit_writer(oracle_mod, tmp_path):
+    # the benchmark's numpy .2bit writer: byte-identical to the plain test
+    # writer, and read by the oracle as the same genome as its FASTA
+    # (odd lengths, a record that is all N, N runs at both ends)
+    import numpy as np
+    import synth
+    import twobit
+    rng = np.random.default_rng(9)
+    gen = synth.make_genome(rng, [70001, 7, 3, 64, 5], n_runs=[(0, 500), (0, 37), (3, 10)])
+    gen.records[2][:] = 15
+    gen.records[4][0] = gen.records[4][-1] = 15
+    gen.write_2bit(str(tmp_path / "a.2bit"))
+    twobit.write_2bit(str(tmp_path / "b.2bit"),
+                      [(n, bytes(synth._CHARS[r]).decode()) for n, r in zip(gen.names, gen.records)])
+    assert (tmp_path / "a.2bit").read_bytes() == (tmp_path / "b.2bit").read_bytes()
+    gen.write_fasta(str(tmp_path / "a.fa"))
+    a = oracle_mod.OracleGenome(str(tmp_path / "a.2bit"))
+    b = oracle_mod.OracleGenome(str(tmp_path / "a.fa"))
+    assert a.decode() == b.decode()
