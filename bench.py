@@ -65,6 +65,8 @@ def parse():
     ap.add_argument("--only-bulge", action="store_true",
                     help="run only the bulge-path measurement (10 Mbp x 20 guides, mm<=4, "
                          "DNA/RNA bulges<=2) and print it")
+    ap.add_argument("--only-cli", action="store_true",
+                    help="run only the whole-process CLI measurement and print it")
     ap.add_argument("--bulge-scale", type=float, default=0.02,
                     help="bulge genome factor (1.0 = 500 Mbp; ~720 k rows per Mbp)")
     return ap.parse_args()
@@ -375,21 +377,27 @@ def bench_cli(cfg, n_rows, runs=2):
             for p in cfg["patterns"]:
                 f.write(f"{p} {cfg['max_mismatches']}\n")
         out = os.path.join(d, "out.txt")
-        secs = []
+        secs, stages = [], []
+        env = dict(os.environ, COF_CLI_TIMES="1")
         for _ in range(runs):
             t1 = time.perf_counter()
             r = subprocess.run([cof_build.CLI, inp, "G", out], capture_output=True, text=True,
-                               timeout=600)
+                               timeout=600, env=env)
             secs.append(time.perf_counter() - t1)
             if r.returncode:
                 raise RuntimeError("cof-offinder failed: " + r.stderr.strip())
+            for ln in r.stderr.splitlines():
+                if ln.startswith("stage seconds:"):
+                    f = ln.split(":", 1)[1].split()
+                    stages.append({f[i]: float(f[i + 1]) for i in range(0, len(f), 2)})
         rows = 0
         with open(out, "rb") as f:
             for line in f:
                 rows += not line.startswith(b"#")
         return {"workload": "cof-offinder input.txt G out.txt, " + cfg["name"],
                 "seconds": min(secs), "runs_s": secs, "rows": rows,
-                "rows_match_c_abi": rows == n_rows,
+                "stage_s": stages[secs.index(min(secs))] if len(stages) == len(secs) else None,
+                "rows_match_c_abi": None if n_rows is None else rows == n_rows,
                 "genome_2bit_bytes": os.path.getsize(path2),
                 "output_bytes": os.path.getsize(out),
                 "includes": "process start, CUDA context, .2bit read + convert, upload, "
@@ -506,6 +514,13 @@ def main():
     t0 = time.perf_counter()
     cfg = make_workload(args, rank)
     t_gen = time.perf_counter() - t0
+    if args.only_cli:
+        if rank == 0:
+            print(json.dumps({"cli_whole_process": bench_cli(cfg, None, max(1, args.steps))}),
+                  flush=True)
+        if dist:
+            dist.destroy_process_group()
+        return
     gen = cfg["genome"]
     n_nt = gen.n_nucl
     g = cof.Genome(device=local)
@@ -569,7 +584,9 @@ def main():
         "e2e": {"value": e2e, "unit": UNIT, "ms_per_step": e2e_s * 1e3 / args.steps,
                 "h2d_bytes_per_step": 100 * 23 * 2 + 4096,
                 "d2h_bytes_per_step": text_bytes},
-        "roofline": {"bound": "alu", "kernel": "scan_kernel",
+        "roofline": {"bound": "alu",
+                     "kernel": "scan_warp_kernel" if g.tuning()["last"].startswith("warp-")
+                               else "scan_kernel",
                      "achieved": achieved, "peak": peaks["popc_per_s"], "unit": "pairs/s",
                      "frac": achieved / peaks["popc_per_s"], "traffic": TRAFFIC,
                      "peak_kind": "measured live: POPC results/s of this GPU (XU pipe); "

@@ -13,6 +13,7 @@
 
 #include <chrono>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <ctime>
 #include <fstream>
@@ -110,9 +111,22 @@ int main(int argc, char **argv) {
     if (lineno < 2) die("Input file must contain at least 3 lines");
     if (!have_mm) die("Input file must contain at least 1 pattern line");
 
+    // COF_CLI_TIMES=1: seconds per stage on stderr (not part of main.rs's output)
+    const char *times_env = std::getenv("COF_CLI_TIMES");
+    const bool times = times_env && *times_env && std::strcmp(times_env, "0") != 0;
+    auto lap = [t = t0]() mutable {
+        const auto now = std::chrono::steady_clock::now();
+        const double d = std::chrono::duration<double>(now - t).count();
+        t = now;
+        return d;
+    };
+    const double t_input = lap();
     cof_genome *g = nullptr;
     if (cof_genome_create(0, &g)) die(cof_last_error());
     if (cof_genome_load(g, genome.c_str())) die(cof_last_error());
+    const double t_load = lap();
+    if (cof_genome_upload(g)) die(cof_last_error());
+    const double t_upload = lap();
     std::vector<const char *> pp;
     for (auto &p : pats) pp.push_back(p.c_str());
     cof_request r{};
@@ -127,11 +141,13 @@ int main(int argc, char **argv) {
     r.chunks_per_search = dev[0] == 'C' ? 64 : 16384;
     cof_result res{};
     if (cof_search(g, &r, &res)) die(cof_last_error());
+    const double t_search = lap();
     FILE *out = out_path == "-" ? stdout : std::fopen(out_path.c_str(), "wb");
     if (!out) die("cannot open output file " + out_path);
     std::fputs(COF_HEADER, out);
     std::fwrite(res.text, 1, res.text_len, out);
     if (out != stdout) std::fclose(out);
+    const double t_write = lap();
     const double secs =
         std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
     std::cerr << "Completed in " << secs << "s\n";
@@ -164,5 +180,9 @@ int main(int argc, char **argv) {
     }
     cof_result_free(&res);
     cof_genome_free(g);
+    if (times)
+        std::fprintf(stderr, "stage seconds: input %.4f load %.4f upload %.4f search %.4f "
+                             "write %.4f free %.4f\n",
+                     t_input, t_load, t_upload, t_search, t_write, lap());
     return 0;
 }

@@ -9,6 +9,7 @@
 #include <map>
 #include <mutex>
 #include <string>
+#include <thread>
 #include <unordered_map>
 #include <vector>
 
@@ -192,6 +193,9 @@ class Engine {
     int run_bulge(const std::vector<Request> &reqs, std::vector<Result> &out, Error &err);
     int run_raw(const Request &req, Result &out, Error &err);
     int device_;
+    // creates the device's CUDA context while the caller reads the genome
+    // file; joined before the first device call
+    std::thread warm_;
     HostGenome host_;
     DeviceGenome *dev_ = nullptr;
     StageTimes times_;

@@ -172,6 +172,7 @@ struct ScanParams {
     const uint64_t *item_begin;  // per group: first work item; [n_groups] = total
     uint32_t n_groups;
     uint32_t span_tiles;         // 1024-start tiles per work item
+    uint32_t n_pats;             // patterns of all groups (the table at pats)
     Hit *hits;
     uint32_t hit_cap;
     Counters *ctr;
@@ -195,7 +196,9 @@ __device__ __forceinline__ FastPattern lds_pattern(uint32_t saddr) {
 
 // Compares the queued windows (32 * kCpt at most, kCpt per lane) with every
 // pattern of the group and appends the hits.  kSmem: the pattern table is in
-// shared memory (all but the largest groups).
+// shared memory (all but the largest groups).  kPair selects how a lane
+// reduces its kCpt mismatch counts per pattern: 1 one minimum chain, 2 two
+// patterns per step (two chains), 4 three-input minima (__vimin3_s32).
 template <int kCpt, int kPair, bool kSmem>
 __device__ __forceinline__ void flush_body(const uint4 *q, int n, const FastPattern *pt,
                                            const ScanGroup &G, uint32_t batch,
@@ -240,6 +243,23 @@ __device__ __forceinline__ void flush_body(const uint4 *q, int n, const FastPatt
                 if (m1 <= f1.k) emit(p + 1, f1);
             }
         }
+        if (kPair == 4) {  // minimum of three per instruction, depth log3(kCpt)
+            for (; p < K.pat_end; ++p) {
+                const FastPattern f0 = load(p);
+                int c[kCpt];
+#pragma unroll
+                for (int j = 0; j < kCpt; ++j)
+                    c[j] = (int)__popc((mh[j] ^ f0.h) | (ml[j] ^ f0.l) | ms[j]);
+#pragma unroll
+                for (int w = 1; w < kCpt; w *= 3)
+#pragma unroll
+                    for (int j = 0; j < kCpt; j += 3 * w)
+                        c[j] = j + 2 * w < kCpt ? __vimin3_s32(c[j], c[j + w], c[j + 2 * w])
+                               : j + w < kCpt   ? min(c[j], c[j + w])
+                                                : c[j];
+                if (c[0] <= f0.k) emit(p, f0);
+            }
+        }
         for (; p < K.pat_end; ++p) {
             const FastPattern f0 = load(p);
             int m0 = 64;
@@ -268,6 +288,76 @@ __device__ __forceinline__ void flush(const uint4 *q, int n, const FastPattern *
     flush_queue<kCpt, kPair>(q, n, pt, pt == spat, G, batch, P, lane);
 }
 
+// One 1024-start tile of a scan segment for one warp: PAM prefilter of the
+// lane's 32 starts, then the passing starts are drained into the warp's
+// queue, which is compared with the group's patterns whenever it fills (or
+// the batch changes: hits carry their batch).
+template <int kCpt, int kPair>
+__device__ __forceinline__ void scan_tile(const ScanParams &P, const ScanGroup &G,
+                                          const ScanSeg &sgm, uint64_t tile, uint4 *q, int &qn,
+                                          uint32_t &qbatch, const FastPattern *pt, bool smem,
+                                          uint32_t npat, unsigned long long &ncand,
+                                          unsigned long long &npairs, int lane) {
+    constexpr int kQCap = 32 * kCpt;
+    const uint32_t lt_mask = (1u << lane) - 1u;
+    if (sgm.batch != qbatch) {
+        if (qn) {
+            __syncwarp();
+            flush_queue<kCpt, kPair>(q, qn, pt, smem, G, qbatch, P, lane);
+            __syncwarp();
+            qn = 0;
+        }
+        qbatch = sgm.batch;
+    }
+    const uint64_t w = sgm.w0 + (tile - sgm.tile_begin) * 32 + lane;
+    const uint32_t h0 = __ldg(P.H + w), h1 = __ldg(P.H + w + 1);
+    const uint32_t l0 = __ldg(P.L + w), l1 = __ldg(P.L + w + 1);
+    const uint32_t s0 = __ldg(P.S + w), s1 = __ldg(P.S + w + 1);
+    // window starts 32w + k in [lo, hi)
+    const uint64_t p0 = w * 32;
+    uint32_t m = 0xFFFFFFFFu;
+    if (p0 < sgm.lo) m = (sgm.lo - p0 >= 32) ? 0u : (m << (uint32_t)(sgm.lo - p0));
+    if (p0 + 32 > sgm.hi) m = (sgm.hi <= p0) ? 0u : (m & (0xFFFFFFFFu >> (uint32_t)(32 - (sgm.hi - p0))));
+    for (uint32_t c = 0; c < G.n_pam && m; ++c) {
+        const PamCell pc = G.pam[c];
+        const uint32_t h = __funnelshift_r(h0, h1, pc.cell);
+        const uint32_t l = __funnelshift_r(l0, l1, pc.cell);
+        const uint32_t s = __funnelshift_r(s0, s1, pc.cell);
+        const uint32_t t0 = (l & pc.fc) | (~l & pc.fa);
+        const uint32_t t1 = (l & pc.ft) | (~l & pc.fg);
+        m &= ((h & t1) | (~h & t0)) & ~s;
+    }
+    const uint32_t nm = __popc(m);
+    ncand += nm;
+    npairs += (unsigned long long)nm * npat;
+    // drain PAM-passing starts into the warp queue, one per lane per step
+    while (__any_sync(0xFFFFFFFFu, m)) {
+        const bool has = m != 0;
+        const uint32_t bal = __ballot_sync(0xFFFFFFFFu, has);
+        if (has) {
+            const uint32_t k = __ffs(m) - 1;
+            m &= m - 1;
+            const int slot = qn + __popc(bal & lt_mask);
+            q[slot] = make_uint4((uint32_t)(p0 + k - sgm.base), __funnelshift_r(h0, h1, k),
+                                 __funnelshift_r(l0, l1, k), __funnelshift_r(s0, s1, k));
+        }
+        qn += __popc(bal);
+        if (qn >= kQCap) {
+            // full pass over kQCap windows; the (< 32) windows beyond it
+            // move to the front of the queue
+            __syncwarp();
+            flush_queue<kCpt, kPair>(q, kQCap, pt, smem, G, qbatch, P, lane);
+            const int rest = qn - kQCap;
+            uint4 e = make_uint4(0, 0, 0, 0);
+            if (lane < rest) e = q[kQCap + lane];
+            __syncwarp();
+            if (lane < rest) q[lane] = e;
+            __syncwarp();
+            qn = rest;
+        }
+    }
+}
+
 // Persistent scan: CTAs pull work items -- a span of kSpanTiles tiles of one
 // scan group -- from a global counter, so groups of very different sizes
 // (few or many patterns, sparse or dense PAMs) share the GPU evenly.  A CTA
@@ -290,7 +380,6 @@ scan_kernel(ScanParams P) {
     uint4 *q = queues + warp * kQSlots;
     int qn = 0;
     uint32_t qbatch = 0xFFFFFFFFu;
-    const uint32_t lt_mask = (1u << lane) - 1u;
     unsigned long long ncand = 0, npairs = 0;
     uint32_t cur_g = 0xFFFFFFFFu, nseg = 0, npat = 0;
     uint64_t g_tiles = 0;
@@ -343,63 +432,8 @@ scan_kernel(ScanParams P) {
         uint32_t sidx = 0;
         for (uint64_t tile = t_begin + warp; tile < t_end; tile += kScanWarps) {
             while (sidx + 1 < nseg && tile >= ssegs[sidx + 1].tile_begin) ++sidx;
-            const ScanSeg &sgm = ssegs[sidx];
-            if (sgm.batch != qbatch) {
-                if (qn) {
-                    __syncwarp();
-                    flush<kCpt, kPair>(q, qn, pt, spat, sg, qbatch, P, lane);
-                    __syncwarp();
-                    qn = 0;
-                }
-                qbatch = sgm.batch;
-            }
-            const uint64_t w = sgm.w0 + (tile - sgm.tile_begin) * 32 + lane;
-            const uint32_t h0 = __ldg(P.H + w), h1 = __ldg(P.H + w + 1);
-            const uint32_t l0 = __ldg(P.L + w), l1 = __ldg(P.L + w + 1);
-            const uint32_t s0 = __ldg(P.S + w), s1 = __ldg(P.S + w + 1);
-            // window starts 32w + k in [lo, hi)
-            const uint64_t p0 = w * 32;
-            uint32_t m = 0xFFFFFFFFu;
-            if (p0 < sgm.lo) m = (sgm.lo - p0 >= 32) ? 0u : (m << (uint32_t)(sgm.lo - p0));
-            if (p0 + 32 > sgm.hi) m = (sgm.hi <= p0) ? 0u : (m & (0xFFFFFFFFu >> (uint32_t)(32 - (sgm.hi - p0))));
-            for (uint32_t c = 0; c < sg.n_pam && m; ++c) {
-                const PamCell pc = sg.pam[c];
-                const uint32_t h = __funnelshift_r(h0, h1, pc.cell);
-                const uint32_t l = __funnelshift_r(l0, l1, pc.cell);
-                const uint32_t s = __funnelshift_r(s0, s1, pc.cell);
-                const uint32_t t0 = (l & pc.fc) | (~l & pc.fa);
-                const uint32_t t1 = (l & pc.ft) | (~l & pc.fg);
-                m &= ((h & t1) | (~h & t0)) & ~s;
-            }
-            const uint32_t nm = __popc(m);
-            ncand += nm;
-            npairs += (unsigned long long)nm * npat;
-            // drain PAM-passing starts into the warp queue, one per lane per step
-            while (__any_sync(0xFFFFFFFFu, m)) {
-                const bool has = m != 0;
-                const uint32_t bal = __ballot_sync(0xFFFFFFFFu, has);
-                if (has) {
-                    const uint32_t k = __ffs(m) - 1;
-                    m &= m - 1;
-                    const int slot = qn + __popc(bal & lt_mask);
-                    q[slot] = make_uint4((uint32_t)(p0 + k - sgm.base), __funnelshift_r(h0, h1, k),
-                                         __funnelshift_r(l0, l1, k), __funnelshift_r(s0, s1, k));
-                }
-                qn += __popc(bal);
-                if (qn >= kQCap) {
-                    // full pass over kQCap windows; the (< 32) windows beyond it
-                    // move to the front of the queue
-                    __syncwarp();
-                    flush<kCpt, kPair>(q, kQCap, pt, spat, sg, qbatch, P, lane);
-                    const int rest = qn - kQCap;
-                    uint4 e = make_uint4(0, 0, 0, 0);
-                    if (lane < rest) e = q[kQCap + lane];
-                    __syncwarp();
-                    if (lane < rest) q[lane] = e;
-                    __syncwarp();
-                    qn = rest;
-                }
-            }
+            scan_tile<kCpt, kPair>(P, sg, ssegs[sidx], tile, q, qn, qbatch, pt, pt == spat, npat,
+                                   ncand, npairs, lane);
         }
         __syncthreads();  // s_item / s_group are rewritten by the next fetch
     }
@@ -418,10 +452,92 @@ scan_kernel(ScanParams P) {
     }
 }
 
+// Persistent scan with per-warp work items: each warp pulls its own span of
+// kSpanTiles tiles from the global counter, so a warp never waits at a CTA
+// barrier while another warp of its CTA compares a full queue.  The pattern
+// table of all groups is staged in shared memory once, up to kSmemPatterns
+// patterns; a group whose patterns lie beyond that prefix reads them from
+// global memory.  Group and segment descriptors are read through L1.
+template <int kCpt, int kScanWarps, int kMinBlocks, int kPair>
+__global__ void __launch_bounds__(kScanWarps * 32, kMinBlocks)
+scan_warp_kernel(ScanParams P) {
+    constexpr int kQSlots = 32 * kCpt + 32;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    uint4 *queues = reinterpret_cast<uint4 *>(smem_raw);
+    FastPattern *spat = reinterpret_cast<FastPattern *>(queues + kScanWarps * kQSlots);
+    const uint32_t n_staged = min(P.n_pats, (uint32_t)kSmemPatterns);
+    for (uint32_t i = threadIdx.x; i < n_staged; i += blockDim.x) spat[i] = P.pats[i];
+    __syncthreads();
+
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    uint4 *q = queues + warp * kQSlots;
+    int qn = 0;
+    uint32_t qbatch = 0xFFFFFFFFu;
+    unsigned long long ncand = 0, npairs = 0;
+    uint32_t cur_g = 0xFFFFFFFFu, nseg = 0, npat = 0;
+    uint64_t g_tiles = 0;
+    const ScanGroup *G = P.groups;
+    const ScanSeg *segs = P.segs;
+    const FastPattern *pt = spat;
+    bool smem = true;
+    const uint64_t total_items = P.item_begin[P.n_groups];
+
+    while (true) {
+        unsigned long long it = 0;
+        if (lane == 0) it = atomicAdd(&P.ctr->next_item, 1ull);
+        it = __shfl_sync(0xFFFFFFFFu, it, 0);
+        if (it >= total_items) break;
+        uint32_t lo = 0, hi = P.n_groups;
+        while (hi - lo > 1) {
+            const uint32_t mid = (lo + hi) >> 1;
+            if (__ldg(P.item_begin + mid) <= it) lo = mid; else hi = mid;
+        }
+        if (lo != cur_g) {
+            if (qn) {  // the queue belongs to the previous group's patterns
+                __syncwarp();
+                flush_queue<kCpt, kPair>(q, qn, pt, smem, *G, qbatch, P, lane);
+                __syncwarp();
+                qn = 0;
+            }
+            cur_g = lo;
+            G = P.groups + lo;
+            segs = P.segs + G->seg_begin;
+            nseg = G->seg_end - G->seg_begin;
+            npat = G->pat_end - G->pat_begin;
+            smem = G->pat_end <= n_staged;
+            pt = (smem ? spat : P.pats) + G->pat_begin;
+            const ScanSeg &last = segs[nseg - 1];
+            g_tiles = last.tile_begin + ((last.hi - last.w0 * 32 + 1023) >> 10);
+            qbatch = 0xFFFFFFFFu;
+        }
+        const uint64_t t_begin = (it - P.item_begin[lo]) * P.span_tiles;
+        const uint64_t t_end = min(t_begin + P.span_tiles, g_tiles);
+        uint32_t sidx = 0;
+        for (uint64_t tile = t_begin; tile < t_end; ++tile) {
+            while (sidx + 1 < nseg && tile >= segs[sidx + 1].tile_begin) ++sidx;
+            scan_tile<kCpt, kPair>(P, *G, segs[sidx], tile, q, qn, qbatch, pt, smem, npat, ncand,
+                                   npairs, lane);
+        }
+    }
+    if (qn) {
+        __syncwarp();
+        flush_queue<kCpt, kPair>(q, qn, pt, smem, *G, qbatch, P, lane);
+    }
+    for (int o = 16; o; o >>= 1) {
+        ncand += __shfl_down_sync(0xFFFFFFFFu, ncand, o);
+        npairs += __shfl_down_sync(0xFFFFFFFFu, npairs, o);
+    }
+    if (lane == 0 && ncand) {
+        atomicAdd(&P.ctr->candidates, ncand);
+        atomicAdd(&P.ctr->pairs, npairs);
+    }
+}
+
 struct ScanVariant {
     int cpt, warps, min_blocks, pair;
     uint32_t span_tiles;
     void (*kernel)(ScanParams);
+    bool per_warp;
     size_t smem() const {
         return (size_t)warps * (32 * cpt + 32) * sizeof(uint4) + kSmemPatterns * sizeof(FastPattern);
     }
@@ -429,7 +545,12 @@ struct ScanVariant {
 
 template <int C, int W, int B, int Q = 1>
 constexpr ScanVariant variant(uint32_t span) {
-    return ScanVariant{C, W, B, Q, span, scan_kernel<C, W, B, Q>};
+    return ScanVariant{C, W, B, Q, span, scan_kernel<C, W, B, Q>, false};
+}
+// span: tiles per warp work item
+template <int C, int W, int B, int Q = 1>
+constexpr ScanVariant warp_variant(uint32_t span) {
+    return ScanVariant{C, W, B, Q, span, scan_warp_kernel<C, W, B, Q>, true};
 }
 
 // Candidate tile shapes (windows per lane x warps x min blocks per SM, and
@@ -437,6 +558,10 @@ constexpr ScanVariant variant(uint32_t span) {
 // genome.  Two patterns per step need registers that only the shapes with
 // fewer blocks per SM have.
 const ScanVariant kScanVariants[] = {
+    // per-warp work items
+    warp_variant<8, 8, 3, 4>(8),  warp_variant<8, 8, 3>(8),  warp_variant<8, 8, 3>(32),
+    warp_variant<16, 8, 2, 4>(8), warp_variant<16, 8, 2>(8), warp_variant<8, 8, 2, 2>(8),
+    // CTA work items
     variant<8, 8, 3>(64),     variant<4, 8, 4>(64),     variant<16, 8, 2>(64),
     variant<8, 4, 6>(32),     variant<16, 4, 4>(32),    variant<4, 16, 2>(128),
     variant<8, 8, 2, 2>(64),  variant<16, 8, 2, 2>(64), variant<8, 4, 4, 2>(32),
@@ -594,8 +719,15 @@ row_write_kernel(GenomeDev G, const Row *__restrict__ rows, const uint32_t *__re
 // device genome + scratch
 // ---------------------------------------------------------------------------
 
-Engine::Engine(int device) : device_(device) {}
+Engine::Engine(int device) : device_(device) {
+    // context creation costs a few hundred ms on a large GPU; it overlaps
+    // the file read that precedes every upload
+    warm_ = std::thread([device] {
+        if (cudaSetDevice(device) == cudaSuccess) cudaFree(nullptr);
+    });
+}
 Engine::~Engine() {
+    if (warm_.joinable()) warm_.join();
     if (dev_) {
         cudaSetDevice(device_);
         delete dev_;
@@ -604,6 +736,7 @@ Engine::~Engine() {
 
 int Engine::upload(Error &err) {
     if (dev_) return kOk;
+    if (warm_.joinable()) warm_.join();
     CU(cudaSetDevice(device_));
     std::unique_ptr<DeviceGenome> d(new DeviceGenome());
     d->device = device_;
@@ -981,6 +1114,7 @@ int Engine::run_popcount(const std::vector<Request> &reqs, std::vector<Result> &
     sp.segs = (const ScanSeg *)tab(o_seg);
     sp.pats = (const FastPattern *)tab(o_fp);
     sp.n_groups = (uint32_t)groups.size();
+    sp.n_pats = (uint32_t)fpats.size();
     sp.hits = d.hits.p;
     sp.ctr = d.ctr.p;
     // launches variant v over the full work list or over the tuning sample
@@ -1053,7 +1187,8 @@ int Engine::run_popcount(const std::vector<Request> &reqs, std::vector<Result> &
         }
         const ScanVariant &v = kScanVariants[vi];
         times_.scan_variant = vi;
-        times_.scan_shape = std::string(v.pair == 2 ? "pp2-" : "") + "cpt" + std::to_string(v.cpt) + "-warps" + std::to_string(v.warps) +
+        static const char *const kMinName[] = {"", "", "pp2-", "", "min3-"};
+        times_.scan_shape = std::string(v.per_warp ? "warp-" : "") + kMinName[v.pair] + "cpt" + std::to_string(v.cpt) + "-warps" + std::to_string(v.warps) +
                             "-minb" + std::to_string(v.min_blocks) + "-span" +
                             std::to_string(v.span_tiles);
         for (int attempt = 0; attempt < 2; ++attempt) {

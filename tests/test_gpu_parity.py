@@ -127,7 +127,10 @@ def test_cli_matches_oracle_cli(cof_mod, oracle_mod, golden, tmp_path):
         assert "=== Cas-OFFinder Rust ===" in log and "Matches found: 117" in log
 
 
-@pytest.mark.parametrize("variant", range(9))
+N_SCAN_VARIANTS = 15  # per-warp work items: 0-5; CTA work items: 6-14
+
+
+@pytest.mark.parametrize("variant", range(N_SCAN_VARIANTS))
 def test_every_scan_tile_shape(cof_mod, oracle_mod, golden, variant, monkeypatch):
     # the autotuner may pick any tile shape; all must give the same rows
     monkeypatch.setenv("COF_SCAN_VARIANT", str(variant))
@@ -142,12 +145,31 @@ def test_every_scan_tile_shape(cof_mod, oracle_mod, golden, variant, monkeypatch
     assert g2.tuning()["variant"] == variant
 
 
+@pytest.mark.parametrize("variant", [0, 5, 6])
+def test_patterns_beyond_the_shared_memory_table(cof_mod, oracle_mod, variant, monkeypatch):
+    # 1500 guides: 3000 patterns in two strand groups; the per-warp scan
+    # stages the first 2048 patterns, so the reverse-strand group reads its
+    # patterns from global memory
+    monkeypatch.setenv("COF_SCAN_VARIANT", str(variant))
+    rng = random.Random(77)
+    _, records = randgen.random_genome(rng, 2, 20000, 30000)
+    pats = ["".join(rng.choice("ACGT") for _ in range(20)) + "NNN" for _ in range(1500)]
+    for p in pats[::100]:
+        randgen.plant_sites(rng, records, p, "N" * 21 + "RG", 2, 3)
+    chunks = randgen.chunk_records(rng, records, 4000)
+    g, o = _both(cof_mod, oracle_mod, chunks)
+    text, n = g.search("N" * 21 + "RG", pats, 4)
+    ref, nref = o.search("N" * 21 + "RG", pats, 4)
+    assert n == nref > 0 and _rows(text) == _rows(ref)
+    assert g.tuning()["variant"] == variant
+
+
 def test_autotuner_records_choice(cof_mod, golden, monkeypatch):
     monkeypatch.delenv("COF_SCAN_VARIANT", raising=False)
     g = cof_mod.Genome(os.path.join(golden, "upstream1000.fa"))
     g.search("N" * 24, KAT_PATS, 11)
     t = g.tuning()
-    assert "cpt" in t["last"] and 0 <= t["variant"] < 9
+    assert "cpt" in t["last"] and 0 <= t["variant"] < N_SCAN_VARIANTS
 
 
 @pytest.mark.parametrize("seed", range(8))
@@ -260,9 +282,11 @@ def test_2bit_loader_matches_fasta(cof_mod, oracle_mod, tmp_path):
     assert sorted(ra.split("\n")) == sorted(ref.split("\n"))
 
 
-def test_more_batches_than_one_scan_group_holds(cof_mod, oracle_mod):
+@pytest.mark.parametrize("variant", [0, 6])
+def test_more_batches_than_one_scan_group_holds(cof_mod, oracle_mod, variant, monkeypatch):
     # ~300 batches (2 chunks each): more batch segments than a scan group
     # stages, as with chunks_per_search 64 (the CLI's C) on a large genome
+    monkeypatch.setenv("COF_SCAN_VARIANT", str(variant))
     rng = random.Random(31)
     _, records = randgen.random_genome(rng, 3, 12000, 16000)
     pats = ["".join(rng.choice("ACGT") for _ in range(20)) + "NNN" for _ in range(3)]
