@@ -88,18 +88,33 @@ int make_request(const char *filter, size_t pattern_len, const char *const *patt
 // caller's cof_result.text; cof_result_free hands it back.  Freed buffers
 // are kept (up to kKeepBytes) and reused, so a steady stream of searches
 // neither pins nor first-touches new host pages.
+//
+// Results of up to kSmallMax bytes (the rows of a few guides) are blocks of
+// a power-of-two size class cut from page-locked slabs of at least
+// kSlabBytes, so that a pass over hundreds of small requests pins memory
+// once instead of once per request.  Slabs stay until exit, kSmallCap bytes
+// at most; beyond that small results are allocated like large ones.
 class PinnedPool {
   public:
     static constexpr size_t kKeepBytes = size_t(4) << 30;
+    static constexpr size_t kMinBlock = size_t(4) << 10;
+    static constexpr int kClasses = 9;  // 4 KiB .. 1 MiB
+    static constexpr size_t kSmallMax = kMinBlock << (kClasses - 1);
+    static constexpr size_t kSlabBytes = size_t(8) << 20;
+    static constexpr size_t kSmallCap = size_t(1) << 30;
     static PinnedPool &get();
     char *acquire(size_t bytes);  // nullptr when page-locked memory runs out
     bool release(char *p);        // false when p did not come from the pool
 
   private:
+    char *alloc_large(size_t want);
     std::mutex mu_;
-    std::unordered_map<char *, size_t> live_;
+    // live buffer -> (bytes, size class; -1 for a buffer of its own)
+    std::unordered_map<char *, std::pair<size_t, int>> live_;
     std::multimap<size_t, char *> free_;
     size_t free_bytes_ = 0;
+    std::vector<char *> small_free_[kClasses];
+    size_t slab_bytes_ = 0;
 };
 
 // A pool buffer owned by one result (move-only; returned to the pool when

@@ -1273,11 +1273,31 @@ int Engine::run_popcount(const std::vector<Request> &reqs, std::vector<Result> &
     // each request's rows (sorted request-major) go straight from the
     // device into its own page-locked result buffer
     CU(cudaEventRecord(d.ev[4], s));
+    // text offset where each request's rows end: one small asynchronous copy
+    // per request into a page-locked array, then a single wait
+    std::vector<uint64_t> tend(reqs.size(), text_bytes);
+    if (reqs.size() > 1) {
+        PooledText bnd;
+        bnd.p = PinnedPool::get().acquire(8 * reqs.size());
+        if (!bnd.p) {
+            err = {kOom, "out of page-locked host memory for result text"};
+            return err.code;
+        }
+        uint64_t *hb = reinterpret_cast<uint64_t *>(bnd.p);
+        uint64_t r1 = 0;
+        for (size_t ri = 0; ri < reqs.size(); ++ri) {
+            r1 += req_rows[ri];
+            hb[ri] = text_bytes;
+            if (r1 < n_rows)
+                CU(cudaMemcpyAsync(hb + ri, d.offs.p + r1, 8, cudaMemcpyDeviceToHost, s));
+        }
+        CU(cudaStreamSynchronize(s));
+        for (size_t ri = 0; ri < reqs.size(); ++ri) tend[ri] = hb[ri];
+    }
     uint64_t r0 = 0, t0 = 0;
     for (size_t ri = 0; ri < reqs.size(); ++ri) {
         const uint64_t r1 = r0 + req_rows[ri];
-        uint64_t t1 = text_bytes;
-        if (r1 < n_rows) CU(cudaMemcpy(&t1, d.offs.p + r1, 8, cudaMemcpyDeviceToHost));
+        const uint64_t t1 = tend[ri];
         char *buf = PinnedPool::get().acquire(t1 - t0 + 1);
         if (!buf) {
             err = {kOom, "out of page-locked host memory for result text"};

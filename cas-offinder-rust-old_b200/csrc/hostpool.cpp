@@ -1,6 +1,8 @@
 // hostpool.cpp -- the page-locked result-buffer pool (PinnedPool in
 // cof_engine.h).  Buffers are portable pinned allocations, usable from every
-// device's stream, rounded up to 2 MiB so that nearby sizes reuse each other.
+// device's stream.  Small results are blocks of size classes cut from shared
+// slabs; larger ones are allocations of their own, rounded up to 2 MiB so
+// that nearby sizes reuse each other.
 #include <cuda_runtime.h>
 
 #include "cof_engine.h"
@@ -12,19 +14,7 @@ PinnedPool &PinnedPool::get() {
     return pool;
 }
 
-char *PinnedPool::acquire(size_t bytes) {
-    const size_t want = ((bytes + 1) + (size_t(2) << 20) - 1) & ~((size_t(2) << 20) - 1);
-    std::lock_guard<std::mutex> lk(mu_);
-    // best fit among the kept buffers, at most twice the size asked for
-    auto it = free_.lower_bound(want);
-    if (it != free_.end() && it->first <= 2 * want) {
-        char *p = it->second;
-        const size_t n = it->first;
-        free_.erase(it);
-        free_bytes_ -= n;
-        live_[p] = n;
-        return p;
-    }
+char *PinnedPool::alloc_large(size_t want) {
     char *p = nullptr;
     if (cudaHostAlloc((void **)&p, want, cudaHostAllocPortable) != cudaSuccess) {
         cudaGetLastError();  // clear the recorded error of the failed call
@@ -37,7 +27,48 @@ char *PinnedPool::acquire(size_t bytes) {
             return nullptr;
         }
     }
-    live_[p] = want;
+    return p;
+}
+
+char *PinnedPool::acquire(size_t bytes) {
+    const size_t need = bytes + 1;
+    std::lock_guard<std::mutex> lk(mu_);
+    if (need <= kSmallMax) {
+        int c = 0;
+        while ((kMinBlock << c) < need) ++c;
+        const size_t block = kMinBlock << c;
+        auto &fl = small_free_[c];
+        if (fl.empty()) {
+            const size_t slab = std::max(kSlabBytes, 16 * block);
+            char *s = nullptr;
+            if (slab_bytes_ + slab <= kSmallCap &&
+                cudaHostAlloc((void **)&s, slab, cudaHostAllocPortable) == cudaSuccess) {
+                slab_bytes_ += slab;
+                for (size_t o = slab; o >= block; o -= block) fl.push_back(s + o - block);
+            } else {
+                cudaGetLastError();
+            }
+        }
+        if (!fl.empty()) {
+            char *p = fl.back();
+            fl.pop_back();
+            live_[p] = {block, c};
+            return p;
+        }
+    }
+    const size_t want = (need + (size_t(2) << 20) - 1) & ~((size_t(2) << 20) - 1);
+    // best fit among the kept buffers, at most twice the size asked for
+    auto it = free_.lower_bound(want);
+    if (it != free_.end() && it->first <= 2 * want) {
+        char *p = it->second;
+        const size_t n = it->first;
+        free_.erase(it);
+        free_bytes_ -= n;
+        live_[p] = {n, -1};
+        return p;
+    }
+    char *p = alloc_large(want);
+    if (p) live_[p] = {want, -1};
     return p;
 }
 
@@ -46,8 +77,13 @@ bool PinnedPool::release(char *p) {
     std::lock_guard<std::mutex> lk(mu_);
     auto it = live_.find(p);
     if (it == live_.end()) return false;
-    const size_t n = it->second;
+    const size_t n = it->second.first;
+    const int c = it->second.second;
     live_.erase(it);
+    if (c >= 0) {  // back to its size class; slabs are kept
+        small_free_[c].push_back(p);
+        return true;
+    }
     free_.emplace(n, p);
     free_bytes_ += n;
     while (free_bytes_ > kKeepBytes && !free_.empty()) {  // keep the newest sizes

@@ -90,6 +90,28 @@ def test_batched_equals_single(cof_mod, oracle_mod):
         assert _rows(text) == _rows(ref)
 
 
+def test_many_small_requests_in_one_pass(cof_mod):
+    # 300 one-guide requests in one pass: their result texts are blocks cut
+    # from shared page-locked slabs and their text boundaries are read in one
+    # wait; every request equals its own search, twice over (blocks reused)
+    rng = random.Random(15)
+    _, records = randgen.random_genome(rng, 3, 20000, 30000)
+    reqs = []
+    for i in range(300):
+        filt, mk, mm = randgen.REQUEST_SHAPES[i % 3]
+        pat = mk("".join(rng.choice("ACGT") for _ in range(25)))
+        if i % 2:
+            randgen.plant_sites(rng, records, pat, filt, 2, 1)
+        reqs.append(dict(search_filter=filt, patterns=[pat], max_mismatches=mm))
+    g = cof_mod.Genome()
+    for name, data, _nibs, s, e in randgen.chunk_records(rng, records, 3000):
+        g.add_chunk(name, data, s, e)
+    singles = [g.search(**r) for r in reqs]
+    assert sum(n for _, n in singles) > 100
+    for _ in range(2):
+        assert g.search_batch(reqs) == singles
+
+
 def test_planted_sites_found(cof_mod, oracle_mod, tmp_path):
     import synth
     cfg = synth.config_plain_small(seed=11, scale=0.05)
