@@ -32,11 +32,11 @@ PKG = os.path.join(ROOT, "cas-offinder-rust-old_b200")
 ORACLE = os.path.join(ROOT, "oracle")
 sys.path.insert(0, PKG)
 
-# dram__bytes_read.sum + dram__bytes_write.sum of one scan_kernel launch,
-# from the ncu capture summarised in profiles/ (620 Mbp case, scaled x5 by
-# genome size to the 3.1 Gbp workload: each strand group reads every plane
-# word once, so traffic grows in proportion to the genome)
-TRAFFIC = (466.45e6 + 17.69e6) * 5
+# dram__bytes_read.sum + dram__bytes_write.sum of one scan_warp_kernel
+# launch, from the ncu capture summarised in profiles/ (620 Mbp case, scaled
+# x5 by genome size to the 3.1 Gbp workload: each strand group reads every
+# plane word once, so traffic grows in proportion to the genome)
+TRAFFIC = (465.71e6 + 20.20e6) * 5
 
 METRIC = "Gbp*guides/s scanned (3.1 Gbp x 100 guides, 20 nt + NRG, mm<=6, both strands)"
 UNIT = "Gbp*guides/s"
