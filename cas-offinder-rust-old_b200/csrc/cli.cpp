@@ -121,6 +121,9 @@ int main(int argc, char **argv) {
         return d;
     };
     const double t_input = lap();
+    // one search per process: timing tile shapes (tens of ms) cannot pay
+    // back, so the default shape is used unless COF_AUTOTUNE says otherwise
+    ::setenv("COF_AUTOTUNE", "0", 0);
     cof_genome *g = nullptr;
     if (cof_genome_create(0, &g)) die(cof_last_error());
     if (cof_genome_load(g, genome.c_str())) die(cof_last_error());

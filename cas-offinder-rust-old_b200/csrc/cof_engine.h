@@ -7,6 +7,7 @@
 #include <cstddef>
 #include <cstdint>
 #include <map>
+#include <memory>
 #include <mutex>
 #include <string>
 #include <thread>
@@ -51,18 +52,40 @@ bool is_mixed_base(char c);    // bit4ops.rs:201-203
 // The chunk stream of the reference (ChromChunkInfo), tight-packed the way
 // chunks_to_searchchunk lays a search batch out (search.rs:1376-1427): chunk
 // k occupies bytes [boff[k], boff[k+1]) of `data`.
+// The bases of a .2bit file, as its chunks will hold them: for each chunk
+// the file offset of its packed bases, its byte offset in the genome's bit4
+// stream, its length, and the N ranges (nucleotides relative to the chunk,
+// [lo, hi) pairs in nr) that the reference's N-block loop (read_2bit.rs)
+// writes into it.  Built from the file's index and N blocks without touching
+// a base; the bases are decoded later, on the host or on the device.
+struct TwoBitPlan {
+    struct Piece {
+        uint64_t raw, out;  // file offset of the packed bases; bit4 byte offset
+        uint32_t rs, nr;    // nucleotides; first N range (index into nr / 2)
+    };
+    std::string path;
+    uint64_t file_bytes = 0;
+    std::vector<Piece> pieces;  // one per chunk, plus a sentinel (nr = end)
+    std::vector<uint32_t> nr;
+    uint64_t raw_begin = 0, raw_end = 0;  // file bytes holding every chunk's bases
+};
+
 struct HostGenome {
     std::vector<std::string> names;
     std::vector<uint32_t> name_idx;  // per chunk
     std::vector<uint64_t> start, end, boff{0};
     std::vector<uint8_t> data;
-    // staging for loaders
-    std::vector<uint8_t> cur;
+    // a .2bit file loaded into an empty genome: its bases are decoded on the
+    // device at upload (data stays empty); any other change to the genome
+    // first decodes them on the host (materialize)
+    std::shared_ptr<TwoBitPlan> deferred;
 
     size_t n_chunks() const { return start.size(); }
     uint64_t n_nucl() const;
+    uint64_t n_bytes() const { return boff.back(); }
     int add_chunk(uint32_t name, uint64_t cs, uint64_t ce, const uint8_t *bytes, Error &err);
     uint32_t add_name(const char *s, size_t n);
+    int materialize(Error &err);
 };
 
 // Genome loaders (read_fasta.rs, read_2bit.rs, read_fasta_folder.rs,

@@ -744,14 +744,18 @@ int Engine::upload(Error &err) {
     for (auto &e : d->ev) CU(cudaEventCreate(&e));
     CU(cudaDeviceGetAttribute(&d->n_sm, cudaDevAttrMultiProcessorCount, device_));
     const HostGenome &h = host_;
-    const uint64_t n_bytes = h.data.size();
+    const uint64_t n_bytes = h.n_bytes();
     const uint64_t n_nucl = 2 * n_bytes;
     // 64 pad words (all non-single) so that a scan tile's last lanes and the
     // funnel-shift neighbour word stay inside the planes
     d->n_words = (n_nucl + 31) / 32 + 64;
     if (d->bit4.ensure(d->n_words * 16 + 64, err)) return err.code;
     CU(cudaMemsetAsync(d->bit4.p, 0, d->n_words * 16 + 64, d->stream));
-    if (n_bytes) CU(cudaMemcpyAsync(d->bit4.p, h.data.data(), n_bytes, cudaMemcpyHostToDevice, d->stream));
+    if (h.deferred) {  // a .2bit file: the packed bases are decoded here
+        if (upload_2bit(*h.deferred, d->bit4.p, device_, d->stream, err)) return err.code;
+    } else if (n_bytes) {
+        CU(cudaMemcpyAsync(d->bit4.p, h.data.data(), n_bytes, cudaMemcpyHostToDevice, d->stream));
+    }
     // each plane starts with one padding word (32 non-single cells before
     // position 0) for windows anchored at a PAM near the genome start
     const uint64_t pw = d->n_words + 1;

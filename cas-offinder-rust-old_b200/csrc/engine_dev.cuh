@@ -136,6 +136,10 @@ struct DevBuf {
     }
 };
 
+// Copies a planned .2bit file's packed bases to the device and decodes them
+// into bit4 (twobit.cu); returns after the decode has finished on s.
+int upload_2bit(const TwoBitPlan &plan, uint8_t *bit4, int device, cudaStream_t s, Error &err);
+
 class DeviceGenome {
   public:
     int device = 0;

@@ -74,6 +74,7 @@ uint32_t HostGenome::add_name(const char *s, size_t n) {
 
 int HostGenome::add_chunk(uint32_t name, uint64_t cs, uint64_t ce, const uint8_t *bytes,
                           Error &err) {
+    if (deferred && materialize(err)) return err.code;
     if (ce < cs || ce - cs > kChunkSize) {
         err = {kBadInput, "chunk must hold 0..65536 nucleotides"};
         return err.code;
@@ -294,9 +295,15 @@ uint32_t rd32(const FileBytes &b, size_t &o, bool &ok) {
     return v;
 }
 
-// read_2bit.rs:33-118.  Sequences are taken one after the other in index
-// order (the stored offsets are skipped, as the reference does).
-int parse_2bit(HostGenome &g, const FileBytes &b, Error &err) {
+// read_2bit.rs:33-118, first half: the header, the index, and per record
+// its length and N blocks.  Sequences are taken one after the other in index
+// order (the stored offsets are skipped, as the reference does).  Appends the
+// chunk table to g and describes every chunk's bases in plan: the file
+// offset of its packed bytes, and the N ranges the reference's loop writes
+// into it.  That loop keeps its N-block index across a record's chunks and
+// steps back by one at each chunk; it is replayed here without touching any
+// bases.
+int index_2bit(HostGenome &g, const FileBytes &b, TwoBitPlan &plan, Error &err) {
     bool ok = true;
     size_t o = 0;
     auto trunc = [&]() {
@@ -322,33 +329,19 @@ int parse_2bit(HostGenome &g, const FileBytes &b, Error &err) {
         names[i] = g.add_name(b.data() + o, nl);
         o += nl + 4;
     }
-    // BIT2_TO_BIT4 (bit4ops.rs:60-75): codes T=0 C=1 A=2 G=3, first base in
-    // the high bits of each byte.
-    uint16_t b2b4[256];
-    for (int i = 0; i < 256; ++i) {
-        uint16_t v = 0;
-        for (int j = 0; j < 4; ++j) v |= (uint16_t)((1u << ((i >> ((3 - j) * 2)) & 3)) << (4 * j));
-        b2b4[i] = v;
-    }
-    // Pass 1 (sequential): record headers, N blocks, and one entry per
-    // 65536-nt chunk with its packed bytes and the N-block index the
-    // reference's loop (read_2bit.rs) has when it reaches the chunk -- the
-    // loop keeps that index across chunks and steps back by one each time,
-    // so it is replayed here without touching any bases.
-    struct Piece {
-        uint32_t rec;
-        uint64_t pos, rs;
-        size_t raw;   // file offset of the chunk's packed bases
-        int64_t bmi;  // N-block index at the chunk's start
-    };
-    std::vector<std::vector<std::pair<uint32_t, uint32_t>>> nblocks(cnt);
-    std::vector<Piece> pieces;
+    plan.file_bytes = b.size();
+    plan.pieces.clear();
+    plan.nr.clear();
+    plan.raw_begin = b.size();
+    plan.raw_end = 0;
+    std::vector<uint32_t> piece_rec;
+    std::vector<uint64_t> piece_pos;
+    std::vector<std::pair<uint32_t, uint32_t>> nb;
     for (uint32_t s = 0; s < cnt; ++s) {
         uint32_t chrlen = rd32(b, o, ok);
         uint32_t nbc = rd32(b, o, ok);
         if (!ok) return trunc();
-        auto &nb = nblocks[s];
-        nb.resize(nbc);
+        nb.assign(nbc, {0, 0});
         for (uint32_t i = 0; i < nbc; ++i) nb[i].first = rd32(b, o, ok);
         for (uint32_t i = 0; i < nbc; ++i) nb[i].second = rd32(b, o, ok);
         if (!ok) return trunc();
@@ -365,33 +358,68 @@ int parse_2bit(HostGenome &g, const FileBytes &b, Error &err) {
             const size_t nbytes = (rs + 3) / 4;
             if (o + nbytes > b.size()) return trunc();
             bmi = std::max<int64_t>(bmi - 1, 0);
-            pieces.push_back({s, pos, rs, o, bmi});
-            while (bmi < (int64_t)nbc && (int64_t)nb[bmi].first - (int64_t)pos <= (int64_t)rs) ++bmi;
+            plan.pieces.push_back({o, 0, (uint32_t)rs, (uint32_t)(plan.nr.size() / 2)});
+            piece_rec.push_back(s);
+            piece_pos.push_back(pos);
+            // memsetbit4 of every N block the loop reaches in this chunk,
+            // clipped to the chunk (the block end wraps at 32 bits, as the
+            // reference's u32 sum does)
+            while (bmi < (int64_t)nbc && (int64_t)nb[bmi].first - (int64_t)pos <= (int64_t)rs) {
+                const int64_t bs = (int64_t)nb[bmi].first - (int64_t)pos;
+                const int64_t be =
+                    (int64_t)(uint32_t)(nb[bmi].first + nb[bmi].second) - (int64_t)pos;
+                const int64_t lo = std::max<int64_t>(bs, 0);
+                const int64_t hi = std::min<int64_t>(std::max<int64_t>(be, 0), (int64_t)rs);
+                if (lo < hi) {
+                    plan.nr.push_back((uint32_t)lo);
+                    plan.nr.push_back((uint32_t)hi);
+                }
+                ++bmi;
+            }
+            plan.raw_begin = std::min<uint64_t>(plan.raw_begin, o);
+            plan.raw_end = std::max<uint64_t>(plan.raw_end, o + nbytes);
             o += nbytes;
             pos += rs;
         }
     }
+    if (plan.pieces.empty()) plan.raw_begin = plan.raw_end = 0;
     // chunk table
-    const size_t k0 = g.start.size();
-    uint64_t total = g.data.size();
-    for (const Piece &pc : pieces) {
-        if (!g.start.empty() && pc.pos != 0 && g.end.back() != pc.pos) {
+    uint64_t total = g.boff.back();
+    for (size_t k = 0; k < plan.pieces.size(); ++k) {
+        TwoBitPlan::Piece &pc = plan.pieces[k];
+        const uint64_t pos = piece_pos[k];
+        if (!g.start.empty() && pos != 0 && g.end.back() != pos) {
             err = {kBadInput, "search expects chromosome chunks to arrive in order"};
             return err.code;
         }
-        g.name_idx.push_back(names[pc.rec]);
-        g.start.push_back(pc.pos);
-        g.end.push_back(pc.pos + pc.rs);
+        g.name_idx.push_back(names[piece_rec[k]]);
+        g.start.push_back(pos);
+        g.end.push_back(pos + pc.rs);
+        pc.out = total;
         total += (pc.rs + 1) / 2;
         g.boff.push_back(total);
     }
-    g.data.resize(total, 0);
-    // Pass 2 (all host threads): bases, padding and N runs per chunk
+    plan.pieces.push_back({0, total, 0, (uint32_t)(plan.nr.size() / 2)});
+    return kOk;
+}
+
+// read_2bit.rs:33-118, second half, on all host threads: each chunk's bases
+// (BIT2_TO_BIT4, bit4ops.rs:60-75: codes T=0 C=1 A=2 G=3, first base in the
+// high bits of each byte), zero padding after the last base, then the N
+// ranges, written into g.data at the chunk's byte offset.
+void convert_2bit_host(HostGenome &g, const FileBytes &b, const TwoBitPlan &plan) {
+    uint16_t b2b4[256];
+    for (int i = 0; i < 256; ++i) {
+        uint16_t v = 0;
+        for (int j = 0; j < 4; ++j) v |= (uint16_t)((1u << ((i >> ((3 - j) * 2)) & 3)) << (4 * j));
+        b2b4[i] = v;
+    }
+    g.data.resize(plan.pieces.back().out, 0);
+    const size_t np = plan.pieces.size() - 1;
     auto convert = [&](size_t a, size_t z) {
         std::vector<uint8_t> cur(kChunkBytes);
         for (size_t k = a; k < z; ++k) {
-            const Piece &pc = pieces[k];
-            const auto &nb = nblocks[pc.rec];
+            const TwoBitPlan::Piece &pc = plan.pieces[k];
             const size_t rs = pc.rs, nbytes = (rs + 3) / 4;
             const uint8_t *raw = (const uint8_t *)b.data() + pc.raw;
             std::fill(cur.begin(), cur.end(), 0);
@@ -407,18 +435,11 @@ int parse_2bit(HostGenome &g, const FileBytes &b, Error &err) {
                 }
             };
             if (rs % 4) setn(rs, nbytes * 4, 0);
-            for (int64_t bmi = pc.bmi; bmi < (int64_t)nb.size(); ++bmi) {
-                int64_t bs = (int64_t)nb[bmi].first - (int64_t)pc.pos;
-                int64_t be = (int64_t)(uint32_t)(nb[bmi].first + nb[bmi].second) - (int64_t)pc.pos;
-                if (bs > (int64_t)rs) break;
-                int64_t lo = std::max<int64_t>(bs, 0);
-                int64_t hi = std::min<int64_t>(std::max<int64_t>(be, 0), (int64_t)rs);
-                if (lo < hi) setn((size_t)lo, (size_t)hi, 0xF);
-            }
-            std::memcpy(g.data.data() + g.boff[k0 + k], cur.data(), (rs + 1) / 2);
+            for (uint32_t r = pc.nr; r < plan.pieces[k + 1].nr; ++r)
+                setn(plan.nr[2 * r], plan.nr[2 * r + 1], 0xF);
+            std::memcpy(g.data.data() + pc.out, cur.data(), (rs + 1) / 2);
         }
     };
-    const size_t np = pieces.size();
     const unsigned nt = std::max(1u, std::min(std::thread::hardware_concurrency(), 32u));
     if (nt == 1 || np < 64) {
         convert(0, np);
@@ -430,12 +451,19 @@ int parse_2bit(HostGenome &g, const FileBytes &b, Error &err) {
         }
         for (auto &x : th) x.join();
     }
+}
+
+int parse_2bit(HostGenome &g, const FileBytes &b, Error &err) {
+    TwoBitPlan plan;
+    if (int rc = index_2bit(g, b, plan, err)) return rc;
+    convert_2bit_host(g, b, plan);
     return kOk;
 }
 
 }  // namespace
 
 int load_genome_path(HostGenome &g, const std::string &path, Error &err) {
+    if (g.deferred && g.materialize(err)) return err.code;  // appending to it
     struct stat st;
     if (::stat(path.c_str(), &st)) {
         err = {kIo, "cannot stat " + path};
@@ -473,7 +501,29 @@ int load_genome_path(HostGenome &g, const std::string &path, Error &err) {
         return err.code;
     }
     if (fv.p[0] == '>') return parse_fasta(g, fv.p, fv.n, err);
+    if (g.n_chunks() == 0 && !g.deferred) {
+        // a .2bit file into an empty genome: only the index is read here;
+        // the device decodes the bases at upload
+        auto plan = std::make_shared<TwoBitPlan>();
+        plan->path = path;
+        if (int rc = index_2bit(g, FileBytes{fv.p, fv.n}, *plan, err)) return rc;
+        if (plan->pieces.size() > 1) g.deferred = plan;
+        return kOk;
+    }
     return parse_2bit(g, FileBytes{fv.p, fv.n}, err);
+}
+
+int HostGenome::materialize(Error &err) {
+    if (!deferred) return kOk;
+    FileView fv;
+    if (int rc = fv.open(deferred->path, err)) return rc;
+    if (fv.n != deferred->file_bytes) {
+        err = {kIo, deferred->path + " changed since it was loaded"};
+        return err.code;
+    }
+    convert_2bit_host(*this, FileBytes{fv.p, fv.n}, *deferred);
+    deferred.reset();
+    return kOk;
 }
 
 bool Tuner::enabled() const {

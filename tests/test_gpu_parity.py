@@ -304,6 +304,59 @@ def test_2bit_loader_matches_fasta(cof_mod, oracle_mod, tmp_path):
     assert sorted(ra.split("\n")) == sorted(ref.split("\n"))
 
 
+def _nrun_records(rng, lengths, n_runs):
+    recs = []
+    for r, n in enumerate(lengths):
+        seq = [rng.choice("ACGTacgt") for _ in range(n)]
+        for _ in range(n_runs):
+            a = rng.randrange(n)
+            for i in range(a, min(n, a + rng.randint(1, 60))):
+                seq[i] = "N"
+        recs.append((f"chr{r}", "".join(seq)))
+    return recs
+
+
+def test_2bit_device_decode_many_n_blocks(cof_mod, oracle_mod, tmp_path):
+    # .2bit bases are decoded on the device at upload; hundreds of short N
+    # blocks per 64 Knt chunk, blocks touching chunk ends, odd record
+    # lengths: every window of the raw stream equals the oracle's
+    import twobit
+    rng = random.Random(23)
+    recs = _nrun_records(rng, (200003, 65536, 65537, 1, 7), 400)
+    tb = tmp_path / "g.2bit"
+    twobit.write_2bit(str(tb), recs)
+    g = cof_mod.Genome(str(tb))
+    o = oracle_mod.OracleGenome(str(tb))
+    assert g.n_nucl == o.n_nucl == sum(len(x) for _, x in recs)
+    ra, na = g.search("N" * 6, ["N" * 6], 5, raw=True)
+    ref, nref = o.search("N" * 6, ["N" * 6], 5, raw=True)
+    assert na == nref > 0 and sorted(ra.split("\n")) == sorted(ref.split("\n"))
+    pats = ["".join(rng.choice("ACGT") for _ in range(20)) + "NNN" for _ in range(4)]
+    text, n = g.search("N" * 21 + "RG", pats, 5)
+    rtext, rn = o.search("N" * 21 + "RG", pats, 5)
+    assert n == rn and _rows(text) == _rows(rtext)
+
+
+def test_chunk_added_after_2bit_load(cof_mod, oracle_mod, tmp_path):
+    # adding a chunk to a genome loaded from .2bit decodes the file's bases
+    # on the host first (the device decode only covers a genome that is one
+    # .2bit file); the result equals the oracle's genome built the same way
+    import twobit
+    rng = random.Random(29)
+    recs = _nrun_records(rng, (70001, 3001), 30)
+    tb = tmp_path / "g.2bit"
+    twobit.write_2bit(str(tb), recs)
+    extra = randgen.chunk_records(rng, ["".join(rng.choice("ACGT") for _ in range(5000))], 5000)
+    g = cof_mod.Genome(str(tb))
+    o = oracle_mod.OracleGenome(str(tb))
+    for name, data, _nibs, s, e in extra:
+        g.add_chunk("extra", data, s, e)
+        o.add_chunk("extra", data, s, e)
+    ra, na = g.search("N" * 6, ["N" * 6], 5, raw=True)
+    ref, nref = o.search("N" * 6, ["N" * 6], 5, raw=True)
+    assert na == nref > 0 and sorted(ra.split("\n")) == sorted(ref.split("\n"))
+
+
 @pytest.mark.parametrize("variant", [0, 6])
 def test_more_batches_than_one_scan_group_holds(cof_mod, oracle_mod, variant, monkeypatch):
     # ~300 batches (2 chunks each): more batch segments than a scan group
