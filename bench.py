@@ -357,23 +357,27 @@ class CpuSample:
                            f"search_compute_cpu + writer, {self.cores} threads, {t:.1f} s")
 
 
-def bench_cli(cfg, n_rows, runs=2):
+def bench_cli(cfg, n_rows, runs=2, fmt="2bit"):
     """The command line tool as a fresh process, the way main.rs is run:
-    `cof-offinder input.txt G out.txt` reads the genome from a .2bit file,
-    uploads it, searches, and writes the rows and the .log summary.  The
-    .2bit file is written once beforehand (page cache warm for every run)."""
+    `cof-offinder input.txt G out.txt` reads the genome file (`fmt`: "2bit"
+    or "fasta", 60-column lines), uploads it, searches, and writes the rows
+    and the .log summary.  The genome file is written once beforehand (page
+    cache warm for every run)."""
     import shutil
     import tempfile
     import build as cof_build
     d = tempfile.mkdtemp(prefix="cof_cli_")
     try:
         t0 = time.perf_counter()
-        path2 = os.path.join(d, "genome.2bit")
-        cfg["genome"].write_2bit(path2)
+        path = os.path.join(d, "genome." + ("2bit" if fmt == "2bit" else "fa"))
+        if fmt == "2bit":
+            cfg["genome"].write_2bit(path)
+        else:
+            cfg["genome"].write_fasta(path)
         t_write = time.perf_counter() - t0
         inp = os.path.join(d, "input.txt")
         with open(inp, "w") as f:
-            f.write(path2 + "\n" + cfg["filter"] + "\n")
+            f.write(path + "\n" + cfg["filter"] + "\n")
             for p in cfg["patterns"]:
                 f.write(f"{p} {cfg['max_mismatches']}\n")
         out = os.path.join(d, "out.txt")
@@ -395,14 +399,14 @@ def bench_cli(cfg, n_rows, runs=2):
             for line in f:
                 rows += not line.startswith(b"#")
         return {"workload": "cof-offinder input.txt G out.txt, " + cfg["name"],
-                "seconds": min(secs), "runs_s": secs, "rows": rows,
+                "genome_file": fmt, "seconds": min(secs), "runs_s": secs, "rows": rows,
                 "stage_s": stages[secs.index(min(secs))] if len(stages) == len(secs) else None,
                 "rows_match_c_abi": None if n_rows is None else rows == n_rows,
-                "genome_2bit_bytes": os.path.getsize(path2),
+                "genome_file_bytes": os.path.getsize(path),
                 "output_bytes": os.path.getsize(out),
-                "includes": "process start, CUDA context, .2bit read + convert, upload, "
+                "includes": "process start, CUDA context, genome file read + convert, upload, "
                             "search, output + .log written",
-                "genome_2bit_write_s": t_write}
+                "genome_file_write_s": t_write}
     finally:
         shutil.rmtree(d, ignore_errors=True)
 
@@ -516,7 +520,9 @@ def main():
     t_gen = time.perf_counter() - t0
     if args.only_cli:
         if rank == 0:
-            print(json.dumps({"cli_whole_process": bench_cli(cfg, None, max(1, args.steps))}),
+            print(json.dumps({"cli_whole_process": bench_cli(cfg, None, max(1, args.steps)),
+                              "cli_whole_process_fasta": bench_cli(cfg, None, max(1, args.steps),
+                                                                   "fasta")}),
                   flush=True)
         if dist:
             dist.destroy_process_group()
@@ -611,6 +617,7 @@ def main():
                                                        2000.0, seed=8, max_guides=4, max_mm=3)
         line["bulge"] = bench_bulge(cof, local, 3, args.bulge_scale)
         line["cli_whole_process"] = bench_cli(cfg, rows_per_step)
+        line["cli_whole_process_fasta"] = bench_cli(cfg, rows_per_step, fmt="fasta")
     if not args.no_cpu_baseline and world == 1:
         base, _ = cpu_baseline(cfg, args.cpu_sample_s)
         line["cpu_baseline"] = base

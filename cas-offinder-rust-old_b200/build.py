@@ -24,7 +24,7 @@ HEADERS = [os.path.join(CSRC, "cof_engine.h"), os.path.join(CSRC, "engine_dev.cu
            os.path.join(ROOT, "include", "cof.h")]
 
 SOURCES = ["engine.cu", "bulge.cu", "raw.cu", "loader.cpp", "cabi.cpp", "server.cpp", "noalloc.cu",
-           "hostpool.cpp", "twobit.cu"]
+           "hostpool.cpp", "twobit.cu", "fasta_dev.cu"]
 
 
 def _stale(out, deps):

@@ -70,6 +70,21 @@ struct TwoBitPlan {
     uint64_t raw_begin = 0, raw_end = 0;  // file bytes holding every chunk's bases
 };
 
+// A FASTA file whose chunks are decided (read_fasta.rs) but whose bases are
+// not yet converted: the chunks as ranges of the file's lines, [first line,
+// next chunk's first line), with their bit4 byte offsets.  Lines are counted
+// as the reader counts them: every '\n' ends one, and a last line without
+// '\n' counts too.
+struct FastaPlan {
+    std::string path;
+    uint64_t file_bytes = 0;
+    uint64_t n_lines = 0;
+    std::vector<uint64_t> first_line;  // per chunk, ascending
+    std::vector<uint64_t> last_line;   // per chunk: one past its last line
+    std::vector<uint64_t> out;         // per chunk: bit4 byte offset
+    std::vector<uint32_t> nt;          // per chunk: nucleotides
+};
+
 struct HostGenome {
     std::vector<std::string> names;
     std::vector<uint32_t> name_idx;  // per chunk
@@ -79,6 +94,7 @@ struct HostGenome {
     // device at upload (data stays empty); any other change to the genome
     // first decodes them on the host (materialize)
     std::shared_ptr<TwoBitPlan> deferred;
+    std::shared_ptr<FastaPlan> deferred_fa;  // the same for one FASTA file
 
     size_t n_chunks() const { return start.size(); }
     uint64_t n_nucl() const;

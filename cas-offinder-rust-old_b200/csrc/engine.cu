@@ -753,6 +753,9 @@ int Engine::upload(Error &err) {
     CU(cudaMemsetAsync(d->bit4.p, 0, d->n_words * 16 + 64, d->stream));
     if (h.deferred) {  // a .2bit file: the packed bases are decoded here
         if (upload_2bit(*h.deferred, d->bit4.p, device_, d->stream, err)) return err.code;
+    } else if (h.deferred_fa) {  // a FASTA file: its lines are converted here
+        if (upload_fasta(*h.deferred_fa, d->bit4.p, d->n_words * 16 + 64, device_, d->stream, err))
+            return err.code;
     } else if (n_bytes) {
         CU(cudaMemcpyAsync(d->bit4.p, h.data.data(), n_bytes, cudaMemcpyHostToDevice, d->stream));
     }

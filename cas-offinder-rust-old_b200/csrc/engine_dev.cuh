@@ -136,9 +136,18 @@ struct DevBuf {
     }
 };
 
+// Copies file bytes [begin, begin + n) to device memory dst through
+// page-locked staging buffers on several host threads (twobit.cu); fails if
+// the file's size is no longer file_bytes.  Returns when the copy is done.
+int copy_file_to_device(const std::string &path, uint64_t file_bytes, uint64_t begin,
+                        uint64_t n, uint8_t *dst, int device, Error &err);
 // Copies a planned .2bit file's packed bases to the device and decodes them
 // into bit4 (twobit.cu); returns after the decode has finished on s.
 int upload_2bit(const TwoBitPlan &plan, uint8_t *bit4, int device, cudaStream_t s, Error &err);
+// Copies a planned FASTA file to the device and converts its chunks' lines
+// into bit4 (fasta_dev.cu); returns after the conversion has finished on s.
+int upload_fasta(const FastaPlan &plan, uint8_t *bit4, uint64_t bit4_bytes, int device,
+                 cudaStream_t s, Error &err);
 
 class DeviceGenome {
   public:

@@ -74,7 +74,7 @@ uint32_t HostGenome::add_name(const char *s, size_t n) {
 
 int HostGenome::add_chunk(uint32_t name, uint64_t cs, uint64_t ce, const uint8_t *bytes,
                           Error &err) {
-    if (deferred && materialize(err)) return err.code;
+    if ((deferred || deferred_fa) && materialize(err)) return err.code;
     if (ce < cs || ce - cs > kChunkSize) {
         err = {kBadInput, "chunk must hold 0..65536 nucleotides"};
         return err.code;
@@ -295,6 +295,122 @@ uint32_t rd32(const FileBytes &b, size_t &o, bool &ok) {
     return v;
 }
 
+// read_fasta.rs:9-71, the chunk decisions only, for a FASTA file whose
+// bases the device converts.  Every host thread measures the lines of its
+// share of the file (a share ends just after a '\n'): each line's length,
+// with one '\r' before its '\n' dropped, and whether it is a header.  Then
+// one sequential pass over those lengths applies parse_fasta's rules -- the
+// same chunks, names and errors -- and records each chunk as a range of line
+// indices.
+int index_fasta(HostGenome &g, const char *buf, size_t n, FastaPlan &plan, Error &err) {
+    constexpr uint32_t kHdr = 0x80000000u;
+    const unsigned nt = (unsigned)std::max<size_t>(
+        1, std::min<size_t>(n >> 20, std::min(32u, std::max(1u, std::thread::hardware_concurrency()))));
+    std::vector<size_t> cut(nt + 1, n);
+    cut[0] = 0;
+    for (unsigned t = 1; t < nt; ++t) {
+        size_t c = std::max(cut[t - 1], n * t / nt);
+        const char *nl = c < n ? (const char *)std::memchr(buf + c, '\n', n - c) : nullptr;
+        cut[t] = nl ? (size_t)(nl - buf) + 1 : n;
+    }
+    std::vector<std::vector<uint32_t>> lens(nt);
+    std::vector<std::vector<uint64_t>> hdrs(nt);  // file offsets of header lines
+    std::vector<int> too_long(nt, 0);
+    auto scan = [&](unsigned t) {
+        const char *p = buf + cut[t], *e = buf + cut[t + 1];
+        auto &L = lens[t];
+        L.reserve((size_t)(e - p) / 61 + 16);
+        while (p < e) {
+            const char *nl = (const char *)std::memchr(p, '\n', (size_t)(e - p));
+            const char *le = nl ? nl : e;
+            size_t len = (size_t)(le - p);
+            if (nl && len && p[len - 1] == '\r') --len;
+            if (len >= kHdr) {
+                too_long[t] = 1;
+                return;
+            }
+            const bool hdr = len >= 1 && p[0] == '>';
+            if (hdr) hdrs[t].push_back((uint64_t)(p - buf));
+            L.push_back((uint32_t)len | (hdr ? kHdr : 0u));
+            p = nl ? nl + 1 : e;
+        }
+    };
+    if (nt == 1) {
+        scan(0);
+    } else {
+        std::vector<std::thread> th;
+        for (unsigned t = 0; t < nt; ++t) th.emplace_back(scan, t);
+        for (auto &x : th) x.join();
+    }
+    for (unsigned t = 0; t < nt; ++t)
+        if (too_long[t]) {
+            err = {kBadInput, "line in fasta too long"};
+            return err.code;
+        }
+    struct Span {
+        uint32_t name;
+        uint64_t cs, ce, fl, el;  // nucleotides [cs, ce); lines [fl, el)
+    };
+    std::vector<Span> spans;
+    bool started = false, have_name = false;
+    uint32_t name = 0;
+    uint64_t cs = 0, ce = 0, fl = 0, li = 0;
+    for (unsigned t = 0; t < nt; ++t) {
+        size_t h = 0;
+        for (uint32_t v : lens[t]) {
+            const size_t len = v & ~kHdr;
+            if (v & kHdr) {
+                if (ce != cs) spans.push_back({name, cs, ce, fl, li});
+                name = g.add_name(buf + hdrs[t][h++] + 1, len - 1);
+                have_name = len > 1;
+                cs = ce = 0;
+                fl = li + 1;
+                started = true;
+            } else {
+                if (!started) {
+                    err = {kBadInput, "fasta file needs to start with >"};
+                    return err.code;
+                }
+                if (!have_name) {
+                    err = {kBadInput, "> must be followed by chromosome name"};
+                    return err.code;
+                }
+                if (len + (size_t)(ce - cs) > kChunkSize) {
+                    spans.push_back({name, cs, ce, fl, li});
+                    cs = ce;
+                    fl = li;
+                }
+                if (len > kChunkSize) {
+                    err = {kBadInput, "line in fasta too long"};
+                    return err.code;
+                }
+                ce += len;
+            }
+            ++li;
+        }
+    }
+    if (ce > cs) spans.push_back({name, cs, ce, fl, li});
+    plan.file_bytes = n;
+    plan.n_lines = li;
+    uint64_t total = g.boff.back();
+    for (const Span &sp : spans) {
+        if (!g.start.empty() && sp.cs != 0 && g.end.back() != sp.cs) {
+            err = {kBadInput, "search expects chromosome chunks to arrive in order"};
+            return err.code;
+        }
+        g.name_idx.push_back(sp.name);
+        g.start.push_back(sp.cs);
+        g.end.push_back(sp.ce);
+        plan.first_line.push_back(sp.fl);
+        plan.last_line.push_back(sp.el);
+        plan.out.push_back(total);
+        plan.nt.push_back((uint32_t)(sp.ce - sp.cs));
+        total += (sp.ce - sp.cs + 1) / 2;
+        g.boff.push_back(total);
+    }
+    return kOk;
+}
+
 // read_2bit.rs:33-118, first half: the header, the index, and per record
 // its length and N blocks.  Sequences are taken one after the other in index
 // order (the stored offsets are skipped, as the reference does).  Appends the
@@ -463,7 +579,7 @@ int parse_2bit(HostGenome &g, const FileBytes &b, Error &err) {
 }  // namespace
 
 int load_genome_path(HostGenome &g, const std::string &path, Error &err) {
-    if (g.deferred && g.materialize(err)) return err.code;  // appending to it
+    if ((g.deferred || g.deferred_fa) && g.materialize(err)) return err.code;  // appending to it
     struct stat st;
     if (::stat(path.c_str(), &st)) {
         err = {kIo, "cannot stat " + path};
@@ -500,8 +616,19 @@ int load_genome_path(HostGenome &g, const std::string &path, Error &err) {
         err = {kIo, "cannot read " + path};
         return err.code;
     }
-    if (fv.p[0] == '>') return parse_fasta(g, fv.p, fv.n, err);
-    if (g.n_chunks() == 0 && !g.deferred) {
+    if (fv.p[0] == '>') {
+        if (g.n_chunks() == 0) {
+            // one FASTA file into an empty genome: the chunks are decided
+            // here; the device converts the bases at upload
+            auto plan = std::make_shared<FastaPlan>();
+            plan->path = path;
+            if (int rc = index_fasta(g, fv.p, fv.n, *plan, err)) return rc;
+            if (!plan->first_line.empty()) g.deferred_fa = plan;
+            return kOk;
+        }
+        return parse_fasta(g, fv.p, fv.n, err);
+    }
+    if (g.n_chunks() == 0) {
         // a .2bit file into an empty genome: only the index is read here;
         // the device decodes the bases at upload
         auto plan = std::make_shared<TwoBitPlan>();
@@ -514,6 +641,23 @@ int load_genome_path(HostGenome &g, const std::string &path, Error &err) {
 }
 
 int HostGenome::materialize(Error &err) {
+    if (deferred_fa) {
+        FileView fv;
+        if (int rc = fv.open(deferred_fa->path, err)) return rc;
+        if (fv.n != deferred_fa->file_bytes) {
+            err = {kIo, deferred_fa->path + " changed since it was loaded"};
+            return err.code;
+        }
+        HostGenome tmp;  // the same chunks, converted on the host
+        if (int rc = parse_fasta(tmp, fv.p, fv.n, err)) return rc;
+        if (tmp.n_bytes() != n_bytes()) {
+            err = {kIo, deferred_fa->path + " changed since it was loaded"};
+            return err.code;
+        }
+        data = std::move(tmp.data);
+        deferred_fa.reset();
+        return kOk;
+    }
     if (!deferred) return kOk;
     FileView fv;
     if (int rc = fv.open(deferred->path, err)) return rc;

@@ -83,30 +83,24 @@ bool read_fully(int fd, char *dst, size_t n, uint64_t off) {
 
 }  // namespace
 
-int upload_2bit(const TwoBitPlan &plan, uint8_t *bit4, int device, cudaStream_t s, Error &err) {
-    const size_t n_pieces = plan.pieces.size() - 1;
-    if (n_pieces == 0) return kOk;
-    const uint64_t raw_n = plan.raw_end - plan.raw_begin;
-    Scratch sc;
-    if (sc.raw.ensure(raw_n, err) || sc.pieces.ensure(plan.pieces.size(), err) ||
-        sc.nr.ensure(std::max<size_t>(plan.nr.size(), 1), err))
-        return err.code;
-
-    const int fd = ::open(plan.path.c_str(), O_RDONLY);
+int copy_file_to_device(const std::string &path, uint64_t file_bytes, uint64_t begin,
+                        uint64_t n, uint8_t *dst, int device, Error &err) {
+    if (n == 0) return kOk;
+    const int fd = ::open(path.c_str(), O_RDONLY);
     if (fd < 0) {
-        err = {kIo, "cannot open " + plan.path + ": " + std::strerror(errno)};
+        err = {kIo, "cannot open " + path + ": " + std::strerror(errno)};
         return err.code;
     }
     struct stat st;
-    if (::fstat(fd, &st) || (uint64_t)st.st_size != plan.file_bytes) {
+    if (::fstat(fd, &st) || (uint64_t)st.st_size != file_bytes) {
         ::close(fd);
-        err = {kIo, plan.path + " changed since it was loaded"};
+        err = {kIo, path + " changed since it was loaded"};
         return err.code;
     }
-    // file -> device: slices of kSlice bytes, every nt-th slice on one host
-    // thread, each thread with two page-locked buffers and its own stream
+    // slices of kSlice bytes, every nt-th slice on one host thread, each
+    // thread with two page-locked buffers and its own stream
     constexpr size_t kSlice = size_t(4) << 20;
-    const size_t n_slices = (size_t)((raw_n + kSlice - 1) / kSlice);
+    const size_t n_slices = (size_t)((n + kSlice - 1) / kSlice);
     const unsigned nt = (unsigned)std::max<size_t>(
         1, std::min<size_t>(n_slices, std::min(8u, std::max(1u, std::thread::hardware_concurrency()))));
     std::atomic<bool> failed{false};
@@ -138,13 +132,12 @@ int upload_2bit(const TwoBitPlan &plan, uint8_t *bit4, int device, cudaStream_t 
                 break;
             }
             const uint64_t off = (uint64_t)i * kSlice;
-            const size_t len = (size_t)std::min<uint64_t>(kSlice, raw_n - off);
-            if (!read_fully(fd, buf[b].p, len, plan.raw_begin + off)) {
-                fail("short read on " + plan.path);
+            const size_t len = (size_t)std::min<uint64_t>(kSlice, n - off);
+            if (!read_fully(fd, buf[b].p, len, begin + off)) {
+                fail("short read on " + path);
                 break;
             }
-            if (cudaMemcpyAsync(sc.raw.p + off, buf[b].p, len, cudaMemcpyHostToDevice, ts) !=
-                    cudaSuccess ||
+            if (cudaMemcpyAsync(dst + off, buf[b].p, len, cudaMemcpyHostToDevice, ts) != cudaSuccess ||
                 cudaEventRecord(ev[b], ts) != cudaSuccess) {
                 fail("genome copy failed");
                 break;
@@ -166,6 +159,20 @@ int upload_2bit(const TwoBitPlan &plan, uint8_t *bit4, int device, cudaStream_t 
         err = {kIo, msg};
         return err.code;
     }
+    return kOk;
+}
+
+int upload_2bit(const TwoBitPlan &plan, uint8_t *bit4, int device, cudaStream_t s, Error &err) {
+    const size_t n_pieces = plan.pieces.size() - 1;
+    if (n_pieces == 0) return kOk;
+    const uint64_t raw_n = plan.raw_end - plan.raw_begin;
+    Scratch sc;
+    if (sc.raw.ensure(raw_n, err) || sc.pieces.ensure(plan.pieces.size(), err) ||
+        sc.nr.ensure(std::max<size_t>(plan.nr.size(), 1), err))
+        return err.code;
+    if (copy_file_to_device(plan.path, plan.file_bytes, plan.raw_begin, raw_n, sc.raw.p, device,
+                            err))
+        return err.code;
     CU(cudaMemcpyAsync(sc.pieces.p, plan.pieces.data(), plan.pieces.size() * sizeof(TwoBitPlan::Piece),
                        cudaMemcpyHostToDevice, s));
     if (!plan.nr.empty())

@@ -69,12 +69,20 @@ class SynthGenome:
                 yield name, packed[s // 2:(e + 1) // 2].tobytes(), s, e
 
     def write_fasta(self, path, line_len=60):
+        """FASTA with `line_len`-column lines, each record's whole lines laid
+        out as one (lines x (line_len + 1)) array with a newline column."""
         with open(path, "wb") as f:
             for name, rec in zip(self.names, self.records):
                 f.write(b">" + name.encode() + b"\n")
                 chars = _CHARS[rec]
-                for s in range(0, len(chars), line_len):
-                    f.write(chars[s:s + line_len].tobytes() + b"\n")
+                full = len(chars) // line_len * line_len
+                if full:
+                    block = np.empty((full // line_len, line_len + 1), dtype=np.uint8)
+                    block[:, :line_len] = chars[:full].reshape(-1, line_len)
+                    block[:, line_len] = ord("\n")
+                    f.write(block.tobytes())
+                if full < len(chars):
+                    f.write(chars[full:].tobytes() + b"\n")
 
     def write_2bit(self, path):
         """UCSC .2bit v0 (the format read_2bit.rs reads): bases packed 2 bits

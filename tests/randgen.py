@@ -116,3 +116,24 @@ def random_case(seed, bulge=False):
         db, rb = rng.choice([(1, 0), (0, 1), (1, 1), (2, 1)])
         mm = min(mm, 3)
     return dict(chunks=chunks, filter=filt, patterns=pats, mm=mm, db=db, rb=rb, cps=cps)
+
+
+def write_messy_fasta(rng, path, final_newline):
+    # CRLF and LF lines, lowercase and IUPAC letters, N runs, blank lines,
+    # odd and varying line lengths (neighbouring lines share a bit4 byte),
+    # lines that push a chunk past 65,536 nt, a header ending in '\r'
+    parts = []
+    for r, n in enumerate((150001, 70003, 5, 131072)):
+        parts.append(f">rec{r} description {r}" + ("\r\n" if r % 2 else "\n"))
+        left = n
+        while left:
+            ln = min(left, rng.choice([1, 59, 60, 61, 997, 4096, 65535]))
+            seq = "".join(rng.choice("ACGTacgtNnRYKMSWBDHVx") for _ in range(ln))
+            eol = rng.choice(["\n", "\r\n", "\n\n"])
+            parts.append(seq + eol)
+            left -= ln
+    text = "".join(parts)
+    if not final_newline:
+        text = text.rstrip("\n") + "ACGTr"
+    with open(path, "w", newline="") as f:
+        f.write(text)

@@ -45,6 +45,30 @@ def test_host_loader_matches_oracle(cof_mod, oracle_mod, golden):
         assert g.n_nucl == o.n_nucl == 12507
 
 
+def test_fasta_index_matches_oracle(cof_mod, oracle_mod, tmp_path):
+    # a FASTA file loaded into an empty genome is only indexed on the host
+    # (all threads measure lines, one pass decides the chunks); the chunk
+    # table must be the oracle reader's
+    import random
+    import randgen
+    for final_newline in (True, False):
+        fa = tmp_path / f"g{final_newline}.fa"
+        randgen.write_messy_fasta(random.Random(7), fa, final_newline)
+        g = cof_mod.Genome(str(fa))
+        o = oracle_mod.OracleGenome(str(fa))
+        assert g.n_chunks == o.n_chunks > 8
+        assert g.n_nucl == o.n_nucl
+
+
+def test_fasta_index_errors(cof_mod, tmp_path):
+    for text in (">\nACGT\n", ">a\n" + "A" * 65537 + "\n"):
+        p = tmp_path / "bad.fa"
+        p.write_text(text)
+        with pytest.raises(cof_mod.CofError) as e:
+            cof_mod.Genome(str(p))
+        assert e.value.code == cof_mod.COF_E_BADINPUT
+
+
 def test_bad_requests_rejected(cof_mod, golden):
     g = cof_mod.Genome(os.path.join(golden, "upstream1000.fa"))
     with pytest.raises(cof_mod.CofError) as e:

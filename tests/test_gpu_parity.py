@@ -357,6 +357,37 @@ def test_chunk_added_after_2bit_load(cof_mod, oracle_mod, tmp_path):
     assert na == nref > 0 and sorted(ra.split("\n")) == sorted(ref.split("\n"))
 
 
+@pytest.mark.parametrize("final_newline", [True, False])
+def test_fasta_device_conversion(cof_mod, oracle_mod, tmp_path, final_newline):
+    # a FASTA file is converted on the device at upload; every window of the
+    # raw stream equals the oracle's own FASTA reader
+    rng = random.Random(41 + final_newline)
+    fa = tmp_path / "g.fa"
+    randgen.write_messy_fasta(rng, fa, final_newline)
+    g = cof_mod.Genome(str(fa))
+    o = oracle_mod.OracleGenome(str(fa))
+    assert g.n_nucl == o.n_nucl and g.n_chunks == o.n_chunks
+    ra, na = g.search("N" * 5, ["N" * 5], 4, raw=True)
+    ref, nref = o.search("N" * 5, ["N" * 5], 4, raw=True)
+    assert na == nref > 0 and sorted(ra.split("\n")) == sorted(ref.split("\n"))
+
+
+def test_chunk_added_after_fasta_load(cof_mod, oracle_mod, tmp_path):
+    # adding a chunk after a FASTA load converts the file on the host first
+    rng = random.Random(43)
+    fa = tmp_path / "g.fa"
+    randgen.write_messy_fasta(rng, fa, True)
+    extra = randgen.chunk_records(rng, ["".join(rng.choice("ACGT") for _ in range(3000))], 3000)
+    g = cof_mod.Genome(str(fa))
+    o = oracle_mod.OracleGenome(str(fa))
+    for name, data, _nibs, s, e in extra:
+        g.add_chunk("extra", data, s, e)
+        o.add_chunk("extra", data, s, e)
+    ra, na = g.search("N" * 5, ["N" * 5], 4, raw=True)
+    ref, nref = o.search("N" * 5, ["N" * 5], 4, raw=True)
+    assert na == nref > 0 and sorted(ra.split("\n")) == sorted(ref.split("\n"))
+
+
 @pytest.mark.parametrize("variant", [0, 6])
 def test_more_batches_than_one_scan_group_holds(cof_mod, oracle_mod, variant, monkeypatch):
     # ~300 batches (2 chunks each): more batch segments than a scan group
