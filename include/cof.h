@@ -84,7 +84,13 @@ COF_API int cof_genome_add_chunk(cof_genome *g, const char *chr_name,
 /* Loads a genome path the way cas-offinder-cli/src/main.rs:106-121 does:
  * a directory -> read_fasta_folder, first byte '>' -> read_fasta, otherwise
  * read_2bit (cas-offinder-lib/src/read_fasta.rs:9-71, read_2bit.rs:33-118,
- * read_fasta_folder.rs:8-23).  May be mixed with cof_genome_add_chunk. */
+ * read_fasta_folder.rs:8-23).  May be mixed with cof_genome_add_chunk.
+ * A single FASTA or .2bit file loaded into an empty genome is only indexed
+ * here (chunk table, names, N ranges); its bases are read from the file
+ * again and converted on the device by cof_genome_upload (or the first
+ * search), so the file must not change in between -- a changed size or line
+ * count fails the upload with COF_E_IO.  Adding chunks or files to such a
+ * genome converts its bases on the host first. */
 COF_API int cof_genome_load(cof_genome *g, const char *path);
 
 /* Packs the chunk stream into HBM (bit4 stream + 2-bit/N-mask planes).
