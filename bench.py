@@ -374,6 +374,7 @@ def bench_cli(cfg, n_rows, runs=2, fmt="2bit"):
             cfg["genome"].write_2bit(path)
         else:
             cfg["genome"].write_fasta(path)
+        os.sync()  # a genome file at rest: no writeback during the timed runs
         t_write = time.perf_counter() - t0
         inp = os.path.join(d, "input.txt")
         with open(inp, "w") as f:

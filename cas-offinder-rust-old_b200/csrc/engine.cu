@@ -579,57 +579,82 @@ __global__ void verify_kernel(GenomeDev G, const BatchDev *__restrict__ batches,
                               uint32_t n_hits, Row *__restrict__ rows, uint64_t *__restrict__ keys,
                               uint32_t *__restrict__ vals, Counters *ctr,
                               uint32_t *__restrict__ req_rows) {
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n_hits;
-         i += gridDim.x * blockDim.x) {
-        const Hit h = hits[i];
-        const BatchDev B = batches[h.batch];
-        const uint32_t pe = fast2exact[h.pattern];
-        const ExactPattern &P = pats[pe];
-        const RequestDev &R = reqs[P.request];
-        const uint32_t L = P.L;
-        // a scan group's windows cover the starts of all its pattern lengths:
-        // keep this length's own range (legacy_match_start_min_nucl,
-        // search.rs:540-546, up to the batch's valid cells)
-        const uint32_t msmin = B.active_start > L - 1 ? B.active_start - (L - 1) : 0;
-        if (h.s_local < msmin || h.s_local >= B.valid) continue;
-        const uint64_t sg = B.base + h.s_local;
-        // search_chunk_cpu count on the N-masked batch buffer (zero past the
-        // batch's valid bytes)
-        uint8_t g[kMaxPatternLen];
-        int matches = 0;
-        for (uint32_t c = 0; c < L; ++c) {
-            uint8_t v = (h.s_local + c < B.valid) ? nib(G.bit4, sg + c) : 0;
-            if (v == 0xF) v = 0;
-            g[c] = v;
-            matches += __popc(v & P.b4[c]);
+    // the block steps through the hits together, so every lane of a warp
+    // reaches the row emission below; rows get their slots and requests
+    // their counts with one atomic per warp (per request), not per row
+    const uint32_t lane = threadIdx.x & 31, lt_mask = (1u << lane) - 1u;
+    for (uint32_t base = blockIdx.x * blockDim.x; base < n_hits; base += gridDim.x * blockDim.x) {
+        const uint32_t i = base + threadIdx.x;
+        bool emit = false;
+        Row row{};
+        uint64_t key = 0;
+        uint32_t req = 0xFFFFFFFFu;
+        do {
+            if (i >= n_hits) break;
+            const Hit h = hits[i];
+            const BatchDev B = batches[h.batch];
+            const uint32_t pe = fast2exact[h.pattern];
+            const ExactPattern &P = pats[pe];
+            const RequestDev &R = reqs[P.request];
+            const uint32_t L = P.L;
+            // a scan group's windows cover the starts of all its pattern
+            // lengths: keep this length's own range
+            // (legacy_match_start_min_nucl, search.rs:540-546, up to the
+            // batch's valid cells)
+            const uint32_t msmin = B.active_start > L - 1 ? B.active_start - (L - 1) : 0;
+            if (h.s_local < msmin || h.s_local >= B.valid) break;
+            const uint64_t sg = B.base + h.s_local;
+            // search_chunk_cpu count on the N-masked batch buffer (zero past
+            // the batch's valid bytes)
+            uint8_t g[kMaxPatternLen];
+            int matches = 0;
+            for (uint32_t c = 0; c < L; ++c) {
+                uint8_t v = (h.s_local + c < B.valid) ? nib(G.bit4, sg + c) : 0;
+                if (v == 0xF) v = 0;
+                g[c] = v;
+                matches += __popc(v & P.b4[c]);
+            }
+            if ((int)L - matches > (int)R.max_mm) break;
+            // convert_matches: owning chunk, record position, record-end drop
+            const uint64_t gbyte = sg >> 1;
+            uint32_t lo = B.first, hi = B.first + B.nch;  // boff[lo] <= gbyte < boff[hi]
+            while (hi - lo > 1) {
+                uint32_t mid = (lo + hi) >> 1;
+                if (G.boff[mid] <= gbyte) lo = mid; else hi = mid;
+            }
+            const uint32_t k = lo;
+            const uint64_t pos = G.start[k] + (sg - 2 * G.boff[k]);
+            const bool end_chrom = (k == B.first + B.nch - 1) || G.start[k + 1] == 0;
+            if (end_chrom && pos + L > G.end[k]) break;
+            // writer: PAM filter and mismatch recount
+            const uint32_t st = P.strand;
+            uint32_t actual = 0;
+            bool pam_ok = true;
+            for (uint32_t c = 0; c < L; ++c) {
+                const bool sb = single_base(g[c]);
+                if (!R.fisn[st][c] && !(sb && (g[c] & R.fset[st][c]))) { pam_ok = false; break; }
+                if (P.b4[c] != 0xF && !(sb && (g[c] & P.b4[c]))) ++actual;
+            }
+            if (!pam_ok || actual > R.max_mm) break;
+            emit = true;
+            row = Row{sg, B.base + B.valid, pos, k, pe, actual, 0};
+            key = ((uint64_t)pe << 34) | sg;
+            req = P.request;
+        } while (false);
+        const uint32_t em = __ballot_sync(0xFFFFFFFFu, emit);
+        if (!em) continue;
+        const int leader = __ffs(em) - 1;
+        uint32_t r0 = 0;
+        if ((int)lane == leader) r0 = atomicAdd(&ctr->rows, (uint32_t)__popc(em));
+        r0 = __shfl_sync(0xFFFFFFFFu, r0, leader);
+        const uint32_t peers = __match_any_sync(0xFFFFFFFFu, req);
+        if (emit) {
+            const uint32_t r = r0 + __popc(em & lt_mask);
+            rows[r] = row;
+            keys[r] = key;
+            vals[r] = r;
+            if ((int)lane == __ffs(peers) - 1) atomicAdd(&req_rows[req], (uint32_t)__popc(peers));
         }
-        if ((int)L - matches > (int)R.max_mm) continue;
-        // convert_matches: owning chunk, record position, record-end drop
-        const uint64_t gbyte = sg >> 1;
-        uint32_t lo = B.first, hi = B.first + B.nch;  // boff[lo] <= gbyte < boff[hi]
-        while (hi - lo > 1) {
-            uint32_t mid = (lo + hi) >> 1;
-            if (G.boff[mid] <= gbyte) lo = mid; else hi = mid;
-        }
-        const uint32_t k = lo;
-        const uint64_t pos = G.start[k] + (sg - 2 * G.boff[k]);
-        const bool end_chrom = (k == B.first + B.nch - 1) || G.start[k + 1] == 0;
-        if (end_chrom && pos + L > G.end[k]) continue;
-        // writer: PAM filter and mismatch recount
-        const uint32_t st = P.strand;
-        uint32_t actual = 0;
-        bool pam_ok = true;
-        for (uint32_t c = 0; c < L; ++c) {
-            const bool sb = single_base(g[c]);
-            if (!R.fisn[st][c] && !(sb && (g[c] & R.fset[st][c]))) { pam_ok = false; break; }
-            if (P.b4[c] != 0xF && !(sb && (g[c] & P.b4[c]))) ++actual;
-        }
-        if (!pam_ok || actual > R.max_mm) continue;
-        const uint32_t r = atomicAdd(&ctr->rows, 1u);
-        rows[r] = Row{sg, B.base + B.valid, pos, k, pe, actual, 0};
-        keys[r] = ((uint64_t)pe << 34) | sg;
-        vals[r] = r;
-        atomicAdd(&req_rows[P.request], 1u);
     }
 }
 
