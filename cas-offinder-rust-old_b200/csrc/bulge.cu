@@ -141,7 +141,7 @@ __global__ void myers_filter_kernel(const uint8_t *__restrict__ bit4,
             if (q >= T.t0 && score <= (int)P.E) {
                 const uint32_t tl = (uint32_t)(q - B.base);
                 if (tl + 1 >= L && pam_quick(bit4, B, tl, P, R.db, R.rb)) {
-                    const uint32_t i = atomicAdd(&ctr->hits, 1u);
+                    const uint32_t i = append_slot(&ctr->hits);
                     if (i < cap) cand[i] = MyersCand{tl, T.batch, p, 0};
                     else ctr->overflow = 1;
                 }
@@ -262,7 +262,7 @@ myers_tile_kernel(const uint8_t *__restrict__ bit4, const BatchDev *__restrict__
                     if (((okb >> (r & 31)) & 1u) && score <= (int)P.E) {
                         const uint32_t tlc = (uint32_t)(q - B.base);
                         if (tlc + 1 >= L) {
-                            const uint32_t c = atomicAdd(&ctr->hits, 1u);
+                            const uint32_t c = append_slot(&ctr->hits);
                             if (c < cap) cand[c] = MyersCand{tlc, T.batch, p, 0};
                             else ctr->overflow = 1;
                         }

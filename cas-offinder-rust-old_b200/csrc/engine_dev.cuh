@@ -3,6 +3,7 @@
 // batches, small device helpers and scratch buffers.
 #pragma once
 
+#include <cooperative_groups.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -113,6 +114,16 @@ __device__ __forceinline__ char *put_u64(char *o, uint64_t v) {
     do { t[k++] = (char)('0' + v % 10); v /= 10; } while (v);
     while (k) *o++ = t[--k];
     return o;
+}
+
+// A slot in an append-only list: the lanes that append together take
+// consecutive slots with one atomic on the list's counter.
+__device__ __forceinline__ uint32_t append_slot(uint32_t *counter) {
+    namespace cg = cooperative_groups;
+    const cg::coalesced_group g = cg::coalesced_threads();
+    uint32_t base = 0;
+    if (g.thread_rank() == 0) base = atomicAdd(counter, g.size());
+    return g.shfl(base, 0) + g.thread_rank();
 }
 
 template <class T>
