@@ -197,8 +197,8 @@ __device__ __forceinline__ FastPattern lds_pattern(uint32_t saddr) {
 // Compares the queued windows (32 * kCpt at most, kCpt per lane) with every
 // pattern of the group and appends the hits.  kSmem: the pattern table is in
 // shared memory (all but the largest groups).  kPair selects how a lane
-// reduces its kCpt mismatch counts per pattern: 1 one minimum chain, 2 two
-// patterns per step (two chains), 4 three-input minima (__vimin3_s32).
+// reduces its kCpt mismatch counts per pattern: 1 one minimum chain, 4
+// three-input minima (__vimin3_s32).
 template <int kCpt, int kPair, bool kSmem>
 __device__ __forceinline__ void flush_body(const uint4 *q, int n, const FastPattern *pt,
                                            const ScanGroup &G, uint32_t batch,
@@ -230,19 +230,6 @@ __device__ __forceinline__ void flush_body(const uint4 *q, int n, const FastPatt
             }
         };
         uint32_t p = K.pat_begin;
-        if (kPair == 2) {  // two independent min chains per iteration
-            for (; p + 1 < K.pat_end; p += 2) {
-                const FastPattern f0 = load(p), f1 = load(p + 1);
-                int m0 = 64, m1 = 64;
-#pragma unroll
-                for (int j = 0; j < kCpt; ++j) {
-                    m0 = min(m0, (int)__popc((mh[j] ^ f0.h) | (ml[j] ^ f0.l) | ms[j]));
-                    m1 = min(m1, (int)__popc((mh[j] ^ f1.h) | (ml[j] ^ f1.l) | ms[j]));
-                }
-                if (m0 <= f0.k) emit(p, f0);
-                if (m1 <= f1.k) emit(p + 1, f1);
-            }
-        }
         if (kPair == 4) {  // minimum of three per instruction, depth log3(kCpt)
             for (; p < K.pat_end; ++p) {
                 const FastPattern f0 = load(p);
@@ -458,14 +445,14 @@ scan_kernel(ScanParams P) {
 // table of all groups is staged in shared memory once, up to kSmemPatterns
 // patterns; a group whose patterns lie beyond that prefix reads them from
 // global memory.  Group and segment descriptors are read through L1.
-template <int kCpt, int kScanWarps, int kMinBlocks, int kPair>
+template <int kCpt, int kScanWarps, int kMinBlocks, int kPair, int kPatCap>
 __global__ void __launch_bounds__(kScanWarps * 32, kMinBlocks)
 scan_warp_kernel(ScanParams P) {
     constexpr int kQSlots = 32 * kCpt + 32;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     uint4 *queues = reinterpret_cast<uint4 *>(smem_raw);
     FastPattern *spat = reinterpret_cast<FastPattern *>(queues + kScanWarps * kQSlots);
-    const uint32_t n_staged = min(P.n_pats, (uint32_t)kSmemPatterns);
+    const uint32_t n_staged = min(P.n_pats, (uint32_t)kPatCap);
     for (uint32_t i = threadIdx.x; i < n_staged; i += blockDim.x) spat[i] = P.pats[i];
     __syncthreads();
 
@@ -538,19 +525,20 @@ struct ScanVariant {
     uint32_t span_tiles;
     void (*kernel)(ScanParams);
     bool per_warp;
+    uint32_t pat_cap;  // patterns staged in shared memory
     size_t smem() const {
-        return (size_t)warps * (32 * cpt + 32) * sizeof(uint4) + kSmemPatterns * sizeof(FastPattern);
+        return (size_t)warps * (32 * cpt + 32) * sizeof(uint4) + pat_cap * sizeof(FastPattern);
     }
 };
 
 template <int C, int W, int B, int Q = 1>
 constexpr ScanVariant variant(uint32_t span) {
-    return ScanVariant{C, W, B, Q, span, scan_kernel<C, W, B, Q>, false};
+    return ScanVariant{C, W, B, Q, span, scan_kernel<C, W, B, Q>, false, kSmemPatterns};
 }
-// span: tiles per warp work item
-template <int C, int W, int B, int Q = 1>
+// span: tiles per warp work item; K: patterns staged in shared memory
+template <int C, int W, int B, int Q = 1, int K = kSmemPatterns>
 constexpr ScanVariant warp_variant(uint32_t span) {
-    return ScanVariant{C, W, B, Q, span, scan_warp_kernel<C, W, B, Q>, true};
+    return ScanVariant{C, W, B, Q, span, scan_warp_kernel<C, W, B, Q, K>, true, (uint32_t)K};
 }
 
 // Candidate tile shapes (windows per lane x warps x min blocks per SM, and
@@ -558,13 +546,11 @@ constexpr ScanVariant warp_variant(uint32_t span) {
 // genome.  Two patterns per step need registers that only the shapes with
 // fewer blocks per SM have.
 const ScanVariant kScanVariants[] = {
-    // per-warp work items
-    warp_variant<8, 8, 3, 4>(8),  warp_variant<8, 8, 3>(8),  warp_variant<8, 8, 3>(32),
-    warp_variant<16, 8, 2, 4>(8), warp_variant<16, 8, 2>(8), warp_variant<8, 8, 2, 2>(8),
+    // per-warp work items: four CTAs per SM (1024 staged patterns), then three
+    warp_variant<8, 8, 4, 4, 1024>(8), warp_variant<8, 8, 4, 1, 1024>(8),
+    warp_variant<4, 8, 4, 4, 1024>(8), warp_variant<8, 8, 3, 4>(8), warp_variant<8, 8, 3>(8),
     // CTA work items
-    variant<8, 8, 3>(64),     variant<4, 8, 4>(64),     variant<16, 8, 2>(64),
-    variant<8, 4, 6>(32),     variant<16, 4, 4>(32),    variant<4, 16, 2>(128),
-    variant<8, 8, 2, 2>(64),  variant<16, 8, 2, 2>(64), variant<8, 4, 4, 2>(32),
+    variant<8, 8, 3>(64), variant<4, 8, 4>(64), variant<4, 16, 2>(128),
 };
 constexpr int kNumScanVariants = sizeof(kScanVariants) / sizeof(kScanVariants[0]);
 
@@ -1219,7 +1205,7 @@ int Engine::run_popcount(const std::vector<Request> &reqs, std::vector<Result> &
         }
         const ScanVariant &v = kScanVariants[vi];
         times_.scan_variant = vi;
-        static const char *const kMinName[] = {"", "", "pp2-", "", "min3-"};
+        static const char *const kMinName[] = {"", "", "", "", "min3-"};
         times_.scan_shape = std::string(v.per_warp ? "warp-" : "") + kMinName[v.pair] + "cpt" + std::to_string(v.cpt) + "-warps" + std::to_string(v.warps) +
                             "-minb" + std::to_string(v.min_blocks) + "-span" +
                             std::to_string(v.span_tiles);

@@ -149,7 +149,7 @@ def test_cli_matches_oracle_cli(cof_mod, oracle_mod, golden, tmp_path):
         assert "=== Cas-OFFinder Rust ===" in log and "Matches found: 117" in log
 
 
-N_SCAN_VARIANTS = 15  # per-warp work items: 0-5; CTA work items: 6-14
+N_SCAN_VARIANTS = 8  # per-warp work items: 0-4; CTA work items: 5-7
 
 
 @pytest.mark.parametrize("variant", range(N_SCAN_VARIANTS))
@@ -167,10 +167,10 @@ def test_every_scan_tile_shape(cof_mod, oracle_mod, golden, variant, monkeypatch
     assert g2.tuning()["variant"] == variant
 
 
-@pytest.mark.parametrize("variant", [0, 5, 6])
+@pytest.mark.parametrize("variant", [0, 3, 5])
 def test_patterns_beyond_the_shared_memory_table(cof_mod, oracle_mod, variant, monkeypatch):
     # 1500 guides: 3000 patterns in two strand groups; the per-warp scan
-    # stages the first 2048 patterns, so the reverse-strand group reads its
+    # stages the first 1024 or 2048 patterns, so later groups read their
     # patterns from global memory
     monkeypatch.setenv("COF_SCAN_VARIANT", str(variant))
     rng = random.Random(77)
@@ -388,7 +388,7 @@ def test_chunk_added_after_fasta_load(cof_mod, oracle_mod, tmp_path):
     assert na == nref > 0 and sorted(ra.split("\n")) == sorted(ref.split("\n"))
 
 
-@pytest.mark.parametrize("variant", [0, 6])
+@pytest.mark.parametrize("variant", [0, 5])
 def test_more_batches_than_one_scan_group_holds(cof_mod, oracle_mod, variant, monkeypatch):
     # ~300 batches (2 chunks each): more batch segments than a scan group
     # stages, as with chunks_per_search 64 (the CLI's C) on a large genome
