@@ -308,7 +308,27 @@ def bench_bulge(cof, device, steps, scale):
             "stages_ms": {k: statistics.median(s[k] for s in stats)
                           for k in ("scan_ms", "verify_ms", "format_ms", "d2h_ms", "total_ms")},
             "rows_per_step": rows, "candidates_per_step": stats[-1]["candidates"],
-            "gpu_launches_per_step": stats[-1]["kernel_launches"], "steps": steps}
+            "gpu_launches_per_step": stats[-1]["kernel_launches"], "steps": steps,
+            "stage_rates": bulge_rates(cfg, stats, rows)}
+
+
+def bulge_rates(cfg, stats, rows):
+    """Per-stage work rates of the bulge path (its kernels are integer DP, so
+    rates of their own units stand in for a roofline): Myers steps (one text
+    position x one pattern, both strands), budget-DP cells of the Myers
+    candidates (L x (L + max_db + 1) per candidate, an upper bound: the test
+    stops early), and rows enumerated by the traceback."""
+    L = len(cfg["patterns"][0])
+    n_pat = 2 * len(cfg["patterns"])
+    scan = statistics.median(s["scan_ms"] for s in stats) * 1e-3
+    verify = statistics.median(s["verify_ms"] for s in stats) * 1e-3
+    fmt = statistics.median(s["format_ms"] for s in stats) * 1e-3
+    cand = stats[-1]["candidates"]
+    return {"myers_steps_per_s": cfg["genome"].n_nucl * n_pat / scan,
+            "budget_dp_cells_per_s": cand * L * (L + cfg["max_dna_bulges"] + 1) / verify,
+            "candidates_per_s": cand / verify, "rows_per_s_traceback": rows / verify,
+            "rows_per_s_format": rows / fmt,
+            "note": "budget pre-test and traceback share one timed stage (verify_ms)"}
 
 
 class CpuSample:
