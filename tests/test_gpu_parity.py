@@ -372,6 +372,37 @@ def test_fasta_device_conversion(cof_mod, oracle_mod, tmp_path, final_newline):
     assert na == nref > 0 and sorted(ra.split("\n")) == sorted(ref.split("\n"))
 
 
+@pytest.mark.parametrize("seed", range(6))
+def test_random_genome_files_device_decode(cof_mod, oracle_mod, tmp_path, seed):
+    # seeded random FASTA and .2bit files of a few records: the device
+    # conversion of each equals the oracle's reader, window by window
+    import twobit
+    rng = random.Random(100 + seed)
+    fa = tmp_path / "r.fa"
+    parts = []
+    recs = []
+    for r in range(rng.randint(1, 4)):
+        n = rng.randint(1, 90000)
+        seq = "".join(rng.choice("ACGTNacgtnRY") for _ in range(n))
+        recs.append((f"s{r}", seq.replace("R", "N").replace("Y", "N")))
+        parts.append(f">s{r} x\n")
+        i = 0
+        while i < n:
+            ln = rng.choice([1, 7, 50, 60, 61, 80, 4000])
+            parts.append(seq[i:i + ln] + rng.choice(["\n", "\r\n"]))
+            i += ln
+    fa.write_text("".join(parts), newline="")
+    tb = tmp_path / "r.2bit"
+    twobit.write_2bit(str(tb), recs)
+    for path in (fa, tb):
+        g = cof_mod.Genome(str(path))
+        o = oracle_mod.OracleGenome(str(path))
+        assert g.n_nucl == o.n_nucl and g.n_chunks == o.n_chunks
+        ra, na = g.search("N" * 4, ["N" * 4], 3, raw=True)
+        ref, nref = o.search("N" * 4, ["N" * 4], 3, raw=True)
+        assert na == nref and sorted(ra.split("\n")) == sorted(ref.split("\n"))
+
+
 def test_chunk_added_after_fasta_load(cof_mod, oracle_mod, tmp_path):
     # adding a chunk after a FASTA load converts the file on the host first
     rng = random.Random(43)
