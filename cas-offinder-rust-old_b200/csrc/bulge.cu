@@ -1387,7 +1387,10 @@ int Engine::run_bulge(const std::vector<Request> &reqs, std::vector<Result> &out
         times_.verify_ms += ms;
         cands = d.mcand2.p;
     }
+    // candidates per chunk; COF_BULGE_CHUNK lowers it (tests: many chunks)
     uint32_t chunk = std::max<uint32_t>(1, std::min<uint32_t>(n_work, 1u << 21));
+    if (const char *e = std::getenv("COF_BULGE_CHUNK"))
+        chunk = std::max<uint32_t>(1, std::min<uint32_t>(chunk, (uint32_t)std::max(1, std::atoi(e))));
     uint32_t c0 = 0;
     while (c0 < n_work) {
         const uint32_t cn = std::min(chunk, n_work - c0);
@@ -1470,7 +1473,10 @@ int Engine::run_bulge(const std::vector<Request> &reqs, std::vector<Result> &out
             uint64_t bytes = 0;
             CU(cudaMemcpyAsync(&bytes, d.offs.p + nr, 8, cudaMemcpyDeviceToHost, s));
             CU(cudaStreamSynchronize(s));
-            if (grow_keep(d.text, arena + bytes + 1, arena, s, err)) return err.code;
+            // each chunk's text starts 16-byte aligned, after the bytes in use
+            const uint64_t in_use = arena;
+            arena = (arena + 15) & ~15ull;
+            if (grow_keep(d.text, arena + bytes + 1, in_use, s, err)) return err.code;
             mrow_write_kernel<<<fb, 256, 0, s>>>(d.view(), d.mrows.p, d.vals2.p, nr, dP, dR,
                                                  d.offs.p, d.text.p + arena);
             CU(cudaGetLastError());

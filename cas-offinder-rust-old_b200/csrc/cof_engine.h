@@ -125,8 +125,9 @@ int make_request(const char *filter, size_t pattern_len, const char *const *patt
 // Page-locked host buffers for result text.  The device copies each
 // request's rows straight into one of them, and that buffer becomes the
 // caller's cof_result.text; cof_result_free hands it back.  Freed buffers
-// are kept (up to kKeepBytes) and reused, so a steady stream of searches
-// neither pins nor first-touches new host pages.
+// are kept (up to kKeepBytes, and always the one returned last) and reused,
+// so a steady stream of searches neither pins nor first-touches new host
+// pages.
 //
 // Results of up to kSmallMax bytes (the rows of a few guides) are blocks of
 // a power-of-two size class cut from page-locked slabs of at least

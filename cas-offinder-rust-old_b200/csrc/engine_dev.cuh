@@ -266,20 +266,26 @@ __device__ __forceinline__ void warp_rows_staged(uint32_t i0, uint32_t n,
     const uint32_t lane = threadIdx.x & 31;
     const uint32_t i = i0 + lane;
     const uint64_t start = off[i0], end = off[min(i0 + 32, n)];
-    const uint64_t base = start & ~3ull;  // stage byte k <-> output byte base + k
-    if (end - base > cap) {
+    // stage byte k <-> output byte start - mis + k, so that 4-byte-aligned
+    // stage words land on 4-byte-aligned output addresses (text itself may
+    // start anywhere)
+    const uintptr_t tb = reinterpret_cast<uintptr_t>(text);
+    const uint32_t mis = (uint32_t)((tb + start) & 3u);
+    if (end - start + mis > cap) {
         if (i < n) row(i, text + off[i]);
         return;
     }
-    if (i < n) row(i, stage + (off[i] - base));
+    if (i < n) row(i, stage + (off[i] - start + mis));
     __syncwarp();
-    const uint64_t a0 = (start + 3) & ~3ull, a1 = end & ~3ull;
+    const uint64_t a0 = start + ((4u - mis) & 3u);           // first aligned output byte
+    const uint64_t a1 = end - (uint64_t)((tb + end) & 3u);  // end of the last aligned word
+    auto sb = [&](uint64_t g) { return stage[g - start + mis]; };
     if (a0 >= a1) {  // no whole aligned word: bytes only
-        for (uint64_t g = start + lane; g < end; g += 32) text[g] = stage[g - base];
+        for (uint64_t g = start + lane; g < end; g += 32) text[g] = sb(g);
     } else {
-        if (start + lane < a0) text[start + lane] = stage[start + lane - base];
-        if (a1 + lane < end) text[a1 + lane] = stage[a1 + lane - base];
-        const uint32_t *sw = reinterpret_cast<const uint32_t *>(stage + (a0 - base));
+        if (start + lane < a0) text[start + lane] = sb(start + lane);
+        if (a1 + lane < end) text[a1 + lane] = sb(a1 + lane);
+        const uint32_t *sw = reinterpret_cast<const uint32_t *>(stage + (a0 - start + mis));
         uint32_t *gw = reinterpret_cast<uint32_t *>(text + a0);
         for (uint64_t w = lane; w < (a1 - a0) / 4; w += 32) gw[w] = sw[w];
     }

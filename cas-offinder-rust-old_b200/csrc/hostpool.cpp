@@ -86,9 +86,12 @@ bool PinnedPool::release(char *p) {
     }
     free_.emplace(n, p);
     free_bytes_ += n;
-    while (free_bytes_ > kKeepBytes && !free_.empty()) {  // keep the newest sizes
+    // over kKeepBytes, free the smallest kept buffers, but never the one just
+    // released: a caller repeating a search whose rows alone pass the limit
+    // reuses it instead of pinning gigabytes again
+    while (free_bytes_ > kKeepBytes && free_.size() > 1) {
         auto victim = free_.begin();
-        if (victim->second == p && free_.size() > 1) ++victim;
+        if (victim->second == p) ++victim;
         free_bytes_ -= victim->first;
         cudaFreeHost(victim->second);
         free_.erase(victim);

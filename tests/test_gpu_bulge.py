@@ -117,3 +117,28 @@ def test_warp_traceback_equals_thread_traceback(cof_mod, oracle_mod, monkeypatch
             o.add_chunk(name, data, s, e)
         ref, nref = o.search(*args)
         assert nref == n and sorted(ref.splitlines()) == sorted(text.splitlines())
+
+
+@pytest.mark.parametrize("per_chunk", [1, 7, 64])
+def test_many_traceback_chunks(cof_mod, oracle_mod, monkeypatch, per_chunk):
+    # the surviving candidates are walked in chunks whose row texts follow
+    # each other in one device arena, which grows as they come (a large
+    # genome makes many chunks; COF_BULGE_CHUNK forces them here); the rows
+    # equal the one-chunk search and the oracle
+    import synth
+    cfg = synth.config_bulge(seed=6, scale=0.0002, n_guides=6, planted=8)
+    g = cof_mod.Genome()
+    cfg["genome"].load_into(g)
+    args = (cfg["filter"], cfg["patterns"], cfg["max_mismatches"], cfg["max_dna_bulges"],
+            cfg["max_rna_bulges"])
+    # many chunks first: the fresh text arena grows chunk by chunk
+    monkeypatch.setenv("COF_BULGE_CHUNK", str(per_chunk))
+    many, nm = g.search(*args)
+    monkeypatch.delenv("COF_BULGE_CHUNK", raising=False)
+    one, n1 = g.search(*args)
+    assert nm == n1 > 0 and sorted(many.splitlines()) == sorted(one.splitlines())
+    o = oracle_mod.OracleGenome()
+    for name, data, s, e in cfg["genome"].chunks():
+        o.add_chunk(name, data, s, e)
+    ref, nref = o.search(*args)
+    assert nref == n1 and sorted(ref.splitlines()) == sorted(one.splitlines())
