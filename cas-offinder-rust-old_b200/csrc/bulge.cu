@@ -1268,7 +1268,7 @@ int Engine::run_bulge(const std::vector<Request> &reqs, std::vector<Result> &out
     const MyersPattern *dP = (const MyersPattern *)tab(o_p);
     const MyersReqDev *dR = (const MyersReqDev *)tab(o_r);
     if (d.ctr.ensure(1, err) || d.req_rows.ensure(reqs.size(), err)) return err.code;
-    if (d.mcand.cap == 0 && d.mcand.ensure(1u << 22, err)) return err.code;
+    if (d.mcand.cap == 0 && d.mcand.ensure(first_cand_cap(), err)) return err.code;
 
     // stage 1: streaming Myers + PAM -> candidates
     Counters hc{};

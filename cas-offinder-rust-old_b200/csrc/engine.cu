@@ -1122,7 +1122,7 @@ int Engine::run_popcount(const std::vector<Request> &reqs, std::vector<Result> &
     CU(cudaMemcpyAsync(d.tables.p, tp.buf.data(), tp.buf.size(), cudaMemcpyHostToDevice, s));
     auto tab = [&](size_t o) { return (const void *)(d.tables.p + o); };
     if (d.ctr.ensure(1, err) || d.req_rows.ensure(reqs.size(), err)) return err.code;
-    if (d.hits.cap == 0 && d.hits.ensure(1u << 22, err)) return err.code;
+    if (d.hits.cap == 0 && d.hits.ensure(first_cand_cap(), err)) return err.code;
 
     ScanParams sp{};
     sp.H = d.planes.p;  // word w holds shifted window starts [32 w, 32 w + 32)

@@ -7,6 +7,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -124,6 +125,18 @@ __device__ __forceinline__ uint32_t append_slot(uint32_t *counter) {
     uint32_t base = 0;
     if (g.thread_rank() == 0) base = atomicAdd(counter, g.size());
     return g.shfl(base, 0) + g.thread_rank();
+}
+
+// Starting entries of a candidate list (scan hits, Myers candidates); a
+// search that overflows it grows it and runs again.  COF_CAND_CAP lowers the
+// start (tests of the overflow path).
+inline size_t first_cand_cap() {
+    size_t cap = size_t(1) << 22;
+    if (const char *e = std::getenv("COF_CAND_CAP")) {
+        const long v = std::atol(e);
+        if (v > 0) cap = std::min(cap, (size_t)v);
+    }
+    return cap;
 }
 
 template <class T>

@@ -142,3 +142,22 @@ def test_many_traceback_chunks(cof_mod, oracle_mod, monkeypatch, per_chunk):
         o.add_chunk(name, data, s, e)
     ref, nref = o.search(*args)
     assert nref == n1 and sorted(ref.splitlines()) == sorted(one.splitlines())
+
+
+def test_myers_candidate_list_overflow(cof_mod, oracle_mod, monkeypatch):
+    # the Myers candidate list starts at 64 entries (COF_CAND_CAP) on a fresh
+    # genome: it overflows, grows and the filter runs again
+    import synth
+    monkeypatch.setenv("COF_CAND_CAP", "1")
+    cfg = synth.config_bulge(seed=7, scale=0.0002, n_guides=4, planted=6)
+    g = cof_mod.Genome()
+    cfg["genome"].load_into(g)
+    args = (cfg["filter"], cfg["patterns"], cfg["max_mismatches"], cfg["max_dna_bulges"],
+            cfg["max_rna_bulges"])
+    text, n = g.search(*args)
+    assert g.last_stats()["candidates"] > 64  # it did overflow
+    o = oracle_mod.OracleGenome()
+    for name, data, s, e in cfg["genome"].chunks():
+        o.add_chunk(name, data, s, e)
+    ref, nref = o.search(*args)
+    assert n == nref > 0 and sorted(ref.splitlines()) == sorted(text.splitlines())

@@ -186,6 +186,16 @@ def test_patterns_beyond_the_shared_memory_table(cof_mod, oracle_mod, variant, m
     assert g.tuning()["variant"] == variant
 
 
+def test_candidate_list_overflow(cof_mod, golden, monkeypatch):
+    # a fresh genome whose scan hit list starts at 64 entries (COF_CAND_CAP):
+    # the KAT's hits overflow it, the list grows and the scan runs again
+    monkeypatch.setenv("COF_CAND_CAP", "1")
+    g = cof_mod.Genome(os.path.join(golden, "upstream1000.fa"))
+    text, n = g.search("N" * 24, KAT_PATS, 11)
+    assert n == 117 and _rows(text) == _golden_rows(golden, "kat_popcount_rows.txt")
+    assert g.last_stats()["raw_hits"] > 64  # it did overflow
+
+
 def test_autotuner_records_choice(cof_mod, golden, monkeypatch):
     monkeypatch.delenv("COF_SCAN_VARIANT", raising=False)
     g = cof_mod.Genome(os.path.join(golden, "upstream1000.fa"))
