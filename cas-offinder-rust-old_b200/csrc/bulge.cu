@@ -1328,7 +1328,11 @@ int Engine::run_bulge(const std::vector<Request> &reqs, std::vector<Result> &out
     std::vector<uint64_t> nrows(reqs.size(), 0);
     std::vector<std::array<uint64_t, 3>> segs;
     uint64_t arena = 0;
-    const size_t row_cap = 1u << 24;
+    // rows one chunk may produce; a chunk that produces more is halved and
+    // walked again (COF_BULGE_ROW_CAP lowers the cap: tests of that path)
+    size_t row_cap = 1u << 24;
+    if (const char *e = std::getenv("COF_BULGE_ROW_CAP"))
+        row_cap = std::min(row_cap, (size_t)std::max(64L, std::atol(e)));
     if (d.mrows.ensure(row_cap, err) || d.keys.ensure(row_cap, err) ||
         d.keys2.ensure(row_cap, err) || d.vals.ensure(row_cap, err) ||
         d.vals2.ensure(row_cap, err) || d.lens.ensure(row_cap + 1, err) ||

@@ -161,3 +161,26 @@ def test_myers_candidate_list_overflow(cof_mod, oracle_mod, monkeypatch):
         o.add_chunk(name, data, s, e)
     ref, nref = o.search(*args)
     assert n == nref > 0 and sorted(ref.splitlines()) == sorted(text.splitlines())
+
+
+def test_row_buffer_overflow_halves_chunks(cof_mod, oracle_mod, monkeypatch):
+    # a chunk whose alignments pass the row buffer is halved and walked
+    # again (COF_BULGE_ROW_CAP lowers the buffer from 16 M rows); the rows
+    # equal the oracle's and take more launches than one chunk does
+    import synth
+    cfg = synth.config_bulge(seed=8, scale=0.0002, n_guides=6, planted=8)
+    g = cof_mod.Genome()
+    cfg["genome"].load_into(g)
+    args = (cfg["filter"], cfg["patterns"], cfg["max_mismatches"], cfg["max_dna_bulges"],
+            cfg["max_rna_bulges"])
+    monkeypatch.delenv("COF_BULGE_ROW_CAP", raising=False)
+    _, n1 = g.search(*args)
+    one = g.last_stats()["kernel_launches"]
+    monkeypatch.setenv("COF_BULGE_ROW_CAP", str(max(64, n1 // 5)))
+    text, n = g.search(*args)
+    assert g.last_stats()["kernel_launches"] > one
+    o = oracle_mod.OracleGenome()
+    for name, data, s, e in cfg["genome"].chunks():
+        o.add_chunk(name, data, s, e)
+    ref, nref = o.search(*args)
+    assert n == n1 == nref > 0 and sorted(ref.splitlines()) == sorted(text.splitlines())
