@@ -542,9 +542,8 @@ constexpr ScanVariant warp_variant(uint32_t span) {
 }
 
 // Candidate tile shapes (windows per lane x warps x min blocks per SM, and
-// patterns per comparison step); the autotuner times them on a sample of the
-// genome.  Two patterns per step need registers that only the shapes with
-// fewer blocks per SM have.
+// how a lane reduces its mismatch counts); the autotuner times them on a
+// sample of the genome.  Four CTAs per SM leave 64 registers per thread.
 const ScanVariant kScanVariants[] = {
     // per-warp work items: four CTAs per SM (1024 staged patterns), then three
     warp_variant<8, 8, 4, 4, 1024>(8), warp_variant<8, 8, 4, 1, 1024>(8),
