@@ -12,6 +12,8 @@
 #include <string>
 #include <thread>
 #include <unordered_map>
+
+#include <pthread.h>
 #include <vector>
 
 namespace cof {
@@ -249,8 +251,13 @@ class Engine {
     int run_raw(const Request &req, Result &out, Error &err);
     int device_;
     // creates the device's CUDA context while the caller reads the genome
-    // file; joined before the first device call
-    std::thread warm_;
+    // file; joined before the first device call, and only by the process
+    // that started it (a forked child holds a copy of this object but not
+    // the thread)
+    pthread_t warm_{};
+    bool warm_live_ = false;
+    int warm_pid_ = 0;
+    void join_warm();
     HostGenome host_;
     DeviceGenome *dev_ = nullptr;
     StageTimes times_;

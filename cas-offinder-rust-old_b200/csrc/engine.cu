@@ -25,6 +25,8 @@
 //            writer PAM filter and mismatch recount (main.rs:159-197).
 //   format : site strings with lowercase mismatches and the 8-column row text
 //            (main.rs:198-242), laid out by an exclusive scan of row lengths.
+#include <unistd.h>
+
 #include <cub/cub.cuh>
 #include <cuda_runtime.h>
 
@@ -729,15 +731,28 @@ row_write_kernel(GenomeDev G, const Row *__restrict__ rows, const uint32_t *__re
 // device genome + scratch
 // ---------------------------------------------------------------------------
 
+namespace {
+void *warm_context(void *arg) {
+    const int device = (int)(intptr_t)arg;
+    if (cudaSetDevice(device) == cudaSuccess) cudaFree(nullptr);
+    return nullptr;
+}
+}  // namespace
+
 Engine::Engine(int device) : device_(device) {
     // context creation costs a few hundred ms on a large GPU; it overlaps
     // the file read that precedes every upload
-    warm_ = std::thread([device] {
-        if (cudaSetDevice(device) == cudaSuccess) cudaFree(nullptr);
-    });
+    warm_pid_ = (int)::getpid();
+    warm_live_ = pthread_create(&warm_, nullptr, warm_context, (void *)(intptr_t)device) == 0;
 }
+
+void Engine::join_warm() {
+    if (warm_live_ && (int)::getpid() == warm_pid_) pthread_join(warm_, nullptr);
+    warm_live_ = false;
+}
+
 Engine::~Engine() {
-    if (warm_.joinable()) warm_.join();
+    join_warm();
     if (dev_) {
         cudaSetDevice(device_);
         delete dev_;
@@ -746,7 +761,7 @@ Engine::~Engine() {
 
 int Engine::upload(Error &err) {
     if (dev_) return kOk;
-    if (warm_.joinable()) warm_.join();
+    join_warm();
     CU(cudaSetDevice(device_));
     std::unique_ptr<DeviceGenome> d(new DeviceGenome());
     d->device = device_;

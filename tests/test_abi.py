@@ -69,6 +69,24 @@ def test_fasta_index_errors(cof_mod, tmp_path):
         assert e.value.code == cof_mod.COF_E_BADINPUT
 
 
+def test_genome_freed_in_forked_child(cof_mod):
+    # a genome starts a thread that creates the CUDA context; a child forked
+    # while the genome exists holds a copy of it but not the thread, and
+    # freeing it there must neither wait on that thread nor fail
+    g = cof_mod.Genome()
+    pid = os.fork()
+    if pid == 0:  # child
+        code = 1
+        try:
+            g.close()
+            code = 0
+        finally:
+            os._exit(code)
+    _, status = os.waitpid(pid, 0)
+    assert os.WIFEXITED(status) and os.WEXITSTATUS(status) == 0
+    g.close()
+
+
 def test_bad_requests_rejected(cof_mod, golden):
     g = cof_mod.Genome(os.path.join(golden, "upstream1000.fa"))
     with pytest.raises(cof_mod.CofError) as e:
