@@ -347,6 +347,83 @@ __device__ __forceinline__ void scan_tile(const ScanParams &P, const ScanGroup &
     }
 }
 
+// scan_tile with the segment's fields held in registers and one ballot per
+// drain step: fewer instructions per tile, which pays with few patterns per
+// group (2-6 %), while with hundreds of patterns the longer live ranges
+// around the flush call cost a few percent; the autotuner picks per shape.
+template <int kCpt, int kPair>
+__device__ __forceinline__ void scan_tile_lean(const ScanParams &P, const ScanGroup &G,
+                                          const ScanSeg &sgm, uint64_t tile, uint4 *q, int &qn,
+                                          uint32_t &qbatch, const FastPattern *pt, bool smem,
+                                          uint32_t npat, unsigned long long &ncand,
+                                          unsigned long long &npairs, int lane) {
+    constexpr int kQCap = 32 * kCpt;
+    const uint32_t lt_mask = (1u << lane) - 1u;
+    // the segment's fields once, in registers: the queue stores below go
+    // through a generic pointer and would otherwise force reloads
+    const uint64_t seg_lo = sgm.lo, seg_hi = sgm.hi, seg_w0 = sgm.w0, seg_t0 = sgm.tile_begin;
+    const uint64_t seg_base = sgm.base;
+    const uint32_t seg_batch = sgm.batch;
+    if (seg_batch != qbatch) {
+        if (qn) {
+            __syncwarp();
+            flush_queue<kCpt, kPair>(q, qn, pt, smem, G, qbatch, P, lane);
+            __syncwarp();
+            qn = 0;
+        }
+        qbatch = seg_batch;
+    }
+    const uint64_t w = seg_w0 + (tile - seg_t0) * 32 + lane;
+    const uint32_t h0 = __ldg(P.H + w), h1 = __ldg(P.H + w + 1);
+    const uint32_t l0 = __ldg(P.L + w), l1 = __ldg(P.L + w + 1);
+    const uint32_t s0 = __ldg(P.S + w), s1 = __ldg(P.S + w + 1);
+    // window starts 32w + k in [lo, hi)
+    const uint64_t p0 = w * 32;
+    uint32_t m = 0xFFFFFFFFu;
+    if (p0 < seg_lo) m = (seg_lo - p0 >= 32) ? 0u : (m << (uint32_t)(seg_lo - p0));
+    if (p0 + 32 > seg_hi) m = (seg_hi <= p0) ? 0u : (m & (0xFFFFFFFFu >> (uint32_t)(32 - (seg_hi - p0))));
+    for (uint32_t c = 0; c < G.n_pam && m; ++c) {
+        const PamCell pc = G.pam[c];
+        const uint32_t h = __funnelshift_r(h0, h1, pc.cell);
+        const uint32_t l = __funnelshift_r(l0, l1, pc.cell);
+        const uint32_t s = __funnelshift_r(s0, s1, pc.cell);
+        const uint32_t t0 = (l & pc.fc) | (~l & pc.fa);
+        const uint32_t t1 = (l & pc.ft) | (~l & pc.fg);
+        m &= ((h & t1) | (~h & t0)) & ~s;
+    }
+    const uint32_t nm = __popc(m);
+    ncand += nm;
+    npairs += (unsigned long long)nm * npat;
+    // drain PAM-passing starts into the warp queue, one per lane per step
+    const uint32_t off0 = (uint32_t)(p0 - seg_base);  // batch-local start of bit 0
+    for (;;) {
+        const bool has = m != 0;
+        const uint32_t bal = __ballot_sync(0xFFFFFFFFu, has);
+        if (!bal) break;
+        if (has) {
+            const uint32_t k = __ffs(m) - 1;
+            m &= m - 1;
+            const int slot = qn + __popc(bal & lt_mask);
+            q[slot] = make_uint4(off0 + k, __funnelshift_r(h0, h1, k), __funnelshift_r(l0, l1, k),
+                                 __funnelshift_r(s0, s1, k));
+        }
+        qn += __popc(bal);
+        if (qn >= kQCap) {
+            // full pass over kQCap windows; the (< 32) windows beyond it
+            // move to the front of the queue
+            __syncwarp();
+            flush_queue<kCpt, kPair>(q, kQCap, pt, smem, G, qbatch, P, lane);
+            const int rest = qn - kQCap;
+            uint4 e = make_uint4(0, 0, 0, 0);
+            if (lane < rest) e = q[kQCap + lane];
+            __syncwarp();
+            if (lane < rest) q[lane] = e;
+            __syncwarp();
+            qn = rest;
+        }
+    }
+}
+
 // Persistent scan: CTAs pull work items -- a span of kSpanTiles tiles of one
 // scan group -- from a global counter, so groups of very different sizes
 // (few or many patterns, sparse or dense PAMs) share the GPU evenly.  A CTA
@@ -447,7 +524,7 @@ scan_kernel(ScanParams P) {
 // table of all groups is staged in shared memory once, up to kSmemPatterns
 // patterns; a group whose patterns lie beyond that prefix reads them from
 // global memory.  Group and segment descriptors are read through L1.
-template <int kCpt, int kScanWarps, int kMinBlocks, int kPair, int kPatCap>
+template <int kCpt, int kScanWarps, int kMinBlocks, int kPair, int kPatCap, int kLean>
 __global__ void __launch_bounds__(kScanWarps * 32, kMinBlocks)
 scan_warp_kernel(ScanParams P) {
     constexpr int kQSlots = 32 * kCpt + 32;
@@ -504,8 +581,12 @@ scan_warp_kernel(ScanParams P) {
         uint32_t sidx = 0;
         for (uint64_t tile = t_begin; tile < t_end; ++tile) {
             while (sidx + 1 < nseg && tile >= segs[sidx + 1].tile_begin) ++sidx;
-            scan_tile<kCpt, kPair>(P, *G, segs[sidx], tile, q, qn, qbatch, pt, smem, npat, ncand,
-                                   npairs, lane);
+            if (kLean)
+                scan_tile_lean<kCpt, kPair>(P, *G, segs[sidx], tile, q, qn, qbatch, pt, smem, npat,
+                                            ncand, npairs, lane);
+            else
+                scan_tile<kCpt, kPair>(P, *G, segs[sidx], tile, q, qn, qbatch, pt, smem, npat,
+                                       ncand, npairs, lane);
         }
     }
     if (qn) {
@@ -528,6 +609,7 @@ struct ScanVariant {
     void (*kernel)(ScanParams);
     bool per_warp;
     uint32_t pat_cap;  // patterns staged in shared memory
+    bool lean;         // scan_tile_lean
     size_t smem() const {
         return (size_t)warps * (32 * cpt + 32) * sizeof(uint4) + pat_cap * sizeof(FastPattern);
     }
@@ -535,12 +617,14 @@ struct ScanVariant {
 
 template <int C, int W, int B, int Q = 1>
 constexpr ScanVariant variant(uint32_t span) {
-    return ScanVariant{C, W, B, Q, span, scan_kernel<C, W, B, Q>, false, kSmemPatterns};
+    return ScanVariant{C, W, B, Q, span, scan_kernel<C, W, B, Q>, false, kSmemPatterns, false};
 }
-// span: tiles per warp work item; K: patterns staged in shared memory
-template <int C, int W, int B, int Q = 1, int K = kSmemPatterns>
+// span: tiles per warp work item; K: patterns staged in shared memory;
+// N: scan_tile_lean (1) or scan_tile (0)
+template <int C, int W, int B, int Q = 1, int K = kSmemPatterns, int N = 0>
 constexpr ScanVariant warp_variant(uint32_t span) {
-    return ScanVariant{C, W, B, Q, span, scan_warp_kernel<C, W, B, Q, K>, true, (uint32_t)K};
+    return ScanVariant{C, W, B, Q, span, scan_warp_kernel<C, W, B, Q, K, N>, true, (uint32_t)K,
+                       N != 0};
 }
 
 // Candidate tile shapes (windows per lane x warps x min blocks per SM, and
@@ -548,10 +632,12 @@ constexpr ScanVariant warp_variant(uint32_t span) {
 // sample of the genome.  Four CTAs per SM leave 64 registers per thread.
 const ScanVariant kScanVariants[] = {
     // per-warp work items: four CTAs per SM (1024 staged patterns), then three
-    warp_variant<8, 8, 4, 4, 1024>(8), warp_variant<8, 8, 4, 1, 1024>(8),
+    warp_variant<8, 8, 4, 4, 1024, 1>(8), warp_variant<8, 8, 4, 1, 1024>(8),
     warp_variant<4, 8, 4, 4, 1024>(8), warp_variant<8, 8, 3, 4>(8), warp_variant<8, 8, 3>(8),
     // CTA work items
     variant<8, 8, 3>(64), variant<4, 8, 4>(64), variant<4, 16, 2>(128),
+    // the default shape without the lean tile (more patterns per group)
+    warp_variant<8, 8, 4, 4, 1024>(8),
 };
 constexpr int kNumScanVariants = sizeof(kScanVariants) / sizeof(kScanVariants[0]);
 
@@ -1158,6 +1244,7 @@ int Engine::run_popcount(const std::vector<Request> &reqs, std::vector<Result> &
         occ = std::max(occ, 1);
         sp.span_tiles = v.span_tiles;
         sp.item_begin = (const uint64_t *)tab(sample ? o_sample[v.span_tiles] : o_items[v.span_tiles]);
+        sp.hits = d.hits.p;  // the list may have grown (and moved) since the last launch
         sp.hit_cap = (uint32_t)std::min<size_t>(d.hits.cap, 0xFFFFFFF0u);
         const uint64_t items = sample ? n_sample[v.span_tiles] : n_items[v.span_tiles];
         const unsigned gx = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>(items, (uint64_t)d.n_sm * occ));
@@ -1220,7 +1307,8 @@ int Engine::run_popcount(const std::vector<Request> &reqs, std::vector<Result> &
         const ScanVariant &v = kScanVariants[vi];
         times_.scan_variant = vi;
         static const char *const kMinName[] = {"", "", "", "", "min3-"};
-        times_.scan_shape = std::string(v.per_warp ? "warp-" : "") + kMinName[v.pair] + "cpt" + std::to_string(v.cpt) + "-warps" + std::to_string(v.warps) +
+        times_.scan_shape = std::string(v.per_warp ? "warp-" : "") + (v.lean ? "lean-" : "") +
+                            kMinName[v.pair] + "cpt" + std::to_string(v.cpt) + "-warps" + std::to_string(v.warps) +
                             "-minb" + std::to_string(v.min_blocks) + "-span" +
                             std::to_string(v.span_tiles);
         for (int attempt = 0; attempt < 2; ++attempt) {

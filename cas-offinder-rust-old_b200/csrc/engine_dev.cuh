@@ -143,13 +143,25 @@ template <class T>
 struct DevBuf {
     T *p = nullptr;
     size_t cap = 0;
+    // Grows to at least n elements; contents are not kept.  The new buffer
+    // is allocated before the old one is freed, so it never reuses the old
+    // address: a pointer still held to the old buffer cannot pass for the
+    // new one (the overflow tests depend on that).
     int ensure(size_t n, Error &err) {
         if (n <= cap) return kOk;
-        if (p) cudaFree(p);
-        p = nullptr;
-        cap = 0;
-        size_t want = std::max<size_t>(n, 64);
-        CU(cudaMalloc((void **)&p, want * sizeof(T)));
+        const size_t want = std::max<size_t>(n, 64);
+        T *q = nullptr;
+        const cudaError_t e = cudaMalloc((void **)&q, want * sizeof(T));
+        if (e != cudaSuccess) {  // retry with the old buffer released first
+            cudaGetLastError();
+            if (p) cudaFree(p);
+            p = nullptr;
+            cap = 0;
+            CU(cudaMalloc((void **)&q, want * sizeof(T)));
+        } else if (p) {
+            cudaFree(p);
+        }
+        p = q;
         cap = want;
         return kOk;
     }

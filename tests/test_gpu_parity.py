@@ -149,7 +149,7 @@ def test_cli_matches_oracle_cli(cof_mod, oracle_mod, golden, tmp_path):
         assert "=== Cas-OFFinder Rust ===" in log and "Matches found: 117" in log
 
 
-N_SCAN_VARIANTS = 8  # per-warp work items: 0-4; CTA work items: 5-7
+N_SCAN_VARIANTS = 9  # per-warp work items: 0-4 and 8; CTA work items: 5-7
 
 
 @pytest.mark.parametrize("variant", range(N_SCAN_VARIANTS))
