@@ -36,7 +36,7 @@ sys.path.insert(0, PKG)
 # launch, from the ncu capture summarised in profiles/ (620 Mbp case, scaled
 # x5 by genome size to the 3.1 Gbp workload: each strand group reads every
 # plane word once, so traffic grows in proportion to the genome)
-TRAFFIC = (465.15e6 + 21.96e6) * 5
+TRAFFIC = (465.17e6 + 22.00e6) * 5
 
 METRIC = "Gbp*guides/s scanned (3.1 Gbp x 100 guides, 20 nt + NRG, mm<=6, both strands)"
 UNIT = "Gbp*guides/s"
