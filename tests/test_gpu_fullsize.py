@@ -119,3 +119,22 @@ def test_mixed_pam_batch_vs_oracle(cof_mod, oracle_mod):
         pats = cfg["requests"][0 if gi < 50 else 1]["patterns"]
         want = pos + (max(_pam_len(pats[0]) - 1, 0) if strand == "-" else 0)
         assert (gen.names[rec], want, strand) in found
+
+
+def test_full_genome_workload_vs_oracle_at_310Mbp(cof_mod, oracle_mod):
+    # the 100-guide workload's generator at a tenth of its size (310 Mbp,
+    # 24 records, N runs, 50 planted sites per guide): every row equals the
+    # oracle's (the oracle takes seconds here on all host threads)
+    import synth
+    cfg = synth.config_full_genome(seed=2, scale=0.1, n_guides=100)
+    gen = cfg["genome"]
+    g = cof_mod.Genome()
+    o = oracle_mod.OracleGenome()
+    for name, data, s, e in gen.chunks():
+        g.add_chunk(name, data, s, e)
+        o.add_chunk(name, data, s, e)
+    args = (cfg["filter"], cfg["patterns"], cfg["max_mismatches"])
+    text, n = g.search(*args)
+    ref, nref = o.search(*args)
+    assert n == nref > 100_000
+    assert sorted(text.splitlines()) == sorted(ref.splitlines())

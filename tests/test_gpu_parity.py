@@ -112,9 +112,12 @@ def test_many_small_requests_in_one_pass(cof_mod):
         assert g.search_batch(reqs) == singles
 
 
-def test_planted_sites_found(cof_mod, oracle_mod, tmp_path):
+@pytest.mark.parametrize("scale", [0.05, 1.0])
+def test_planted_sites_found(cof_mod, oracle_mod, tmp_path, scale):
+    # the plain small workload (10 Mbp x 1 guide at scale 1.0) through a
+    # FASTA file: every planted site, and exactly the oracle's rows
     import synth
-    cfg = synth.config_plain_small(seed=11, scale=0.05)
+    cfg = synth.config_plain_small(seed=11, scale=scale)
     gen = cfg["genome"]
     g = cof_mod.Genome()
     gen.load_into(g)
@@ -130,6 +133,9 @@ def test_planted_sites_found(cof_mod, oracle_mod, tmp_path):
     ref, nref = oracle_mod.OracleGenome(str(fa)).search(cfg["filter"], cfg["patterns"],
                                                          cfg["max_mismatches"])
     assert _rows(text) == _rows(ref) and n == nref
+    text2, n2 = cof_mod.Genome(str(fa)).search(cfg["filter"], cfg["patterns"],
+                                               cfg["max_mismatches"])
+    assert _rows(text2) == _rows(ref) and n2 == nref  # the file converted on the device
 
 
 def test_cli_matches_oracle_cli(cof_mod, oracle_mod, golden, tmp_path):
