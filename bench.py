@@ -10,8 +10,15 @@ formatting, rows copied to host memory.
           CUDA events on the library's stream), genome resident.
   e2e   : same metric over the whole cof_search call (request tables
           host->device, row text device->host into a host buffer).
-  roofline : the scan kernel against the measured peak of its own inner loop
-          (window x pattern comparisons per second, microbenchmarked live).
+  roofline : the scan kernel against the measured POPC peak of this GPU (one
+          POPC per window x pattern comparison, microbenchmarked live).
+
+Extra measurements on one GPU (--no-extras skips them): two PAMs batched in
+one pass, the serving loop (spec mix and small requests, batched vs one
+request per pass, p50/p99 latency), the bulge path (--only-bulge), and the
+command line tool as a whole process on .2bit and FASTA genome files
+(--only-cli).  cpu_baseline times the oracle port of the reference CPU path
+on a slice of the genome.
 
 Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
 Multi-GPU (torchrun): each rank searches its own 100-guide set over its own
