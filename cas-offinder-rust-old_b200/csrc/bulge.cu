@@ -1278,17 +1278,39 @@ int Engine::run_bulge(const std::vector<Request> &reqs, std::vector<Result> &out
         CU(cudaEventRecord(d.ev[1], s));
         const uint32_t cap = (uint32_t)std::min<size_t>(d.mcand.cap, 0xFFFFFFF0u);
         if (forms.size() <= kMfMaxForms) {
-            // PAM test per tile in shared memory; enough tiles per block
-            // that its (tile, pattern) items fill the block
-            const uint32_t tpb = std::min<uint32_t>(
-                kMfMaxTiles, std::max<uint32_t>(1, (kMfThreads + n_pat - 1) / n_pat));
-            const size_t smem = (size_t)tpb * forms.size() * (kMfQWords + 32) * 4 +
-                                (n_pat <= (uint32_t)kSmemMyers ? (size_t)n_pat * 64 : 0);
+            // PAM test per tile in shared memory.  Tiles per block: a block
+            // walks its tpb x n_pat (tile, pattern) items in rounds of
+            // kMfThreads, and the grid walks the tile blocks in waves of
+            // n_sm x (blocks per SM); take the tpb with the fewest
+            // waves x rounds (ties: more tiles per block)
+            auto smem_of = [&](uint32_t t) {
+                return (size_t)t * forms.size() * (kMfQWords + 32) * 4 +
+                       (n_pat <= (uint32_t)kSmemMyers ? (size_t)n_pat * 64 : 0);
+            };
+            uint32_t tpb = 1;
+            uint64_t best = ~0ull;
+            int per_sm = 1;
+            for (uint32_t t = 1; t <= kMfMaxTiles; ++t) {
+                const size_t sm = smem_of(t);
+                CU(cudaFuncSetAttribute(myers_tile_kernel,
+                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+                int occ = 1;
+                CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, myers_tile_kernel,
+                                                                 kMfThreads, sm));
+                occ = std::max(occ, 1);
+                const uint64_t rounds = ((uint64_t)t * n_pat + kMfThreads - 1) / kMfThreads;
+                const uint64_t tblk = (tiles.size() + t - 1) / t;
+                const uint64_t slots = (uint64_t)d.n_sm * occ;
+                const uint64_t cost = ((tblk + slots - 1) / slots) * rounds;
+                if (cost <= best) {
+                    best = cost;
+                    tpb = t;
+                    per_sm = occ;
+                }
+            }
+            const size_t smem = smem_of(tpb);
             CU(cudaFuncSetAttribute(myers_tile_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     (int)smem));
-            int per_sm = 1;
-            CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, myers_tile_kernel, kMfThreads,
-                                                             smem));
             const uint64_t tblocks = (tiles.size() + tpb - 1) / tpb;
             const unsigned blocks = (unsigned)std::max<uint64_t>(
                 1, std::min<uint64_t>(tblocks, (uint64_t)d.n_sm * std::max(1, per_sm)));
