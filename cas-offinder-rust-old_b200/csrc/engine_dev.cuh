@@ -205,22 +205,19 @@ class DeviceGenome {
     DevBuf<uint64_t> keys, keys2, offs;
     DevBuf<uint32_t> vals, vals2, lens, req_rows;
     DevBuf<Counters> ctr;
-    DevBuf<char> text, text2;
+    DevBuf<char> text;
     DevBuf<unsigned char> cub_tmp;
     DevBuf<MyersCand> mcand, mcand2;
     DevBuf<MyersRow> mrows;
     DevBuf<unsigned char> tb_items;  // two queues of handed-on traceback subtrees
-    char *h_text = nullptr;
-    size_t h_text_cap = 0;
 
     ~DeviceGenome() {
         bit4.release(); planes.release(); boff.release(); start.release(); end.release();
         name_idx.release(); name_off.release(); names.release(); tables.release();
         hits.release(); rows.release(); keys.release(); keys2.release(); offs.release();
         vals.release(); vals2.release(); lens.release(); req_rows.release(); ctr.release();
-        text.release(); text2.release(); cub_tmp.release(); mcand.release(); mcand2.release(); mrows.release();
+        text.release(); cub_tmp.release(); mcand.release(); mcand2.release(); mrows.release();
         tb_items.release();
-        if (h_text) cudaFreeHost(h_text);
         for (auto &e : ev)
             if (e) cudaEventDestroy(e);
         if (stream) cudaStreamDestroy(stream);
