@@ -1044,11 +1044,16 @@ int Engine::run_popcount(const std::vector<Request> &reqs, std::vector<Result> &
                 last = (int)c;
             }
             const bool end_anchor = last == (int)L - 1 && first > 0;
-            off[st] = end_anchor ? kMaxPatternLen - L : 0;
+            // window cell of pattern cell 0: the 32-cell window ends at the
+            // pattern end (END anchor) or starts at its start; a pattern
+            // longer than the window has cells outside it (negative offset,
+            // kept as a wrapped uint32) that only verify compares
+            off[st] = end_anchor ? kScanWindow - L : 0;
             key[st] = std::string(end_anchor ? "E" : "S") + (st ? "-" : "+");
             for (uint32_t c = 0; c < L; ++c)
                 if (!rd.fisn[st][c])
-                    key[st] += std::to_string(c + off[st]) + ":" + std::to_string(rd.fset[st][c]) + ",";
+                    key[st] += std::to_string((int)c + (int)off[st]) + ":" +
+                               std::to_string(rd.fset[st][c]) + ",";
         }
         const size_t np = r.patterns.size(), nfwd = np / 2;
         for (size_t p = 0; p < np; ++p) {
@@ -1075,8 +1080,10 @@ int Engine::run_popcount(const std::vector<Request> &reqs, std::vector<Result> &
         for (uint32_t c = 0; c < rd.L; ++c) {  // the same cells for every member
             if (rd.fisn[strand][c]) continue;
             if (proto.n_pam == kMaxPamCells) break;
+            const int wc = (int)c + (int)off0;  // window cell
+            if (wc < 0 || wc >= (int)kScanWindow) continue;  // verify tests it
             const uint8_t fs = rd.fset[strand][c];
-            PamCell pc{c + off0, (fs & 4) ? ~0u : 0u, (fs & 2) ? ~0u : 0u, (fs & 8) ? ~0u : 0u,
+            PamCell pc{(uint32_t)wc, (fs & 4) ? ~0u : 0u, (fs & 2) ? ~0u : 0u, (fs & 8) ? ~0u : 0u,
                        (fs & 1) ? ~0u : 0u};
             proto.pam[proto.n_pam++] = pc;
         }
@@ -1099,14 +1106,17 @@ int Engine::run_popcount(const std::vector<Request> &reqs, std::vector<Result> &
                 const uint32_t L = lo_.first, o = lo_.second;
                 const uint64_t msmin = c1 > L - 1 ? c1 - (L - 1) : 0;
                 if (msmin >= b.valid) continue;
-                lo = std::min<uint64_t>(lo, b.base + msmin + kMaxPatternLen - o);
-                hi = std::max<uint64_t>(hi, b.base + b.valid + kMaxPatternLen - o);
+                // shifted window start of pattern start s: s + kScanWindow - o
+                // (a 32-bit difference: L for an END anchor of any length)
+                const uint32_t shift = kScanWindow - o;
+                lo = std::min<uint64_t>(lo, b.base + msmin + shift);
+                hi = std::max<uint64_t>(hi, b.base + b.valid + shift);
             }
             if (hi <= lo) continue;
             ScanSeg sgm{};
             sgm.lo = lo;
             sgm.hi = hi;
-            sgm.base = b.base + kMaxPatternLen;
+            sgm.base = b.base + kScanWindow;
             sgm.w0 = sgm.lo / 32;
             sgm.tile_begin = tiles;
             sgm.batch = (uint32_t)bi;
@@ -1127,11 +1137,12 @@ int Engine::run_popcount(const std::vector<Request> &reqs, std::vector<Result> &
             FastPattern fp{0, 0, 0, (int32_t)ep.max_mm};
             for (uint32_t c = 0; c < ep.L; ++c) {
                 const uint8_t v = ep.b4[c];
-                if (v && !(v & (v - 1))) {
+                const int wc = (int)c + (int)o;  // window cell; outside: verify only
+                if (wc >= 0 && wc < (int)kScanWindow && v && !(v & (v - 1))) {
                     const uint32_t cd = code2(v);
-                    fp.care |= 1u << (c + o);
-                    fp.h |= ((cd >> 1) & 1u) << (c + o);
-                    fp.l |= (cd & 1u) << (c + o);
+                    fp.care |= 1u << wc;
+                    fp.h |= ((cd >> 1) & 1u) << wc;
+                    fp.l |= (cd & 1u) << wc;
                 }
             }
             comp.push_back({fp, o, e});

@@ -99,7 +99,13 @@ def test_bad_requests_rejected(cof_mod, golden):
         g.search("NNNN", ["ACGT"], 4)  # mm >= pattern length
     assert e.value.code == cof_mod.COF_E_BADINPUT
     with pytest.raises(cof_mod.CofError) as e:
-        g.search("N" * 40, ["A" * 40], 3)  # above the 32-cell word
+        g.search("N" * 65, ["A" * 65], 3)  # above 64 cells
+    assert e.value.code == cof_mod.COF_E_UNSUPPORTED
+    with pytest.raises(cof_mod.CofError) as e:
+        g.search("N" * 40, ["A" * 40], 3, 1, 1)  # bulges: at most 32 cells
+    assert e.value.code == cof_mod.COF_E_UNSUPPORTED
+    with pytest.raises(cof_mod.CofError) as e:
+        g.search("N" * 40, ["A" * 40], 3, raw=True)  # raw matches: at most 32 cells
     assert e.value.code == cof_mod.COF_E_UNSUPPORTED
 
 

@@ -202,6 +202,43 @@ def test_candidate_list_overflow(cof_mod, golden, monkeypatch):
     assert g.last_stats()["raw_hits"] > 64  # it did overflow
 
 
+@pytest.mark.parametrize("L", [33, 40, 51, 64])
+def test_patterns_longer_than_the_scan_window(cof_mod, oracle_mod, L):
+    # patterns of 33-64 cells: the 32-cell scan window holds the PAM end
+    # (3' PAM) or start (5' PAM) of the pattern, and verify recounts all of
+    # it; rows equal the oracle's for a 3' PAM, a 5' PAM and no PAM, and in a
+    # batch that mixes 23- and L-cell NRG requests (one scan group)
+    rng = random.Random(700 + L)
+    _, records = randgen.random_genome(rng, 3, 30000, 50000)
+    guide = lambda n: "".join(rng.choice("ACGT") for _ in range(n))
+    shapes = [
+        ("N" * (L - 2) + "RG", [guide(L - 3) + "NNN" for _ in range(3)], 6),
+        ("TTTN" + "N" * (L - 4), ["NNNN" + guide(L - 4) for _ in range(3)], 6),
+        ("N" * L, [guide(L) for _ in range(2)], 5),
+    ]
+    for filt, pats, mm in shapes:
+        for p in pats:
+            randgen.plant_sites(rng, records, p, filt, 6, mm)
+    short = ("N" * 21 + "RG", [guide(20) + "NNN" for _ in range(2)], 4)
+    for p in short[1]:
+        randgen.plant_sites(rng, records, p, short[0], 4, 3)
+    g, o = _both(cof_mod, oracle_mod, randgen.chunk_records(rng, records, 5000))
+    for filt, pats, mm in shapes:
+        text, n = g.search(filt, pats, mm)
+        ref, nref = o.search(filt, pats, mm)
+        assert n == nref and _rows(text) == _rows(ref), filt
+    assert sum(o.search(f, p, m)[1] for f, p, m in shapes) > 10
+    reqs = [dict(search_filter=short[0], patterns=short[1], max_mismatches=short[2]),
+            dict(search_filter=shapes[0][0], patterns=shapes[0][1], max_mismatches=shapes[0][2])]
+    for r, (text, n) in zip(reqs, g.search_batch(reqs)):
+        ref, nref = o.search(r["search_filter"], r["patterns"], r["max_mismatches"])
+        assert n == nref and _rows(text) == _rows(ref)
+    with pytest.raises(cof_mod.CofError):  # bulges and raw matches stay at 32 cells
+        g.search(shapes[0][0], shapes[0][1], 3, 1, 1)
+    with pytest.raises(cof_mod.CofError):
+        g.search(shapes[0][0], shapes[0][1], 3, raw=True)
+
+
 def test_autotuner_records_choice(cof_mod, golden, monkeypatch):
     monkeypatch.delenv("COF_SCAN_VARIANT", raising=False)
     g = cof_mod.Genome(os.path.join(golden, "upstream1000.fa"))
