@@ -11,8 +11,10 @@
 //
 // Kernels:
 //   myers_filter_kernel  one thread per (1024-position tile, pattern): a
-//       streaming Myers sweep (Myers 1999, semi-global, 32-bit words) started
-//       >= 48 positions before the tile.  Its score at t bounds the windowed
+//       streaming Myers sweep (Myers 1999, semi-global; 32-bit words for
+//       patterns of at most 32 cells, 64-bit words up to 64 cells, the
+//       single-u64 limit of myers.rs:3) started >= W - 1 positions before
+//       the tile (W = L + max_db, the reference's text window).  Its score at t bounds the windowed
 //       score from below (more start positions), which bounds the DP cost from
 //       below (the DP forbids padding cells and may forbid bulges), so
 //       "score <= max_edits" keeps every position the reference can emit.
@@ -41,15 +43,22 @@ namespace cof {
 
 namespace {
 
-constexpr int kMaxCells = 40;          // L <= 32, L + max_db <= 40
+constexpr int kMaxCells = 72;          // L <= 64, L + max_db <= 72
 constexpr uint32_t kTile = 1024;       // end positions per filter work item
-constexpr uint32_t kWarm = 48;         // Myers warm-up before a tile (>= W - 1)
+constexpr uint32_t kWarmMin = 48;      // Myers warm-up before a tile (>= W - 1)
 constexpr int kSmemMyers = 512;        // patterns whose eq tables fit in smem
+
+// Myers warm-up for windows of at most wmax cells: W - 1, in whole 16-cell
+// words, and never below the 48 cells every window of <= 40 cells uses
+inline uint32_t myers_warm(uint32_t wmax) {
+    const uint32_t need = wmax > 0 ? ((wmax - 1 + 15) & ~15u) : 0;
+    return need > kWarmMin ? need : kWarmMin;
+}
 
 struct MyersPattern {
     uint32_t request, strand, L, E;    // E = max edits = mm + db + rb
     uint32_t W, pam_off, pam_n, pad;
-    uint32_t eq16[16];                 // Myers Eq per genome nibble value
+    uint32_t eq_lo[16], eq_hi[16];     // Myers Eq per genome nibble value, cells 0..31 / 32..63
     uint8_t b4[kMaxCells];             // pattern bit4 cells
     uint8_t isn[kMaxCells];            // pattern char is N/n (pam_is_n)
     uint8_t eff[kMaxCells];            // effective filter bit4 per cell
@@ -97,16 +106,45 @@ __device__ bool pam_quick(const uint8_t *bit4, const BatchDev &B, uint32_t end_p
     return false;
 }
 
+// one column of the streaming Myers sweep (Myers 1999, the step of
+// myers.rs:56-90) over a Word-wide pattern bit vector; returns the score change
+template <typename Word>
+__device__ __forceinline__ int myers_step(Word eq, Word &vp, Word &vn, Word mask, uint32_t sh) {
+    const Word x = eq | vn;
+    const Word d0 = (((x & vp) + vp) ^ vp) | x;
+    const Word hn = vp & d0;
+    const Word hp = vn | ~(vp | d0);
+    const Word xs = hp << 1;
+    vn = xs & d0;
+    vp = ((hn << 1) | ~(xs | d0)) & mask;
+    vn &= mask;
+    return (int)((hp >> sh) & 1u) - (int)((hn >> sh) & 1u);
+}
+
+// the Word-wide Eq vector of genome nibble b
+template <typename Word>
+__device__ __forceinline__ Word eq_word(const MyersPattern &P, uint32_t b) {
+    if constexpr (sizeof(Word) == 4) return P.eq_lo[b];
+    else return ((uint64_t)P.eq_hi[b] << 32) | P.eq_lo[b];
+}
+
+template <typename Word>
+__device__ __forceinline__ Word myers_mask(uint32_t L) {
+    return L >= 8 * sizeof(Word) ? ~(Word)0 : (((Word)1 << L) - 1);
+}
+
+template <typename Word>
 __global__ void myers_filter_kernel(const uint8_t *__restrict__ bit4,
                                     const BatchDev *__restrict__ batches,
                                     const MyersTile *__restrict__ tiles, uint64_t n_tiles,
                                     const MyersPattern *__restrict__ pats, uint32_t n_pat,
-                                    const MyersReqDev *__restrict__ reqs, MyersCand *cand,
-                                    uint32_t cap, Counters *ctr) {
-    __shared__ uint32_t seq[kSmemMyers * 16];
-    const bool staged = n_pat <= (uint32_t)kSmemMyers;
+                                    const MyersReqDev *__restrict__ reqs, uint32_t warm,
+                                    MyersCand *cand, uint32_t cap, Counters *ctr) {
+    constexpr uint32_t kStaged = kSmemMyers * 4 / sizeof(Word);  // 32 KB of eq tables
+    __shared__ Word seq[kStaged * 16];
+    const bool staged = n_pat <= kStaged;
     if (staged)
-        for (uint32_t i = threadIdx.x; i < n_pat * 16; i += blockDim.x) seq[i] = pats[i / 16].eq16[i % 16];
+        for (uint32_t i = threadIdx.x; i < n_pat * 16; i += blockDim.x) seq[i] = eq_word<Word>(pats[i / 16], i % 16);
     __syncthreads();
     const uint64_t n_items = n_tiles * n_pat;
     for (uint64_t item = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; item < n_items;
@@ -117,27 +155,18 @@ __global__ void myers_filter_kernel(const uint8_t *__restrict__ bit4,
         const BatchDev B = batches[T.batch];
         const MyersPattern &P = pats[p];
         const MyersReqDev R = reqs[P.request];
-        const uint32_t *eq = staged ? seq + 16 * p : P.eq16;
         const uint32_t L = P.L;
-        const uint32_t mask = L == 32 ? 0xFFFFFFFFu : ((1u << L) - 1u);
+        const Word mask = myers_mask<Word>(L);
         const uint32_t sh = L - 1;
-        uint32_t vp = mask, vn = 0;
+        Word vp = mask, vn = 0;
         int score = (int)L;
-        const uint64_t ws = T.t0 >= kWarm ? ((T.t0 - kWarm) & ~15ull) : 0;
+        const uint64_t ws = T.t0 >= warm ? ((T.t0 - warm) & ~15ull) : 0;
         unsigned long long word = 0;
         for (uint64_t q = ws; q < T.t1; ++q) {
             if ((q & 15) == 0 || q == ws)
                 word = __ldg(reinterpret_cast<const unsigned long long *>(bit4 + ((q >> 1) & ~7ull)));
             const uint32_t b = (uint32_t)(word >> ((q & 15) * 4)) & 0xF;
-            const uint32_t x = eq[b] | vn;
-            const uint32_t d0 = (((x & vp) + vp) ^ vp) | x;
-            const uint32_t hn = vp & d0;
-            const uint32_t hp = vn | ~(vp | d0);
-            const uint32_t xs = hp << 1;
-            vn = xs & d0;
-            vp = ((hn << 1) | ~(xs | d0)) & mask;
-            vn &= mask;
-            score += (int)((hp >> sh) & 1u) - (int)((hn >> sh) & 1u);
+            score += myers_step<Word>(staged ? seq[16 * p + b] : eq_word<Word>(P, b), vp, vn, mask, sh);
             if (q >= T.t0 && score <= (int)P.E) {
                 const uint32_t tl = (uint32_t)(q - B.base);
                 if (tl + 1 >= L && pam_quick(bit4, B, tl, P, R.db, R.rb)) {
@@ -172,19 +201,21 @@ struct PamForm {
     uint8_t f[kMaxCells];                        // filter bit4 of the PAM cells
 };
 
+template <typename Word>
 __global__ void __launch_bounds__(kMfThreads)
 myers_tile_kernel(const uint8_t *__restrict__ bit4, const BatchDev *__restrict__ batches,
                   const MyersTile *__restrict__ tiles, uint64_t n_tiles,
                   const MyersPattern *__restrict__ pats, uint32_t n_pat,
                   const PamForm *__restrict__ forms, uint32_t n_forms, uint32_t tpb,
-                  MyersCand *cand, uint32_t cap, Counters *ctr) {
-    extern __shared__ uint32_t mf_smem[];
+                  uint32_t warm, MyersCand *cand, uint32_t cap, Counters *ctr) {
+    extern __shared__ __align__(16) uint32_t mf_smem[];
     uint32_t *q_bits = mf_smem;                            // [tpb][n_forms][kMfQWords]
     uint32_t *ok_bits = q_bits + tpb * n_forms * kMfQWords; // [tpb][n_forms][32]
-    uint32_t *seq = ok_bits + tpb * n_forms * 32;          // [n_pat][16] when staged
+    // [n_pat][16] when staged; 8-byte aligned (kMfQWords and 32 words are even)
+    Word *seq = reinterpret_cast<Word *>(ok_bits + tpb * n_forms * 32);
     const bool staged = n_pat <= (uint32_t)kSmemMyers;
     if (staged)
-        for (uint32_t i = threadIdx.x; i < n_pat * 16; i += blockDim.x) seq[i] = pats[i / 16].eq16[i % 16];
+        for (uint32_t i = threadIdx.x; i < n_pat * 16; i += blockDim.x) seq[i] = eq_word<Word>(pats[i / 16], i % 16);
     for (uint64_t tb = blockIdx.x; tb * tpb < n_tiles; tb += gridDim.x) {
         const uint64_t tile0 = tb * tpb;
         const uint32_t nt = (uint32_t)(n_tiles - tile0 < tpb ? n_tiles - tile0 : tpb);
@@ -233,29 +264,25 @@ myers_tile_kernel(const uint8_t *__restrict__ bit4, const BatchDev *__restrict__
             const MyersTile T = tiles[tile0 + tl];
             const BatchDev B = batches[T.batch];
             const MyersPattern &P = pats[p];
-            const uint32_t *eq = staged ? seq + 16 * p : P.eq16;
+            const Word *eq = staged ? seq + 16 * p
+                                    : (sizeof(Word) == 4 ? reinterpret_cast<const Word *>(P.eq_lo) : nullptr);
             const uint32_t *okw = ok_bits + (tl * n_forms + P.pad) * 32;
             const uint32_t L = P.L;
-            const uint32_t mask = L == 32 ? 0xFFFFFFFFu : ((1u << L) - 1u);
+            const Word mask = myers_mask<Word>(L);
             const uint32_t sh = L - 1;
-            uint32_t vp = mask, vn = 0;
+            Word vp = mask, vn = 0;
             int score = (int)L;
-            const uint64_t ws = T.t0 >= kWarm ? ((T.t0 - kWarm) & ~15ull) : 0;
+            const uint64_t ws = T.t0 >= warm ? ((T.t0 - warm) & ~15ull) : 0;
             unsigned long long word = 0;
             uint32_t okb = 0;
             for (uint64_t q = ws; q < T.t1; ++q) {
                 if ((q & 15) == 0 || q == ws)
                     word = __ldg(reinterpret_cast<const unsigned long long *>(bit4 + ((q >> 1) & ~7ull)));
                 const uint32_t b = (uint32_t)(word >> ((q & 15) * 4)) & 0xF;
-                const uint32_t x = eq[b] | vn;
-                const uint32_t d0 = (((x & vp) + vp) ^ vp) | x;
-                const uint32_t hn = vp & d0;
-                const uint32_t hp = vn | ~(vp | d0);
-                const uint32_t xs = hp << 1;
-                vn = xs & d0;
-                vp = ((hn << 1) | ~(xs | d0)) & mask;
-                vn &= mask;
-                score += (int)((hp >> sh) & 1u) - (int)((hn >> sh) & 1u);
+                Word e;
+                if constexpr (sizeof(Word) == 4) e = eq[b];
+                else e = staged ? eq[b] : eq_word<Word>(P, b);
+                score += myers_step<Word>(e, vp, vn, mask, sh);
                 if (q >= T.t0) {
                     const uint32_t r = (uint32_t)(q - T.t0);
                     if ((r & 31) == 0) okb = okw[r >> 5];
@@ -347,10 +374,12 @@ traceback_kernel(GenomeDev G, const BatchDev *__restrict__ batches,
                     bool ok = true;
                     uint32_t pi = 0, gi = f.j;
                     uint64_t o0 = 0, o1 = 0;
+                    uint32_t o2 = 0;
                     for (int k = 0; k < n_ops; ++k) {
                         const uint8_t op = ops[n_ops - 1 - k];
                         if (k < 32) o0 |= (uint64_t)op << (2 * k);
-                        else o1 |= (uint64_t)op << (2 * (k - 32));
+                        else if (k < 64) o1 |= (uint64_t)op << (2 * (k - 32));
+                        else o2 |= (uint32_t)op << (2 * (k - 64));
                         if (op <= 1) {
                             const uint8_t g = text[gi], fl = P.eff[pi];
                             const bool good = fl == 0xF ? g != 0 : (g != 0 && g != 0xF && (g & fl));
@@ -390,7 +419,7 @@ traceback_kernel(GenomeDev G, const BatchDev *__restrict__ batches,
                                 w.mm = f.mm;
                                 w.db = f.db;
                                 w.rb = f.rb;
-                                w.pad = 0;
+                                w.ops_hi = o2;
                                 rows[r] = w;
                                 keys[r] = ((uint64_t)c.pattern << 34) | start;
                                 vals[r] = r;
@@ -482,49 +511,71 @@ traceback_kernel(GenomeDev G, const BatchDev *__restrict__ batches,
 // spends kTbBudget iterations on one tree hands its remaining stack to a
 // global queue, which the next pass spreads over all warps, so a candidate
 // with thousands of alignments cannot serialise the launch.
-constexpr int kTbWarps = 4;                  // warps per block
-constexpr int kTbCap = 160;                  // stack slots per warp
-constexpr int kTbMargin = 2 * kMaxCells;     // slots a one-node-at-a-time walk can add
+//
+// Patterns of more than 32 cells: the wavefront runs in passes of 32 rows,
+// lane 0 of a later pass reading its upper row from the table.
+constexpr int kTbWarps = 4;                  // warps per block (fewer for large tables)
+constexpr uint32_t kTbSpare = 80;            // stack slots beyond the walk margin
 constexpr uint32_t kTbMaxBits = 128;         // budget bits per cell (NW <= 2)
 constexpr uint32_t kTbBudget = 384;          // iterations on one tree before handing it on
 constexpr uint32_t kTbQueue = 1u << 21;      // subtrees per hand-on queue
 constexpr int kTbMaxPasses = 24;             // the last pass finishes every tree
+constexpr uint32_t kTbText = 80;             // staged window text bytes (>= kMaxCells)
+constexpr uint32_t kTbPat = 64;              // staged bytes per pattern array (>= L)
 
+// Stack slots a one-node-at-a-time walk can add to a warp's stack: at most
+// two per level (three children, one popped), levels <= W; never below the
+// 80 of a 40-cell window.
+inline uint32_t tb_margin(uint32_t wmax) { return 2 * std::max(wmax, 40u); }
+
+// A node of the enumeration.  NO 64-bit words and ops_hi hold its walk-back
+// ops, 2 bits per op: depths 0..32 NO - 1 in ops, the next 16 in ops_hi
+// (NO = 1: windows of <= 48 cells, NO = 2: <= 80).  Its depth is L - i + d
+// (each step consumes a pattern cell, or a text cell for a DNA bulge).
+template <int NO>
 struct TbNode {
-    uint64_t ops;     // walk-back order, 2 bits per op, depths 0..31
-    uint32_t ops_hi;  // depths 32..39
-    uint32_t st;      // i | j << 6 | m << 12 | d << 18 | r << 22 | depth << 26
+    uint64_t ops[NO];
+    uint32_t ops_hi;
+    uint32_t st;      // i | j << 7 | m << 14 | d << 20 | r << 24
 };
 
 // one unit of enumeration work: a candidate's root, or a subtree handed on
 // by a warp that spent its iteration budget (cand == ~0u: an empty slot)
+template <int NO>
 struct TbItem {
     uint32_t cand, pad;
-    TbNode node;
+    TbNode<NO> node;
 };
 
-// walk-back ops (2 bits per step, n_ops steps, steps 32.. in hi) into
-// alignment order: reverse all 64 two-bit groups of the 128-bit value, then
-// drop the 64 - n_ops unused groups
-__device__ __forceinline__ void ops_forward(uint64_t lo, uint64_t hi, uint32_t n_ops,
-                                            uint64_t &o0, uint64_t &o1) {
+// the 32 two-bit groups of x in reverse order
+__device__ __forceinline__ uint64_t rev2(uint64_t x) {
     const uint64_t k5 = 0x5555555555555555ull;
-    uint64_t rl = __brevll(hi), rh = __brevll(lo);
-    rl = ((rl >> 1) & k5) | ((rl & k5) << 1);
-    rh = ((rh >> 1) & k5) | ((rh & k5) << 1);
-    const uint32_t sh = 2 * (64 - n_ops);  // 48..126
-    if (sh >= 64) {
-        o0 = rh >> (sh - 64);
-        o1 = 0;
-    } else {
-        o0 = (rl >> sh) | (rh << (64 - sh));
-        o1 = rh >> sh;
-    }
+    x = __brevll(x);
+    return ((x >> 1) & k5) | ((x & k5) << 1);
+}
+
+// walk-back ops (2 bits per step: steps 0..31 in a0, 32..63 in a1, 64..79
+// in a2) into alignment order: reverse the 96 two-bit groups of
+// (a2:a1:a0), which puts step g at group 95 - g, then shift right by
+// 2 (96 - n_ops) so that op k = step n_ops - 1 - k lands at group k
+__device__ __forceinline__ void ops_forward(uint64_t a0, uint64_t a1, uint32_t a2,
+                                            uint32_t n_ops, uint64_t &o0, uint64_t &o1,
+                                            uint32_t &o2) {
+    const uint64_t r[3] = {rev2((uint64_t)a2), rev2(a1), rev2(a0)};
+    const uint32_t sh = 2 * (96 - n_ops), w = sh >> 6, b = sh & 63;  // sh in 48..190
+    auto word = [&](uint32_t k) -> uint64_t { return k == 0 ? r[0] : k == 1 ? r[1] : k == 2 ? r[2] : 0; };
+    auto out = [&](uint32_t q) -> uint64_t {
+        const uint64_t lo = word(w + q), hi = word(w + q + 1);
+        return b ? (lo >> b) | (hi << (64 - b)) : lo;
+    };
+    o0 = out(0);
+    o1 = out(1);
+    o2 = (uint32_t)out(2);
 }
 
 __device__ __forceinline__ uint32_t tb_st(uint32_t i, uint32_t j, uint32_t m, uint32_t d,
-                                          uint32_t r, uint32_t dep) {
-    return i | (j << 6) | (m << 12) | (d << 18) | (r << 22) | (dep << 26);
+                                          uint32_t r) {
+    return i | (j << 7) | (m << 14) | (d << 20) | (r << 24);
 }
 
 // classify's filter test of a match / substitution cell
@@ -580,27 +631,31 @@ __device__ __forceinline__ void budget_cell(const uint64_t (&dg)[NW], const uint
     }
 }
 
-// shared-memory bytes one warp needs for tables of tbl_words 64-bit words
-__host__ __device__ constexpr size_t tb_warp_bytes(uint32_t tbl_words) {
-    return (kTbCap * sizeof(TbNode) + (size_t)tbl_words * 8 + 64 + 3 * 48 + 15) & ~(size_t)15;
+// shared-memory bytes one warp needs: a stack of cap nodes, tables of
+// tbl_words 64-bit words, the window text and three pattern arrays
+template <int NO>
+__host__ __device__ constexpr size_t tb_warp_bytes(uint32_t tbl_words, uint32_t cap) {
+    return ((size_t)cap * sizeof(TbNode<NO>) + (size_t)tbl_words * 8 + kTbText + 3 * kTbPat + 15) &
+           ~(size_t)15;
 }
 
-template <int NW>
+template <int NW, int NO>
 __global__ void __launch_bounds__(kTbWarps * 32)
 traceback_warp_kernel(GenomeDev G, const BatchDev *__restrict__ batches,
                       const MyersPattern *__restrict__ pats, const MyersReqDev *__restrict__ reqs,
                       const MyersCand *__restrict__ cand, uint32_t n_cand,
-                      const TbItem *__restrict__ items, uint32_t n_items, TbItem *spill,
+                      const TbItem<NO> *__restrict__ items, uint32_t n_items, TbItem<NO> *spill,
                       uint32_t spill_cap, uint32_t iter_budget, uint32_t tbl_words,
-                      MyersRow *rows, uint32_t row_cap, uint64_t *keys, uint32_t *vals,
-                      Counters *ctr, uint32_t *req_rows) {
+                      uint32_t stk_cap, uint32_t margin, MyersRow *rows, uint32_t row_cap,
+                      uint64_t *keys, uint32_t *vals, Counters *ctr, uint32_t *req_rows) {
+    using Node = TbNode<NO>;
     extern __shared__ __align__(16) unsigned char tb_smem[];
     const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    unsigned char *wbase = tb_smem + warp * tb_warp_bytes(tbl_words);
-    TbNode *stk = reinterpret_cast<TbNode *>(wbase);
-    uint64_t *tbl = reinterpret_cast<uint64_t *>(wbase + kTbCap * sizeof(TbNode));
-    uint8_t *stext = wbase + kTbCap * sizeof(TbNode) + (size_t)tbl_words * 8;
-    uint8_t *spb = stext + 64, *sisn = spb + 48, *seff = sisn + 48;
+    unsigned char *wbase = tb_smem + warp * tb_warp_bytes<NO>(tbl_words, stk_cap);
+    Node *stk = reinterpret_cast<Node *>(wbase);
+    uint64_t *tbl = reinterpret_cast<uint64_t *>(wbase + stk_cap * sizeof(Node));
+    uint8_t *stext = wbase + stk_cap * sizeof(Node) + (size_t)tbl_words * 8;
+    uint8_t *spb = stext + kTbText, *sisn = spb + kTbPat, *seff = sisn + kTbPat;
     const unsigned full = 0xFFFFFFFFu;
 
     const uint32_t n_work = items ? n_items : n_cand;
@@ -611,9 +666,9 @@ traceback_warp_kernel(GenomeDev G, const BatchDev *__restrict__ batches,
         if (wi >= n_work) break;
         __syncwarp();  // the previous item's readers are done
         uint32_t ci = wi;
-        TbNode start_node{0, 0, 0};
+        Node start_node{};
         if (items) {
-            const TbItem it = items[wi];
+            const TbItem<NO> it = items[wi];
             if (it.cand == ~0u) continue;
             ci = it.cand;
             start_node = it.node;
@@ -641,54 +696,58 @@ traceback_warp_kernel(GenomeDev G, const BatchDev *__restrict__ batches,
         }
         __syncwarp();
 
-        // -- 1. budget DP wavefront
-        const uint32_t i = lane + 1;
-        const bool row_on = i <= L;
-        uint8_t pbi = 0, effi = 0;
-        bool isn1 = false, rna_ok = false, dna_ok = false;
-        if (row_on) {
-            pbi = spb[i - 1];
-            effi = seff[i - 1];
-            isn1 = sisn[i - 1];
-            const bool isn0 = i < L && sisn[i];
-            const bool isn2 = i >= 2 && sisn[i - 2];
-            rna_ok = R.rb > 0 && !isn1 && !isn0 && !isn2;
-            dna_ok = R.db > 0 && i < L && !(isn1 && isn0);
-        }
-        uint64_t left[NW], upc[NW], upp[NW];
-#pragma unroll
-        for (int w = 0; w < NW; ++w) left[w] = upc[w] = upp[w] = 0;
-        for (uint32_t s = 0; s < L + n; ++s) {
-#pragma unroll
-            for (int w = 0; w < NW; ++w) {
-                uint64_t u = __shfl_up_sync(full, left[w], 1);
-                if (lane == 0) u = valid[w];  // row 0
-                upp[w] = upc[w];
-                upc[w] = u;
+        // -- 1. budget DP wavefront, 32 pattern rows per pass
+        for (uint32_t r0 = 0; r0 < L; r0 += 32) {
+            const uint32_t i = r0 + lane + 1;
+            const bool row_on = i <= L;
+            uint8_t pbi = 0, effi = 0;
+            bool isn1 = false, rna_ok = false, dna_ok = false;
+            if (row_on) {
+                pbi = spb[i - 1];
+                effi = seff[i - 1];
+                isn1 = sisn[i - 1];
+                const bool isn0 = i < L && sisn[i];
+                const bool isn2 = i >= 2 && sisn[i - 2];
+                rna_ok = R.rb > 0 && !isn1 && !isn0 && !isn2;
+                dna_ok = R.db > 0 && i < L && !(isn1 && isn0);
             }
-            const int j = (int)s - (int)lane;
-            if (row_on && j >= 0 && j <= (int)n) {
-                uint64_t v[NW];
-                const uint8_t tx = j ? stext[j - 1] : 0;
-                if (j == 0) {
-                    budget_cell<NW>(upp, upc, left, false, 0, rna_ok, false, T, dsh, R, v);
-                } else if (tx == 0) {  // a node over a padding cell is dead
+            uint64_t left[NW], upc[NW], upp[NW];
 #pragma unroll
-                    for (int w = 0; w < NW; ++w) v[w] = 0;
-                } else {
-                    const uint32_t mc = loose(pbi, tx) ? 0u : 1u;
-                    const bool dok = !(mc && isn1) && filt_ok(effi, tx);
-                    budget_cell<NW>(upp, upc, left, dok, mc, rna_ok, dna_ok, T, dsh, R, v);
-                }
-                uint64_t *cell = tbl + (i * cols + (uint32_t)j) * NW;
+            for (int w = 0; w < NW; ++w) left[w] = upc[w] = upp[w] = 0;
+            const uint32_t n_rows = min(32u, L - r0);
+            for (uint32_t s = 0; s < n_rows + n; ++s) {
 #pragma unroll
                 for (int w = 0; w < NW; ++w) {
-                    left[w] = v[w];
-                    cell[w] = v[w];
+                    uint64_t u = __shfl_up_sync(full, left[w], 1);
+                    if (lane == 0)  // row r0, column s: row 0, or the previous pass
+                        u = r0 == 0 ? valid[w] : (s <= n ? tbl[(r0 * cols + s) * NW + w] : 0);
+                    upp[w] = upc[w];
+                    upc[w] = u;
+                }
+                const int j = (int)s - (int)lane;
+                if (row_on && j >= 0 && j <= (int)n) {
+                    uint64_t v[NW];
+                    const uint8_t tx = j ? stext[j - 1] : 0;
+                    if (j == 0) {
+                        budget_cell<NW>(upp, upc, left, false, 0, rna_ok, false, T, dsh, R, v);
+                    } else if (tx == 0) {  // a node over a padding cell is dead
+#pragma unroll
+                        for (int w = 0; w < NW; ++w) v[w] = 0;
+                    } else {
+                        const uint32_t mc = loose(pbi, tx) ? 0u : 1u;
+                        const bool dok = !(mc && isn1) && filt_ok(effi, tx);
+                        budget_cell<NW>(upp, upc, left, dok, mc, rna_ok, dna_ok, T, dsh, R, v);
+                    }
+                    uint64_t *cell = tbl + (i * cols + (uint32_t)j) * NW;
+#pragma unroll
+                    for (int w = 0; w < NW; ++w) {
+                        left[w] = v[w];
+                        cell[w] = v[w];
+                    }
                 }
             }
+            __syncwarp();
         }
-        __syncwarp();
         // F[b](ii, jj) <= mm - m ?
         auto feas = [&](uint32_t ii, uint32_t jj, uint32_t b, uint32_t m) -> bool {
             const uint32_t bit = b * T + (mm - m);
@@ -696,7 +755,8 @@ traceback_warp_kernel(GenomeDev G, const BatchDev *__restrict__ batches,
         };
         if (!items) {
             if (!feas(L, n, R.db * rb1 + R.rb, 0)) continue;  // no alignment within the caps
-            start_node = TbNode{0, 0, tb_st(L, n, 0, 0, 0, 0)};
+            start_node = Node{};
+            start_node.st = tb_st(L, n, 0, 0, 0);
         }
         // every leaf starts in [t + 1 - n, t + 1]: one chunk lookup serves
         // them all unless that range crosses a chunk boundary
@@ -724,7 +784,7 @@ traceback_warp_kernel(GenomeDev G, const BatchDev *__restrict__ batches,
                 if (lane == 0) sb = atomicAdd(&ctr->hits, size);
                 sb = __shfl_sync(full, sb, 0);
                 if ((uint64_t)sb + size <= spill_cap) {
-                    for (uint32_t q = lane; q < size; q += 32) spill[sb + q] = TbItem{ci, 0, stk[q]};
+                    for (uint32_t q = lane; q < size; q += 32) spill[sb + q] = TbItem<NO>{ci, 0, stk[q]};
                     __syncwarp();
                     break;
                 }
@@ -734,10 +794,10 @@ traceback_warp_kernel(GenomeDev G, const BatchDev *__restrict__ batches,
             ++iters;
             // pop k nodes; with size + 2k <= cap - margin the stack cannot
             // overflow, and below that a one-node walk adds <= margin slots
-            const int room = kTbCap - kTbMargin - (int)size;
+            const int room = (int)stk_cap - (int)margin - (int)size;
             const uint32_t k = room >= 2 ? min(min(32u, size), (uint32_t)room / 2) : 1u;
             const bool have = lane < k;
-            TbNode nd{0, 0, 0};
+            Node nd{};
             if (have) nd = stk[size - 1 - lane];
             size -= k;
             __syncwarp();
@@ -750,9 +810,9 @@ traceback_warp_kernel(GenomeDev G, const BatchDev *__restrict__ batches,
             uint32_t dep = 0;
             if (have) {
                 const uint32_t st = nd.st;
-                const uint32_t ni = st & 63, nj = (st >> 6) & 63, m = (st >> 12) & 63;
-                const uint32_t d = (st >> 18) & 15, r = (st >> 22) & 15;
-                dep = st >> 26;
+                const uint32_t ni = st & 127, nj = (st >> 7) & 127, m = (st >> 14) & 63;
+                const uint32_t d = (st >> 20) & 15, r = (st >> 24) & 15;
+                dep = L - ni + d;
                 // convert_matches_myers: owning chunk and record-end drop
                 auto leaf = [&](Leaf &o, uint32_t jf, uint32_t lm, uint32_t ld, uint32_t lr,
                                 uint32_t op) {
@@ -771,7 +831,7 @@ traceback_warp_kernel(GenomeDev G, const BatchDev *__restrict__ batches,
                         if (ni == 1)
                             leaf(la, nj - 1, m + mc, d, r, mc);
                         else if (feas(ni - 1, nj - 1, (R.db - d) * rb1 + (R.rb - r), m + mc))
-                            ka = Kid{tb_st(ni - 1, nj - 1, m + mc, d, r, dep + 1), mc, true};
+                            ka = Kid{tb_st(ni - 1, nj - 1, m + mc, d, r), mc, true};
                     }
                 }
                 // RNA bulge: pattern cell skipped
@@ -781,20 +841,23 @@ traceback_warp_kernel(GenomeDev G, const BatchDev *__restrict__ batches,
                         if (ni == 1)
                             leaf(lb, nj, m, d, r + 1, 3);
                         else if (feas(ni - 1, nj, (R.db - d) * rb1 + (R.rb - r - 1), m))
-                            kb = Kid{tb_st(ni - 1, nj, m, d, r + 1, dep + 1), 3, true};
+                            kb = Kid{tb_st(ni - 1, nj, m, d, r + 1), 3, true};
                     }
                 }
                 // DNA bulge: text cell skipped
                 if (d < R.db && nj >= 1 && ni < L && !(sisn[ni - 1] && sisn[ni])) {
                     if (feas(ni, nj - 1, (R.db - d - 1) * rb1 + (R.rb - r), m))
-                        kc = Kid{tb_st(ni, nj - 1, m, d + 1, r, dep + 1), 2, true};
+                        kc = Kid{tb_st(ni, nj - 1, m, d + 1, r), 2, true};
                 }
             }
-            auto ops_with = [&](uint32_t op, uint64_t &o, uint32_t &oh) {
-                o = nd.ops;
-                oh = nd.ops_hi;
-                if (dep < 32) o |= (uint64_t)op << (2 * dep);
-                else oh |= op << (2 * (dep - 32));
+            // nd's ops with op at depth dep
+            auto ops_with = [&](uint32_t op, Node &o) {
+#pragma unroll
+                for (int q = 0; q < NO; ++q) o.ops[q] = nd.ops[q];
+                o.ops_hi = nd.ops_hi;
+                if (dep < 32) o.ops[0] |= (uint64_t)op << (2 * dep);
+                else if (NO == 2 && dep < 64) o.ops[NO - 1] |= (uint64_t)op << (2 * (dep - 32));
+                else o.ops_hi |= op << (2 * (dep - 32 * NO));
             };
             const uint32_t nc = (uint32_t)ka.on + kb.on + kc.on;
             const uint32_t ne = (uint32_t)la.on + lb.on;
@@ -809,8 +872,8 @@ traceback_warp_kernel(GenomeDev G, const BatchDev *__restrict__ batches,
             uint32_t at = size + incl - nc;
             auto push = [&](const Kid &k2) {
                 if (!k2.on) return;
-                TbNode o;
-                ops_with(k2.op, o.ops, o.ops_hi);
+                Node o;
+                ops_with(k2.op, o);
                 o.st = k2.st;
                 stk[at++] = o;
             };
@@ -837,22 +900,22 @@ traceback_warp_kernel(GenomeDev G, const BatchDev *__restrict__ batches,
                 auto put = [&](const Leaf &l2) {
                     if (!l2.on) return;
                     if (rr < row_cap) {
-                        uint64_t o, oh32;
-                        uint32_t oh;
-                        ops_with(l2.op, o, oh);
-                        oh32 = oh;
+                        Node o;
+                        ops_with(l2.op, o);
                         const uint32_t n_ops = dep + 1;
                         MyersRow w;
                         w.start = l2.start;
                         w.pos = l2.pos;
-                        ops_forward(o, oh32, n_ops, w.ops[0], w.ops[1]);
+                        // steps 0..31, 32..63, 64..79 of the walk-back ops
+                        const uint64_t a1 = NO == 1 ? (uint64_t)o.ops_hi : o.ops[NO - 1];
+                        const uint32_t a2 = NO == 1 ? 0u : o.ops_hi;
+                        ops_forward(o.ops[0], a1, a2, n_ops, w.ops[0], w.ops[1], w.ops_hi);
                         w.chunk = l2.chunk;
                         w.pattern = c.pattern;
                         w.n_ops = (uint8_t)n_ops;
                         w.mm = (uint8_t)l2.m;
                         w.db = (uint8_t)l2.d;
                         w.rb = (uint8_t)l2.r;
-                        w.pad = 0;
                         rows[rr] = w;
                         keys[rr] = ((uint64_t)c.pattern << 34) | l2.start;
                         vals[rr] = rr;
@@ -880,7 +943,9 @@ traceback_warp_kernel(GenomeDev G, const BatchDev *__restrict__ batches,
 // are passed on.
 constexpr int kBfThreads = 128;
 
-template <int NW>
+// TW: 64-bit words of window text, 16 cells each (3: windows of <= 48
+// cells, 5: <= 80)
+template <int NW, int TW>
 __global__ void __launch_bounds__(kBfThreads)
 budget_filter_kernel(GenomeDev G, const BatchDev *__restrict__ batches,
                      const MyersPattern *__restrict__ pats, const MyersReqDev *__restrict__ reqs,
@@ -910,12 +975,17 @@ budget_filter_kernel(GenomeDev G, const BatchDev *__restrict__ batches,
                 fullg[w] = R.m_full[w];
                 valid[w] = R.m_valid[w];
             }
-            // the window's n text cells, cell k in bits 4k of (t2:t1:t0)
+            // the window's n text cells, cell k in bits 4 (k % 16) of word k / 16
+            // of (tw4:tw3:tw2:tw1:tw0)
             const uint64_t tbase = B.base + t + 1 - n;
-            uint64_t tw0 = 0, tw1 = 0, tw2 = 0;
+            uint64_t tw0 = 0, tw1 = 0, tw2 = 0, tw3 = 0, tw4 = 0;
             for (uint32_t k = 0; k < n; ++k) {
                 const uint64_t x = (uint64_t)nib(G.bit4, tbase + k) << (4 * (k & 15));
-                if (k < 16) tw0 |= x; else if (k < 32) tw1 |= x; else tw2 |= x;
+                if (k < 16) tw0 |= x;
+                else if (k < 32) tw1 |= x;
+                else if (TW == 3 || k < 48) tw2 |= x;
+                else if (k < 64) tw3 |= x;
+                else tw4 |= x;
             }
             for (uint32_t j = 0; j <= n; ++j) {
 #pragma unroll
@@ -939,12 +1009,18 @@ budget_filter_kernel(GenomeDev G, const BatchDev *__restrict__ batches,
                     Rw(0, w) = left[w];
                     row_or |= left[w] & fullg[w];
                 }
-                uint64_t a0 = tw0, a1 = tw1, a2 = tw2;  // text shift register
+                uint64_t a0 = tw0, a1 = tw1, a2 = tw2, a3 = tw3, a4 = tw4;  // text shift register
                 for (uint32_t j = 1; j <= n; ++j) {
                     const uint8_t tx = (uint8_t)(a0 & 0xF);
                     a0 = (a0 >> 4) | (a1 << 60);
                     a1 = (a1 >> 4) | (a2 << 60);
-                    a2 >>= 4;
+                    if (TW == 3) {
+                        a2 >>= 4;
+                    } else {
+                        a2 = (a2 >> 4) | (a3 << 60);
+                        a3 = (a3 >> 4) | (a4 << 60);
+                        a4 >>= 4;
+                    }
 #pragma unroll
                     for (int w = 0; w < NW; ++w) up[w] = Rw(j, w);
                     if (tx == 0) {  // a node over a padding cell is dead
@@ -1058,7 +1134,7 @@ mrow_write_kernel(GenomeDev G, const MyersRow *__restrict__ rows,
             uint32_t pi = 0;
             uint64_t gi = w.start;
             for (uint32_t k = 0; k < no; ++k) {
-                const uint32_t op = (uint32_t)((k < 32 ? w.ops[0] >> (2 * k) : w.ops[1] >> (2 * (k - 32))) & 3);
+                const uint32_t op = mrow_op(w, k);
                 uint8_t pv = 0, gv = 0;
                 bool pgap = false, ggap = false;
                 if (op <= 1) {
@@ -1102,23 +1178,57 @@ mrow_write_kernel(GenomeDev G, const MyersRow *__restrict__ rows,
     }
 }
 
+// One launch of the warp traceback; the work queues are untyped here
+// because the node width is a template parameter.
+struct TbLaunch {
+    unsigned grid, threads;
+    size_t smem;
+    cudaStream_t s;
+    GenomeDev G;
+    const BatchDev *batches;
+    const MyersPattern *pats;
+    const MyersReqDev *reqs;
+    const MyersCand *cand;
+    uint32_t n_cand;
+    const char *items;
+    uint32_t n_items;
+    char *spill;
+    uint32_t spill_cap, iter_budget, tbl_words, stk_cap, margin;
+    MyersRow *rows;
+    uint32_t row_cap;
+    uint64_t *keys;
+    uint32_t *vals;
+    Counters *ctr;
+    uint32_t *req_rows;
+};
+
+template <int NW, int NO>
+void launch_tb(const TbLaunch &a) {
+    traceback_warp_kernel<NW, NO><<<a.grid, a.threads, a.smem, a.s>>>(
+        a.G, a.batches, a.pats, a.reqs, a.cand, a.n_cand,
+        reinterpret_cast<const TbItem<NO> *>(a.items), a.n_items,
+        reinterpret_cast<TbItem<NO> *>(a.spill), a.spill_cap, a.iter_budget, a.tbl_words,
+        a.stk_cap, a.margin, a.rows, a.row_cap, a.keys, a.vals, a.ctr, a.req_rows);
+}
+
 // Myers Eq table of one pattern (build_peq, myers.rs:32-50, and the eq rule
 // of search.rs:846-858): nibble 0 -> 0, 0xF -> peq_n, else OR of the peqs of
 // its set bits (A=4, C=2, G=8, T=1).
-void build_eq16(const std::string &p, uint32_t eq16[16]) {
-    uint32_t peq[4] = {0, 0, 0, 0}, peq_n = 0;
+// Patterns of up to 64 cells: the low 32 bits go to eq_lo, the rest to eq_hi.
+void build_eq16(const std::string &p, uint32_t eq_lo[16], uint32_t eq_hi[16]) {
+    uint64_t peq[4] = {0, 0, 0, 0}, peq_n = 0;
     for (size_t i = 0; i < p.size(); ++i) {
         const char u = (char)((p[i] >= 'a' && p[i] <= 'z') ? p[i] - 32 : p[i]);
         const int idx = u == 'A' ? 0 : u == 'C' ? 1 : u == 'G' ? 2 : u == 'T' ? 3 : 4;
         if (idx < 4) {
-            peq[idx] |= 1u << i;
+            peq[idx] |= 1ull << i;
         } else {
-            for (int k = 0; k < 4; ++k) peq[k] |= 1u << i;
-            peq_n |= 1u << i;
+            for (int k = 0; k < 4; ++k) peq[k] |= 1ull << i;
+            peq_n |= 1ull << i;
         }
     }
     for (int b = 0; b < 16; ++b) {
-        uint32_t e = 0;
+        uint64_t e = 0;
         if (b == 15) e = peq_n;
         else {
             if (b & 4) e |= peq[0];
@@ -1126,7 +1236,8 @@ void build_eq16(const std::string &p, uint32_t eq16[16]) {
             if (b & 8) e |= peq[2];
             if (b & 1) e |= peq[3];
         }
-        eq16[b] = e;
+        eq_lo[b] = (uint32_t)e;
+        eq_hi[b] = (uint32_t)(e >> 32);
     }
 }
 
@@ -1206,8 +1317,8 @@ int Engine::run_bulge(const std::vector<Request> &reqs, std::vector<Result> &out
                 if (b == nbud - 1) setb(rd.m_full, bit);
             }
         }
-        if (rd.W > (uint32_t)kMaxCells) {
-            err = {kUnsupported, "pattern length + max_dna_bulges above 40"};
+        if (rd.L > 64 || rd.W > (uint32_t)kMaxCells) {
+            err = {kUnsupported, "bulge search needs pattern length <= 64 and length + max_dna_bulges <= 72"};
             return err.code;
         }
         rdev.push_back(rd);
@@ -1225,7 +1336,7 @@ int Engine::run_bulge(const std::vector<Request> &reqs, std::vector<Result> &out
             mp.W = rd.W;
             const std::string &pa = r.patterns[p];
             const std::string &fa = p < nfwd ? r.filter : rf;
-            build_eq16(pa, mp.eq16);
+            build_eq16(pa, mp.eq_lo, mp.eq_hi);
             for (uint32_t c = 0; c < L; ++c) {
                 mp.b4[c] = t.str2b4[1][(uint8_t)pa[c]];
                 mp.isn[c] = pa[c] == 'N' || pa[c] == 'n';
@@ -1256,6 +1367,15 @@ int Engine::run_bulge(const std::vector<Request> &reqs, std::vector<Result> &out
         }
     }
     if (tiles.empty() || pats.empty()) return kOk;
+    // longest pattern and window: 64-bit Myers words above 32 cells, and
+    // the warm-up every window needs
+    uint32_t lmax = 0, wmax = 0;
+    for (const MyersReqDev &rd : rdev) {
+        lmax = std::max(lmax, rd.L);
+        wmax = std::max(wmax, rd.W);
+    }
+    const bool wide = lmax > 32;
+    const uint32_t warm = myers_warm(wmax);
 
     TablePack tp;
     const size_t o_b = tp.add(batches), o_t = tp.add(tiles), o_p = tp.add(pats),
@@ -1283,20 +1403,20 @@ int Engine::run_bulge(const std::vector<Request> &reqs, std::vector<Result> &out
             // kMfThreads, and the grid walks the tile blocks in waves of
             // n_sm x (blocks per SM); take the tpb with the fewest
             // waves x rounds (ties: more tiles per block)
+            auto mf_fn = wide ? myers_tile_kernel<uint64_t> : myers_tile_kernel<uint32_t>;
+            const size_t eq_bytes = wide ? 8 : 4;
             auto smem_of = [&](uint32_t t) {
                 return (size_t)t * forms.size() * (kMfQWords + 32) * 4 +
-                       (n_pat <= (uint32_t)kSmemMyers ? (size_t)n_pat * 64 : 0);
+                       (n_pat <= (uint32_t)kSmemMyers ? (size_t)n_pat * 16 * eq_bytes : 0);
             };
             uint32_t tpb = 1;
             uint64_t best = ~0ull;
             int per_sm = 1;
             for (uint32_t t = 1; t <= kMfMaxTiles; ++t) {
                 const size_t sm = smem_of(t);
-                CU(cudaFuncSetAttribute(myers_tile_kernel,
-                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+                CU(cudaFuncSetAttribute(mf_fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
                 int occ = 1;
-                CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, myers_tile_kernel,
-                                                                 kMfThreads, sm));
+                CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, mf_fn, kMfThreads, sm));
                 occ = std::max(occ, 1);
                 const uint64_t rounds = ((uint64_t)t * n_pat + kMfThreads - 1) / kMfThreads;
                 const uint64_t tblk = (tiles.size() + t - 1) / t;
@@ -1309,21 +1429,21 @@ int Engine::run_bulge(const std::vector<Request> &reqs, std::vector<Result> &out
                 }
             }
             const size_t smem = smem_of(tpb);
-            CU(cudaFuncSetAttribute(myers_tile_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    (int)smem));
+            CU(cudaFuncSetAttribute(mf_fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
             const uint64_t tblocks = (tiles.size() + tpb - 1) / tpb;
             const unsigned blocks = (unsigned)std::max<uint64_t>(
                 1, std::min<uint64_t>(tblocks, (uint64_t)d.n_sm * std::max(1, per_sm)));
-            myers_tile_kernel<<<blocks, kMfThreads, smem, s>>>(
+            mf_fn<<<blocks, kMfThreads, smem, s>>>(
                 d.bit4.p, dB, (const MyersTile *)tab(o_t), tiles.size(), dP, n_pat,
-                (const PamForm *)tab(o_f), (uint32_t)forms.size(), tpb, d.mcand.p, cap, d.ctr.p);
+                (const PamForm *)tab(o_f), (uint32_t)forms.size(), tpb, warm, d.mcand.p, cap,
+                d.ctr.p);
         } else {
             const uint64_t items = (uint64_t)tiles.size() * n_pat;
             const unsigned blocks = (unsigned)std::max<uint64_t>(
                 1, std::min<uint64_t>((items + 127) / 128, (uint64_t)d.n_sm * 16));
-            myers_filter_kernel<<<blocks, 128, 0, s>>>(d.bit4.p, dB, (const MyersTile *)tab(o_t),
-                                                       tiles.size(), dP, n_pat, dR, d.mcand.p, cap,
-                                                       d.ctr.p);
+            auto ff = wide ? myers_filter_kernel<uint64_t> : myers_filter_kernel<uint32_t>;
+            ff<<<blocks, 128, 0, s>>>(d.bit4.p, dB, (const MyersTile *)tab(o_t), tiles.size(), dP,
+                                      n_pat, dR, warm, d.mcand.p, cap, d.ctr.p);
         }
         CU(cudaGetLastError());
         CU(cudaEventRecord(d.ev[2], s));
@@ -1364,25 +1484,44 @@ int Engine::run_bulge(const std::vector<Request> &reqs, std::vector<Result> &out
     // fits 128 bits ((db + 1)(rb + 1)(mm + 1)); COF_BULGE_WARP=0 selects the
     // thread-per-candidate kernel
     bool warp_tb = true;
-    uint32_t nw = 1, wmax = 0;
+    uint32_t nw = 1;
     for (const MyersReqDev &rd : rdev) {
         if (rd.nbits > kTbMaxBits) warp_tb = false;
         nw = std::max(nw, (rd.nbits + 63) / 64);
-        wmax = std::max(wmax, rd.W);
     }
     uint32_t tbl_words = 0;  // 64-bit words of one warp's table
     for (const MyersReqDev &rd : rdev) tbl_words = std::max(tbl_words, (rd.L + 1) * (rd.W + 1) * nw);
     if (const char *e = std::getenv("COF_BULGE_WARP"))
         if (e[0] == '0') warp_tb = false;
-    if (warp_tb && d.tb_items.ensure(2 * (size_t)kTbQueue * sizeof(TbItem), err)) return err.code;
+    // nodes with two op words for windows of more than 48 cells; a stack of
+    // the walk margin plus kTbSpare slots
+    const bool wide_nodes = wmax > 48;
+    const size_t item_bytes = wide_nodes ? sizeof(TbItem<2>) : sizeof(TbItem<1>);
+    const uint32_t tb_mrg = tb_margin(wmax), stk_cap = tb_mrg + kTbSpare;
+    if (warp_tb && d.tb_items.ensure(2 * (size_t)kTbQueue * item_bytes, err)) return err.code;
     uint32_t tb_budget = kTbBudget;  // COF_TB_BUDGET: iterations before a tree is handed on
     if (const char *e = std::getenv("COF_TB_BUDGET")) tb_budget = (uint32_t)std::max(1, std::atoi(e));
-    const size_t tb_smem = (size_t)kTbWarps * tb_warp_bytes(tbl_words);
-    auto tb_fn = nw == 1 ? traceback_warp_kernel<1> : traceback_warp_kernel<2>;
+    const size_t warp_bytes = wide_nodes ? tb_warp_bytes<2>(tbl_words, stk_cap)
+                                         : tb_warp_bytes<1>(tbl_words, stk_cap);
+    // warps per block: kTbWarps, fewer when their tables exceed a block's
+    // shared memory (patterns of more than 32 cells with two-word cells)
+    int smem_optin = 0;
+    CU(cudaDeviceGetAttribute(&smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, d.device));
+    const uint32_t tb_wpb = (uint32_t)std::max<size_t>(
+        1, std::min<size_t>(kTbWarps, (size_t)smem_optin / warp_bytes));
+    if (warp_tb && warp_bytes > (size_t)smem_optin) warp_tb = false;
+    const size_t tb_smem = (size_t)tb_wpb * warp_bytes;
+    const void *tb_fn = wide_nodes ? (nw == 1 ? (const void *)traceback_warp_kernel<1, 2>
+                                              : (const void *)traceback_warp_kernel<2, 2>)
+                                   : (nw == 1 ? (const void *)traceback_warp_kernel<1, 1>
+                                              : (const void *)traceback_warp_kernel<2, 1>);
+    void (*tb_launch)(const TbLaunch &) =
+        wide_nodes ? (nw == 1 ? launch_tb<1, 2> : launch_tb<2, 2>)
+                   : (nw == 1 ? launch_tb<1, 1> : launch_tb<2, 1>);
     int tb_blocks_per_sm = 1;
     if (warp_tb) {
         CU(cudaFuncSetAttribute(tb_fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tb_smem));
-        CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&tb_blocks_per_sm, tb_fn, kTbWarps * 32,
+        CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&tb_blocks_per_sm, tb_fn, tb_wpb * 32,
                                                          tb_smem));
         tb_blocks_per_sm = std::max(1, tb_blocks_per_sm);
     }
@@ -1393,7 +1532,8 @@ int Engine::run_bulge(const std::vector<Request> &reqs, std::vector<Result> &out
     if (warp_tb && n_cand) {
         const size_t bf_smem = (size_t)(wmax + 1) * nw * kBfThreads * 8;
         if (d.mcand2.ensure(n_cand, err)) return err.code;
-        auto kfn = nw == 1 ? budget_filter_kernel<1> : budget_filter_kernel<2>;
+        auto kfn = wmax > 48 ? (nw == 1 ? budget_filter_kernel<1, 5> : budget_filter_kernel<2, 5>)
+                             : (nw == 1 ? budget_filter_kernel<1, 3> : budget_filter_kernel<2, 3>);
         CU(cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bf_smem));
         int bf_per_sm = 1;
         CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bf_per_sm, kfn, kBfThreads, bf_smem));
@@ -1428,9 +1568,9 @@ int Engine::run_bulge(const std::vector<Request> &reqs, std::vector<Result> &out
             // iterations on one tree hands its remaining stack on, and the
             // next pass spreads those subtrees over all warps
             const unsigned grid = (unsigned)((uint64_t)d.n_sm * tb_blocks_per_sm);
-            TbItem *q[2] = {reinterpret_cast<TbItem *>(d.tb_items.p),
-                            reinterpret_cast<TbItem *>(d.tb_items.p) + kTbQueue};
-            const TbItem *in = nullptr;
+            char *tq = reinterpret_cast<char *>(d.tb_items.p);
+            char *q[2] = {tq, tq + kTbQueue * item_bytes};
+            const char *in = nullptr;
             uint32_t n_in = 0;
             for (int pass = 0;; ++pass) {
                 const bool last = pass >= kTbMaxPasses;
@@ -1438,12 +1578,13 @@ int Engine::run_bulge(const std::vector<Request> &reqs, std::vector<Result> &out
                 CU(cudaMemsetAsync(&d.ctr.p->hits, 0, sizeof(uint32_t), s));
                 const uint64_t work = in ? n_in : cn;
                 const unsigned tb = (unsigned)std::max<uint64_t>(
-                    1, std::min<uint64_t>((work + kTbWarps - 1) / kTbWarps, grid));
-                TbItem *out_q = q[pass & 1];
-                tb_fn<<<tb, kTbWarps * 32, tb_smem, s>>>(
-                    d.view(), dB, dP, dR, cands + c0, cn, in, n_in, last ? nullptr : out_q,
-                    kTbQueue, tb_budget, tbl_words, d.mrows.p, (uint32_t)row_cap, d.keys.p,
-                    d.vals.p, d.ctr.p, d.req_rows.p);
+                    1, std::min<uint64_t>((work + tb_wpb - 1) / tb_wpb, grid));
+                char *out_q = q[pass & 1];
+                TbLaunch a{tb, tb_wpb * 32, tb_smem, s, d.view(), dB, dP, dR, cands + c0, cn,
+                           in, n_in, last ? nullptr : out_q, kTbQueue, tb_budget, tbl_words,
+                           stk_cap, tb_mrg, d.mrows.p, (uint32_t)row_cap, d.keys.p, d.vals.p,
+                           d.ctr.p, d.req_rows.p};
+                tb_launch(a);
                 CU(cudaGetLastError());
                 ++times_.kernel_launches;
                 if (last) break;

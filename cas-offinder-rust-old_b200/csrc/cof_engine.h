@@ -21,11 +21,10 @@ namespace cof {
 constexpr uint32_t kChunkSize = 65536;           // chrom_chunk.rs:1
 constexpr uint32_t kChunkBytes = kChunkSize / 2;  // chrom_chunk.rs:2
 constexpr uint32_t kDefaultCps = 16384;          // search.rs:22 (GPU batch)
-constexpr uint32_t kMaxPatternLen = 64;          // popcount rows path
+constexpr uint32_t kMaxPatternLen = 64;          // every path (Myers: one u64, myers.rs:3)
 constexpr uint32_t kScanWindow = 32;             // cells a scan window holds (one
                                                  // 32-bit plane word); also the
                                                  // planes' leading padding
-constexpr uint32_t kMaxWindowPatternLen = 32;    // raw stream and bulge path
 
 // Status codes mirrored from include/cof.h.
 enum Status : int {

@@ -83,8 +83,16 @@ struct MyersRow {
     uint64_t ops[2];     // 2 bits per op, forward order: 0 M, 1 S, 2 DNA bulge, 3 RNA bulge
     uint32_t chunk, pattern;
     uint8_t n_ops, mm, db, rb;
-    uint32_t pad;
+    uint32_t ops_hi;     // ops 64..79 (patterns of 33..64 cells with DNA bulges)
 };
+
+// op k (forward order) of an alignment row
+__device__ __forceinline__ uint32_t mrow_op(const MyersRow &w, uint32_t k) {
+    const uint64_t x = k < 32 ? w.ops[0] >> (2 * k)
+                     : k < 64 ? w.ops[1] >> (2 * (k - 32))
+                              : (uint64_t)(w.ops_hi >> (2 * (k - 64)));
+    return (uint32_t)(x & 3);
+}
 
 __device__ __forceinline__ uint8_t nib(const uint8_t *__restrict__ g, uint64_t i) {
     uint8_t b = __ldg(g + (i >> 1));

@@ -35,7 +35,7 @@ struct RawSeg {
 };
 
 struct RawPattern {
-    uint32_t w[4];         // bit4 cells, 8 per word, zero past L
+    uint32_t w[8];         // bit4 cells, 8 per word, zero past L (L <= 64)
     uint32_t strand, pad[3];
 };
 
@@ -50,6 +50,8 @@ __device__ __forceinline__ uint32_t masked_word(const uint8_t *bit4, uint64_t j,
     return x & ~(t * 0xFu);
 }
 
+// NWD: pattern words compared (4: patterns of <= 32 cells, 8: <= 64)
+template <int NWD>
 __global__ void raw_scan_kernel(const uint8_t *__restrict__ bit4, const RawSeg *__restrict__ segs,
                                 uint32_t nseg, uint64_t n_blocks, const RawPattern *__restrict__ pats,
                                 uint32_t npat, uint32_t L, int max_mm, Hit *hits, uint32_t cap,
@@ -64,9 +66,9 @@ __global__ void raw_scan_kernel(const uint8_t *__restrict__ bit4, const RawSeg *
         while (si + 1 < nseg && blk >= segs[si + 1].blk_begin) ++si;
         const RawSeg S = segs[si];
         const uint64_t p0 = (S.lo & ~31ull) + 32 * (blk - S.blk_begin);  // 32-aligned
-        uint32_t W[9];
+        uint32_t W[NWD + 5];
 #pragma unroll
-        for (int k = 0; k < 9; ++k) W[k] = masked_word(bit4, p0 / 8 + k, S.clip);
+        for (int k = 0; k < NWD + 5; ++k) W[k] = masked_word(bit4, p0 / 8 + k, S.clip);
         const RawPattern P = pats[p];
 #pragma unroll
         for (int o = 0; o < 32; ++o) {
@@ -74,7 +76,7 @@ __global__ void raw_scan_kernel(const uint8_t *__restrict__ bit4, const RawSeg *
             const int sh = 4 * (o & 7);
             int matches = 0;
 #pragma unroll
-            for (int j = 0; j < 4; ++j) {
+            for (int j = 0; j < NWD; ++j) {
                 if (j < (int)nw) {
                     const uint32_t w = __funnelshift_r(W[(o >> 3) + j], W[(o >> 3) + j + 1], sh);
                     matches += __popc(w & P.w[j]);
@@ -226,10 +228,11 @@ int Engine::run_raw(const Request &r, Result &out, Error &err) {
         const uint64_t items = blocks * np;
         const unsigned gb = (unsigned)std::max<uint64_t>(
             1, std::min<uint64_t>((items + 255) / 256, (uint64_t)d.n_sm * 16));
-        raw_scan_kernel<<<gb, 256, 0, s>>>(d.bit4.p, (const RawSeg *)tab(o_s), (uint32_t)segs.size(),
-                                           blocks, (const RawPattern *)tab(o_p), (uint32_t)np, L,
-                                           (int)r.max_mm, d.hits.p,
-                                           (uint32_t)std::min<size_t>(d.hits.cap, 0xFFFFFFF0u), d.ctr.p);
+        auto scan_fn = L > 32 ? raw_scan_kernel<8> : raw_scan_kernel<4>;
+        scan_fn<<<gb, 256, 0, s>>>(d.bit4.p, (const RawSeg *)tab(o_s), (uint32_t)segs.size(), blocks,
+                                   (const RawPattern *)tab(o_p), (uint32_t)np, L, (int)r.max_mm,
+                                   d.hits.p, (uint32_t)std::min<size_t>(d.hits.cap, 0xFFFFFFF0u),
+                                   d.ctr.p);
         CU(cudaGetLastError());
         CU(cudaEventRecord(d.ev[2], s));
         ++times_.kernel_launches;

@@ -110,8 +110,9 @@ COF_API void cof_genome_free(cof_genome *g);
  * exactly as search.rs:1513 does.
  * chunks_per_search: 64 Knt chunks per search batch; 0 selects 16384, the
  * batch search() uses with a GPU device (search.rs:22, :44-50).
- * pattern_len: at most 64, and at most 32 with bulges or COF_F_RAW_MATCHES;
- * longer requests fail with COF_E_UNSUPPORTED. */
+ * pattern_len: at most 64 on every path (the bulge path's Myers filter is
+ * one u64 word in the reference, myers.rs:3), and pattern_len +
+ * max_dna_bulges at most 72; longer requests fail with COF_E_UNSUPPORTED. */
 typedef struct {
     const char *search_filter;
     size_t pattern_len;

@@ -102,10 +102,13 @@ def test_bad_requests_rejected(cof_mod, golden):
         g.search("N" * 65, ["A" * 65], 3)  # above 64 cells
     assert e.value.code == cof_mod.COF_E_UNSUPPORTED
     with pytest.raises(cof_mod.CofError) as e:
-        g.search("N" * 40, ["A" * 40], 3, 1, 1)  # bulges: at most 32 cells
+        g.search("N" * 65, ["A" * 65], 3, 1, 1)  # bulges: at most 64 cells
     assert e.value.code == cof_mod.COF_E_UNSUPPORTED
     with pytest.raises(cof_mod.CofError) as e:
-        g.search("N" * 40, ["A" * 40], 3, raw=True)  # raw matches: at most 32 cells
+        g.search("N" * 65, ["A" * 65], 3, raw=True)  # raw matches: at most 64 cells
+    assert e.value.code == cof_mod.COF_E_UNSUPPORTED
+    with pytest.raises(cof_mod.CofError) as e:
+        g.search("N" * 40, ["A" * 40], 3, 9, 1)  # more than 8 DNA bulges
     assert e.value.code == cof_mod.COF_E_UNSUPPORTED
 
 

@@ -184,3 +184,98 @@ def test_row_buffer_overflow_halves_chunks(cof_mod, oracle_mod, monkeypatch):
         o.add_chunk(name, data, s, e)
     ref, nref = o.search(*args)
     assert n == n1 == nref > 0 and sorted(ref.splitlines()) == sorted(text.splitlines())
+
+
+def _plant_bulged(rng, records, pattern, filt, count, subs):
+    """Near-copies of pattern with subs substitutions and one inserted or
+    deleted cell outside the PAM, on either strand."""
+    comp = {"A": "T", "C": "G", "G": "C", "T": "A"}
+    free = [i for i, c in enumerate(pattern) if c in "ACGT" and filt[i] == "N"]
+    for _ in range(count):
+        r = rng.randrange(len(records))
+        seq = records[r]
+        site = []
+        for i, c in enumerate(pattern):
+            f = filt[i]
+            if c not in "ACGT":
+                site.append(rng.choice([b for b in "ACGT" if randgen.B4[b] & randgen.B4[f]]))
+            else:
+                site.append(c)
+        for i in rng.sample(free, subs):
+            site[i] = rng.choice([b for b in "ACGT" if b != site[i]])
+        k = rng.choice(free[2:-2])
+        if rng.random() < 0.5:
+            site.insert(k, rng.choice("ACGT"))  # a DNA bulge
+        else:
+            del site[k]  # an RNA bulge
+        s = "".join(site)
+        if rng.random() < 0.5:
+            s = "".join(comp[c] for c in reversed(s))
+        p = rng.randrange(0, len(seq) - len(s))
+        records[r] = seq[:p] + s + seq[p + len(s):]
+
+
+# (L, PAM side, mm, db, rb): 64-bit Myers words for every L > 32; windows
+# W = L + db of <= 48 cells (one op word per traceback node) and above
+# (two, with ops past 64 in the row's third word); (db + 1)(rb + 1)(mm + 1)
+# budget bits of one word and of two
+LONG_BULGE_CASES = [
+    (33, "3", 3, 1, 1),
+    (40, "5", 3, 2, 1),
+    (48, "3", 2, 1, 2),
+    (57, "5", 8, 1, 3),
+    (64, "3", 3, 8, 0),
+    (64, "-", 2, 2, 2),
+]
+
+
+@pytest.mark.parametrize("L,pam,mm,db,rb", LONG_BULGE_CASES)
+def test_bulge_patterns_longer_than_32_cells(cof_mod, oracle_mod, monkeypatch, L, pam, mm, db,
+                                             rb):
+    rng = random.Random(900 + L + db)
+    _, records = randgen.random_genome(rng, 3, 20000, 30000)
+    guide = lambda n: "".join(rng.choice("ACGT") for _ in range(n))
+    if pam == "3":
+        filt, pats = "N" * (L - 2) + "RG", [guide(L - 3) + "NNN" for _ in range(2)]
+    elif pam == "5":
+        filt, pats = "TTTN" + "N" * (L - 4), ["NNNN" + guide(L - 4) for _ in range(2)]
+    else:
+        filt, pats = "N" * L, [guide(L) for _ in range(2)]
+    for p in pats:
+        _plant_bulged(rng, records, p, filt, 4, min(mm, 2))
+        randgen.plant_sites(rng, records, p, filt, 2, mm)
+    g, o = _both(cof_mod, oracle_mod, randgen.chunk_records(rng, records, 5000))
+    args = (filt, pats, mm, db, rb)
+    monkeypatch.delenv("COF_BULGE_WARP", raising=False)
+    text, n = g.search(*args)
+    ref, nref = o.search(*args)
+    assert n == nref > 0
+    assert _rows(text) == _rows(ref)
+    assert any(r.split("\t")[0] in ("DNA", "RNA") for r in ref.splitlines())
+    if L + db > 64 and db > 0:  # alignments of more than 64 ops
+        assert any(len(r.split("\t")[1]) > 64 for r in ref.splitlines())
+    raw, nraw = g.search(*args, raw=True)
+    rref, nrref = o.search(*args, raw=True)
+    assert nraw == nrref and sorted(raw.split("\n")[:-1]) == sorted(rref.split("\n")[:-1])
+    monkeypatch.setenv("COF_BULGE_WARP", "0")  # the thread-per-candidate traceback
+    text0, n0 = g.search(*args)
+    assert n0 == n and _rows(text0) == _rows(text)
+
+
+def test_long_and_short_bulge_requests_in_one_batch(cof_mod, oracle_mod):
+    # a 23-cell and a 60-cell request share one launch: 64-bit Myers words,
+    # two-word nodes and the five-word budget filter serve both
+    rng = random.Random(31)
+    _, records = randgen.random_genome(rng, 3, 15000, 25000)
+    guide = lambda n: "".join(rng.choice("ACGT") for _ in range(n))
+    short = ("N" * 21 + "RG", [guide(20) + "NNN" for _ in range(2)], 3, 1, 1)
+    long_ = ("N" * 58 + "RG", [guide(57) + "NNN" for _ in range(2)], 3, 2, 1)
+    for filt, pats, mm, _db, _rb in (short, long_):
+        for p in pats:
+            _plant_bulged(rng, records, p, filt, 4, 2)
+    g, o = _both(cof_mod, oracle_mod, randgen.chunk_records(rng, records, 4000))
+    reqs = [dict(search_filter=f, patterns=p, max_mismatches=m, max_dna_bulges=d,
+                 max_rna_bulges=r) for f, p, m, d, r in (short, long_)]
+    for (f, p, m, d, r), (text, n) in zip((short, long_), g.search_batch(reqs)):
+        ref, nref = o.search(f, p, m, d, r)
+        assert n == nref > 0 and _rows(text) == _rows(ref)

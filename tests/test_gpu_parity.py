@@ -233,10 +233,10 @@ def test_patterns_longer_than_the_scan_window(cof_mod, oracle_mod, L):
     for r, (text, n) in zip(reqs, g.search_batch(reqs)):
         ref, nref = o.search(r["search_filter"], r["patterns"], r["max_mismatches"])
         assert n == nref and _rows(text) == _rows(ref)
-    with pytest.raises(cof_mod.CofError):  # bulges and raw matches stay at 32 cells
-        g.search(shapes[0][0], shapes[0][1], 3, 1, 1)
-    with pytest.raises(cof_mod.CofError):
-        g.search(shapes[0][0], shapes[0][1], 3, raw=True)
+    for filt, pats, mm in shapes:  # the raw Match stream compares all L cells
+        raw, nraw = g.search(filt, pats, mm, raw=True)
+        rref, nrref = o.search(filt, pats, mm, raw=True)
+        assert nraw == nrref and sorted(raw.split("\n")[:-1]) == sorted(rref.split("\n")[:-1])
 
 
 def test_autotuner_records_choice(cof_mod, golden, monkeypatch):
