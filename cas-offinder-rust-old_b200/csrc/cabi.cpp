@@ -222,14 +222,15 @@ COF_API int cof_genome_last_stats(const cof_genome *g, double *ms5, uint64_t *co
 }
 
 // Autotuner state of a genome: JSON {"last": tile shape of the last scan,
-// "variant": its index, "cache": {shape key: variant index}}.  No reference
-// counterpart.
+// "variant": its index, "slices": slices the last scan ran in (0: one pass),
+// "cache": {shape key: variant index}}.  No reference counterpart.
 COF_API int cof_genome_tuning(cof_genome *g, char *buf, size_t len) {
     if (!g || !buf || !len) return fail(COF_E_BADINPUT, "null argument");
     std::lock_guard<std::mutex> lk(g->mu);
     const cof::StageTimes &t = g->engine.last_times();
     std::string js = "{\"last\": \"" + t.scan_shape + "\", \"variant\": " +
-                     std::to_string(t.scan_variant) + ", \"cache\": " +
+                     std::to_string(t.scan_variant) + ", \"slices\": " +
+                     std::to_string(t.slices) + ", \"cache\": " +
                      g->engine.tuner().report() + "}";
     std::snprintf(buf, len, "%s", js.c_str());
     return js.size() < len ? COF_OK : fail(COF_E_BADINPUT, "buffer too small");

@@ -207,6 +207,7 @@ struct StageTimes {
     double scan_ms = 0, verify_ms = 0, format_ms = 0, d2h_ms = 0, total_ms = 0;
     uint64_t candidates = 0, pairs = 0, raw_hits = 0, rows = 0, kernel_launches = 0;
     int scan_variant = -1;        // tile shape the scan ran with
+    int slices = 0;               // slices of a sliced scan (0: one pass)
     std::string scan_shape;
 };
 
@@ -253,6 +254,8 @@ class Engine {
     int run_bulge(const std::vector<Request> &reqs, std::vector<Result> &out, Error &err);
     int run_raw(const Request &req, Result &out, Error &err);
     int device_;
+    uint64_t slice_text_hint_ = 0;  // bytes of the last sliced result (+2 %)
+    int scan_occ_[16] = {};          // resident CTAs per SM of each scan shape (0: not set up)
     // creates the device's CUDA context while the caller reads the genome
     // file; joined before the first device call, and only by the process
     // that started it (a forked child holds a copy of this object but not

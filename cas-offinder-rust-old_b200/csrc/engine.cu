@@ -640,6 +640,7 @@ const ScanVariant kScanVariants[] = {
     warp_variant<8, 8, 4, 4, 1024>(8),
 };
 constexpr int kNumScanVariants = sizeof(kScanVariants) / sizeof(kScanVariants[0]);
+static_assert(kNumScanVariants <= 16, "Engine::scan_occ_ holds 16 shapes");
 
 // ---------------------------------------------------------------------------
 // verify: the reference's exact decision per candidate hit
@@ -649,13 +650,21 @@ __global__ void verify_kernel(GenomeDev G, const BatchDev *__restrict__ batches,
                               const ExactPattern *__restrict__ pats,
                               const uint32_t *__restrict__ fast2exact,
                               const RequestDev *__restrict__ reqs, const Hit *__restrict__ hits,
-                              uint32_t n_hits, Row *__restrict__ rows, uint64_t *__restrict__ keys,
+                              const Counters *__restrict__ scan_ctr, uint32_t hit_cap,
+                              uint32_t sg_bits, uint32_t e_bits,
+                              Row *__restrict__ rows, uint64_t *__restrict__ keys,
                               uint32_t *__restrict__ vals, Counters *ctr,
                               uint32_t *__restrict__ req_rows) {
+    // row sort key: request, then genome position, then the pattern's index
+    // within its request (sg < 2^sg_bits, index < 2^e_bits)
     // the block steps through the hits together, so every lane of a warp
     // reaches the row emission below; rows get their slots and requests
     // their counts with one atomic per warp (per request), not per row
     const uint32_t lane = threadIdx.x & 31, lt_mask = (1u << lane) - 1u;
+    // the scan's hit count (read on the device: no host round trip between
+    // the two kernels); an overflowed list is verified up to its capacity
+    // and the whole pass is rerun
+    const uint32_t n_hits = min(*(volatile const uint32_t *)&scan_ctr->hits, hit_cap);
     for (uint32_t base = blockIdx.x * blockDim.x; base < n_hits; base += gridDim.x * blockDim.x) {
         const uint32_t i = base + threadIdx.x;
         bool emit = false;
@@ -711,7 +720,8 @@ __global__ void verify_kernel(GenomeDev G, const BatchDev *__restrict__ batches,
             if (!pam_ok || actual > R.max_mm) break;
             emit = true;
             row = Row{sg, B.base + B.valid, pos, k, pe, actual, 0};
-            key = ((uint64_t)pe << 34) | sg;
+            key = ((uint64_t)P.request << (sg_bits + e_bits)) | (sg << e_bits) |
+                  (pe - R.first_pattern);
             req = P.request;
         } while (false);
         const uint32_t em = __ballot_sync(0xFFFFFFFFu, emit);
@@ -852,7 +862,10 @@ int Engine::upload(Error &err) {
     std::unique_ptr<DeviceGenome> d(new DeviceGenome());
     d->device = device_;
     CU(cudaStreamCreateWithFlags(&d->stream, cudaStreamNonBlocking));
+    CU(cudaStreamCreateWithFlags(&d->copy_stream, cudaStreamNonBlocking));
     for (auto &e : d->ev) CU(cudaEventCreate(&e));
+    CU(cudaEventCreate(&d->fmt_done));
+    CU(cudaEventCreate(&d->copy_done));
     CU(cudaDeviceGetAttribute(&d->n_sm, cudaDevAttrMultiProcessorCount, device_));
     const HostGenome &h = host_;
     const uint64_t n_bytes = h.n_bytes();
@@ -1013,6 +1026,9 @@ int Engine::run_popcount(const std::vector<Request> &reqs, std::vector<Result> &
     // window start -- so that one PAM sweep serves requests of different
     // guide lengths and mismatch limits.
     std::vector<uint32_t> fast2exact;
+    // per scan group: shifted window start - pattern start, when all of its
+    // patterns have one length (always so within one request); else ~0u
+    std::vector<uint32_t> group_shift;
     std::map<std::string, std::vector<uint32_t>> by_key;
     std::vector<std::string> key_order;
     std::vector<uint32_t> ep_off;  // window offset of each exact pattern's first cell
@@ -1070,6 +1086,21 @@ int Engine::run_popcount(const std::vector<Request> &reqs, std::vector<Result> &
             ep_off.push_back(off[strand]);
         }
     }
+    // row sort key (verify_kernel): request | genome position | pattern
+    // index within the request, each field as wide as this pass needs
+    auto width = [](uint64_t v) {  // bits of v's binary form
+        uint32_t b = 0;
+        while (b < 64 && (v >> b) != 0) ++b;
+        return b;
+    };
+    size_t max_np = 1;
+    for (const Request &r : reqs) max_np = std::max(max_np, r.patterns.size());
+    const uint32_t sg_bits = width(2 * h.boff.back()), e_bits = width(max_np - 1),
+                   key_bits = width(reqs.size() - 1) + sg_bits + e_bits;
+    if (key_bits > 64) {
+        err = {kUnsupported, "too many requests x patterns in one pass for the row sort key"};
+        return err.code;
+    }
     for (const auto &key : key_order) {
         const std::vector<uint32_t> &members = by_key[key];
         const ExactPattern &e0 = epats[members[0]];
@@ -1092,6 +1123,7 @@ int Engine::run_popcount(const std::vector<Request> &reqs, std::vector<Result> &
         for (uint32_t e : members) lens.push_back({epats[e].L, ep_off[e]});
         std::sort(lens.begin(), lens.end());
         lens.erase(std::unique(lens.begin(), lens.end()), lens.end());
+        const uint32_t key_shift = lens.size() == 1 ? kScanWindow - lens[0].second : ~0u;
         // scan segments: one per batch, the union of the members' window
         // ranges; verify re-applies each length's own head-overlap threshold
         std::vector<ScanSeg> kseg;
@@ -1174,6 +1206,7 @@ int Engine::run_popcount(const std::vector<Request> &reqs, std::vector<Result> &
                 if (new_class && g.n_class == (uint32_t)kMaxCareClasses) {
                     g.pat_end = (uint32_t)fpats.size();
                     groups.push_back(g);
+                    group_shift.push_back(key_shift);
                     g = proto;
                     g.pat_begin = (uint32_t)fpats.size();
                     g.n_class = 0;
@@ -1187,6 +1220,7 @@ int Engine::run_popcount(const std::vector<Request> &reqs, std::vector<Result> &
             }
             g.pat_end = (uint32_t)fpats.size();
             groups.push_back(g);
+            group_shift.push_back(key_shift);
         }
     }
 
@@ -1227,6 +1261,76 @@ int Engine::run_popcount(const std::vector<Request> &reqs, std::vector<Result> &
         o_items[v.span_tiles] = tp.add(full);
         o_sample[v.span_tiles] = tp.add(samp);
     }
+
+    // Slices: one request on a large genome is scanned in slices of pattern
+    // start positions, [cut_j, cut_j+1) of the global start coordinate.  A
+    // slice's rows are verified, sorted and written while the previous
+    // slice's text is still crossing to the host, so the copy runs beside
+    // the scan.  Rows sort by position first, so the slices' texts follow
+    // each other in the order of one unsliced pass.  A scan group's segment
+    // holds shifted window starts (start + the group's shift), clipped here
+    // to the slice.
+    struct SliceTab {
+        size_t o_grp = 0, o_seg = 0;
+        uint32_t n_groups = 0;
+        std::map<uint32_t, size_t> o_items;
+        std::map<uint32_t, uint64_t> n_items;
+    };
+    std::vector<SliceTab> slices;
+    {
+        // 768 Mnt: 4 slices of a 3.1 Gbp genome (3, 4 and 6 slices measured
+        // 18.99, 18.83 and 19.40 ms per 100-guide search; one pass 20.02)
+        uint64_t slice_nt = uint64_t(768) << 20;  // COF_SLICE_NT: tests of many slices
+        if (const char *e = std::getenv("COF_SLICE_NT"))
+            slice_nt = std::max<uint64_t>(1024, std::strtoull(e, nullptr, 10));
+        const uint64_t total_nt = 2 * h.boff.back();
+        bool ok = reqs.size() == 1 && !groups.empty() && total_nt >= 2 * slice_nt;
+        for (uint32_t sh : group_shift) ok = ok && sh != ~0u;
+        const uint64_t n_slices = ok ? (total_nt + slice_nt - 1) / slice_nt : 0;
+        for (uint64_t j = 0; j < n_slices; ++j) {
+            const uint64_t c0 = total_nt * j / n_slices;
+            const uint64_t c1 = j + 1 == n_slices ? ~0ull : total_nt * (j + 1) / n_slices;
+            std::vector<ScanGroup> gj;
+            std::vector<ScanSeg> sj;
+            for (size_t gi = 0; gi < groups.size(); ++gi) {
+                ScanGroup ng = groups[gi];
+                const uint64_t sh = group_shift[gi];
+                const uint64_t lo_cut = c0 + sh, hi_cut = c1 == ~0ull ? ~0ull : c1 + sh;
+                ng.seg_begin = (uint32_t)sj.size();
+                uint64_t tiles = 0;
+                for (uint32_t k = groups[gi].seg_begin; k < groups[gi].seg_end; ++k) {
+                    ScanSeg x = segs[k];
+                    const uint64_t lo = std::max(x.lo, lo_cut), hi = std::min(x.hi, hi_cut);
+                    if (hi <= lo) continue;
+                    x.lo = lo;
+                    x.hi = hi;
+                    x.w0 = lo / 32;
+                    x.tile_begin = tiles;
+                    tiles += (hi - x.w0 * 32 + 1023) / 1024;
+                    sj.push_back(x);
+                }
+                ng.seg_end = (uint32_t)sj.size();
+                if (ng.seg_end > ng.seg_begin) gj.push_back(ng);
+            }
+            if (gj.empty()) continue;
+            SliceTab st;
+            st.n_groups = (uint32_t)gj.size();
+            st.o_grp = tp.add(gj);
+            st.o_seg = tp.add(sj);
+            for (const ScanVariant &v : kScanVariants) {
+                if (st.o_items.count(v.span_tiles)) continue;
+                std::vector<uint64_t> ib{0};
+                for (const ScanGroup &g : gj) {
+                    const ScanSeg &last = sj[g.seg_end - 1];
+                    const uint64_t t = last.tile_begin + (last.hi - last.w0 * 32 + 1023) / 1024;
+                    ib.push_back(ib.back() + (t + v.span_tiles - 1) / v.span_tiles);
+                }
+                st.n_items[v.span_tiles] = ib.back();
+                st.o_items[v.span_tiles] = tp.add(ib);
+            }
+            slices.push_back(std::move(st));
+        }
+    }
     if (d.tables.ensure(tp.buf.size(), err)) return err.code;
     cudaStream_t s = d.stream;
     CU(cudaEventRecord(d.ev[0], s));
@@ -1246,18 +1350,29 @@ int Engine::run_popcount(const std::vector<Request> &reqs, std::vector<Result> &
     sp.n_pats = (uint32_t)fpats.size();
     sp.hits = d.hits.p;
     sp.ctr = d.ctr.p;
-    // launches variant v over the full work list or over the tuning sample
-    auto launch = [&](const ScanVariant &v, bool sample) -> int {
+    // launches variant v over the full work list, over the tuning sample or
+    // over one slice's work list
+    auto launch = [&](const ScanVariant &v, bool sample, const SliceTab *sl = nullptr) -> int {
         const size_t smem = v.smem();
-        CU(cudaFuncSetAttribute(v.kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        int occ = 0;
-        CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, v.kernel, v.warps * 32, smem));
-        occ = std::max(occ, 1);
+        // the shape's shared-memory opt-in and occupancy, once per engine
+        int &occ = scan_occ_[&v - kScanVariants];
+        if (occ == 0) {
+            CU(cudaFuncSetAttribute(v.kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+            CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, v.kernel, v.warps * 32, smem));
+            occ = std::max(occ, 1);
+        }
         sp.span_tiles = v.span_tiles;
-        sp.item_begin = (const uint64_t *)tab(sample ? o_sample[v.span_tiles] : o_items[v.span_tiles]);
+        sp.groups = (const ScanGroup *)tab(sl ? sl->o_grp : o_grp);
+        sp.segs = (const ScanSeg *)tab(sl ? sl->o_seg : o_seg);
+        sp.n_groups = sl ? sl->n_groups : (uint32_t)groups.size();
+        sp.item_begin = (const uint64_t *)tab(sl ? sl->o_items.at(v.span_tiles)
+                                              : sample ? o_sample[v.span_tiles]
+                                                       : o_items[v.span_tiles]);
         sp.hits = d.hits.p;  // the list may have grown (and moved) since the last launch
         sp.hit_cap = (uint32_t)std::min<size_t>(d.hits.cap, 0xFFFFFFF0u);
-        const uint64_t items = sample ? n_sample[v.span_tiles] : n_items[v.span_tiles];
+        const uint64_t items = sl       ? sl->n_items.at(v.span_tiles)
+                               : sample ? n_sample[v.span_tiles]
+                                        : n_items[v.span_tiles];
         const unsigned gx = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>(items, (uint64_t)d.n_sm * occ));
         CU(cudaMemsetAsync(d.ctr.p, 0, sizeof(Counters), s));
         v.kernel<<<gx, v.warps * 32, smem, s>>>(sp);
@@ -1266,7 +1381,102 @@ int Engine::run_popcount(const std::vector<Request> &reqs, std::vector<Result> &
         return kOk;
     };
 
+    // the scan over one work list (the full one, or a slice's) and the
+    // verify of its hits, with one host wait; rerun once with a larger
+    // candidate list if the scan overflowed.  n_rows and the rows per
+    // request come back.
     Counters hc{};
+    auto scan_verify = [&](const ScanVariant *v, const SliceTab *sl, uint32_t &n_rows,
+                           std::vector<uint32_t> &req_rows) -> int {
+        for (int attempt = 0; attempt < 2; ++attempt) {
+            CU(cudaEventRecord(d.ev[1], s));
+            if (v) {
+                if (launch(*v, false, sl)) return err.code;
+            } else {
+                CU(cudaMemsetAsync(d.ctr.p, 0, sizeof(Counters), s));
+            }
+            CU(cudaEventRecord(d.ev[2], s));
+            const size_t cap = std::max<size_t>(d.hits.cap, 1);
+            if (d.rows.ensure(cap + 1, err) || d.keys.ensure(cap + 1, err) ||
+                d.keys2.ensure(cap + 1, err) || d.vals.ensure(cap + 1, err) ||
+                d.vals2.ensure(cap + 1, err))
+                return err.code;
+            CU(cudaMemsetAsync(d.req_rows.p, 0, reqs.size() * 4, s));
+            if (v) {
+                verify_kernel<<<d.n_sm * 8, 256, 0, s>>>(
+                    d.view(), (const BatchDev *)tab(o_batch), (const ExactPattern *)tab(o_ep),
+                    (const uint32_t *)tab(o_f2e), (const RequestDev *)tab(o_rdev), d.hits.p, d.ctr.p,
+                    (uint32_t)std::min<size_t>(d.hits.cap, 0xFFFFFFF0u), sg_bits, e_bits, d.rows.p,
+                    d.keys.p, d.vals.p, d.ctr.p, d.req_rows.p);
+                CU(cudaGetLastError());
+                ++times_.kernel_launches;
+            }
+            CU(cudaEventRecord(d.ev[3], s));
+            CU(cudaMemcpyAsync(&hc, d.ctr.p, sizeof(Counters), cudaMemcpyDeviceToHost, s));
+            req_rows.assign(reqs.size(), 0);
+            CU(cudaMemcpyAsync(req_rows.data(), d.req_rows.p, reqs.size() * 4,
+                               cudaMemcpyDeviceToHost, s));
+            CU(cudaStreamSynchronize(s));
+            if (!hc.overflow && hc.hits <= d.hits.cap) break;
+            if (attempt == 1) {
+                err = {kOom, "candidate buffer overflow after resize"};
+                return err.code;
+            }
+            if (d.hits.ensure((size_t)hc.hits + hc.hits / 4 + 1024, err)) return err.code;
+        }
+        float ms = 0;
+        cudaEventElapsedTime(&ms, d.ev[1], d.ev[2]);
+        times_.scan_ms += ms;
+        cudaEventElapsedTime(&ms, d.ev[2], d.ev[3]);
+        times_.verify_ms += ms;
+        times_.raw_hits += hc.hits;
+        times_.candidates += hc.candidates;
+        times_.pairs += hc.pairs;
+        n_rows = hc.rows;
+        times_.rows += n_rows;
+        return kOk;
+    };
+    // sort the verified rows by (request, position, pattern) and write their
+    // text into d.text; the text bytes come back.  before_write runs just
+    // before the text is written (the sliced path waits there for the
+    // previous copy).
+    auto format_rows = [&](uint32_t n_rows, uint64_t &text_bytes, auto &&before_write) -> int {
+        CU(cudaEventRecord(d.ev[6], s));  // format interval: ev[6] -> ev[4]
+        text_bytes = 0;
+        if (!n_rows) return kOk;
+        size_t tmp = 0;
+        CU(cub::DeviceRadixSort::SortPairs(nullptr, tmp, d.keys.p, d.keys2.p, d.vals.p, d.vals2.p,
+                                           (int)n_rows, 0, (int)key_bits, s));
+        size_t tmp2 = 0;
+        CU(cub::DeviceScan::ExclusiveSum(nullptr, tmp2, d.lens.p, d.offs.p, (int)n_rows + 1, s));
+        if (d.cub_tmp.ensure(std::max(tmp, tmp2), err)) return err.code;
+        tmp = d.cub_tmp.cap;
+        CU(cub::DeviceRadixSort::SortPairs(d.cub_tmp.p, tmp, d.keys.p, d.keys2.p, d.vals.p,
+                                           d.vals2.p, (int)n_rows, 0, (int)key_bits, s));
+        const uint32_t *order = d.vals2.p;
+        if (d.lens.ensure(n_rows + 1, err) || d.offs.ensure(n_rows + 1, err)) return err.code;
+        unsigned fb = (unsigned)std::min<uint64_t>((n_rows + 255) / 256, (uint64_t)d.n_sm * 8);
+        row_len_kernel<<<fb, 256, 0, s>>>(d.view(), d.rows.p, order, n_rows,
+                                          (const ExactPattern *)tab(o_ep),
+                                          (const RequestDev *)tab(o_rdev), d.lens.p);
+        CU(cudaGetLastError());
+        CU(cudaMemsetAsync(d.lens.p + n_rows, 0, 4, s));
+        // widen lengths to 64-bit offsets
+        tmp2 = d.cub_tmp.cap;
+        CU(cub::DeviceScan::ExclusiveSum(d.cub_tmp.p, tmp2, d.lens.p, d.offs.p, (int)n_rows + 1, s));
+        CU(cudaMemcpyAsync(&text_bytes, d.offs.p + n_rows, 8, cudaMemcpyDeviceToHost, s));
+        CU(cudaStreamSynchronize(s));
+        if (before_write(text_bytes)) return err.code;
+        if (d.text.ensure(text_bytes + 1, err)) return err.code;
+        row_write_kernel<<<fb, 256, 0, s>>>(d.view(), d.rows.p, order, n_rows,
+                                            (const ExactPattern *)tab(o_ep),
+                                            (const RequestDev *)tab(o_rdev), d.offs.p, d.text.p);
+        CU(cudaGetLastError());
+        times_.kernel_launches += 4;
+        return kOk;
+    };
+
+    const ScanVariant *vsel = nullptr;
     if (!groups.empty()) {
         // autotuner: the fastest tile shape for this request shape, timed on
         // the first kTuneTiles tiles of every group; cached per shape
@@ -1322,85 +1532,95 @@ int Engine::run_popcount(const std::vector<Request> &reqs, std::vector<Result> &
                             kMinName[v.pair] + "cpt" + std::to_string(v.cpt) + "-warps" + std::to_string(v.warps) +
                             "-minb" + std::to_string(v.min_blocks) + "-span" +
                             std::to_string(v.span_tiles);
-        for (int attempt = 0; attempt < 2; ++attempt) {
-            CU(cudaEventRecord(d.ev[1], s));
-            if (launch(v, false)) return err.code;
-            CU(cudaEventRecord(d.ev[2], s));
-            CU(cudaMemcpyAsync(&hc, d.ctr.p, sizeof(Counters), cudaMemcpyDeviceToHost, s));
-            CU(cudaStreamSynchronize(s));
-            if (!hc.overflow && hc.hits <= d.hits.cap) break;
-            if (attempt == 1) {
-                err = {kOom, "candidate buffer overflow after resize"};
+        vsel = &v;
+    }
+    if (!slices.empty()) {
+        // one request, scanned slice by slice (slices need scan groups, so a
+        // tile shape was chosen above); each slice's text is copied into the
+        // page-locked result on the copy stream while the next slice scans
+        PooledText hbuf;  // the result text, released on every early return
+        // destroyed before hbuf: no copy may still write into it then
+        struct CopyDrain {
+            cudaStream_t cs;
+            ~CopyDrain() { cudaStreamSynchronize(cs); }
+        } drain{d.copy_stream};
+        size_t hcap = 0;
+        uint64_t host_off = 0, rows_total = 0;
+        bool copy_pending = false;
+        float ms = 0;
+        // grows the result buffer to `need` bytes, keeping the text copied so far
+        auto reserve = [&](size_t need) -> int {
+            if (need <= hcap) return kOk;
+            CU(cudaStreamSynchronize(d.copy_stream));
+            PooledText nb;
+            nb.p = PinnedPool::get().acquire(need);
+            if (!nb.p) {
+                err = {kOom, "out of page-locked host memory for result text"};
                 return err.code;
             }
-            if (d.hits.ensure((size_t)hc.hits + hc.hits / 4 + 1024, err)) return err.code;
+            if (hbuf.p) std::memcpy(nb.p, hbuf.p, host_off);
+            hbuf = std::move(nb);
+            hcap = need;
+            return kOk;
+        };
+        times_.slices = (int)slices.size();
+        for (size_t j = 0; j < slices.size(); ++j) {
+            uint32_t nr = 0;
+            std::vector<uint32_t> rq;
+            if (scan_verify(vsel, &slices[j], nr, rq)) return err.code;  // ends with a stream sync
+            if (j > 0) {  // the previous slice's text write has finished
+                cudaEventElapsedTime(&ms, d.ev[6], d.ev[4]);
+                times_.format_ms += ms;
+            }
+            auto before_write = [&](uint64_t bytes) -> int {
+                // d.text still feeds the previous slice's copy
+                if (copy_pending) CU(cudaEventSynchronize(d.copy_done));
+                size_t need = host_off + bytes + 1;
+                if (need > hcap)  // room for the rest at this slice's rate (+20 %)
+                    need = std::max<size_t>({need, (size_t)slice_text_hint_,
+                                             (size_t)((double)(host_off + bytes) * slices.size() /
+                                                      (double)(j + 1) * 1.2) + (1u << 20)});
+                return reserve(need);
+            };
+            uint64_t tb = 0;
+            if (format_rows(nr, tb, before_write)) return err.code;
+            CU(cudaEventRecord(d.ev[4], s));
+            rows_total += nr;
+            if (tb) {
+                CU(cudaEventRecord(d.fmt_done, s));
+                CU(cudaStreamWaitEvent(d.copy_stream, d.fmt_done, 0));
+                CU(cudaMemcpyAsync(hbuf.p + host_off, d.text.p, tb, cudaMemcpyDeviceToHost,
+                                   d.copy_stream));
+                CU(cudaEventRecord(d.copy_done, d.copy_stream));
+                copy_pending = true;
+                host_off += tb;
+            }
         }
-    } else {
-        CU(cudaEventRecord(d.ev[1], s));
-        CU(cudaEventRecord(d.ev[2], s));
-    }
-    times_.raw_hits = hc.hits;
-    times_.candidates = hc.candidates;
-    times_.pairs = hc.pairs;
-
-    // verify
-    const uint32_t n_hits = hc.hits;
-    if (d.rows.ensure(n_hits + 1, err) || d.keys.ensure(n_hits + 1, err) ||
-        d.keys2.ensure(n_hits + 1, err) || d.vals.ensure(n_hits + 1, err) ||
-        d.vals2.ensure(n_hits + 1, err))
-        return err.code;
-    CU(cudaMemsetAsync(d.req_rows.p, 0, reqs.size() * 4, s));
-    if (n_hits) {
-        unsigned vb = (unsigned)std::min<uint64_t>((n_hits + 255) / 256, (uint64_t)d.n_sm * 8);
-        verify_kernel<<<vb, 256, 0, s>>>(d.view(), (const BatchDev *)tab(o_batch),
-                                         (const ExactPattern *)tab(o_ep),
-                                         (const uint32_t *)tab(o_f2e),
-                                         (const RequestDev *)tab(o_rdev), d.hits.p, n_hits,
-                                         d.rows.p, d.keys.p, d.vals.p, d.ctr.p, d.req_rows.p);
-        CU(cudaGetLastError());
-        ++times_.kernel_launches;
-    }
-    CU(cudaEventRecord(d.ev[3], s));
-    CU(cudaMemcpyAsync(&hc, d.ctr.p, sizeof(Counters), cudaMemcpyDeviceToHost, s));
-    std::vector<uint32_t> req_rows(reqs.size());
-    CU(cudaMemcpyAsync(req_rows.data(), d.req_rows.p, reqs.size() * 4, cudaMemcpyDeviceToHost, s));
-    CU(cudaStreamSynchronize(s));
-    const uint32_t n_rows = hc.rows;
-    times_.rows = n_rows;
-
-    // sort rows by (pattern, position), then lay out the text
-    const uint32_t *order = d.vals.p;
-    uint64_t text_bytes = 0;
-    if (n_rows) {
-        size_t tmp = 0;
-        CU(cub::DeviceRadixSort::SortPairs(nullptr, tmp, d.keys.p, d.keys2.p, d.vals.p, d.vals2.p,
-                                           (int)n_rows, 0, 64, s));
-        size_t tmp2 = 0;
-        CU(cub::DeviceScan::ExclusiveSum(nullptr, tmp2, d.lens.p, d.offs.p, (int)n_rows + 1, s));
-        if (d.cub_tmp.ensure(std::max(tmp, tmp2), err)) return err.code;
-        tmp = d.cub_tmp.cap;
-        CU(cub::DeviceRadixSort::SortPairs(d.cub_tmp.p, tmp, d.keys.p, d.keys2.p, d.vals.p,
-                                           d.vals2.p, (int)n_rows, 0, 64, s));
-        order = d.vals2.p;
-        if (d.lens.ensure(n_rows + 1, err) || d.offs.ensure(n_rows + 1, err)) return err.code;
-        unsigned fb = (unsigned)std::min<uint64_t>((n_rows + 255) / 256, (uint64_t)d.n_sm * 8);
-        row_len_kernel<<<fb, 256, 0, s>>>(d.view(), d.rows.p, order, n_rows,
-                                          (const ExactPattern *)tab(o_ep),
-                                          (const RequestDev *)tab(o_rdev), d.lens.p);
-        CU(cudaGetLastError());
-        CU(cudaMemsetAsync(d.lens.p + n_rows, 0, 4, s));
-        // widen lengths to 64-bit offsets
-        tmp2 = d.cub_tmp.cap;
-        CU(cub::DeviceScan::ExclusiveSum(d.cub_tmp.p, tmp2, d.lens.p, d.offs.p, (int)n_rows + 1, s));
-        CU(cudaMemcpyAsync(&text_bytes, d.offs.p + n_rows, 8, cudaMemcpyDeviceToHost, s));
+        CU(cudaEventRecord(d.ev[5], d.copy_stream));
+        CU(cudaStreamSynchronize(d.copy_stream));
         CU(cudaStreamSynchronize(s));
-        if (d.text.ensure(text_bytes + 1, err)) return err.code;
-        row_write_kernel<<<fb, 256, 0, s>>>(d.view(), d.rows.p, order, n_rows,
-                                            (const ExactPattern *)tab(o_ep),
-                                            (const RequestDev *)tab(o_rdev), d.offs.p, d.text.p);
-        CU(cudaGetLastError());
-        times_.kernel_launches += 4;
+        cudaEventElapsedTime(&ms, d.ev[6], d.ev[4]);
+        times_.format_ms += ms;
+        if (copy_pending) {  // the copy time left after the last slice's text
+            cudaEventElapsedTime(&ms, d.ev[4], d.ev[5]);
+            times_.d2h_ms += std::max(0.0f, ms);
+        }
+        if (reserve(host_off + 1)) return err.code;
+        hbuf.p[host_off] = 0;
+        out[0].text = hbuf.p;
+        out[0].pooled = std::move(hbuf);
+        out[0].text_len = host_off;
+        out[0].n_rows = rows_total;
+        slice_text_hint_ = host_off + host_off / 50 + 1;
+        return kOk;
     }
+
+    uint32_t n_rows = 0;
+    uint64_t text_bytes = 0;
+    std::vector<uint32_t> req_rows;
+    if (scan_verify(vsel, nullptr, n_rows, req_rows) ||
+        format_rows(n_rows, text_bytes, [](uint64_t) { return 0; }))
+        return err.code;
     // each request's rows (sorted request-major) go straight from the
     // device into its own page-locked result buffer
     CU(cudaEventRecord(d.ev[4], s));
@@ -1446,14 +1666,10 @@ int Engine::run_popcount(const std::vector<Request> &reqs, std::vector<Result> &
     CU(cudaStreamSynchronize(s));
     for (Result &r : out) r.pooled.p[r.text_len] = 0;
     float ms;
-    cudaEventElapsedTime(&ms, d.ev[1], d.ev[2]);
-    times_.scan_ms = ms;
-    cudaEventElapsedTime(&ms, d.ev[2], d.ev[3]);
-    times_.verify_ms = ms;
-    cudaEventElapsedTime(&ms, d.ev[3], d.ev[4]);
-    times_.format_ms = ms;
+    cudaEventElapsedTime(&ms, d.ev[6], d.ev[4]);
+    times_.format_ms += ms;
     cudaEventElapsedTime(&ms, d.ev[4], d.ev[5]);
-    times_.d2h_ms = ms;
+    times_.d2h_ms += ms;
     return kOk;
 }
 

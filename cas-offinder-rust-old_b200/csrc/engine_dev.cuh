@@ -197,7 +197,9 @@ class DeviceGenome {
   public:
     int device = 0;
     cudaStream_t stream = nullptr;
+    cudaStream_t copy_stream = nullptr;  // result text to the host, beside the next slice's scan
     cudaEvent_t ev[10] = {};
+    cudaEvent_t fmt_done = nullptr, copy_done = nullptr;  // a slice's text written / copied
     int n_sm = 0;
     DevBuf<uint8_t> bit4;
     DevBuf<uint32_t> planes;
@@ -228,6 +230,9 @@ class DeviceGenome {
         tb_items.release();
         for (auto &e : ev)
             if (e) cudaEventDestroy(e);
+        if (fmt_done) cudaEventDestroy(fmt_done);
+        if (copy_done) cudaEventDestroy(copy_done);
+        if (copy_stream) cudaStreamDestroy(copy_stream);
         if (stream) cudaStreamDestroy(stream);
     }
     GenomeDev view() const {

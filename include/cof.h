@@ -126,8 +126,10 @@ typedef struct {
 } cof_request;
 
 /* Output of one request: the writer's rows (main.rs:130-245) without the
- * header line, '\n'-terminated, ordered by genome position then pattern
- * (the reference's order is unspecified; compare sorted). */
+ * header line, '\n'-terminated.  Popcount rows are ordered by genome
+ * position, then by pattern (the order of cof_request.patterns, then their
+ * reverse complements); bulge rows by pattern, then position.  The
+ * reference's order is unspecified; compare sorted. */
 typedef struct {
     char *text;
     size_t text_len;

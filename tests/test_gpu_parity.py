@@ -488,3 +488,66 @@ def test_more_batches_than_one_scan_group_holds(cof_mod, oracle_mod, variant, mo
     text, n = g.search("N" * 21 + "RG", pats, 4, chunks_per_search=2)
     ref, nref = o.search("N" * 21 + "RG", pats, 4, chunks_per_search=2)
     assert _rows(text) == _rows(ref) and n == nref > 0
+
+
+@pytest.mark.parametrize("shape", ["nrg", "tttn", "nrg40"])
+@pytest.mark.parametrize("cps", [16384, 3])
+def test_sliced_scan_equals_one_pass(cof_mod, oracle_mod, monkeypatch, shape, cps):
+    # one request on a genome scanned in slices of pattern starts (forced on a
+    # small genome by COF_SLICE_NT), each slice's text copied out while the
+    # next one scans: rows sort by position first, so the text equals the
+    # one-pass text byte for byte, and a two-request batch (one pass) gives
+    # the same text; the rows equal the oracle's.  cps = 3 puts many batch
+    # heads (overlapping starts) across the slice cuts; the 40-cell pattern
+    # has a window shift above 32 on one strand.
+    rng = random.Random(1234 + cps + len(shape))
+    _, records = randgen.random_genome(rng, 3, 30000, 60000)
+    guide = lambda n: "".join(rng.choice("ACGT") for _ in range(n))
+    if shape == "nrg":
+        filt, pats, mm = "N" * 21 + "RG", [guide(20) + "NNN" for _ in range(3)], 5
+    elif shape == "tttn":
+        filt, pats, mm = "TTTN" + "N" * 25, ["NNNN" + guide(25) for _ in range(3)], 6
+    else:
+        filt, pats, mm = "N" * 38 + "RG", [guide(37) + "NNN" for _ in range(2)], 6
+    for p in pats:
+        randgen.plant_sites(rng, records, p, filt, 12, min(mm, 4))
+    g, o = _both(cof_mod, oracle_mod, randgen.chunk_records(rng, records, 3000))
+    monkeypatch.delenv("COF_SLICE_NT", raising=False)
+    one, n1 = g.search(filt, pats, mm, chunks_per_search=cps)
+    assert g.tuning()["slices"] == 0
+    monkeypatch.setenv("COF_SLICE_NT", "5000")
+    sliced, n2 = g.search(filt, pats, mm, chunks_per_search=cps)
+    assert g.tuning()["slices"] > 10
+    assert sliced == one and n2 == n1
+    req = dict(search_filter=filt, patterns=pats, max_mismatches=mm, chunks_per_search=cps)
+    other = dict(req, patterns=pats[:1], max_mismatches=2)
+    (bt, bn), _ = g.search_batch([req, other])
+    assert bt == one and bn == n1
+    ref, nref = o.search(filt, pats, mm, chunks_per_search=cps)
+    assert n1 == nref > 0 and _rows(one) == _rows(ref)
+
+
+def test_sliced_result_buffer_grows(cof_mod, oracle_mod, monkeypatch):
+    # one row in the first slices and thousands in the last: the page-locked
+    # result buffer, sized from the first slices' rate, has to grow while
+    # copies are in flight and keep the text already copied; a second call
+    # starts from the last result's size
+    rng = random.Random(5)
+    site = "".join(rng.choice("ACGT") for _ in range(20)) + "AGG"
+    pattern = site[:20] + "NNN"
+    head = randgen.random_seq(rng, 60000, n_rate=0, iupac_rate=0)
+    head = head[:1000] + site + head[1000 + len(site):]
+    tail = "".join(site + "".join(rng.choice("ACGT") for _ in range(7)) for _ in range(20000))
+    records = [head, randgen.random_seq(rng, 40000, n_rate=0, iupac_rate=0), tail]
+    g, o = _both(cof_mod, oracle_mod, randgen.chunk_records(rng, records, 60000))
+    monkeypatch.setenv("COF_SLICE_NT", "20000")
+    text, n = g.search("N" * 21 + "RG", [pattern], 2)
+    assert g.tuning()["slices"] > 20
+    assert len(text) > (1 << 20) + 2 * 35 * 75  # beyond the first estimate
+    again, n2 = g.search("N" * 21 + "RG", [pattern], 2)
+    assert again == text and n2 == n
+    monkeypatch.delenv("COF_SLICE_NT")
+    one, n1 = g.search("N" * 21 + "RG", [pattern], 2)
+    assert one == text and n1 == n
+    ref, nref = o.search("N" * 21 + "RG", [pattern], 2)
+    assert nref == n > 19000 and _rows(ref) == _rows(text)
