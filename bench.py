@@ -7,9 +7,12 @@ ABI (cof_search): PAM prefilter + popcount scan, exact verification, row
 formatting, rows copied to host memory.
 
   value : Gbp*guides/s over the device pipeline (scan + verify + format,
-          CUDA events on the library's stream), genome resident.
+          CUDA events on the library's stream), genome resident.  The
+          library scans one request on a genome this large in 4 slices and
+          sums their stage times.
   e2e   : same metric over the whole cof_search call (request tables
-          host->device, row text device->host into a host buffer).
+          host->device, row text device->host into a host buffer; each
+          slice's text crosses while the next slice scans).
   roofline : the scan kernel against the measured POPC peak of this GPU (one
           POPC per window x pattern comparison, microbenchmarked live).
 
