@@ -1280,11 +1280,44 @@ int Engine::run_popcount(const std::vector<Request> &reqs, std::vector<Result> &
     {
         // 768 Mnt: 4 slices of a 3.1 Gbp genome (3, 4 and 6 slices measured
         // 18.99, 18.83 and 19.40 ms per 100-guide search; one pass 20.02)
-        uint64_t slice_nt = uint64_t(768) << 20;  // COF_SLICE_NT: tests of many slices
-        if (const char *e = std::getenv("COF_SLICE_NT"))
-            slice_nt = std::max<uint64_t>(1024, std::strtoull(e, nullptr, 10));
+        uint64_t slice_nt = uint64_t(768) << 20;
+        const char *force = std::getenv("COF_SLICE_NT");  // tests: slice small genomes too
+        if (force) slice_nt = std::max<uint64_t>(1024, std::strtoull(force, nullptr, 10));
         const uint64_t total_nt = 2 * h.boff.back();
         bool ok = reqs.size() == 1 && !groups.empty() && total_nt >= 2 * slice_nt;
+        if (ok && !force) {
+            // slice only when the text is expected to be large enough for
+            // its copy to outweigh the slices' own cost (about 0.2 ms each).
+            // For i.i.d. uniform bases, rows per pattern ~ starts x P(the
+            // filter cells under the pattern's N cells match) x P(<= mm of
+            // the pattern's other cells mismatch); a reverse-strand pattern
+            // meets the filter reversed
+            const Request &r = reqs[0];
+            const uint32_t L = (uint32_t)r.filter.size();
+            const size_t nfwd = r.patterns.size() / 2;
+            double rows = 0;
+            for (size_t pi = 0; pi < r.patterns.size(); ++pi) {
+                const std::string &pat = r.patterns[pi];
+                double p_pam = 1;
+                std::vector<double> q;  // match probability of each care cell
+                for (uint32_t c = 0; c < L; ++c) {
+                    const uint8_t pb = t.str2b4[1][(uint8_t)pat[c]];
+                    const uint8_t fb = t.str2b4[1][(uint8_t)r.filter[pi < nfwd ? c : L - 1 - c]];
+                    if (pb == 0xF) p_pam *= __builtin_popcount(fb) / 4.0;
+                    else q.push_back(__builtin_popcount(pb) / 4.0);
+                }
+                // P(at most max_mm of the care cells mismatch), by DP
+                std::vector<double> dp(r.max_mm + 2, 0.0);
+                dp[0] = 1;
+                for (double m : q)
+                    for (int k = (int)r.max_mm + 1; k >= 0; --k)
+                        dp[k] = dp[k] * m + (k ? dp[k - 1] * (1 - m) : 0);
+                double p_mm = 0;
+                for (uint32_t k = 0; k <= r.max_mm; ++k) p_mm += dp[k];
+                rows += (double)total_nt * p_pam * p_mm;
+            }
+            ok = rows * (2.0 * L + 30) >= 32.0 * (1 << 20);
+        }
         for (uint32_t sh : group_shift) ok = ok && sh != ~0u;
         const uint64_t n_slices = ok ? (total_nt + slice_nt - 1) / slice_nt : 0;
         for (uint64_t j = 0; j < n_slices; ++j) {
