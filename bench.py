@@ -60,11 +60,10 @@ def parse():
     ap.add_argument("--impl", default="cof", choices=["cof", "reference"])
     ap.add_argument("--scale", type=float, default=1.0, help="genome size factor (1.0 = 3.1 Gbp)")
     ap.add_argument("--guides", type=int, default=100)
-    ap.add_argument("--cpu-sample-s", type=float, default=15.0,
-                    help="target seconds of CPU work for the CPU baseline")
+    ap.add_argument("--cpu-rounds", type=int, default=4,
+                    help="CPU baseline and --impl reference: the genome slice is this many "
+                         "4.19 Mnt batches per host thread (about 1 s each at 100 guides)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--ref-step-s", type=float, default=4.0,
-                    help="seconds of CPU work per step of --impl reference")
     ap.add_argument("--no-ref-gpu", action="store_true",
                     help="--impl reference: skip timing the reference's own GPU kernel")
     ap.add_argument("--serving-requests", type=int, default=64)
@@ -375,10 +374,18 @@ def bulge_rates(cfg, stats, rows):
 
 class CpuSample:
     """The reference CPU path (C restatement, oracle/) over a leading slice of
-    the workload's genome: all host threads, CPU batch size (64 chunks).  The
-    slice is calibrated once to about `target_s` seconds of work."""
+    the workload's genome, with the CPU batch size (64 chunks of 65,520 nt,
+    4.19 Mnt) and all host threads.  The oracle, like search_compute_cpu
+    (search.rs:549-569), gives each worker thread whole batches, so the slice
+    is `rounds` batches per thread: every thread has the same work, no thread
+    idles for want of a batch, and the slice follows from the thread count
+    alone.  Both the product's cpu_baseline and the reference arm
+    (--impl reference) use this rule, so on one machine they time the same
+    slice."""
 
-    def __init__(self, cfg, target_s, n_threads=0):
+    BATCH_CHUNKS = 64
+
+    def __init__(self, cfg, rounds=4, n_threads=0):
         sys.path.insert(0, ORACLE)
         import oracle
         oracle.build()
@@ -386,13 +393,17 @@ class CpuSample:
         self.cfg = cfg
         self.n_threads = n_threads
         self.cores = n_threads or os.cpu_count()
+        self.rounds = rounds
         self.chunks = list(cfg["genome"].chunks())
-        t, nt = self._time(self._genome(min(len(self.chunks), 64)))  # one 4 Mnt batch
-        per_nt = t / max(nt, 1)
-        want = int(target_s / max(per_nt, 1e-12))
-        self.n_chunks = max(64, min(len(self.chunks), want // 65520 // 64 * 64))
+        # batches after the first start with the previous batch's last chunk
+        # (the head overlap of search.rs:1531-1572): B batches hold
+        # 64 + 63 (B - 1) chunks
+        n_batches = rounds * self.cores
+        self.n_chunks = min(len(self.chunks),
+                            self.BATCH_CHUNKS + (self.BATCH_CHUNKS - 1) * (n_batches - 1))
         self.genome = self._genome(self.n_chunks)
         self.nt = self.genome.n_nucl
+        self.batches = self.genome.n_batches(self.BATCH_CHUNKS)
 
     def _genome(self, n_chunks):
         o = self.oracle.OracleGenome()
@@ -403,8 +414,8 @@ class CpuSample:
     def _time(self, o):
         c = self.cfg
         t0 = time.perf_counter()
-        o.search(c["filter"], c["patterns"], c["max_mismatches"], chunks_per_search=64,
-                 n_threads=self.n_threads)
+        o.search(c["filter"], c["patterns"], c["max_mismatches"],
+                 chunks_per_search=self.BATCH_CHUNKS, n_threads=self.n_threads)
         return time.perf_counter() - t0, o.n_nucl
 
     def run(self):
@@ -414,7 +425,9 @@ class CpuSample:
 
     def describe(self, value, t):
         return dict(value=value, unit=UNIT, cores=self.cores, kind="port",
-                    sample=f"first {self.nt / 1e6:.1f} Mbp of the genome x "
+                    sample_nt=self.nt, sample_batches=self.batches,
+                    sample=f"first {self.nt / 1e6:.1f} Mbp of the genome ({self.batches} "
+                           f"batches of 64 chunks: {self.rounds} per thread) x "
                            f"{len(self.cfg['patterns'])} guides, oracle/ C restatement of "
                            f"search_compute_cpu + writer, {self.cores} threads, {t:.1f} s")
 
@@ -484,8 +497,8 @@ def bench_cli(cfg, n_rows, runs=2, fmt="2bit"):
         shutil.rmtree(d, ignore_errors=True)
 
 
-def cpu_baseline(cfg, target_s, n_threads=0):
-    smp = CpuSample(cfg, target_s, n_threads)
+def cpu_baseline(cfg, rounds, n_threads=0):
+    smp = CpuSample(cfg, rounds, n_threads)
     v, t = smp.run()
     return smp.describe(v, t), t
 
@@ -526,12 +539,13 @@ def reference_gpu_kernel(cfg):
 def run_reference(args, rank, world):
     """The reference arm: the reference's CPU search path on the host cores
     (oracle/ C restatement; Rust cannot be built here), each step one pass
-    over a fixed slice of the workload calibrated to --ref-step-s seconds.
-    Under torchrun only rank 0 runs."""
+    over the slice CpuSample picks (--cpu-rounds batches per host thread, the
+    same slice as the product's cpu_baseline).  Under torchrun only rank 0
+    runs."""
     if rank != 0:
         return
     cfg = make_workload(args, 0)
-    smp = CpuSample(cfg, args.ref_step_s)
+    smp = CpuSample(cfg, args.cpu_rounds)
     vals, times = [], []
     for i in range(args.warmup + args.steps):
         v, t = smp.run()
@@ -694,7 +708,7 @@ def main():
         line["cli_whole_process"] = bench_cli(cfg, rows_per_step)
         line["cli_whole_process_fasta"] = bench_cli(cfg, rows_per_step, fmt="fasta")
     if not args.no_cpu_baseline and world == 1:
-        base, _ = cpu_baseline(cfg, args.cpu_sample_s)
+        base, _ = cpu_baseline(cfg, args.cpu_rounds)
         line["cpu_baseline"] = base
     print(json.dumps(line), flush=True)
     if dist:

@@ -36,6 +36,8 @@ constexpr size_t kNaTableBytes = 32u << 10;
 constexpr size_t kNaCandOffset = kNaCounterBytes + kNaTableBytes;
 constexpr uint32_t kNaMaxCandidates =
     (uint32_t)((kNaScratchBytes - kNaCandOffset) / sizeof(uint2));  // 1,044,448
+// rows a call may count before its 32-bit row counter could wrap
+constexpr uint32_t kNaRowCountLimit = 0xFFFFFFF0u;
 
 struct NaPam {
     uint32_t cell, fa, fc, fg, ft;
@@ -56,7 +58,8 @@ struct NaTables {
 };
 static_assert(sizeof(NaTables) <= kNaTableBytes, "pattern tables exceed their scratch slot");
 
-// counters: [0] candidates, [1] candidate overflow, [2] rows
+// counters: [0] candidates, [1] candidate overflow, [2] rows, [3] row-count
+// overflow (the 32-bit row counter came within 16 of wrapping)
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNaScratchBytes];
 
 __device__ __forceinline__ uint32_t na_gather(uint32_t v) {
@@ -167,10 +170,12 @@ __global__ void na_verify_kernel(const uint8_t *__restrict__ bit4, uint64_t n_nu
         }
         if ((int)L - matches > (int)T.max_mm || !pam_ok || actual > T.max_mm) continue;
         const uint32_t r = atomicAdd(&ctr[2], 1u);
+        if (r >= kNaRowCountLimit) ctr[3] = 1;  // every value is returned once: none is missed
         if (r < rows_cap) {
-            rows[3 * r] = s;
-            rows[3 * r + 1] = p;
-            rows[3 * r + 2] = actual;
+            const uint64_t o = 3ull * r;  // rows_cap may exceed 2^32 / 3
+            rows[o] = s;
+            rows[o + 1] = p;
+            rows[o + 2] = actual;
         }
     }
 }
@@ -202,6 +207,10 @@ extern "C" COF_API int cof_search_seq_noalloc(const uint8_t *d_bit4, uint64_t n_
         return na_fail(COF_E_UNSUPPORTED,
                        "n_patterns must be 1.." + std::to_string(kNaMaxPatterns) +
                            " (fwd + reverse) for the fixed scratch tables");
+    if (n_patterns % 2)
+        return na_fail(COF_E_BADINPUT,
+                       "n_patterns must be even: the forward patterns, then their reverse "
+                       "complements (search.rs:1455 takes index < n / 2 as '+')");
     if (n_nucl >= (1ull << 31))
         return na_fail(COF_E_UNSUPPORTED, "sequence longer than 2^31 - 1 nucleotides");
     if (max_mismatches >= L)
@@ -252,9 +261,23 @@ extern "C" COF_API int cof_search_seq_noalloc(const uint8_t *d_bit4, uint64_t n_
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64)
         return na_fail(COF_E_CUDA, "no usable CUDA device");
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    if (s) {
+        // the scratch address below belongs to the current device: a stream
+        // of another device would run the kernels against the wrong array
+        int sdev = -1;
+        const cudaError_t e = cudaStreamGetDevice(s, &sdev);
+        if (e != cudaSuccess)
+            return na_fail(COF_E_BADINPUT, std::string("stream: ") + cudaGetErrorString(e));
+        if (sdev != dev)
+            return na_fail(COF_E_BADINPUT, "stream belongs to device " + std::to_string(sdev) +
+                                                ", the current device is " + std::to_string(dev));
+    }
     if (!g_na_ptr[dev]) {
         // once per device, with that device current: the array's name is only
-        // a host-side stand-in, the kernels need its device address
+        // a host-side stand-in, the kernels need its device address.  The
+        // address is kept for the process; a cudaDeviceReset of this device
+        // by the caller invalidates it (and the array itself)
         void *p = nullptr;
         cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
         if (e != cudaSuccess || !p)
@@ -262,7 +285,6 @@ extern "C" COF_API int cof_search_seq_noalloc(const uint8_t *d_bit4, uint64_t n_
         g_na_ptr[dev] = p;
     }
     unsigned char *scratch = static_cast<unsigned char *>(g_na_ptr[dev]);
-    cudaStream_t s = static_cast<cudaStream_t>(stream);
     auto cu = [&](cudaError_t e, const char *what) {
         if (e == cudaSuccess) return 0;
         na_fail(COF_E_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
@@ -313,10 +335,16 @@ extern "C" COF_API int cof_search_seq_noalloc(const uint8_t *d_bit4, uint64_t n_
             if (cu(cudaGetLastError(), "verify launch")) return COF_E_CUDA;
         }
     }
-    uint32_t nr = 0;
-    if (cu(cudaMemcpyAsync(&nr, scratch + 8, 4, cudaMemcpyDeviceToHost, s), "row count") ||
+    uint32_t c23[2] = {0, 0};  // rows, row-count overflow
+    if (cu(cudaMemcpyAsync(c23, scratch + 8, 8, cudaMemcpyDeviceToHost, s), "row count") ||
         cu(cudaStreamSynchronize(s), "verify"))
         return COF_E_CUDA;
+    if (c23[1]) {
+        *n_rows = 0xFFFFFFFFu;
+        return na_fail(COF_E_UNSUPPORTED,
+                       "more than 2^32 - 16 rows: the row count does not fit its 32-bit counter");
+    }
+    const uint32_t nr = c23[0];
     *n_rows = nr;
     if (nr > rows_cap)
         return na_fail(COF_E_UNSUPPORTED, "rows_cap too small: " + std::to_string(nr) +

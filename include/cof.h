@@ -204,19 +204,27 @@ COF_API int cof_genome_last_stats(const cof_genome *g, double *ms5, uint64_t *co
  * d_bit4: one record of n_nucl nucleotides in the reference's bit4 one-hot
  * encoding (two per byte, even index in the low nibble), 16-byte aligned,
  * n_nucl < 2^31.  patterns: the full fwd + reverse list as search() takes
- * it, 1..512 patterns of the filter's length (<= 32).  Rows are the writer's
+ * it (the forward patterns, then as many reverse complements: an odd count
+ * is rejected with COF_E_BADINPUT), 2..512 patterns of the filter's length
+ * (<= 32).  Rows are the writer's
  * rows of cof_search for a genome made of this one record: every window start
  * s with s + L <= n_nucl that passes the PAM filter and the mismatch
  * recount.  Each row is three uint32 in d_rows: s (0-based, the scan
  * orientation start), pattern index, mismatches; order unspecified.
- * *n_rows receives the number of rows found; if it exceeds rows_cap only the
- * first rows_cap are written and COF_E_UNSUPPORTED is returned.  Requests
+ * *n_rows receives the number of rows found; if it exceeds rows_cap, rows_cap
+ * of them (in no particular order) are written and COF_E_UNSUPPORTED is
+ * returned.  Requests
  * beyond the stated maximums are rejected with COF_E_UNSUPPORTED and a
- * message in cof_last_error().  stream: a cudaStream_t (NULL = default).
+ * message in cof_last_error(), and so is a call whose row count would not
+ * fit 32 bits (*n_rows is then 0xFFFFFFFF).  stream: a cudaStream_t
+ * (NULL = default) of the current device; a stream of another device is
+ * rejected with COF_E_BADINPUT.
  *
  * The first call on a device looks up the array's device address
  * (cudaGetSymbolAddress) with that device current; make it before any
- * stream capture.  All calls share the array and leave their data in it;
+ * stream capture.  The address is kept until the process exits, so a
+ * cudaDeviceReset of that device ends the use of this entry point there.
+ * All calls share the array and leave their data in it;
  * each call clears its counters first.  Calls are serialised inside the
  * library and wait for their stream before returning; work from two calls
  * that overlapped on the GPU would race on the shared array. */

@@ -15,16 +15,20 @@ def build():
     subprocess.run(["make", "-s", "-C", _HERE], check=True)
 
 
-REFERENCE_SRC = "/root/reference/cas-offinder-lib/src"
+def reference_src():
+    """The reference's cas-offinder-lib/src directory, from the environment
+    variable COF_REFERENCE_DIR (the reference project's root), or None."""
+    root = os.environ.get("COF_REFERENCE_DIR")
+    return os.path.join(root, "cas-offinder-lib", "src") if root else None
 
 
 def build_reference_kernels():
     """Builds _ref/ (the reference's kernel.cu / kernel_myers.cu for sm_100a
-    and the launcher ref_gpu.cu) when the reference tree is present; a
-    machine without it keeps the files built where it was."""
-    if os.path.exists(os.path.join(REFERENCE_SRC, "kernel.cu")):
-        subprocess.run(["make", "-s", "-j8", "-C", _HERE, "ref", "REF=" + REFERENCE_SRC],
-                       check=True)
+    and the launcher ref_gpu.cu) when COF_REFERENCE_DIR names the reference
+    tree; without it, the files built earlier (if any) are kept."""
+    src = reference_src()
+    if src and os.path.exists(os.path.join(src, "kernel.cu")):
+        subprocess.run(["make", "-s", "-j8", "-C", _HERE, "ref", "REF=" + src], check=True)
 
 
 class _Req(ctypes.Structure):

@@ -583,4 +583,96 @@ int refgpu_myers_run(refgpu_ctx *c, const char *cubin, const char *search_filter
     return rc;
 }
 
+char *refgpu_myers_lines(refgpu_ctx *c, const char *const *chunk_names,
+                         const char *const *patterns, size_t n_patterns, size_t n_fwd_patterns,
+                         const refgpu_mmatch *recs, const uint64_t *batch_offsets,
+                         uint64_t *text_len, uint64_t *n_lines) {
+    static const char kDec[16] = {0,   'T', 'C', 'Y', 'A', 'W', 'M', 'H',
+                                  'G', 'K', 'S', 'B', 'R', 'D', 'V', 'N'};
+    const size_t L = n_patterns ? std::strlen(patterns[0]) : 0;
+    std::string out;
+    uint64_t lines = 0;
+    std::string rna, dna;
+    char num[64];
+    for (size_t bi = 0; bi < c->batches.size(); bi++) {
+        const Batch &b = c->batches[bi];
+        c->pack(b, false);  // the batch buffer and its chunk byte offsets
+        const uint8_t *buf = c->host.data();
+        const uint64_t nbytes = c->offs.back();
+        auto nib = [&](uint64_t i) -> uint8_t {
+            if (i / 2 >= nbytes) return 0;
+            const uint8_t x = buf[i / 2];
+            return (i & 1) ? (uint8_t)(x >> 4) : (uint8_t)(x & 0xF);
+        };
+        for (uint64_t r = batch_offsets[bi]; r < batch_offsets[bi + 1]; r++) {
+            const refgpu_mmatch &m = recs[r];
+            const char *pat = patterns[m.pattern_idx];
+            // decode_gpu_enum_match (search.rs:152-206): ops last to first;
+            // an M / S / D op over a zero nibble drops the record
+            rna.clear();
+            dna.clear();
+            uint64_t gi = m.chunk_idx;
+            size_t pi = 0;
+            bool ok = true;
+            for (int k = (int)m.ops_count - 1; k >= 0; k--) {
+                const unsigned op = (unsigned)(m.ops_packed >> (2 * k)) & 3u;
+                if (op != 3) {
+                    const uint8_t v = nib(gi);
+                    if (!v) {
+                        ok = false;
+                        break;
+                    }
+                    dna.push_back(kDec[v]);
+                    rna.push_back(op != 2 ? pat[pi] : '-');
+                    pi += op != 2;
+                    gi++;
+                } else {
+                    rna.push_back(pat[pi]);
+                    dna.push_back('-');
+                    pi++;
+                }
+            }
+            if (!ok) continue;
+            // convert_matches_myers (search.rs:1316-1374): owning chunk and
+            // the record-end drop with extent L + db - rb
+            const uint64_t start = m.chunk_idx;
+            size_t idx = (size_t)(std::upper_bound(c->offs.begin(), c->offs.end(),
+                                                   (uint32_t)(start / 2)) -
+                                  c->offs.begin()) - 1;
+            idx = std::min(idx, b.n - 1);
+            const size_t k = b.first + idx;
+            const uint64_t pos = c->start[k] + (start - (uint64_t)c->offs[idx] * 2);
+            const bool end_chrom = idx == b.n - 1 || c->start[k + 1] == 0;
+            const uint64_t extent = L + m.dna_bulge_size - m.rna_bulge_size;
+            if (end_chrom && pos + extent > c->end[k]) continue;
+            const bool fwd = m.pattern_idx < n_fwd_patterns;
+            if (!fwd) {
+                std::reverse(rna.begin(), rna.end());
+                std::reverse(dna.begin(), dna.end());
+                for (char &ch : rna) ch = ch == '-' ? ch : comp_char(ch);
+                for (char &ch : dna) ch = ch == '-' ? ch : comp_char(ch);
+            }
+            out += chunk_names[k];
+            std::snprintf(num, sizeof num, "\t%llu\t%u\t%c\t%u\t%u\t%u\t",
+                          (unsigned long long)pos, m.pattern_idx, fwd ? '+' : '-', m.mismatches,
+                          (unsigned)m.dna_bulge_size, (unsigned)m.rna_bulge_size);
+            out += num;
+            out += rna;
+            out += '\t';
+            out += dna;
+            out += '\n';
+            lines++;
+        }
+    }
+    char *p = static_cast<char *>(std::malloc(out.size() + 1));
+    if (!p) return nullptr;
+    std::memcpy(p, out.data(), out.size());
+    p[out.size()] = 0;
+    *text_len = out.size();
+    *n_lines = lines;
+    return p;
+}
+
+void refgpu_free(void *p) { std::free(p); }
+
 }  // extern "C"

@@ -103,6 +103,18 @@ int refgpu_myers_run(refgpu_ctx *c, const char *cubin, const char *search_filter
                      uint32_t out_buf_size, refgpu_mmatch *out, uint64_t out_cap,
                      uint64_t *batch_offsets, refgpu_times *t, char *err, size_t errlen);
 
+/* search()'s raw Match lines of the Myers records `recs` (from
+ * refgpu_myers_run, batch_offsets as it filled them): decode_gpu_enum_match
+ * (search.rs:152-206) and convert_matches_myers (search.rs:1316-1374), the
+ * line format of the product's COF_F_RAW_MATCHES.  chunk_names: the record
+ * name of every chunk.  Returns a malloc'd NUL-terminated text (free with
+ * refgpu_free), or NULL when out of memory. */
+char *refgpu_myers_lines(refgpu_ctx *c, const char *const *chunk_names,
+                         const char *const *patterns, size_t n_patterns, size_t n_fwd_patterns,
+                         const refgpu_mmatch *recs, const uint64_t *batch_offsets,
+                         uint64_t *text_len, uint64_t *n_lines);
+void refgpu_free(void *p);
+
 #ifdef __cplusplus
 }
 #endif

@@ -84,6 +84,10 @@ def lib():
         L.refgpu_myers_run.restype = ctypes.c_int
         L.refgpu_myers_run.argtypes = [vp, cp, cp, pp, sz, sz, u32, vp, u64, vp,
                                        ctypes.POINTER(Times), cp, sz]
+        L.refgpu_myers_lines.restype = vp
+        L.refgpu_myers_lines.argtypes = [vp, pp, pp, sz, sz, vp, vp, ctypes.POINTER(u64),
+                                         ctypes.POINTER(u64)]
+        L.refgpu_free.argtypes = [vp]
         _lib = L
     return _lib
 
@@ -190,6 +194,38 @@ class RefGpu:
             for b in range(nb):
                 per.append([out[i] for i in range(offs[b], offs[b + 1])])
         return per, t.as_dict()
+
+    def myers_text(self, search_filter, patterns, n_fwd, mm, db, rb, out_cap):
+        """find_matches_myers over every batch, decoded in C into search()'s
+        raw Match lines (refgpu_myers_lines: the decode of myers_raw_lines
+        below, for millions of records).  Returns (text, lines, times)."""
+        L = len(patterns[0])
+        pam_len = max(sum(1 for ch in p if ch in "Nn") for p in patterns)
+        cub = myers_cubin(L, pam_len, mm, db, rb)
+        if not os.path.exists(cub):
+            raise RefGpuError(f"no reference Myers cubin for {os.path.basename(cub)}")
+        enc, arr = _pats(patterns)
+        nb = len(self.batches)
+        out = (MMatch * out_cap)()
+        offs = (ctypes.c_uint64 * (nb + 1))()
+        t = Times()
+        err = ctypes.create_string_buffer(512)
+        if lib().refgpu_myers_run(self._h, cub.encode(), search_filter.encode(), arr, len(enc),
+                                  n_fwd, OUT_BUF_SIZE, out, out_cap, offs, ctypes.byref(t),
+                                  err, 512):
+            raise RefGpuError(err.value.decode())
+        names = [c[0].encode() for c in self.chunks]
+        name_arr = (ctypes.c_char_p * max(len(names), 1))(*names)
+        n_text, n_lines = ctypes.c_uint64(), ctypes.c_uint64()
+        p = lib().refgpu_myers_lines(self._h, name_arr, arr, len(enc), n_fwd, out, offs,
+                                     ctypes.byref(n_text), ctypes.byref(n_lines))
+        if not p:
+            raise RefGpuError("out of host memory for the decoded lines")
+        try:
+            text = ctypes.string_at(p, n_text.value).decode("latin-1")
+        finally:
+            lib().refgpu_free(p)
+        return text, n_lines.value, t.as_dict()
 
 
 # -- host-side decode into search()'s raw Match lines -----------------------

@@ -11,7 +11,8 @@ which run without the reference tree, compare against the same rows:
   kat_bulge_rows.txt     N x 25 + GG filter, db 1 rb 1, mm 5, one pattern
                          (integration_bulge.rs:208-259; CPU == GPU only)
 
-Run from the repository root:  python tests/golden/make_golden.py
+Run from the repository root, with COF_REFERENCE_DIR naming the reference
+project's root:  COF_REFERENCE_DIR=<reference> python tests/golden/make_golden.py
 """
 import os
 import shutil
@@ -19,7 +20,6 @@ import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
-REF = "/root/reference/cas-offinder-lib/tests/test_data"
 
 KAT_POPCOUNT = dict(search_filter="N" * 24,
                     patterns=["CCGTGGTTCAACATTTGCTTAGCA", "GATGTTGGTAAGTGGGATATGGCA"],
@@ -29,8 +29,9 @@ KAT_BULGE = dict(search_filter="N" * 25 + "GG", patterns=["CCGTGGTTCAACATTTGCTTA
 
 
 def main():
+    ref = os.path.join(os.environ["COF_REFERENCE_DIR"], "cas-offinder-lib", "tests", "test_data")
     for f in ("upstream1000.fa", "upstream1000.2bit", "expected.txt"):
-        shutil.copyfile(os.path.join(REF, f), os.path.join(HERE, f))
+        shutil.copyfile(os.path.join(ref, f), os.path.join(HERE, f))
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle
     oracle.build()

@@ -89,3 +89,6 @@ def test_reference_myers_kernel(cof_mod, mm, db, rb):
                                               raw=True)
     assert sorted(ref_lines) == sorted(_lines(text))
     assert n == len(ref_lines) > 0
+    # the C decode used at the benchmark's size gives the same lines
+    ctext, nc, _t = ref.myers_text(filt, full, len(pats), mm, db, rb, out_cap=1 << 20)
+    assert sorted(_lines(ctext)) == sorted(ref_lines) and nc == n
