@@ -78,6 +78,9 @@ def parse():
                     help="run only the whole-process CLI measurement and print it")
     ap.add_argument("--bulge-scale", type=float, default=0.02,
                     help="bulge genome factor (1.0 = 500 Mbp; ~720 k rows per Mbp)")
+    ap.add_argument("--bulge-full-scale", type=float, default=1.0,
+                    help="--only-bulge: genome factor of the streamed bulge measurement "
+                         "(0 skips it)")
     return ap.parse_args()
 
 
@@ -353,6 +356,82 @@ def bench_bulge(cof, device, steps, scale):
             "stage_rates": bulge_rates(cfg, stats, rows)}
 
 
+def bench_bulge_full(cof, device, steps, scale=1.0, cpu_nt=2_000_000):
+    """The bulge workload at its stated size: 500 Mbp in 5 records x 20
+    guides of 20 nt + NRG, mm<=4, DNA and RNA bulges <= 2 (about 3.6e8
+    alignment rows, ~27 GB of row text per search).  The rows are streamed
+    through cof_search_stream to a sink that counts them (the dest channel
+    of search.rs:1490-1500): each candidate chunk's text crosses to a
+    page-locked staging buffer while the next chunk's traceback runs, so
+    host memory holds a few chunks, not the result.  value = Gbp*guides /
+    device time (Myers filter + budget pre-test + traceback + format); e2e =
+    the same over the whole streamed call, every row delivered to the sink.
+    cpu_baseline: the oracle's restatement of the reference's Myers CPU
+    path (search.rs:951-1031, traceback.rs:181-381) on the genome's first
+    cpu_nt nucleotides, all host threads."""
+    import synth
+    t0 = time.perf_counter()
+    cfg = synth.config_bulge(seed=4, scale=scale)
+    t_gen = time.perf_counter() - t0
+    g = cof.Genome(device=device)
+    cfg["genome"].load_into(g)
+    g.upload()
+    req = dict(search_filter=cfg["filter"], patterns=cfg["patterns"],
+               max_mismatches=cfg["max_mismatches"], max_dna_bulges=cfg["max_dna_bulges"],
+               max_rna_bulges=cfg["max_rna_bulges"])
+    prep = g.prepare([req])
+    g.stream_count(prep)  # warm-up: buffers, page-locked staging
+    dev, wall, stats, res = [], [], [], []
+    for _ in range(steps):
+        t1 = time.perf_counter()
+        res.append(g.stream_count(prep))
+        wall.append(time.perf_counter() - t1)
+        st = g.last_stats()
+        stats.append(st)
+        dev.append(st["scan_ms"] + st["verify_ms"] + st["format_ms"])
+    g.close()
+    rows, nbytes, pieces = res[-1]
+    assert all(r == res[0] for r in res), "streamed row counts differ between steps"
+    n_nt = cfg["genome"].n_nucl
+    units = n_nt * 1e-9 * len(cfg["patterns"])
+    d, w = statistics.median(dev), statistics.median(wall)
+    out = {"workload": f"{n_nt / 1e6:.0f} Mbp x 20 guides (20 nt + NRG), mm<=4, "
+                       f"DNA/RNA bulges<=2, rows streamed to a counting sink",
+           "value": units / (d * 1e-3), "unit": UNIT, "device_ms": d,
+           "e2e": {"value": units / w, "unit": UNIT, "ms_per_step": w * 1e3,
+                   "h2d_bytes_per_step": 20 * 23 * 2 + 4096, "d2h_bytes_per_step": nbytes},
+           "rows_per_step": rows, "rows_per_s_e2e": rows / w, "text_gb_per_step": nbytes / 1e9,
+           "pieces_per_step": pieces,
+           "stages_ms": {k: statistics.median(s[k] for s in stats)
+                         for k in ("scan_ms", "verify_ms", "format_ms", "d2h_ms", "total_ms")},
+           "candidates_per_step": stats[-1]["candidates"],
+           "gpu_launches_per_step": stats[-1]["kernel_launches"], "steps": steps,
+           "genome_generate_s": t_gen, "stage_rates": bulge_rates(cfg, stats, rows)}
+    # the reference's Myers CPU path (oracle port) on a leading slice
+    sys.path.insert(0, ORACLE)
+    import oracle
+    oracle.build()
+    o = oracle.OracleGenome()
+    nt = 0
+    for name, data, s0, e0 in cfg["genome"].chunks():
+        if nt >= cpu_nt:
+            break
+        o.add_chunk(name, data, s0, e0)
+        nt += e0 - s0
+    t1 = time.perf_counter()
+    _text, crow = o.search(cfg["filter"], cfg["patterns"], cfg["max_mismatches"],
+                           cfg["max_dna_bulges"], cfg["max_rna_bulges"])
+    tc = time.perf_counter() - t1
+    o.close()
+    out["cpu_baseline"] = {
+        "value": nt * 1e-9 * len(cfg["patterns"]) / tc, "unit": UNIT, "cores": os.cpu_count(),
+        "kind": "port",
+        "sample": f"first {nt / 1e6:.1f} Mbp x 20 guides, oracle/ C restatement of the Myers "
+                  f"CPU path (check_pam_quick, Myers sweep, traceback_all, classify, writer), "
+                  f"{os.cpu_count()} threads, {tc:.1f} s, {crow} rows"}
+    return out
+
+
 def bulge_rates(cfg, stats, rows):
     """Per-stage work rates of the bulge path (its kernels are integer DP, so
     rates of their own units stand in for a roofline): Myers steps (one text
@@ -596,8 +675,11 @@ def main():
     import cof
     if args.only_bulge:
         if rank == 0:
-            print(json.dumps({"bulge": bench_bulge(cof, local, max(1, args.steps),
-                                                   args.bulge_scale)}), flush=True)
+            res = {"bulge": bench_bulge(cof, local, max(1, args.steps), args.bulge_scale)}
+            if args.bulge_full_scale > 0:
+                res["bulge_full"] = bench_bulge_full(cof, local, max(1, args.steps),
+                                                     args.bulge_full_scale)
+            print(json.dumps(res), flush=True)
         if dist:
             dist.destroy_process_group()
         return
@@ -703,6 +785,7 @@ def main():
         line["serving_small_requests"] = bench_serving(cof, g, n_nt, 4 * args.serving_requests,
                                                        2000.0, seed=8, max_guides=4, max_mm=3)
         line["bulge"] = bench_bulge(cof, local, 3, args.bulge_scale)
+        line["bulge_full"] = bench_bulge_full(cof, local, 2)
         line["serving_bulge_mix"] = bench_serving_bulge(cof, local)
         g.close()  # the CLI runs as its own process: free this one's device genome first
         line["cli_whole_process"] = bench_cli(cfg, rows_per_step)

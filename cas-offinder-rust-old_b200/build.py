@@ -21,9 +21,11 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC,-fvisibility=hidden",
           "-I" + os.path.join(ROOT, "include")]
 HEADERS = [os.path.join(CSRC, "cof_engine.h"), os.path.join(CSRC, "engine_dev.cuh"),
+           os.path.join(CSRC, "textout.h"),
            os.path.join(ROOT, "include", "cof.h")]
 
 SOURCES = ["engine.cu", "bulge.cu", "raw.cu", "loader.cpp", "cabi.cpp", "server.cpp", "noalloc.cu",
+           "textout.cpp",
            "hostpool.cpp", "twobit.cu", "fasta_dev.cu"]
 
 

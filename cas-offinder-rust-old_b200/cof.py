@@ -26,8 +26,10 @@ COF_E_IO = -4
 COF_E_UNSUPPORTED = -5
 COF_E_STATE = -6
 COF_E_TIMEOUT = -7
+COF_E_CANCELLED = -8
 COF_F_ADD_REVCOMP = 1
 COF_F_RAW_MATCHES = 2
+COF_STREAM_MATCHES = 1
 
 HEADER = "#Bulge type\tcrRNA\tDNA\tChromosome\tPosition\tDirection\tMismatches\tBulge Size\n"
 
@@ -38,6 +40,7 @@ EXPORTS = (
     "cof_search_batch", "cof_result_free", "cof_genome_last_stats", "cof_last_error",
     "cof_abi_version", "cof_search_seq_noalloc", "cof_server_create", "cof_server_submit",
     "cof_server_wait", "cof_server_stats", "cof_server_free", "cof_genome_tuning",
+    "cof_search_stream", "cof_genome_record_name", "cof_genome_n_records",
 )
 
 
@@ -68,6 +71,34 @@ class _Result(ctypes.Structure):
         ("n_rows", ctypes.c_uint64),
         ("device_ms", ctypes.c_double),
     ]
+
+
+class Match(ctypes.Structure):
+    """cof_match: one Match of search()'s stream (chrom_chunk.rs:19-29)."""
+    _fields_ = [
+        ("chrom_idx", ctypes.c_uint64),
+        ("text_offset", ctypes.c_uint64),
+        ("record", ctypes.c_uint32),
+        ("pattern_idx", ctypes.c_uint32),
+        ("mismatches", ctypes.c_uint8),
+        ("dna_bulge_size", ctypes.c_uint8),
+        ("rna_bulge_size", ctypes.c_uint8),
+        ("is_forward", ctypes.c_uint8),
+        ("pad", ctypes.c_uint32),
+    ]
+
+
+class _Piece(ctypes.Structure):
+    _fields_ = [
+        ("request", ctypes.c_size_t),
+        ("text", ctypes.c_void_p),
+        ("text_len", ctypes.c_size_t),
+        ("n_rows", ctypes.c_uint64),
+        ("matches", ctypes.POINTER(Match)),
+    ]
+
+
+_SINK = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.POINTER(_Piece))
 
 
 class _ServerConfig(ctypes.Structure):
@@ -112,6 +143,12 @@ def load_library(path=LIB_PATH):
     lib.cof_server_stats.argtypes = [vp, c.POINTER(c.c_uint64)]
     lib.cof_server_free.argtypes = [vp]
     lib.cof_server_free.restype = None
+    lib.cof_search_stream.argtypes = [vp, c.POINTER(_Request), c.c_size_t, c.c_uint32, _SINK,
+                                      vp, c.POINTER(c.c_uint64)]
+    lib.cof_genome_record_name.argtypes = [vp, c.c_uint32]
+    lib.cof_genome_record_name.restype = c.c_char_p
+    lib.cof_genome_n_records.argtypes = [vp]
+    lib.cof_genome_n_records.restype = c.c_uint32
     lib.cof_search_seq_noalloc.argtypes = [c.c_void_p, c.c_uint64, c.c_char_p,
                                            c.POINTER(c.c_char_p), c.c_size_t, c.c_uint32,
                                            c.c_void_p, c.c_uint32, c.POINTER(c.c_uint32),
@@ -215,6 +252,67 @@ class Genome:
     def search_batch(self, requests):
         """Many requests in one pass; returns [(rows_text, n_rows), ...]."""
         return self.run_prepared(self.prepare(requests))
+
+    def search_stream(self, requests, on_piece, matches=False, prepared=None):
+        """cof_search_stream: calls on_piece(request, text_bytes, n_rows,
+        match_list_or_None) for every piece of output, in order, on this
+        thread; a truthy return stops the search (CofError COF_E_CANCELLED).
+        Returns each request's row count.  match_list: (chrom_idx,
+        text_offset, record, pattern_idx, mismatches, dna_bulge_size,
+        rna_bulge_size, is_forward) tuples."""
+        reqs, _keep = prepared if prepared is not None else self.prepare(requests)
+        err = []
+
+        def cb(_user, pp):
+            try:
+                p = pp.contents
+                text = ctypes.string_at(p.text, p.text_len) if p.text_len else b""
+                recs = None
+                if p.matches:
+                    recs = [(m.chrom_idx, m.text_offset, m.record, m.pattern_idx, m.mismatches,
+                             m.dna_bulge_size, m.rna_bulge_size, m.is_forward)
+                            for m in p.matches[:p.n_rows]]
+                return 1 if on_piece(p.request, text, p.n_rows, recs) else 0
+            except BaseException as e:  # noqa: BLE001 -- re-raised after the call
+                err.append(e)
+                return 1
+
+        fn = _SINK(cb)
+        n = (ctypes.c_uint64 * max(len(reqs), 1))()
+        rc = _lib.cof_search_stream(self._h, reqs, len(reqs),
+                                    COF_STREAM_MATCHES if matches else 0, fn, None, n)
+        if err:
+            raise err[0]
+        _check(rc)
+        return [n[i] for i in range(len(reqs))]
+
+    def stream_count(self, prepared, matches=False):
+        """cof_search_stream with a sink that only counts: returns (rows,
+        text bytes, pieces).  The rows pass through page-locked staging
+        buffers and are never held, so the result may exceed host memory."""
+        reqs, _keep = prepared
+        tot = [0, 0, 0]
+
+        def cb(_user, pp):
+            p = pp.contents
+            tot[0] += p.n_rows
+            tot[1] += p.text_len
+            tot[2] += 1
+            return 0
+
+        fn = _SINK(cb)
+        n = (ctypes.c_uint64 * max(len(reqs), 1))()
+        _check(_lib.cof_search_stream(self._h, reqs, len(reqs),
+                                      COF_STREAM_MATCHES if matches else 0, fn, None, n))
+        return tot[0], tot[1], tot[2]
+
+    def record_name(self, record):
+        v = _lib.cof_genome_record_name(self._h, record)
+        return None if v is None else v.decode()
+
+    @property
+    def n_records(self):
+        return _lib.cof_genome_n_records(self._h)
 
     def last_stats(self):
         ms = (ctypes.c_double * 5)()

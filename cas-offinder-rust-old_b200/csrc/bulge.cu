@@ -38,12 +38,17 @@
 
 #include "cof_engine.h"
 #include "engine_dev.cuh"
+#include "textout.h"
 
 namespace cof {
 
 namespace {
 
 constexpr int kMaxCells = 72;          // L <= 64, L + max_db <= 72
+constexpr uint32_t kBulgeSplit = 4;        // candidate chunks of a large surviving set
+constexpr uint32_t kBulgeSplitMin = 1u << 15;  // surviving candidates worth splitting
+constexpr uint32_t kBulgeChunkMax = 1u << 21;  // candidates per chunk at most
+constexpr uint32_t kBulgeProbe = 1u << 18;     // probe chunk of a very large set
 constexpr uint32_t kTile = 1024;       // end positions per filter work item
 constexpr uint32_t kWarmMin = 48;      // Myers warm-up before a tile (>= W - 1)
 constexpr int kSmemMyers = 512;        // patterns whose eq tables fit in smem
@@ -1180,6 +1185,32 @@ mrow_write_kernel(GenomeDev G, const MyersRow *__restrict__ rows,
 
 // One launch of the warp traceback; the work queues are untyped here
 // because the node width is a template parameter.
+// Match records of formatted alignment rows, in text order: the fields of
+// search()'s Match (chrom_chunk.rs:19-29) and the offset of the row's line
+// in its piece, which holds one request's rows from row req_first[request].
+__global__ void mrow_rec_kernel(GenomeDev G, const MyersRow *__restrict__ rows,
+                                const uint32_t *__restrict__ order, uint32_t n,
+                                const MyersPattern *__restrict__ pats,
+                                const MyersReqDev *__restrict__ reqs,
+                                const uint64_t *__restrict__ off,
+                                const uint32_t *__restrict__ req_first,
+                                MatchRec *__restrict__ recs) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const MyersRow w = rows[order[i]];
+        const MyersPattern &P = pats[w.pattern];
+        MatchRec m{};
+        m.chrom_idx = w.pos;
+        m.text_offset = off[i] - off[req_first[P.request]];
+        m.record = G.name_idx[w.chunk];
+        m.pattern_idx = w.pattern - reqs[P.request].first_pattern;
+        m.mismatches = w.mm;
+        m.dna_bulge_size = w.db;
+        m.rna_bulge_size = w.rb;
+        m.is_forward = P.strand == 0;
+        recs[i] = m;
+    }
+}
+
 struct TbLaunch {
     unsigned grid, threads;
     size_t smem;
@@ -1241,24 +1272,10 @@ void build_eq16(const std::string &p, uint32_t eq_lo[16], uint32_t eq_hi[16]) {
     }
 }
 
-// Grows a device byte buffer to hold `need` bytes, keeping its first `used`
-// bytes (capacity at least doubles, so appends stay amortised).
-int grow_keep(DevBuf<char> &b, size_t need, size_t used, cudaStream_t s, Error &err) {
-    if (need <= b.cap) return kOk;
-    const size_t cap = std::max(need, 2 * b.cap);
-    char *p = nullptr;
-    CU(cudaMalloc((void **)&p, cap));
-    if (used) CU(cudaMemcpyAsync(p, b.p, used, cudaMemcpyDeviceToDevice, s));
-    CU(cudaStreamSynchronize(s));
-    if (b.p) cudaFree(b.p);
-    b.p = p;
-    b.cap = cap;
-    return kOk;
-}
-
 }  // namespace
 
-int Engine::run_bulge(const std::vector<Request> &reqs, std::vector<Result> &out, Error &err) {
+int Engine::run_bulge(const std::vector<Request> &reqs, std::vector<Result> &out, Error &err,
+                      const Sink *sink) {
     DeviceGenome &d = *dev_;
     const HostGenome &h = host_;
     const Bit4Tables &t = bit4();
@@ -1464,12 +1481,11 @@ int Engine::run_bulge(const std::vector<Request> &reqs, std::vector<Result> &out
     const uint32_t n_cand = hc.hits;
 
     // stage 2: traceback over candidate chunks; each chunk's rows are sorted
-    // (pattern, start), formatted and appended to the requests' texts
-    // every chunk's rows go to one device text arena; segs = (arena offset,
-    // bytes, request) per chunk and request
-    std::vector<uint64_t> nrows(reqs.size(), 0);
-    std::vector<std::array<uint64_t, 3>> segs;
-    uint64_t arena = 0;
+    // (pattern, start), formatted, and copied to the host on the copy
+    // stream while the next chunk's traceback runs: appended to each
+    // request's result, or handed to the sink of a streamed search
+    TextOut tout(d.copy_stream, sink, out);
+    bool text_out = false;  // a chunk's text has been put
     // rows one chunk may produce; a chunk that produces more is halved and
     // walked again (COF_BULGE_ROW_CAP lowers the cap: tests of that path)
     size_t row_cap = 1u << 24;
@@ -1553,10 +1569,22 @@ int Engine::run_bulge(const std::vector<Request> &reqs, std::vector<Result> &out
         times_.verify_ms += ms;
         cands = d.mcand2.p;
     }
-    // candidates per chunk; COF_BULGE_CHUNK lowers it (tests: many chunks)
-    uint32_t chunk = std::max<uint32_t>(1, std::min<uint32_t>(n_work, 1u << 21));
-    if (const char *e = std::getenv("COF_BULGE_CHUNK"))
+    // candidates per chunk: a large surviving set is split into kBulgeSplit
+    // chunks, so that one chunk's rows cross to the host while the next
+    // chunk's traceback runs; COF_BULGE_CHUNK lowers it (tests: many chunks)
+    // A very large set (hundreds of millions of rows) first walks a probe
+    // chunk; the later chunks are sized from its rows per candidate to fill
+    // most of the row buffer, and a chunk that overflows it is cut in
+    // proportion to its row count and walked again.
+    uint32_t chunk = n_work >= kBulgeSplitMin ? (n_work + kBulgeSplit - 1) / kBulgeSplit : n_work;
+    chunk = std::max<uint32_t>(1, std::min<uint32_t>(chunk, kBulgeChunkMax));
+    bool probe = n_work > 4 * kBulgeProbe;
+    if (probe) chunk = std::min(chunk, kBulgeProbe);
+    if (const char *e = std::getenv("COF_BULGE_CHUNK")) {
         chunk = std::max<uint32_t>(1, std::min<uint32_t>(chunk, (uint32_t)std::max(1, std::atoi(e))));
+        probe = false;
+    }
+    const double row_fill = 0.85 * (double)row_cap;  // rows a sized chunk aims at
     uint32_t c0 = 0;
     while (c0 < n_work) {
         const uint32_t cn = std::min(chunk, n_work - c0);
@@ -1587,6 +1615,8 @@ int Engine::run_bulge(const std::vector<Request> &reqs, std::vector<Result> &out
                 tb_launch(a);
                 CU(cudaGetLastError());
                 ++times_.kernel_launches;
+                // the previous chunk's rows go to the sink beside this traceback
+                if (pass == 0 && tout.streaming() && tout.drain(err)) return err.code;
                 if (last) break;
                 uint32_t n_spill = 0;
                 CU(cudaMemcpyAsync(&n_spill, &d.ctr.p->hits, 4, cudaMemcpyDeviceToHost, s));
@@ -1608,6 +1638,7 @@ int Engine::run_bulge(const std::vector<Request> &reqs, std::vector<Result> &out
         CU(cudaMemcpyAsync(&hc, d.ctr.p, sizeof(Counters), cudaMemcpyDeviceToHost, s));
         std::vector<uint32_t> rq(reqs.size());
         CU(cudaMemcpyAsync(rq.data(), d.req_rows.p, reqs.size() * 4, cudaMemcpyDeviceToHost, s));
+        if (tout.streaming() && tout.drain(err)) return err.code;  // beside this traceback
         CU(cudaStreamSynchronize(s));
         cudaEventElapsedTime(&ms, d.ev[3], d.ev[4]);
         times_.verify_ms += ms;
@@ -1616,10 +1647,19 @@ int Engine::run_bulge(const std::vector<Request> &reqs, std::vector<Result> &out
                 err = {kUnsupported, "one bulge candidate has more alignments than the row buffer"};
                 return err.code;
             }
-            chunk = std::max<uint32_t>(1, cn / 2);
+            // hc.rows counts every alignment of the chunk (the walk goes on
+            // past the buffer): cut the chunk in proportion
+            const uint64_t fit = (uint64_t)((double)cn * row_fill / std::max<double>(hc.rows, row_cap + 1.0));
+            chunk = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(fit, cn / 2));
+            probe = false;
             continue;
         }
         const uint32_t nr = hc.rows;
+        if (probe) {  // size the remaining chunks from the probe's rows per candidate
+            const double per = std::max(1.0, (double)nr) / (double)cn;
+            chunk = (uint32_t)std::max(1.0, std::min((double)kBulgeChunkMax, row_fill / per));
+            probe = false;
+        }
         times_.rows += nr;
         if (nr) {
             CU(cudaEventRecord(d.ev[5], s));
@@ -1640,62 +1680,63 @@ int Engine::run_bulge(const std::vector<Request> &reqs, std::vector<Result> &out
             uint64_t bytes = 0;
             CU(cudaMemcpyAsync(&bytes, d.offs.p + nr, 8, cudaMemcpyDeviceToHost, s));
             CU(cudaStreamSynchronize(s));
-            // each chunk's text starts 16-byte aligned, after the bytes in use
-            const uint64_t in_use = arena;
-            arena = (arena + 15) & ~15ull;
-            if (grow_keep(d.text, arena + bytes + 1, in_use, s, err)) return err.code;
+            // d.text is rewritten below: the previous chunk's copy has run
+            // beside this chunk's traceback and is waited for here
+            if (tout.drain(err)) return err.code;
+            if (d.text.ensure(bytes + 1, err)) return err.code;
             mrow_write_kernel<<<fb, 256, 0, s>>>(d.view(), d.mrows.p, d.vals2.p, nr, dP, dR,
-                                                 d.offs.p, d.text.p + arena);
+                                                 d.offs.p, d.text.p);
             CU(cudaGetLastError());
-            CU(cudaEventRecord(d.ev[6], s));
             times_.kernel_launches += 4;
-            // request boundaries inside this chunk's sorted rows
+            // each request's first row inside this chunk's sorted rows
+            std::vector<uint32_t> first(reqs.size());
+            for (size_t ri = 0, r0 = 0; ri < reqs.size(); r0 += rq[ri], ++ri)
+                first[ri] = (uint32_t)r0;
+            if (tout.records()) {
+                if (d.recs.ensure(nr, err) || d.req_first.ensure(reqs.size(), err)) return err.code;
+                CU(cudaMemcpyAsync(d.req_first.p, first.data(), reqs.size() * 4,
+                                   cudaMemcpyHostToDevice, s));
+                mrow_rec_kernel<<<fb, 256, 0, s>>>(d.view(), d.mrows.p, d.vals2.p, nr, dP, dR,
+                                                   d.offs.p, d.req_first.p, d.recs.p);
+                CU(cudaGetLastError());
+                ++times_.kernel_launches;
+            }
+            CU(cudaEventRecord(d.ev[6], s));
+            CU(cudaEventRecord(d.fmt_done, s));
+            // request boundaries (text bytes) inside this chunk
             std::vector<uint64_t> bound(reqs.size() + 1, bytes);
-            uint64_t r0 = 0;
             for (size_t ri = 0; ri < reqs.size(); ++ri) {
-                bound[ri] = 0;
-                if (r0 < nr) CU(cudaMemcpyAsync(&bound[ri], d.offs.p + r0, 8, cudaMemcpyDeviceToHost, s));
-                else bound[ri] = bytes;
-                r0 += rq[ri];
+                bound[ri] = bytes;
+                if (first[ri] < nr)
+                    CU(cudaMemcpyAsync(&bound[ri], d.offs.p + first[ri], 8, cudaMemcpyDeviceToHost, s));
             }
             CU(cudaStreamSynchronize(s));
             cudaEventElapsedTime(&ms, d.ev[5], d.ev[6]);
             times_.format_ms += ms;
+            const uint64_t done = (uint64_t)c0 + cn;
             for (size_t ri = 0; ri < reqs.size(); ++ri) {
-                if (bound[ri + 1] > bound[ri])
-                    segs.push_back({arena + bound[ri], bound[ri + 1] - bound[ri], (uint64_t)ri});
-                nrows[ri] += rq[ri];
+                const uint64_t b = bound[ri + 1] - bound[ri];
+                if (!rq[ri]) continue;
+                if (!text_out) {  // result size from the first chunk's share of the work
+                    const double f = done >= n_work ? 1.0 : 1.15 * (double)n_work / (double)done;
+                    if (tout.reserve(ri, (size_t)(b * f) + (done >= n_work ? 0 : 65536), err))
+                        return err.code;
+                }
+                if (tout.put(ri, d.text.p + bound[ri], b, rq[ri], d.recs.p + first[ri],
+                             d.fmt_done, err))
+                    return err.code;
             }
-            arena += bytes;
+            text_out = true;
         }
         c0 += cn;
     }
-    // each request's rows go from the arena straight into its own
-    // page-locked result buffer, segment by segment in chunk order
-    std::vector<uint64_t> req_len(reqs.size(), 0), at(reqs.size(), 0);
-    for (const auto &sg : segs) req_len[sg[2]] += sg[1];
-    for (size_t ri = 0; ri < reqs.size(); ++ri) {
-        char *buf = PinnedPool::get().acquire(req_len[ri] + 1);
-        if (!buf) {
-            err = {kOom, "out of page-locked host memory for result text"};
-            return err.code;
-        }
-        out[ri].pooled.p = buf;
-        out[ri].text = buf;
-        out[ri].text_len = req_len[ri];
-        out[ri].n_rows = nrows[ri];
+    // the copy time left after the last chunk's text
+    CU(cudaEventRecord(d.ev[7], d.copy_stream));
+    if (tout.finish(err)) return err.code;
+    if (text_out) {
+        cudaEventElapsedTime(&ms, d.ev[6], d.ev[7]);
+        times_.d2h_ms += std::max(0.0f, ms);
     }
-    CU(cudaEventRecord(d.ev[6], s));
-    for (const auto &sg : segs) {
-        CU(cudaMemcpyAsync(out[sg[2]].pooled.p + at[sg[2]], d.text.p + sg[0], sg[1],
-                           cudaMemcpyDeviceToHost, s));
-        at[sg[2]] += sg[1];
-    }
-    CU(cudaEventRecord(d.ev[7], s));
-    CU(cudaStreamSynchronize(s));
-    cudaEventElapsedTime(&ms, d.ev[6], d.ev[7]);
-    times_.d2h_ms += ms;
-    for (Result &r : out) r.pooled.p[r.text_len] = 0;
     return kOk;
 }
 

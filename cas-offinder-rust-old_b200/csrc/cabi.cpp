@@ -1,4 +1,5 @@
 // cabi.cpp -- extern "C" entry points of libcof.so (declared in include/cof.h).
+#include <cstddef>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -191,6 +192,49 @@ COF_API int cof_search_batch(cof_genome *g, const cof_request *reqs, size_t n_re
 
 COF_API int cof_search(cof_genome *g, const cof_request *req, cof_result *out) {
     return cof_search_batch(g, req, 1, out);
+}
+
+static_assert(sizeof(cof_match) == sizeof(cof::MatchRec) &&
+                  offsetof(cof_match, text_offset) == offsetof(cof::MatchRec, text_offset) &&
+                  offsetof(cof_match, record) == offsetof(cof::MatchRec, record) &&
+                  offsetof(cof_match, mismatches) == offsetof(cof::MatchRec, mismatches) &&
+                  offsetof(cof_match, is_forward) == offsetof(cof::MatchRec, is_forward),
+              "cof_match and the engine's match record differ");
+
+COF_API int cof_search_stream(cof_genome *g, const cof_request *reqs, size_t n_reqs,
+                              uint32_t stream_flags, cof_sink sink, void *user,
+                              uint64_t *n_rows) {
+    if (!g || (!reqs && n_reqs) || !sink) return fail(COF_E_BADINPUT, "null argument");
+    if (stream_flags & ~COF_STREAM_MATCHES) return fail(COF_E_BADINPUT, "unknown stream flag");
+    cof::Error err;
+    std::vector<cof::Request> rq;
+    if (to_requests(reqs, n_reqs, rq, err)) return fail(err);
+    cof::Sink sk;
+    sk.records = (stream_flags & COF_STREAM_MATCHES) != 0;
+    sk.fn = [sink, user](const cof::Piece &p) {
+        cof_piece c;
+        c.request = p.request;
+        c.text = p.text;
+        c.text_len = p.text_len;
+        c.n_rows = p.n_rows;
+        c.matches = reinterpret_cast<const cof_match *>(p.recs);
+        return sink(user, &c);
+    };
+    std::vector<cof::Result> res;
+    std::lock_guard<std::mutex> lk(g->mu);
+    if (g->engine.search(rq, res, err, &sk)) return fail(err);
+    if (n_rows)
+        for (size_t i = 0; i < n_reqs; ++i) n_rows[i] = res[i].n_rows;
+    return COF_OK;
+}
+
+COF_API uint32_t cof_genome_n_records(const cof_genome *g) {
+    return g ? (uint32_t)g->engine.host().names.size() : 0;
+}
+
+COF_API const char *cof_genome_record_name(const cof_genome *g, uint32_t record) {
+    if (!g || record >= g->engine.host().names.size()) return nullptr;
+    return g->engine.host().names[record].c_str();
 }
 
 COF_API void cof_result_free(cof_result *r) {

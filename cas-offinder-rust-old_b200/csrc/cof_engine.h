@@ -6,6 +6,7 @@
 
 #include <cstddef>
 #include <cstdint>
+#include <functional>
 #include <map>
 #include <memory>
 #include <mutex>
@@ -36,6 +37,7 @@ enum Status : int {
     kUnsupported = -5,
     kState = -6,
     kTimeout = -7,
+    kCancelled = -8,
 };
 
 struct Error {
@@ -202,6 +204,34 @@ struct Result {
     PooledText pooled;
 };
 
+// One Match of search()'s stream as plain data (cof_match of include/cof.h,
+// chrom_chunk.rs:19-29): 32 bytes.
+struct MatchRec {
+    uint64_t chrom_idx;    // position of the site's first cell in its record
+    uint64_t text_offset;  // this match's line in its piece's text
+    uint32_t record;       // record (name) index
+    uint32_t pattern_idx;  // index in the request's full pattern list
+    uint8_t mismatches, dna_bulge_size, rna_bulge_size, is_forward;
+    uint32_t pad;
+};
+static_assert(sizeof(MatchRec) == 32, "MatchRec is cof_match");
+
+// A piece of one request's output, handed to a streaming caller: rows (or
+// raw Match lines) in the order of the request's result, valid only during
+// the call.
+struct Piece {
+    size_t request = 0;
+    const char *text = nullptr;
+    size_t text_len = 0;
+    uint64_t n_rows = 0;
+    const MatchRec *recs = nullptr;  // n_rows records when Sink::records
+};
+// Receiver of a streamed search; a nonzero return stops the search.
+struct Sink {
+    std::function<int(const Piece &)> fn;
+    bool records = false;  // pieces carry MatchRec records
+};
+
 // Per-stage device timings of the last search (milliseconds, CUDA events).
 struct StageTimes {
     double scan_ms = 0, verify_ms = 0, format_ms = 0, d2h_ms = 0, total_ms = 0;
@@ -243,15 +273,20 @@ class Engine {
     const HostGenome &host() const { return host_; }
     bool uploaded() const { return dev_ != nullptr; }
     int upload(Error &err);
-    int search(const std::vector<Request> &reqs, std::vector<Result> &out, Error &err);
+    // With a sink, the rows are handed to it piece by piece and `out` only
+    // receives each request's row count.
+    int search(const std::vector<Request> &reqs, std::vector<Result> &out, Error &err,
+               const Sink *sink = nullptr);
     int free_device_bytes(uint64_t *free_bytes, Error &err);
     const StageTimes &last_times() const { return times_; }
     Tuner &tuner() { return tuner_; }
     int device() const { return device_; }
 
   private:
-    int run_popcount(const std::vector<Request> &reqs, std::vector<Result> &out, Error &err);
-    int run_bulge(const std::vector<Request> &reqs, std::vector<Result> &out, Error &err);
+    int run_popcount(const std::vector<Request> &reqs, std::vector<Result> &out, Error &err,
+                     const Sink *sink);
+    int run_bulge(const std::vector<Request> &reqs, std::vector<Result> &out, Error &err,
+                  const Sink *sink);
     int run_raw(const Request &req, Result &out, Error &err);
     int device_;
     uint64_t slice_text_hint_ = 0;  // bytes of the last sliced result (+2 %)

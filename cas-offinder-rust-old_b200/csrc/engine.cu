@@ -40,6 +40,7 @@
 
 #include "cof_engine.h"
 #include "engine_dev.cuh"
+#include "textout.h"
 
 namespace cof {
 
@@ -823,6 +824,31 @@ row_write_kernel(GenomeDev G, const Row *__restrict__ rows, const uint32_t *__re
     }
 }
 
+// Match records of formatted rows, in text order (row i of the sorted
+// order): the fields of search()'s Match (chrom_chunk.rs:19-29) and the
+// offset of the row's line in its piece, which holds the rows of one request
+// from row req_first[request] on.
+__global__ void row_rec_kernel(GenomeDev G, const Row *__restrict__ rows,
+                               const uint32_t *__restrict__ order, uint32_t n,
+                               const ExactPattern *__restrict__ pats,
+                               const RequestDev *__restrict__ reqs,
+                               const uint64_t *__restrict__ off,
+                               const uint32_t *__restrict__ req_first, MatchRec *__restrict__ recs) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const Row w = rows[order[i]];
+        const ExactPattern &P = pats[w.pattern];
+        const RequestDev &R = reqs[P.request];
+        MatchRec m{};
+        m.chrom_idx = w.pos;
+        m.text_offset = off[i] - off[req_first[P.request]];
+        m.record = G.name_idx[w.chunk];
+        m.pattern_idx = w.pattern - R.first_pattern;
+        m.mismatches = (uint8_t)w.mm;
+        m.is_forward = P.strand == 0;
+        recs[i] = m;
+    }
+}
+
 // ---------------------------------------------------------------------------
 // device genome + scratch
 // ---------------------------------------------------------------------------
@@ -939,7 +965,8 @@ int Engine::free_device_bytes(uint64_t *free_bytes, Error &err) {
     return kOk;
 }
 
-int Engine::search(const std::vector<Request> &reqs, std::vector<Result> &out, Error &err) {
+int Engine::search(const std::vector<Request> &reqs, std::vector<Result> &out, Error &err,
+                   const Sink *sink) {
     times_ = StageTimes();
     out.clear();
     out.resize(reqs.size());
@@ -962,6 +989,21 @@ int Engine::search(const std::vector<Request> &reqs, std::vector<Result> &out, E
             // search()'s raw stream: every window, no PAM prefilter
             if (run_raw(reqs[i], out[i], err)) return err.code;
             if (out[i].text) out[i].text = out[i].owned.data();
+            if (sink) {  // one piece, without match records
+                Piece pc;
+                pc.request = i;
+                pc.text = out[i].text ? out[i].text : "";
+                pc.text_len = out[i].text_len;
+                pc.n_rows = out[i].n_rows;
+                if (sink->fn(pc)) {
+                    err = {kCancelled, "the result sink stopped the search"};
+                    return err.code;
+                }
+                out[i].owned.clear();
+                out[i].owned.shrink_to_fit();
+                out[i].text = nullptr;
+                out[i].text_len = 0;
+            }
             continue;
         }
         if (reqs[i].max_db || reqs[i].max_rb) {
@@ -972,15 +1014,28 @@ int Engine::search(const std::vector<Request> &reqs, std::vector<Result> &out, E
             pr.push_back(reqs[i]);
         }
     }
+    // a path sees its own requests; the sink hears the caller's indices
+    auto sub_sink = [&](const std::vector<size_t> &idx, Sink &sub) -> const Sink * {
+        if (!sink) return nullptr;
+        sub.records = sink->records;
+        sub.fn = [sink, &idx](const Piece &p) {
+            Piece q = p;
+            q.request = idx[p.request];
+            return sink->fn(q);
+        };
+        return &sub;
+    };
     if (!pr.empty()) {
         std::vector<Result> po;
-        if (run_popcount(pr, po, err)) return err.code;
+        Sink sub;
+        if (run_popcount(pr, po, err, sub_sink(pi, sub))) return err.code;
         for (size_t k = 0; k < pi.size(); ++k) out[pi[k]] = std::move(po[k]);
     }
     if (!br.empty()) {
         std::vector<Result> bo;
-        if (run_bulge(br, bo, err)) return err.code;
-        for (size_t k = 0; k < bi.size(); ++k) out[bi[k]] = std::move(bo[k]);  // views
+        Sink sub;
+        if (run_bulge(br, bo, err, sub_sink(bi, sub))) return err.code;
+        for (size_t k = 0; k < bi.size(); ++k) out[bi[k]] = std::move(bo[k]);
     }
     CU(cudaEventRecord(d.ev[9], d.stream));
     CU(cudaEventSynchronize(d.ev[9]));
@@ -991,7 +1046,8 @@ int Engine::search(const std::vector<Request> &reqs, std::vector<Result> &out, E
     return kOk;
 }
 
-int Engine::run_popcount(const std::vector<Request> &reqs, std::vector<Result> &out, Error &err) {
+int Engine::run_popcount(const std::vector<Request> &reqs, std::vector<Result> &out, Error &err,
+                         const Sink *sink) {
     out.clear();
     out.resize(reqs.size());
     DeviceGenome &d = *dev_;
@@ -1419,6 +1475,9 @@ int Engine::run_popcount(const std::vector<Request> &reqs, std::vector<Result> &
     // candidate list if the scan overflowed.  n_rows and the rows per
     // request come back.
     Counters hc{};
+    // runs while a scan is on the device, just before the host waits for it
+    // (a streamed search hands the previous slice's rows to its sink here)
+    std::function<int()> before_wait;
     auto scan_verify = [&](const ScanVariant *v, const SliceTab *sl, uint32_t &n_rows,
                            std::vector<uint32_t> &req_rows) -> int {
         for (int attempt = 0; attempt < 2; ++attempt) {
@@ -1449,6 +1508,7 @@ int Engine::run_popcount(const std::vector<Request> &reqs, std::vector<Result> &
             req_rows.assign(reqs.size(), 0);
             CU(cudaMemcpyAsync(req_rows.data(), d.req_rows.p, reqs.size() * 4,
                                cudaMemcpyDeviceToHost, s));
+            if (before_wait && before_wait()) return err.code;
             CU(cudaStreamSynchronize(s));
             if (!hc.overflow && hc.hits <= d.hits.cap) break;
             if (attempt == 1) {
@@ -1506,6 +1566,23 @@ int Engine::run_popcount(const std::vector<Request> &reqs, std::vector<Result> &
                                             (const RequestDev *)tab(o_rdev), d.offs.p, d.text.p);
         CU(cudaGetLastError());
         times_.kernel_launches += 4;
+        return kOk;
+    };
+
+    // match records of the n_rows formatted rows (streamed searches that ask
+    // for them); first[r]: the first sorted row of request r in this piece
+    auto write_records = [&](uint32_t n_rows, const std::vector<uint32_t> &first) -> int {
+        if (!n_rows) return kOk;
+        if (d.recs.ensure(n_rows, err) || d.req_first.ensure(first.size(), err)) return err.code;
+        CU(cudaMemcpyAsync(d.req_first.p, first.data(), first.size() * 4, cudaMemcpyHostToDevice,
+                           s));
+        const unsigned fb = (unsigned)std::min<uint64_t>((n_rows + 255) / 256, (uint64_t)d.n_sm * 8);
+        row_rec_kernel<<<fb, 256, 0, s>>>(d.view(), d.rows.p, d.vals2.p, n_rows,
+                                          (const ExactPattern *)tab(o_ep),
+                                          (const RequestDev *)tab(o_rdev), d.offs.p,
+                                          d.req_first.p, d.recs.p);
+        CU(cudaGetLastError());
+        ++times_.kernel_launches;
         return kOk;
     };
 
@@ -1597,6 +1674,13 @@ int Engine::run_popcount(const std::vector<Request> &reqs, std::vector<Result> &
             return kOk;
         };
         times_.slices = (int)slices.size();
+        // a streamed search: each slice's rows are one piece, handed to the
+        // sink while the next slice scans
+        std::unique_ptr<TextOut> tout;
+        if (sink) {
+            tout.reset(new TextOut(d.copy_stream, sink, out));
+            before_wait = [&]() { return tout->drain(err); };
+        }
         for (size_t j = 0; j < slices.size(); ++j) {
             uint32_t nr = 0;
             std::vector<uint32_t> rq;
@@ -1607,6 +1691,7 @@ int Engine::run_popcount(const std::vector<Request> &reqs, std::vector<Result> &
             }
             auto before_write = [&](uint64_t bytes) -> int {
                 // d.text still feeds the previous slice's copy
+                if (tout) return tout->drain(err);
                 if (copy_pending) CU(cudaEventSynchronize(d.copy_done));
                 size_t need = host_off + bytes + 1;
                 if (need > hcap)  // room for the rest at this slice's rate (+20 %)
@@ -1617,8 +1702,15 @@ int Engine::run_popcount(const std::vector<Request> &reqs, std::vector<Result> &
             };
             uint64_t tb = 0;
             if (format_rows(nr, tb, before_write)) return err.code;
+            if (tout && tout->records() && write_records(nr, {0u})) return err.code;
             CU(cudaEventRecord(d.ev[4], s));
             rows_total += nr;
+            if (tout) {
+                CU(cudaEventRecord(d.fmt_done, s));
+                if (tout->put(0, d.text.p, tb, nr, d.recs.p, d.fmt_done, err)) return err.code;
+                copy_pending = tb != 0;
+                continue;
+            }
             if (tb) {
                 CU(cudaEventRecord(d.fmt_done, s));
                 CU(cudaStreamWaitEvent(d.copy_stream, d.fmt_done, 0));
@@ -1629,6 +1721,7 @@ int Engine::run_popcount(const std::vector<Request> &reqs, std::vector<Result> &
                 host_off += tb;
             }
         }
+        before_wait = nullptr;
         CU(cudaEventRecord(d.ev[5], d.copy_stream));
         CU(cudaStreamSynchronize(d.copy_stream));
         CU(cudaStreamSynchronize(s));
@@ -1638,6 +1731,7 @@ int Engine::run_popcount(const std::vector<Request> &reqs, std::vector<Result> &
             cudaEventElapsedTime(&ms, d.ev[4], d.ev[5]);
             times_.d2h_ms += std::max(0.0f, ms);
         }
+        if (tout) return tout->finish(err);
         if (reserve(host_off + 1)) return err.code;
         hbuf.p[host_off] = 0;
         out[0].text = hbuf.p;
@@ -1677,6 +1771,30 @@ int Engine::run_popcount(const std::vector<Request> &reqs, std::vector<Result> &
         }
         CU(cudaStreamSynchronize(s));
         for (size_t ri = 0; ri < reqs.size(); ++ri) tend[ri] = hb[ri];
+    }
+    if (sink) {
+        // a streamed search: each request's rows are one piece
+        TextOut tout(d.copy_stream, sink, out);
+        std::vector<uint32_t> first(reqs.size());
+        for (size_t ri = 0, r = 0; ri < reqs.size(); r += req_rows[ri], ++ri)
+            first[ri] = (uint32_t)r;
+        if (tout.records() && write_records(n_rows, first)) return err.code;
+        CU(cudaEventRecord(d.fmt_done, s));
+        uint64_t t0 = 0;
+        for (size_t ri = 0; ri < reqs.size(); ++ri) {
+            if (tout.put(ri, d.text.p + t0, tend[ri] - t0, req_rows[ri], d.recs.p + first[ri],
+                         d.fmt_done, err))
+                return err.code;
+            t0 = tend[ri];
+        }
+        CU(cudaEventRecord(d.ev[5], d.copy_stream));
+        if (tout.finish(err)) return err.code;
+        float ms;
+        cudaEventElapsedTime(&ms, d.ev[6], d.ev[4]);
+        times_.format_ms += ms;
+        cudaEventElapsedTime(&ms, d.ev[4], d.ev[5]);
+        times_.d2h_ms += std::max(0.0f, ms);
+        return kOk;
     }
     uint64_t r0 = 0, t0 = 0;
     for (size_t ri = 0; ri < reqs.size(); ++ri) {

@@ -220,6 +220,8 @@ class DeviceGenome {
     DevBuf<MyersCand> mcand, mcand2;
     DevBuf<MyersRow> mrows;
     DevBuf<unsigned char> tb_items;  // two queues of handed-on traceback subtrees
+    DevBuf<MatchRec> recs;           // match records of a streamed piece
+    DevBuf<uint32_t> req_first;      // first sorted row of each request in a piece
 
     ~DeviceGenome() {
         bit4.release(); planes.release(); boff.release(); start.release(); end.release();
@@ -227,7 +229,7 @@ class DeviceGenome {
         hits.release(); rows.release(); keys.release(); keys2.release(); offs.release();
         vals.release(); vals2.release(); lens.release(); req_rows.release(); ctr.release();
         text.release(); cub_tmp.release(); mcand.release(); mcand2.release(); mrows.release();
-        tb_items.release();
+        tb_items.release(); recs.release(); req_first.release();
         for (auto &e : ev)
             if (e) cudaEventDestroy(e);
         if (fmt_done) cudaEventDestroy(fmt_done);

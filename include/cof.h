@@ -50,6 +50,7 @@ extern "C" {
 #define COF_E_UNSUPPORTED (-5) /* valid input outside this build's limits  */
 #define COF_E_STATE (-6)       /* call order (e.g. add_chunk after upload) */
 #define COF_E_TIMEOUT (-7)     /* a bounded device wait gave up            */
+#define COF_E_CANCELLED (-8)   /* a result sink stopped the search         */
 
 /* Request flags. */
 #define COF_F_ADD_REVCOMP 1u   /* patterns are user patterns; append their
@@ -128,7 +129,8 @@ typedef struct {
 /* Output of one request: the writer's rows (main.rs:130-245) without the
  * header line, '\n'-terminated.  Popcount rows are ordered by genome
  * position, then by pattern (the order of cof_request.patterns, then their
- * reverse complements); bulge rows by pattern, then position.  The
+ * reverse complements); bulge rows by pattern, then position, within each
+ * candidate chunk (a large result is walked in several chunks).  The
  * reference's order is unspecified; compare sorted. */
 typedef struct {
     char *text;
@@ -153,6 +155,68 @@ COF_API int cof_search_batch(cof_genome *g, const cof_request *reqs, size_t n_re
                              cof_result *outs);
 
 COF_API void cof_result_free(cof_result *r);
+
+/* Streamed results: search()'s `dest: SyncSender<Vec<Match>>` channel
+ * (search.rs:1490-1500), through which the reference hands batches of
+ * matches to the writer thread while the search runs (the Myers host emits
+ * them per sub-range, search.rs:1106-1168).  Instead of one whole-result
+ * buffer per request, the rows reach a callback piece by piece -- a
+ * popcount genome slice, a bulge candidate chunk, or one request's rows of
+ * a pass -- while the GPU works on the next piece, so a result may be far
+ * larger than host memory.  Host memory in use stays at a few pieces. */
+
+/* One Match (cas-offinder-lib/src/chrom_chunk.rs:19-29) as plain data,
+ * 32 bytes.  The dna and rna strings of the Match are the fields of its
+ * line in the piece's text: columns 2 and 3 of a row, 8 and 9 of a raw
+ * Match line. */
+typedef struct {
+    uint64_t chrom_idx;      /* Match.chrom_idx: position of the site's first
+                                cell in its record (the writer prints
+                                chrom_idx + pam_len - 1 - db for '-' rows,
+                                main.rs:229-236) */
+    uint64_t text_offset;    /* byte offset of this match's line in the
+                                piece's text */
+    uint32_t record;         /* record index (cof_genome_record_name) */
+    uint32_t pattern_idx;    /* Match.pattern_idx: index into the request's
+                                full pattern list (forward, then reverse) */
+    uint8_t mismatches;      /* Match.mismatches (the writer's recount) */
+    uint8_t dna_bulge_size;  /* Match.dna_bulge_size */
+    uint8_t rna_bulge_size;  /* Match.rna_bulge_size */
+    uint8_t is_forward;      /* Match.is_forward */
+    uint32_t pad;
+} cof_match;
+
+/* A piece of one request's output, in the order of that request's
+ * cof_search text: concatenating a request's pieces gives its cof_search
+ * text (for the bulge path, whose row order depends on candidate order,
+ * the same rows).  text and matches are valid only during the callback. */
+typedef struct {
+    size_t request;             /* index into the call's request array */
+    const char *text;           /* rows (or raw Match lines), each ending '\n' */
+    size_t text_len;
+    uint64_t n_rows;
+    const cof_match *matches;   /* n_rows records in text order with
+                                   COF_STREAM_MATCHES, else NULL (always NULL
+                                   for the popcount path's raw stream) */
+} cof_piece;
+
+/* Receives each piece on the calling thread; a nonzero return stops the
+ * search, which then returns COF_E_CANCELLED. */
+typedef int (*cof_sink)(void *user, const cof_piece *piece);
+
+#define COF_STREAM_MATCHES 1u  /* pieces carry cof_match records */
+
+/* cof_search_batch with results streamed to `sink`.  n_rows (nullable, n_reqs
+ * entries) receives each request's row count. */
+COF_API int cof_search_stream(cof_genome *g, const cof_request *reqs, size_t n_reqs,
+                              uint32_t stream_flags, cof_sink sink, void *user,
+                              uint64_t *n_rows);
+
+/* Name of record `record` (cof_match.record): the FASTA header line after
+ * '>' or the .2bit sequence name (Match.chr_name); NULL if out of range.
+ * Valid while the genome lives. */
+COF_API const char *cof_genome_record_name(const cof_genome *g, uint32_t record);
+COF_API uint32_t cof_genome_n_records(const cof_genome *g);
 
 /* Continuous-batching request server over a resident genome.  No reference
  * counterpart.  A worker thread repeatedly admits queued requests in arrival
@@ -246,7 +310,7 @@ COF_API int cof_genome_tuning(cof_genome *g, char *buf, size_t len);
 COF_API const char *cof_last_error(void);
 
 /* ABI version of this header. */
-#define COF_ABI_VERSION 1
+#define COF_ABI_VERSION 2
 COF_API int cof_abi_version(void);
 
 #ifdef __cplusplus

@@ -24,7 +24,7 @@ def test_exports_every_declared_symbol(cof_mod):
     for n in names:
         assert hasattr(lib, n), n
     assert set(names) == set(cof_mod.EXPORTS)
-    assert lib.cof_abi_version() == 1
+    assert lib.cof_abi_version() == 2
 
 
 def test_nm_dynamic_symbols(cof_mod):
@@ -43,6 +43,20 @@ def test_host_loader_matches_oracle(cof_mod, oracle_mod, golden):
         o = oracle_mod.OracleGenome(path)
         assert g.n_chunks == o.n_chunks == 13
         assert g.n_nucl == o.n_nucl == 12507
+
+
+def test_record_names(cof_mod, oracle_mod, golden):
+    # cof_match.record indexes the genome's record names (Match.chr_name)
+    for name in ("upstream1000.fa", "upstream1000.2bit"):
+        path = os.path.join(golden, name)
+        g = cof_mod.Genome(path)
+        want = []
+        for nm, _d, s, _e in oracle_mod.OracleGenome(path).chunks():
+            if s == 0:
+                want.append(nm)
+        assert g.n_records == len(want) > 1
+        assert [g.record_name(i) for i in range(g.n_records)] == want
+        assert g.record_name(g.n_records) is None
 
 
 def test_fasta_index_matches_oracle(cof_mod, oracle_mod, tmp_path):
