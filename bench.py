@@ -64,6 +64,8 @@ def parse():
                     help="CPU baseline and --impl reference: the genome slice is this many "
                          "4.19 Mnt batches per host thread (about 1 s each at 100 guides)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-few-guide", action="store_true",
+                    help="skip the 1-guide scan measurement (few_guide)")
     ap.add_argument("--no-ref-gpu", action="store_true",
                     help="--impl reference: skip timing the reference's own GPU kernel")
     ap.add_argument("--serving-requests", type=int, default=64)
@@ -218,6 +220,47 @@ def bench_mixed_pam(g, n_nt, steps):
     return {"workload": "50 x (25 nt + NNGRRT) + 50 x (TTTN + 25 nt), mm<=6, same genome",
             "batched_value": work / (b * 1e-3), "plain_value": work / (p * 1e-3),
             "unit": UNIT, "batched_ms": b, "plain_ms": p, "speedup": p / b}
+
+
+def bench_few_guide(g, cfg, steps, guides=1, max_mm=3):
+    """The few-guide end of the scan on the resident genome: `guides` of the
+    workload's guides (20 nt + NRG) at mm <= max_mm, the reference's
+    1-guide NRG row (README.md:73).  Here the comparisons are few and the
+    scan's bound is the plane reads: 0.375 B per nucleotide (H, L and S
+    bits) of algorithmic traffic, so the line reports the scan's achieved
+    GB/s against the measured HBM copy bandwidth.  value = Gbp*guides /
+    device time of the search; e2e = the same over the C-ABI call."""
+    req = dict(search_filter=cfg["filter"], patterns=cfg["patterns"][:guides],
+               max_mismatches=max_mm)
+    prep = g.prepare([req])
+    for _ in range(3):
+        g.run_prepared(prep, as_text=None)
+    stats, wall = [], []
+    for _ in range(steps):
+        t0 = time.perf_counter()
+        (nbytes, rows), = g.run_prepared(prep, as_text=None)
+        wall.append(time.perf_counter() - t0)
+        stats.append(g.last_stats())
+    n_nt = cfg["genome"].n_nucl
+    scan = statistics.median(s["scan_ms"] for s in stats)
+    dev = statistics.median(s["scan_ms"] + s["verify_ms"] + s["format_ms"] for s in stats)
+    w = statistics.median(wall)
+    hbm, kind = hbm_peak()
+    plane_bytes = n_nt * 0.375
+    achieved = plane_bytes / (scan * 1e-3) / 1e9
+    units = n_nt * 1e-9 * guides
+    return {"workload": f"{n_nt / 1e9:.1f} Gbp x {guides} guide (20 nt + NRG), mm<={max_mm}",
+            "value": units / (dev * 1e-3), "unit": UNIT, "device_ms": dev,
+            "e2e": {"value": units / w, "unit": UNIT, "ms_per_step": w * 1e3,
+                    "d2h_bytes_per_step": nbytes},
+            "scan_ms": scan, "scan_tile_shape": g.tuning()["last"],
+            "kernel": scan_kernel_name(g.tuning()["last"]),
+            "hbm_gbs_achieved": achieved, "hbm_peak_gbs": hbm, "hbm_peak_kind": kind,
+            "hbm_frac": achieved / hbm,
+            "algorithmic_bytes": plane_bytes,
+            "note": "algorithmic bytes = 0.375 B/nt of H/L/S planes, read once for both "
+                    "strands; hbm_frac = achieved / the measured copy bandwidth",
+            "rows_per_step": rows, "steps": steps}
 
 
 def serving_requests(n, seed=5, max_guides=500, max_mm=4):
@@ -430,6 +473,13 @@ def bench_bulge_full(cof, device, steps, scale=1.0, cpu_nt=2_000_000):
                   f"CPU path (check_pam_quick, Myers sweep, traceback_all, classify, writer), "
                   f"{os.cpu_count()} threads, {tc:.1f} s, {crow} rows"}
     return out
+
+
+def scan_kernel_name(shape):
+    """The scan kernel a tile shape name (cof_genome_tuning "last") runs."""
+    if shape.startswith("pair-"):
+        return "scan_pair_kernel"
+    return "scan_warp_kernel" if shape.startswith("warp-") else "scan_kernel"
 
 
 def bulge_rates(cfg, stats, rows):
@@ -760,8 +810,7 @@ def main():
                 "h2d_bytes_per_step": 100 * 23 * 2 + 4096,
                 "d2h_bytes_per_step": text_bytes},
         "roofline": {"bound": "alu",
-                     "kernel": "scan_warp_kernel" if g.tuning()["last"].startswith("warp-")
-                               else "scan_kernel",
+                     "kernel": scan_kernel_name(g.tuning()["last"]),
                      "achieved": achieved, "peak": peaks["popc_per_s"], "unit": "pairs/s",
                      "frac": achieved / peaks["popc_per_s"], "traffic": TRAFFIC,
                      "peak_kind": "measured live: POPC results/s of this GPU (XU pipe); "
@@ -779,6 +828,8 @@ def main():
         "genome_upload_s": t_upload, "genome_generate_s": t_gen,
         "clocks": clk,
     }
+    if world == 1 and not args.no_few_guide:
+        line["few_guide"] = bench_few_guide(g, cfg, max(5, args.steps))
     if not args.no_extras and world == 1:
         line["batched_mixed_pam"] = bench_mixed_pam(g, n_nt, max(3, args.steps // 2))
         line["serving"] = bench_serving(cof, g, n_nt, args.serving_requests, args.serving_rate)

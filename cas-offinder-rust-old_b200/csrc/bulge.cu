@@ -45,8 +45,6 @@ namespace cof {
 namespace {
 
 constexpr int kMaxCells = 72;          // L <= 64, L + max_db <= 72
-constexpr uint32_t kBulgeSplit = 4;        // candidate chunks of a large surviving set
-constexpr uint32_t kBulgeSplitMin = 1u << 15;  // surviving candidates worth splitting
 constexpr uint32_t kBulgeChunkMax = 1u << 21;  // candidates per chunk at most
 constexpr uint32_t kBulgeProbe = 1u << 18;     // probe chunk of a very large set
 constexpr uint32_t kTile = 1024;       // end positions per filter work item
@@ -1569,15 +1567,16 @@ int Engine::run_bulge(const std::vector<Request> &reqs, std::vector<Result> &out
         times_.verify_ms += ms;
         cands = d.mcand2.p;
     }
-    // candidates per chunk: a large surviving set is split into kBulgeSplit
-    // chunks, so that one chunk's rows cross to the host while the next
-    // chunk's traceback runs; COF_BULGE_CHUNK lowers it (tests: many chunks)
-    // A very large set (hundreds of millions of rows) first walks a probe
-    // chunk; the later chunks are sized from its rows per candidate to fill
-    // most of the row buffer, and a chunk that overflows it is cut in
-    // proportion to its row count and walked again.
-    uint32_t chunk = n_work >= kBulgeSplitMin ? (n_work + kBulgeSplit - 1) / kBulgeSplit : n_work;
-    chunk = std::max<uint32_t>(1, std::min<uint32_t>(chunk, kBulgeChunkMax));
+    // candidates per chunk; a chunk's rows cross to the host while the next
+    // chunk's traceback runs.  COF_BULGE_CHUNK lowers it (tests: many
+    // chunks).  Every chunk ends in a tail of a few long trees, so a set
+    // that fits one chunk is walked whole (splitting the 10 Mbp benchmark
+    // into four chunks to hide its copy made the traceback 9 ms slower
+    // than the copy it hid).  A very large set (hundreds of millions of
+    // rows) first walks a probe chunk; the later chunks are sized from its
+    // rows per candidate to fill most of the row buffer, and a chunk that
+    // overflows it is cut in proportion to its row count and walked again.
+    uint32_t chunk = std::max<uint32_t>(1, std::min<uint32_t>(n_work, kBulgeChunkMax));
     bool probe = n_work > 4 * kBulgeProbe;
     if (probe) chunk = std::min(chunk, kBulgeProbe);
     if (const char *e = std::getenv("COF_BULGE_CHUNK")) {
@@ -1615,8 +1614,8 @@ int Engine::run_bulge(const std::vector<Request> &reqs, std::vector<Result> &out
                 tb_launch(a);
                 CU(cudaGetLastError());
                 ++times_.kernel_launches;
-                // the previous chunk's rows go to the sink beside this traceback
-                if (pass == 0 && tout.streaming() && tout.drain(err)) return err.code;
+                // pieces whose copies are done go to the sink beside this pass
+                if (tout.poll(err)) return err.code;
                 if (last) break;
                 uint32_t n_spill = 0;
                 CU(cudaMemcpyAsync(&n_spill, &d.ctr.p->hits, 4, cudaMemcpyDeviceToHost, s));
@@ -1638,7 +1637,7 @@ int Engine::run_bulge(const std::vector<Request> &reqs, std::vector<Result> &out
         CU(cudaMemcpyAsync(&hc, d.ctr.p, sizeof(Counters), cudaMemcpyDeviceToHost, s));
         std::vector<uint32_t> rq(reqs.size());
         CU(cudaMemcpyAsync(rq.data(), d.req_rows.p, reqs.size() * 4, cudaMemcpyDeviceToHost, s));
-        if (tout.streaming() && tout.drain(err)) return err.code;  // beside this traceback
+        if (tout.poll(err)) return err.code;  // beside this traceback
         CU(cudaStreamSynchronize(s));
         cudaEventElapsedTime(&ms, d.ev[3], d.ev[4]);
         times_.verify_ms += ms;

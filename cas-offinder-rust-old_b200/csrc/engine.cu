@@ -167,18 +167,40 @@ constexpr int kSmemPatterns = 2048;    // patterns staged in shared memory
 constexpr int kMaxSegs = 64;
 
 
+// The two strand groups of one filter (or one group alone) scanned by one
+// work item: their windows come from the same plane words, so each tile's
+// words are loaded and its place resolved once for both.  g[1] = ~0u for a
+// group scanned alone.
+struct ScanPair {
+    uint32_t g[2];
+    uint32_t seg_begin, seg_end;  // PairSeg range
+};
+
+// One batch of a pair: each group's range of shifted window starts, and the
+// tiles of their union.
+struct PairSeg {
+    uint64_t lo[2], hi[2];
+    uint64_t base;        // batch base + 32 (the same for both groups)
+    uint64_t w0;          // first plane word of the union
+    uint64_t tile_begin;  // prefix count of 1024-start tiles within the pair
+    uint32_t batch, pad;
+};
+
 struct ScanParams {
     const uint32_t *H, *L, *S;
     const ScanGroup *groups;
     const ScanSeg *segs;
     const FastPattern *pats;
-    const uint64_t *item_begin;  // per group: first work item; [n_groups] = total
+    const uint64_t *item_begin;  // per group (pair): first work item; [n] = total
     uint32_t n_groups;
     uint32_t span_tiles;         // 1024-start tiles per work item
     uint32_t n_pats;             // patterns of all groups (the table at pats)
     Hit *hits;
     uint32_t hit_cap;
     Counters *ctr;
+    const ScanPair *pairs;       // scan_pair_kernel: work items over pairs
+    const PairSeg *psegs;
+    uint32_t n_pairs;
 };
 
 // Compares the first n <= 32 x CPT queued windows with every pattern of the
@@ -604,6 +626,235 @@ scan_warp_kernel(ScanParams P) {
     }
 }
 
+// ---------------------------------------------------------------------------
+// scan of strand pairs (few patterns per group)
+// ---------------------------------------------------------------------------
+
+// Queued windows of a pair carry the groups whose PAM they passed in bits
+// 30 (first group) and 31 (second) of their start; starts stay below 2^30
+// (checked on the host before pairs are used).
+constexpr uint32_t kPairTagShift = 30;
+constexpr uint32_t kPairStartMask = (1u << kPairTagShift) - 1u;
+
+// Compares the first n queued windows of a pair with the patterns of both
+// groups; a window meets a group's patterns only if it passed that group's
+// PAM prefilter (its tag bit).
+template <int kCpt>
+__device__ __noinline__ void flush_pair(const uint4 *q, int n, const FastPattern *spat,
+                                        uint32_t n_staged, const ScanGroup *Gp0,
+                                        const ScanGroup *Gp1, uint32_t batch,
+                                        const ScanParams &P, int lane) {
+    const uint32_t spat_s = (uint32_t)__cvta_generic_to_shared(spat);
+    for (int gi = 0; gi < 2; ++gi) {
+        const ScanGroup *Gp = gi ? Gp1 : Gp0;
+        if (!Gp) break;
+        const uint32_t tag = 1u << (kPairTagShift + gi);
+        const uint32_t pb = Gp->pat_begin, n_class = Gp->n_class;
+        const bool smem = Gp->pat_end <= n_staged;
+        for (uint32_t c = 0; c < n_class; ++c) {
+            const CareClass K = Gp->cls[c];
+            uint32_t mh[kCpt], ml[kCpt], ms[kCpt];
+            bool any = false;
+#pragma unroll
+            for (int j = 0; j < kCpt; ++j) {
+                const int idx = lane + 32 * j;
+                const uint4 e = idx < n ? q[idx] : make_uint4(0, 0, 0, 0);
+                const bool on = (e.x & tag) != 0;
+                any |= on;
+                mh[j] = e.y & K.care;
+                ml[j] = e.z & K.care;
+                ms[j] = on ? (e.w & K.care) : 0xFFFFFFFFu;
+            }
+            if (!__any_sync(0xFFFFFFFFu, any)) continue;
+            for (uint32_t p = pb + K.pat_begin; p < pb + K.pat_end; ++p) {
+                const FastPattern f = smem ? lds_pattern(spat_s + p * (uint32_t)sizeof(FastPattern))
+                                           : P.pats[p];
+                int c3[kCpt];
+#pragma unroll
+                for (int j = 0; j < kCpt; ++j)
+                    c3[j] = (int)__popc((mh[j] ^ f.h) | (ml[j] ^ f.l) | ms[j]);
+#pragma unroll
+                for (int w = 1; w < kCpt; w *= 3)
+#pragma unroll
+                    for (int j = 0; j < kCpt; j += 3 * w)
+                        c3[j] = j + 2 * w < kCpt ? __vimin3_s32(c3[j], c3[j + w], c3[j + 2 * w])
+                                : j + w < kCpt   ? min(c3[j], c3[j + w])
+                                                 : c3[j];
+                if (c3[0] > f.k) continue;
+#pragma unroll
+                for (int j = 0; j < kCpt; ++j) {
+                    const int idx = lane + 32 * j;
+                    if (idx < n && (int)__popc((mh[j] ^ f.h) | (ml[j] ^ f.l) | ms[j]) <= f.k) {
+                        const uint32_t i = atomicAdd(&P.ctr->hits, 1u);
+                        if (i < P.hit_cap)
+                            P.hits[i] = Hit{(q[idx].x & kPairStartMask) + K.off, p, batch, 0};
+                        else
+                            P.ctr->overflow = 1;
+                    }
+                }
+            }
+        }
+    }
+}
+
+// The PAM prefilter of one group over a lane's 32 window starts.
+__device__ __forceinline__ uint32_t pam_mask(const ScanGroup *G, uint32_t m, uint32_t h0,
+                                             uint32_t h1, uint32_t l0, uint32_t l1, uint32_t s0,
+                                             uint32_t s1) {
+    const uint32_t n_pam = G->n_pam;
+    for (uint32_t c = 0; c < n_pam && m; ++c) {
+        const PamCell pc = G->pam[c];
+        const uint32_t h = __funnelshift_r(h0, h1, pc.cell);
+        const uint32_t l = __funnelshift_r(l0, l1, pc.cell);
+        const uint32_t sv = __funnelshift_r(s0, s1, pc.cell);
+        const uint32_t t0 = (l & pc.fc) | (~l & pc.fa);
+        const uint32_t t1 = (l & pc.ft) | (~l & pc.fg);
+        m &= ((h & t1) | (~h & t0)) & ~sv;
+    }
+    return m;
+}
+
+// Window starts 32w + k in [lo, hi) of a lane's word starting at p0.
+__device__ __forceinline__ uint32_t range_mask(uint64_t p0, uint64_t lo, uint64_t hi) {
+    uint32_t m = 0xFFFFFFFFu;
+    if (p0 < lo) m = (lo - p0 >= 32) ? 0u : (m << (uint32_t)(lo - p0));
+    if (p0 + 32 > hi) m = (hi <= p0) ? 0u : (m & (0xFFFFFFFFu >> (uint32_t)(32 - (hi - p0))));
+    return m;
+}
+
+// Persistent scan over strand pairs with per-warp work items (a span of
+// tiles of one pair).  Per 1024-start tile: one load of the lane's plane
+// words, both groups' PAM prefilters, and one drain of the starts that pass
+// either group into the warp queue.  For few patterns per group the fixed
+// per-tile work dominates the scan, and the pair halves it.
+template <int kCpt, int kScanWarps, int kMinBlocks, int kPatCap>
+__global__ void __launch_bounds__(kScanWarps * 32, kMinBlocks)
+scan_pair_kernel(ScanParams P) {
+    constexpr int kQCap = 32 * kCpt;
+    constexpr int kQSlots = kQCap + 32;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    uint4 *queues = reinterpret_cast<uint4 *>(smem_raw);
+    FastPattern *spat = reinterpret_cast<FastPattern *>(queues + kScanWarps * kQSlots);
+    const uint32_t n_staged = min(P.n_pats, (uint32_t)kPatCap);
+    for (uint32_t i = threadIdx.x; i < n_staged; i += blockDim.x) spat[i] = P.pats[i];
+    __syncthreads();
+
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const uint32_t lt_mask = (1u << lane) - 1u;
+    uint4 *q = queues + warp * kQSlots;
+    int qn = 0;
+    uint32_t qbatch = 0xFFFFFFFFu;
+    unsigned long long ncand = 0, npairs = 0;
+    uint32_t cur = 0xFFFFFFFFu, nseg = 0, npat0 = 0, npat1 = 0;
+    uint64_t p_tiles = 0;
+    const ScanGroup *G0 = nullptr, *G1 = nullptr;
+    const PairSeg *segs = P.psegs;
+    const uint64_t total_items = P.item_begin[P.n_pairs];
+
+    while (true) {
+        unsigned long long it = 0;
+        if (lane == 0) it = atomicAdd(&P.ctr->next_item, 1ull);
+        it = __shfl_sync(0xFFFFFFFFu, it, 0);
+        if (it >= total_items) break;
+        uint32_t lo = 0, hi = P.n_pairs;
+        while (hi - lo > 1) {
+            const uint32_t mid = (lo + hi) >> 1;
+            if (__ldg(P.item_begin + mid) <= it) lo = mid; else hi = mid;
+        }
+        if (lo != cur) {
+            if (qn) {  // the queue belongs to the previous pair's patterns
+                __syncwarp();
+                flush_pair<kCpt>(q, qn, spat, n_staged, G0, G1, qbatch, P, lane);
+                __syncwarp();
+                qn = 0;
+            }
+            cur = lo;
+            const ScanPair pr = P.pairs[lo];
+            G0 = P.groups + pr.g[0];
+            G1 = pr.g[1] == 0xFFFFFFFFu ? nullptr : P.groups + pr.g[1];
+            npat0 = G0->pat_end - G0->pat_begin;
+            npat1 = G1 ? G1->pat_end - G1->pat_begin : 0;
+            segs = P.psegs + pr.seg_begin;
+            nseg = pr.seg_end - pr.seg_begin;
+            const PairSeg &last = segs[nseg - 1];
+            const uint64_t hi_u = max(last.hi[0], last.hi[1]);
+            p_tiles = last.tile_begin + ((hi_u - last.w0 * 32 + 1023) >> 10);
+            qbatch = 0xFFFFFFFFu;
+        }
+        const uint64_t t_begin = (it - P.item_begin[lo]) * P.span_tiles;
+        const uint64_t t_end = min(t_begin + P.span_tiles, p_tiles);
+        uint32_t sidx = 0;
+        for (uint64_t tile = t_begin; tile < t_end; ++tile) {
+            while (sidx + 1 < nseg && tile >= segs[sidx + 1].tile_begin) ++sidx;
+            const PairSeg &sg = segs[sidx];
+            const uint64_t lo0 = sg.lo[0], hi0 = sg.hi[0], lo1 = sg.lo[1], hi1 = sg.hi[1];
+            const uint64_t base = sg.base;
+            const uint32_t batch = sg.batch;
+            if (batch != qbatch) {
+                if (qn) {
+                    __syncwarp();
+                    flush_pair<kCpt>(q, qn, spat, n_staged, G0, G1, qbatch, P, lane);
+                    __syncwarp();
+                    qn = 0;
+                }
+                qbatch = batch;
+            }
+            const uint64_t w = sg.w0 + (tile - sg.tile_begin) * 32 + lane;
+            const uint32_t h0 = __ldg(P.H + w), h1 = __ldg(P.H + w + 1);
+            const uint32_t l0 = __ldg(P.L + w), l1 = __ldg(P.L + w + 1);
+            const uint32_t s0 = __ldg(P.S + w), s1 = __ldg(P.S + w + 1);
+            const uint64_t p0 = w * 32;
+            uint32_t m0 = pam_mask(G0, range_mask(p0, lo0, hi0), h0, h1, l0, l1, s0, s1);
+            uint32_t m1 = G1 ? pam_mask(G1, range_mask(p0, lo1, hi1), h0, h1, l0, l1, s0, s1) : 0u;
+            const uint32_t n0 = __popc(m0), n1 = __popc(m1);
+            ncand += n0 + n1;
+            npairs += (unsigned long long)n0 * npat0 + (unsigned long long)n1 * npat1;
+            // drain the starts that pass either group, tagged, one per lane
+            // per step
+            uint32_t m = m0 | m1;
+            const uint32_t off0 = (uint32_t)(p0 - base);
+            for (;;) {
+                const bool has = m != 0;
+                const uint32_t bal = __ballot_sync(0xFFFFFFFFu, has);
+                if (!bal) break;
+                if (has) {
+                    const uint32_t k = __ffs(m) - 1;
+                    m &= m - 1;
+                    const uint32_t tag = (((m0 >> k) & 1u) << kPairTagShift) |
+                                         (((m1 >> k) & 1u) << (kPairTagShift + 1));
+                    const int slot = qn + __popc(bal & lt_mask);
+                    q[slot] = make_uint4((off0 + k) | tag, __funnelshift_r(h0, h1, k),
+                                         __funnelshift_r(l0, l1, k), __funnelshift_r(s0, s1, k));
+                }
+                qn += __popc(bal);
+                if (qn >= kQCap) {
+                    __syncwarp();
+                    flush_pair<kCpt>(q, kQCap, spat, n_staged, G0, G1, qbatch, P, lane);
+                    const int rest = qn - kQCap;
+                    uint4 e = make_uint4(0, 0, 0, 0);
+                    if (lane < rest) e = q[kQCap + lane];
+                    __syncwarp();
+                    if (lane < rest) q[lane] = e;
+                    __syncwarp();
+                    qn = rest;
+                }
+            }
+        }
+    }
+    if (qn) {
+        __syncwarp();
+        flush_pair<kCpt>(q, qn, spat, n_staged, G0, G1, qbatch, P, lane);
+    }
+    for (int o = 16; o; o >>= 1) {
+        ncand += __shfl_down_sync(0xFFFFFFFFu, ncand, o);
+        npairs += __shfl_down_sync(0xFFFFFFFFu, npairs, o);
+    }
+    if (lane == 0 && ncand) {
+        atomicAdd(&P.ctr->candidates, ncand);
+        atomicAdd(&P.ctr->pairs, npairs);
+    }
+}
+
 struct ScanVariant {
     int cpt, warps, min_blocks, pair;
     uint32_t span_tiles;
@@ -611,6 +862,7 @@ struct ScanVariant {
     bool per_warp;
     uint32_t pat_cap;  // patterns staged in shared memory
     bool lean;         // scan_tile_lean
+    bool paired;       // scan_pair_kernel: work items over strand pairs
     size_t smem() const {
         return (size_t)warps * (32 * cpt + 32) * sizeof(uint4) + pat_cap * sizeof(FastPattern);
     }
@@ -618,14 +870,20 @@ struct ScanVariant {
 
 template <int C, int W, int B, int Q = 1>
 constexpr ScanVariant variant(uint32_t span) {
-    return ScanVariant{C, W, B, Q, span, scan_kernel<C, W, B, Q>, false, kSmemPatterns, false};
+    return ScanVariant{C, W, B, Q, span, scan_kernel<C, W, B, Q>, false, kSmemPatterns, false,
+                       false};
+}
+template <int C, int W, int B, int K>
+constexpr ScanVariant pair_variant(uint32_t span) {
+    return ScanVariant{C, W, B, 4, span, scan_pair_kernel<C, W, B, K>, true, (uint32_t)K, false,
+                       true};
 }
 // span: tiles per warp work item; K: patterns staged in shared memory;
 // N: scan_tile_lean (1) or scan_tile (0)
 template <int C, int W, int B, int Q = 1, int K = kSmemPatterns, int N = 0>
 constexpr ScanVariant warp_variant(uint32_t span) {
     return ScanVariant{C, W, B, Q, span, scan_warp_kernel<C, W, B, Q, K, N>, true, (uint32_t)K,
-                       N != 0};
+                       N != 0, false};
 }
 
 // Candidate tile shapes (windows per lane x warps x min blocks per SM, and
@@ -639,7 +897,11 @@ const ScanVariant kScanVariants[] = {
     variant<8, 8, 3>(64), variant<4, 8, 4>(64), variant<4, 16, 2>(128),
     // the default shape without the lean tile (more patterns per group)
     warp_variant<8, 8, 4, 4, 1024>(8),
+    // strand pairs (the default for few patterns per group)
+    pair_variant<8, 8, 4, 256>(8), pair_variant<4, 8, 4, 256>(8),
 };
+constexpr int kFirstPairVariant = 9;
+constexpr uint32_t kPairMaxPatterns = 8;  // patterns per group up to which pairs are the default
 constexpr int kNumScanVariants = sizeof(kScanVariants) / sizeof(kScanVariants[0]);
 static_assert(kNumScanVariants <= 16, "Engine::scan_occ_ holds 16 shapes");
 
@@ -1309,13 +1571,99 @@ int Engine::run_popcount(const std::vector<Request> &reqs, std::vector<Result> &
                  o_ep = tp.add(epats), o_grp = tp.add(groups), o_seg = tp.add(segs),
                  o_f2e = tp.add(fast2exact);
     for (const ScanVariant &v : kScanVariants) {
-        if (o_items.count(v.span_tiles)) continue;
+        if (v.paired || o_items.count(v.span_tiles)) continue;
         auto full = make_items(v.span_tiles, ~0ull);
         auto samp = make_items(v.span_tiles, tune_tiles);
         n_items[v.span_tiles] = full.back();
         n_sample[v.span_tiles] = samp.back();
         o_items[v.span_tiles] = tp.add(full);
         o_sample[v.span_tiles] = tp.add(samp);
+    }
+
+    // Strand pairs for scan_pair_kernel: a group and the next one whose
+    // segments cover the same batches (the two strands of a filter) become
+    // one work unit over the union of their window ranges; a group without
+    // such a partner is scanned alone.  Queue entries tag their start with
+    // the groups it passed in bits 30-31, so pairs need every batch-local
+    // start below 2^30.
+    bool pairs_ok = !groups.empty();
+    for (const ScanSeg &x : segs) pairs_ok = pairs_ok && x.hi - x.base <= (1ull << kPairTagShift);
+    auto make_pairs = [&](const std::vector<ScanGroup> &G, const std::vector<ScanSeg> &S,
+                          std::vector<ScanPair> &pairs, std::vector<PairSeg> &ps) {
+        std::vector<char> used(G.size(), 0);
+        for (size_t i = 0; i < G.size(); ++i) {
+            if (used[i]) continue;
+            used[i] = 1;
+            const uint32_t ni = G[i].seg_end - G[i].seg_begin;
+            size_t j = G.size();
+            for (size_t k = i + 1; k < G.size() && j == G.size(); ++k) {
+                if (used[k] || G[k].seg_end - G[k].seg_begin != ni) continue;
+                bool same = true;
+                for (uint32_t t = 0; t < ni && same; ++t) {
+                    const ScanSeg &a = S[G[i].seg_begin + t], &b = S[G[k].seg_begin + t];
+                    same = a.batch == b.batch && a.base == b.base;
+                }
+                if (same) j = k;
+            }
+            const bool two = j < G.size();
+            if (two) used[j] = 1;
+            ScanPair pr{{(uint32_t)i, two ? (uint32_t)j : 0xFFFFFFFFu}, (uint32_t)ps.size(), 0};
+            uint64_t tiles = 0;
+            for (uint32_t t = 0; t < ni; ++t) {
+                const ScanSeg &a = S[G[i].seg_begin + t];
+                PairSeg x{};
+                x.lo[0] = a.lo;
+                x.hi[0] = a.hi;
+                uint64_t lo = a.lo, hi = a.hi;
+                if (two) {
+                    const ScanSeg &b = S[G[j].seg_begin + t];
+                    x.lo[1] = b.lo;
+                    x.hi[1] = b.hi;
+                    lo = std::min(lo, b.lo);
+                    hi = std::max(hi, b.hi);
+                }
+                x.base = a.base;
+                x.w0 = lo / 32;
+                x.tile_begin = tiles;
+                x.batch = a.batch;
+                tiles += (hi - x.w0 * 32 + 1023) / 1024;
+                ps.push_back(x);
+            }
+            pr.seg_end = (uint32_t)ps.size();
+            pairs.push_back(pr);
+        }
+    };
+    // work-item tables of pairs: spans of `span` tiles of each pair's union
+    auto pair_items = [](const std::vector<ScanPair> &pairs, const std::vector<PairSeg> &ps,
+                         uint32_t span, uint64_t cap_tiles) {
+        std::vector<uint64_t> ib{0};
+        for (const ScanPair &pr : pairs) {
+            const PairSeg &last = ps[pr.seg_end - 1];
+            const uint64_t hi = std::max(last.hi[0], last.hi[1]);
+            const uint64_t tiles =
+                std::min<uint64_t>(last.tile_begin + (hi - last.w0 * 32 + 1023) / 1024, cap_tiles);
+            ib.push_back(ib.back() + (tiles + span - 1) / span);
+        }
+        return ib;
+    };
+    std::vector<ScanPair> pairs;
+    std::vector<PairSeg> psegs;
+    std::map<uint32_t, size_t> o_pitems, o_psample;
+    std::map<uint32_t, uint64_t> n_pitems, n_psample;
+    size_t o_pairs = 0, o_psegs = 0;
+    if (pairs_ok) {
+        make_pairs(groups, segs, pairs, psegs);
+        o_pairs = tp.add(pairs);
+        o_psegs = tp.add(psegs);
+        for (const ScanVariant &v : kScanVariants) {
+            if (!v.paired || o_pitems.count(v.span_tiles)) continue;
+            auto full = pair_items(pairs, psegs, v.span_tiles, ~0ull);
+            auto samp = pair_items(pairs, psegs, v.span_tiles, tune_tiles);
+            n_pitems[v.span_tiles] = full.back();
+            n_psample[v.span_tiles] = samp.back();
+            o_pitems[v.span_tiles] = tp.add(full);
+            o_psample[v.span_tiles] = tp.add(samp);
+        }
     }
 
     // Slices: one request on a large genome is scanned in slices of pattern
@@ -1331,6 +1679,10 @@ int Engine::run_popcount(const std::vector<Request> &reqs, std::vector<Result> &
         uint32_t n_groups = 0;
         std::map<uint32_t, size_t> o_items;
         std::map<uint32_t, uint64_t> n_items;
+        size_t o_pairs = 0, o_psegs = 0;  // strand pairs of the slice (pairs_ok)
+        uint32_t n_pairs = 0;
+        std::map<uint32_t, size_t> o_pitems;
+        std::map<uint32_t, uint64_t> n_pitems;
     };
     std::vector<SliceTab> slices;
     {
@@ -1406,8 +1758,22 @@ int Engine::run_popcount(const std::vector<Request> &reqs, std::vector<Result> &
             st.n_groups = (uint32_t)gj.size();
             st.o_grp = tp.add(gj);
             st.o_seg = tp.add(sj);
+            if (pairs_ok) {
+                std::vector<ScanPair> pj;
+                std::vector<PairSeg> psj;
+                make_pairs(gj, sj, pj, psj);
+                st.n_pairs = (uint32_t)pj.size();
+                st.o_pairs = tp.add(pj);
+                st.o_psegs = tp.add(psj);
+                for (const ScanVariant &v : kScanVariants) {
+                    if (!v.paired || st.o_pitems.count(v.span_tiles)) continue;
+                    auto ib = pair_items(pj, psj, v.span_tiles, ~0ull);
+                    st.n_pitems[v.span_tiles] = ib.back();
+                    st.o_pitems[v.span_tiles] = tp.add(ib);
+                }
+            }
             for (const ScanVariant &v : kScanVariants) {
-                if (st.o_items.count(v.span_tiles)) continue;
+                if (v.paired || st.o_items.count(v.span_tiles)) continue;
                 std::vector<uint64_t> ib{0};
                 for (const ScanGroup &g : gj) {
                     const ScanSeg &last = sj[g.seg_end - 1];
@@ -1454,14 +1820,25 @@ int Engine::run_popcount(const std::vector<Request> &reqs, std::vector<Result> &
         sp.groups = (const ScanGroup *)tab(sl ? sl->o_grp : o_grp);
         sp.segs = (const ScanSeg *)tab(sl ? sl->o_seg : o_seg);
         sp.n_groups = sl ? sl->n_groups : (uint32_t)groups.size();
-        sp.item_begin = (const uint64_t *)tab(sl ? sl->o_items.at(v.span_tiles)
-                                              : sample ? o_sample[v.span_tiles]
-                                                       : o_items[v.span_tiles]);
+        uint64_t items = 0;
+        if (v.paired) {
+            sp.pairs = (const ScanPair *)tab(sl ? sl->o_pairs : o_pairs);
+            sp.psegs = (const PairSeg *)tab(sl ? sl->o_psegs : o_psegs);
+            sp.n_pairs = sl ? sl->n_pairs : (uint32_t)pairs.size();
+            sp.item_begin = (const uint64_t *)tab(sl ? sl->o_pitems.at(v.span_tiles)
+                                                  : sample ? o_psample[v.span_tiles]
+                                                           : o_pitems[v.span_tiles]);
+            items = sl ? sl->n_pitems.at(v.span_tiles)
+                       : sample ? n_psample[v.span_tiles] : n_pitems[v.span_tiles];
+        } else {
+            sp.item_begin = (const uint64_t *)tab(sl ? sl->o_items.at(v.span_tiles)
+                                                  : sample ? o_sample[v.span_tiles]
+                                                           : o_items[v.span_tiles]);
+            items = sl ? sl->n_items.at(v.span_tiles)
+                       : sample ? n_sample[v.span_tiles] : n_items[v.span_tiles];
+        }
         sp.hits = d.hits.p;  // the list may have grown (and moved) since the last launch
         sp.hit_cap = (uint32_t)std::min<size_t>(d.hits.cap, 0xFFFFFFF0u);
-        const uint64_t items = sl       ? sl->n_items.at(v.span_tiles)
-                               : sample ? n_sample[v.span_tiles]
-                                        : n_items[v.span_tiles];
         const unsigned gx = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>(items, (uint64_t)d.n_sm * occ));
         CU(cudaMemsetAsync(d.ctr.p, 0, sizeof(Counters), s));
         v.kernel<<<gx, v.warps * 32, smem, s>>>(sp);
@@ -1611,16 +1988,23 @@ int Engine::run_popcount(const std::vector<Request> &reqs, std::vector<Result> &
                                 std::to_string(max_l) + "-mm" + std::to_string(max_mm);
         // tuning pays off only when the search is much larger than its sample
         const bool worth = full_tiles >= 8 * tune_tiles * groups.size();
-        int vi = 0;
+        // the default: strand pairs for few patterns per group (the fixed
+        // work per tile dominates there), else the per-warp lean tile
+        uint32_t max_group_pats = 0;
+        for (const ScanGroup &g : groups) max_group_pats = std::max(max_group_pats, g.pat_end - g.pat_begin);
+        const int v_default = pairs_ok && max_group_pats <= kPairMaxPatterns ? kFirstPairVariant : 0;
+        int vi = v_default;
         const char *force = std::getenv("COF_SCAN_VARIANT");  // testing: pin a shape
         if (force && *force) {
             vi = std::max(0, std::min(kNumScanVariants - 1, std::atoi(force)));
+            if (kScanVariants[vi].paired && !pairs_ok) vi = 0;
         } else if (!tuner_.lookup(key, vi) && tuner_.enabled() && worth) {
-            if (launch(kScanVariants[0], true)) return err.code;  // warm-up
+            if (launch(kScanVariants[vi], true)) return err.code;  // warm-up
             float t[kNumScanVariants];
             for (int k = 0; k < kNumScanVariants; ++k) t[k] = 1e30f;
             for (int rep = 0; rep < 2; ++rep) {  // interleaved repeats, best of two
                 for (int k = 0; k < kNumScanVariants; ++k) {
+                    if (kScanVariants[k].paired && !pairs_ok) continue;
                     CU(cudaEventRecord(d.ev[1], s));
                     if (launch(kScanVariants[k], true)) return err.code;
                     CU(cudaEventRecord(d.ev[2], s));
@@ -1631,14 +2015,16 @@ int Engine::run_popcount(const std::vector<Request> &reqs, std::vector<Result> &
                 }
             }
             // the default shape wins unless another is clearly faster
-            for (int k = 1; k < kNumScanVariants; ++k)
-                if (t[k] < 0.97f * t[vi]) vi = k;
+            for (int k = 0; k < kNumScanVariants; ++k)
+                if (k != v_default && t[k] < 0.97f * t[vi]) vi = k;
             tuner_.store(key, vi);
         }
+        if (kScanVariants[vi].paired && !pairs_ok) vi = 0;  // a cached choice from another genome
         const ScanVariant &v = kScanVariants[vi];
         times_.scan_variant = vi;
         static const char *const kMinName[] = {"", "", "", "", "min3-"};
-        times_.scan_shape = std::string(v.per_warp ? "warp-" : "") + (v.lean ? "lean-" : "") +
+        times_.scan_shape = std::string(v.paired ? "pair-" : "") + (v.per_warp ? "warp-" : "") +
+                            (v.lean ? "lean-" : "") +
                             kMinName[v.pair] + "cpt" + std::to_string(v.cpt) + "-warps" + std::to_string(v.warps) +
                             "-minb" + std::to_string(v.min_blocks) + "-span" +
                             std::to_string(v.span_tiles);

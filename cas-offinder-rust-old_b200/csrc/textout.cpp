@@ -17,6 +17,9 @@ int cuda_fail(Error &err, cudaError_t e, const char *what) {
 TextOut::~TextOut() {
     // no copy may still write into a buffer that is released here
     if (in_flight_) cudaStreamSynchronize(cs_);
+    for (Pending &pc : pending_)
+        if (pc.done) events_.push_back(pc.done);
+    for (cudaEvent_t e : events_) cudaEventDestroy(e);
 }
 
 int TextOut::grow(size_t req, size_t need, Error &err) {
@@ -86,9 +89,54 @@ int TextOut::put(size_t req, const char *d_text, size_t len, uint64_t n_rows,
         if (e != cudaSuccess) return cuda_fail(err, e, "match record copy");
         in_flight_ = true;
     }
+    if (events_.empty()) {
+        cudaEvent_t ev = nullptr;
+        e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
+        if (e != cudaSuccess) return cuda_fail(err, e, "piece event");
+        events_.push_back(ev);
+    }
+    pc.done = events_.back();
+    events_.pop_back();
+    e = cudaEventRecord(pc.done, cs_);
+    if (e != cudaSuccess) {
+        events_.push_back(pc.done);
+        return cuda_fail(err, e, "piece event");
+    }
     out_[req].n_rows += n_rows;
     copied_ += len + (recs ? n_rows * sizeof(MatchRec) : 0);
     pending_.push_back(std::move(pc));
+    return kOk;
+}
+
+int TextOut::deliver(Pending &pc, Error &err) {
+    events_.push_back(pc.done);
+    pc.done = nullptr;
+    pc.text.p[pc.len] = 0;
+    Piece piece;
+    piece.request = pc.req;
+    piece.text = pc.text.p;
+    piece.text_len = pc.len;
+    piece.n_rows = pc.n_rows;
+    piece.recs = reinterpret_cast<const MatchRec *>(pc.recs.p);
+    if (sink_->fn(piece)) {
+        for (Pending &q : pending_)
+            if (q.done) events_.push_back(q.done);
+        pending_.clear();
+        err = {kCancelled, "the result sink stopped the search"};
+        return err.code;
+    }
+    return kOk;
+}
+
+int TextOut::poll(Error &err) {
+    while (sink_ && !pending_.empty()) {
+        const cudaError_t e = cudaEventQuery(pending_.front().done);
+        if (e == cudaErrorNotReady) return kOk;
+        if (e != cudaSuccess) return cuda_fail(err, e, "result piece copy");
+        Pending pc = std::move(pending_.front());
+        pending_.pop_front();
+        if (deliver(pc, err)) return err.code;
+    }
     return kOk;
 }
 
@@ -101,18 +149,7 @@ int TextOut::drain(Error &err) {
     while (!pending_.empty()) {
         Pending pc = std::move(pending_.front());
         pending_.pop_front();
-        pc.text.p[pc.len] = 0;
-        Piece piece;
-        piece.request = pc.req;
-        piece.text = pc.text.p;
-        piece.text_len = pc.len;
-        piece.n_rows = pc.n_rows;
-        piece.recs = reinterpret_cast<const MatchRec *>(pc.recs.p);
-        if (sink_->fn(piece)) {
-            pending_.clear();
-            err = {kCancelled, "the result sink stopped the search"};
-            return err.code;
-        }
+        if (deliver(pc, err)) return err.code;
     }
     return kOk;
 }

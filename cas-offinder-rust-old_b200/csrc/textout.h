@@ -52,6 +52,9 @@ class TextOut {
     // to the sink in the order they were put.  A sink that returns nonzero
     // cancels the search (kCancelled).
     int drain(Error &err);
+    // Sink mode: hands on the pieces, in order, whose copies have finished,
+    // without waiting for the others (nothing in assemble mode).
+    int poll(Error &err);
     // drain(), then NUL-terminates the assembled texts.
     int finish(Error &err);
     uint64_t bytes_copied() const { return copied_; }
@@ -62,8 +65,11 @@ class TextOut {
         size_t len;
         uint64_t n_rows;
         PooledText text, recs;
+        cudaEvent_t done = nullptr;  // recorded on the copy stream after its copies
     };
     int grow(size_t req, size_t need, Error &err);
+    int deliver(Pending &pc, Error &err);
+    std::vector<cudaEvent_t> events_;  // spare completion events
     cudaStream_t cs_;
     const Sink *sink_;
     std::vector<Result> &out_;
