@@ -631,10 +631,13 @@ scan_warp_kernel(ScanParams P) {
 // ---------------------------------------------------------------------------
 
 // Queued windows of a pair carry the groups whose PAM they passed in bits
-// 30 (first group) and 31 (second) of their start; starts stay below 2^30
-// (checked on the host before pairs are used).
+// 30 (first group) and 31 (second) of their start.  A window anchored at a
+// PAM that ends its pattern starts up to 31 cells before its batch, so the
+// start is stored plus kPairBias; biased starts stay below 2^30 (checked on
+// the host before pairs are used).
 constexpr uint32_t kPairTagShift = 30;
 constexpr uint32_t kPairStartMask = (1u << kPairTagShift) - 1u;
+constexpr uint32_t kPairBias = 64;
 
 // Compares the first n queued windows of a pair with the patterns of both
 // groups; a window meets a group's patterns only if it passed that group's
@@ -687,7 +690,8 @@ __device__ __noinline__ void flush_pair(const uint4 *q, int n, const FastPattern
                     if (idx < n && (int)__popc((mh[j] ^ f.h) | (ml[j] ^ f.l) | ms[j]) <= f.k) {
                         const uint32_t i = atomicAdd(&P.ctr->hits, 1u);
                         if (i < P.hit_cap)
-                            P.hits[i] = Hit{(q[idx].x & kPairStartMask) + K.off, p, batch, 0};
+                            P.hits[i] = Hit{(q[idx].x & kPairStartMask) - kPairBias + K.off,
+                                            p, batch, 0};
                         else
                             P.ctr->overflow = 1;
                     }
@@ -812,7 +816,7 @@ scan_pair_kernel(ScanParams P) {
             // drain the starts that pass either group, tagged, one per lane
             // per step
             uint32_t m = m0 | m1;
-            const uint32_t off0 = (uint32_t)(p0 - base);
+            const uint32_t off0 = (uint32_t)(p0 - base) + kPairBias;  // biased start of bit 0
             for (;;) {
                 const bool has = m != 0;
                 const uint32_t bal = __ballot_sync(0xFFFFFFFFu, has);
@@ -1583,11 +1587,16 @@ int Engine::run_popcount(const std::vector<Request> &reqs, std::vector<Result> &
     // Strand pairs for scan_pair_kernel: a group and the next one whose
     // segments cover the same batches (the two strands of a filter) become
     // one work unit over the union of their window ranges; a group without
-    // such a partner is scanned alone.  Queue entries tag their start with
-    // the groups it passed in bits 30-31, so pairs need every batch-local
-    // start below 2^30.
+    // such a partner is scanned alone.  Queue entries tag their (biased)
+    // start with the groups it passed in bits 30-31, so pairs need every
+    // biased batch-local start below 2^30.
     bool pairs_ok = !groups.empty();
-    for (const ScanSeg &x : segs) pairs_ok = pairs_ok && x.hi - x.base <= (1ull << kPairTagShift);
+    for (const ScanSeg &x : segs) {
+        // window starts lie in [lo - base, hi - base) of the batch, at most
+        // 31 cells before it
+        pairs_ok = pairs_ok && x.lo + kPairBias >= x.base &&
+                   x.hi - x.base + kPairBias <= (1ull << kPairTagShift);
+    }
     auto make_pairs = [&](const std::vector<ScanGroup> &G, const std::vector<ScanSeg> &S,
                           std::vector<ScanPair> &pairs, std::vector<PairSeg> &ps) {
         std::vector<char> used(G.size(), 0);
