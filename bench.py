@@ -478,7 +478,7 @@ def bench_bulge_full(cof, device, steps, scale=1.0, cpu_nt=2_000_000):
 def scan_kernel_name(shape):
     """The scan kernel a tile shape name (cof_genome_tuning "last") runs."""
     if shape.startswith("pair-"):
-        return "scan_pair_kernel"
+        return "scan_direct_kernel"
     return "scan_warp_kernel" if shape.startswith("warp-") else "scan_kernel"
 
 

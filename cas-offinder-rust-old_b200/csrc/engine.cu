@@ -627,79 +627,8 @@ scan_warp_kernel(ScanParams P) {
 }
 
 // ---------------------------------------------------------------------------
-// scan of strand pairs (few patterns per group)
+// direct scan of strand pairs (few patterns per group)
 // ---------------------------------------------------------------------------
-
-// Queued windows of a pair carry the groups whose PAM they passed in bits
-// 30 (first group) and 31 (second) of their start.  A window anchored at a
-// PAM that ends its pattern starts up to 31 cells before its batch, so the
-// start is stored plus kPairBias; biased starts stay below 2^30 (checked on
-// the host before pairs are used).
-constexpr uint32_t kPairTagShift = 30;
-constexpr uint32_t kPairStartMask = (1u << kPairTagShift) - 1u;
-constexpr uint32_t kPairBias = 64;
-
-// Compares the first n queued windows of a pair with the patterns of both
-// groups; a window meets a group's patterns only if it passed that group's
-// PAM prefilter (its tag bit).
-template <int kCpt>
-__device__ __noinline__ void flush_pair(const uint4 *q, int n, const FastPattern *spat,
-                                        uint32_t n_staged, const ScanGroup *Gp0,
-                                        const ScanGroup *Gp1, uint32_t batch,
-                                        const ScanParams &P, int lane) {
-    const uint32_t spat_s = (uint32_t)__cvta_generic_to_shared(spat);
-    for (int gi = 0; gi < 2; ++gi) {
-        const ScanGroup *Gp = gi ? Gp1 : Gp0;
-        if (!Gp) break;
-        const uint32_t tag = 1u << (kPairTagShift + gi);
-        const uint32_t pb = Gp->pat_begin, n_class = Gp->n_class;
-        const bool smem = Gp->pat_end <= n_staged;
-        for (uint32_t c = 0; c < n_class; ++c) {
-            const CareClass K = Gp->cls[c];
-            uint32_t mh[kCpt], ml[kCpt], ms[kCpt];
-            bool any = false;
-#pragma unroll
-            for (int j = 0; j < kCpt; ++j) {
-                const int idx = lane + 32 * j;
-                const uint4 e = idx < n ? q[idx] : make_uint4(0, 0, 0, 0);
-                const bool on = (e.x & tag) != 0;
-                any |= on;
-                mh[j] = e.y & K.care;
-                ml[j] = e.z & K.care;
-                ms[j] = on ? (e.w & K.care) : 0xFFFFFFFFu;
-            }
-            if (!__any_sync(0xFFFFFFFFu, any)) continue;
-            for (uint32_t p = pb + K.pat_begin; p < pb + K.pat_end; ++p) {
-                const FastPattern f = smem ? lds_pattern(spat_s + p * (uint32_t)sizeof(FastPattern))
-                                           : P.pats[p];
-                int c3[kCpt];
-#pragma unroll
-                for (int j = 0; j < kCpt; ++j)
-                    c3[j] = (int)__popc((mh[j] ^ f.h) | (ml[j] ^ f.l) | ms[j]);
-#pragma unroll
-                for (int w = 1; w < kCpt; w *= 3)
-#pragma unroll
-                    for (int j = 0; j < kCpt; j += 3 * w)
-                        c3[j] = j + 2 * w < kCpt ? __vimin3_s32(c3[j], c3[j + w], c3[j + 2 * w])
-                                : j + w < kCpt   ? min(c3[j], c3[j + w])
-                                                 : c3[j];
-                if (c3[0] > f.k) continue;
-#pragma unroll
-                for (int j = 0; j < kCpt; ++j) {
-                    const int idx = lane + 32 * j;
-                    if (idx < n && (int)__popc((mh[j] ^ f.h) | (ml[j] ^ f.l) | ms[j]) <= f.k) {
-                        const uint32_t i = atomicAdd(&P.ctr->hits, 1u);
-                        if (i < P.hit_cap)
-                            P.hits[i] = Hit{(q[idx].x & kPairStartMask) - kPairBias + K.off,
-                                            p, batch, 0};
-                        else
-                            P.ctr->overflow = 1;
-                    }
-                }
-            }
-        }
-    }
-}
 
 // The PAM prefilter of one group over a lane's 32 window starts.
 __device__ __forceinline__ uint32_t pam_mask(const ScanGroup *G, uint32_t m, uint32_t h0,
@@ -726,33 +655,78 @@ __device__ __forceinline__ uint32_t range_mask(uint64_t p0, uint64_t lo, uint64_
     return m;
 }
 
-// Persistent scan over strand pairs with per-warp work items (a span of
-// tiles of one pair).  Per 1024-start tile: one load of the lane's plane
-// words, both groups' PAM prefilters, and one drain of the starts that pass
-// either group into the warp queue.  For few patterns per group the fixed
-// per-tile work dominates the scan, and the pair halves it.
-template <int kCpt, int kScanWarps, int kMinBlocks, int kPatCap>
-__global__ void __launch_bounds__(kScanWarps * 32, kMinBlocks)
-scan_pair_kernel(ScanParams P) {
-    constexpr int kQCap = 32 * kCpt;
-    constexpr int kQSlots = kQCap + 32;
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    uint4 *queues = reinterpret_cast<uint4 *>(smem_raw);
-    FastPattern *spat = reinterpret_cast<FastPattern *>(queues + kScanWarps * kQSlots);
-    const uint32_t n_staged = min(P.n_pats, (uint32_t)kPatCap);
-    for (uint32_t i = threadIdx.x; i < n_staged; i += blockDim.x) spat[i] = P.pats[i];
-    __syncthreads();
+// The patterns of one group (at most kNP), in registers: scan form, the
+// window cell of each pattern's first cell (its care class offset) and its
+// index in the pattern table.  Unused slots never match (k = -1).
+template <int kNP>
+struct RegPats {
+    uint32_t h[kNP], l[kNP], care[kNP], off[kNP], idx[kNP];
+    int32_t k[kNP];
+};
 
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const uint32_t lt_mask = (1u << lane) - 1u;
-    uint4 *q = queues + warp * kQSlots;
-    int qn = 0;
-    uint32_t qbatch = 0xFFFFFFFFu;
+template <int kNP>
+__device__ __forceinline__ void load_reg_pats(const ScanGroup *G, const FastPattern *pats,
+                                              RegPats<kNP> &R) {
+    const uint32_t n = G ? G->pat_end - G->pat_begin : 0;
+#pragma unroll
+    for (int j = 0; j < kNP; ++j) {
+        R.h[j] = R.l[j] = R.care[j] = R.off[j] = R.idx[j] = 0;
+        R.k[j] = -1;
+        if ((uint32_t)j < n) {
+            const uint32_t p = G->pat_begin + j;
+            const FastPattern f = pats[p];
+            R.h[j] = f.h;
+            R.l[j] = f.l;
+            R.care[j] = f.care;
+            R.k[j] = f.k;
+            R.idx[j] = p;
+            for (uint32_t c = 0; c < G->n_class; ++c)
+                if ((uint32_t)j >= G->cls[c].pat_begin && (uint32_t)j < G->cls[c].pat_end)
+                    R.off[j] = G->cls[c].off;
+        }
+    }
+}
+
+// Every PAM-passing start of a lane's word (mask m) against the group's
+// patterns, straight from the lane's plane words: no queue, no loads.
+template <int kNP>
+__device__ __forceinline__ void compare_direct(uint32_t m, const RegPats<kNP> &R, uint32_t h0,
+                                               uint32_t h1, uint32_t l0, uint32_t l1,
+                                               uint32_t s0, uint32_t s1, uint32_t off0,
+                                               uint32_t batch, const ScanParams &P) {
+    while (m) {
+        const uint32_t k = __ffs(m) - 1;
+        m &= m - 1;
+        const uint32_t wh = __funnelshift_r(h0, h1, k), wl = __funnelshift_r(l0, l1, k),
+                       ws = __funnelshift_r(s0, s1, k);
+#pragma unroll
+        for (int j = 0; j < kNP; ++j) {
+            if ((int)__popc(((wh ^ R.h[j]) | (wl ^ R.l[j]) | ws) & R.care[j]) <= R.k[j]) {
+                const uint32_t i = atomicAdd(&P.ctr->hits, 1u);
+                if (i < P.hit_cap) P.hits[i] = Hit{off0 + k + R.off[j], R.idx[j], batch, 0};
+                else P.ctr->overflow = 1;
+            }
+        }
+    }
+}
+
+// Persistent scan over strand pairs with per-warp work items (a span of
+// tiles of one pair), for groups of at most kNP patterns.  Per 1024-start
+// tile a lane loads its plane words once, runs both groups' PAM prefilters
+// on them, and compares each PAM-passing start with the group's patterns in
+// registers.  With few patterns the queue of scan_warp_kernel costs more
+// than the comparisons it batches: a queued window is stored, reloaded and
+// masked per care class, while here it costs three funnel shifts.
+template <int kNP, int kScanWarps, int kMinBlocks>
+__global__ void __launch_bounds__(kScanWarps * 32, kMinBlocks)
+scan_direct_kernel(ScanParams P) {
+    const int lane = threadIdx.x & 31;
     unsigned long long ncand = 0, npairs = 0;
     uint32_t cur = 0xFFFFFFFFu, nseg = 0, npat0 = 0, npat1 = 0;
     uint64_t p_tiles = 0;
     const ScanGroup *G0 = nullptr, *G1 = nullptr;
     const PairSeg *segs = P.psegs;
+    RegPats<kNP> R0, R1;
     const uint64_t total_items = P.item_begin[P.n_pairs];
 
     while (true) {
@@ -766,24 +740,19 @@ scan_pair_kernel(ScanParams P) {
             if (__ldg(P.item_begin + mid) <= it) lo = mid; else hi = mid;
         }
         if (lo != cur) {
-            if (qn) {  // the queue belongs to the previous pair's patterns
-                __syncwarp();
-                flush_pair<kCpt>(q, qn, spat, n_staged, G0, G1, qbatch, P, lane);
-                __syncwarp();
-                qn = 0;
-            }
             cur = lo;
             const ScanPair pr = P.pairs[lo];
             G0 = P.groups + pr.g[0];
             G1 = pr.g[1] == 0xFFFFFFFFu ? nullptr : P.groups + pr.g[1];
             npat0 = G0->pat_end - G0->pat_begin;
             npat1 = G1 ? G1->pat_end - G1->pat_begin : 0;
+            load_reg_pats<kNP>(G0, P.pats, R0);
+            load_reg_pats<kNP>(G1, P.pats, R1);
             segs = P.psegs + pr.seg_begin;
             nseg = pr.seg_end - pr.seg_begin;
             const PairSeg &last = segs[nseg - 1];
             const uint64_t hi_u = max(last.hi[0], last.hi[1]);
             p_tiles = last.tile_begin + ((hi_u - last.w0 * 32 + 1023) >> 10);
-            qbatch = 0xFFFFFFFFu;
         }
         const uint64_t t_begin = (it - P.item_begin[lo]) * P.span_tiles;
         const uint64_t t_end = min(t_begin + P.span_tiles, p_tiles);
@@ -791,63 +760,23 @@ scan_pair_kernel(ScanParams P) {
         for (uint64_t tile = t_begin; tile < t_end; ++tile) {
             while (sidx + 1 < nseg && tile >= segs[sidx + 1].tile_begin) ++sidx;
             const PairSeg &sg = segs[sidx];
-            const uint64_t lo0 = sg.lo[0], hi0 = sg.hi[0], lo1 = sg.lo[1], hi1 = sg.hi[1];
-            const uint64_t base = sg.base;
-            const uint32_t batch = sg.batch;
-            if (batch != qbatch) {
-                if (qn) {
-                    __syncwarp();
-                    flush_pair<kCpt>(q, qn, spat, n_staged, G0, G1, qbatch, P, lane);
-                    __syncwarp();
-                    qn = 0;
-                }
-                qbatch = batch;
-            }
             const uint64_t w = sg.w0 + (tile - sg.tile_begin) * 32 + lane;
             const uint32_t h0 = __ldg(P.H + w), h1 = __ldg(P.H + w + 1);
             const uint32_t l0 = __ldg(P.L + w), l1 = __ldg(P.L + w + 1);
             const uint32_t s0 = __ldg(P.S + w), s1 = __ldg(P.S + w + 1);
             const uint64_t p0 = w * 32;
-            uint32_t m0 = pam_mask(G0, range_mask(p0, lo0, hi0), h0, h1, l0, l1, s0, s1);
-            uint32_t m1 = G1 ? pam_mask(G1, range_mask(p0, lo1, hi1), h0, h1, l0, l1, s0, s1) : 0u;
+            const uint32_t m0 = pam_mask(G0, range_mask(p0, sg.lo[0], sg.hi[0]), h0, h1, l0, l1, s0, s1);
+            const uint32_t m1 =
+                G1 ? pam_mask(G1, range_mask(p0, sg.lo[1], sg.hi[1]), h0, h1, l0, l1, s0, s1) : 0u;
             const uint32_t n0 = __popc(m0), n1 = __popc(m1);
             ncand += n0 + n1;
             npairs += (unsigned long long)n0 * npat0 + (unsigned long long)n1 * npat1;
-            // drain the starts that pass either group, tagged, one per lane
-            // per step
-            uint32_t m = m0 | m1;
-            const uint32_t off0 = (uint32_t)(p0 - base) + kPairBias;  // biased start of bit 0
-            for (;;) {
-                const bool has = m != 0;
-                const uint32_t bal = __ballot_sync(0xFFFFFFFFu, has);
-                if (!bal) break;
-                if (has) {
-                    const uint32_t k = __ffs(m) - 1;
-                    m &= m - 1;
-                    const uint32_t tag = (((m0 >> k) & 1u) << kPairTagShift) |
-                                         (((m1 >> k) & 1u) << (kPairTagShift + 1));
-                    const int slot = qn + __popc(bal & lt_mask);
-                    q[slot] = make_uint4((off0 + k) | tag, __funnelshift_r(h0, h1, k),
-                                         __funnelshift_r(l0, l1, k), __funnelshift_r(s0, s1, k));
-                }
-                qn += __popc(bal);
-                if (qn >= kQCap) {
-                    __syncwarp();
-                    flush_pair<kCpt>(q, kQCap, spat, n_staged, G0, G1, qbatch, P, lane);
-                    const int rest = qn - kQCap;
-                    uint4 e = make_uint4(0, 0, 0, 0);
-                    if (lane < rest) e = q[kQCap + lane];
-                    __syncwarp();
-                    if (lane < rest) q[lane] = e;
-                    __syncwarp();
-                    qn = rest;
-                }
-            }
+            // batch-local start of bit 0 (a window may begin before its
+            // batch; the class offset brings every hit's start back into it)
+            const uint32_t off0 = (uint32_t)(p0 - sg.base);
+            compare_direct<kNP>(m0, R0, h0, h1, l0, l1, s0, s1, off0, sg.batch, P);
+            compare_direct<kNP>(m1, R1, h0, h1, l0, l1, s0, s1, off0, sg.batch, P);
         }
-    }
-    if (qn) {
-        __syncwarp();
-        flush_pair<kCpt>(q, qn, spat, n_staged, G0, G1, qbatch, P, lane);
     }
     for (int o = 16; o; o >>= 1) {
         ncand += __shfl_down_sync(0xFFFFFFFFu, ncand, o);
@@ -866,8 +795,10 @@ struct ScanVariant {
     bool per_warp;
     uint32_t pat_cap;  // patterns staged in shared memory
     bool lean;         // scan_tile_lean
-    bool paired;       // scan_pair_kernel: work items over strand pairs
+    bool paired;       // scan_direct_kernel: work items over strand pairs
+    uint32_t max_pats; // patterns per group the kernel holds (0: any)
     size_t smem() const {
+        if (paired) return 0;
         return (size_t)warps * (32 * cpt + 32) * sizeof(uint4) + pat_cap * sizeof(FastPattern);
     }
 };
@@ -875,19 +806,20 @@ struct ScanVariant {
 template <int C, int W, int B, int Q = 1>
 constexpr ScanVariant variant(uint32_t span) {
     return ScanVariant{C, W, B, Q, span, scan_kernel<C, W, B, Q>, false, kSmemPatterns, false,
-                       false};
+                       false, 0};
 }
-template <int C, int W, int B, int K>
-constexpr ScanVariant pair_variant(uint32_t span) {
-    return ScanVariant{C, W, B, 4, span, scan_pair_kernel<C, W, B, K>, true, (uint32_t)K, false,
-                       true};
+// NP: patterns per group held in registers
+template <int NP, int W, int B>
+constexpr ScanVariant direct_variant(uint32_t span) {
+    return ScanVariant{0, W, B, 0, span, scan_direct_kernel<NP, W, B>, true, 0, false, true,
+                       (uint32_t)NP};
 }
 // span: tiles per warp work item; K: patterns staged in shared memory;
 // N: scan_tile_lean (1) or scan_tile (0)
 template <int C, int W, int B, int Q = 1, int K = kSmemPatterns, int N = 0>
 constexpr ScanVariant warp_variant(uint32_t span) {
     return ScanVariant{C, W, B, Q, span, scan_warp_kernel<C, W, B, Q, K, N>, true, (uint32_t)K,
-                       N != 0, false};
+                       N != 0, false, 0};
 }
 
 // Candidate tile shapes (windows per lane x warps x min blocks per SM, and
@@ -901,11 +833,12 @@ const ScanVariant kScanVariants[] = {
     variant<8, 8, 3>(64), variant<4, 8, 4>(64), variant<4, 16, 2>(128),
     // the default shape without the lean tile (more patterns per group)
     warp_variant<8, 8, 4, 4, 1024>(8),
-    // strand pairs (the default for few patterns per group)
-    pair_variant<8, 8, 4, 256>(8), pair_variant<4, 8, 4, 256>(8),
+    // strand pairs compared directly (the default for up to 4 patterns per
+    // group): 1, 2 and 4 patterns in registers
+    direct_variant<1, 8, 4>(8), direct_variant<2, 8, 3>(8), direct_variant<4, 8, 3>(8),
 };
-constexpr int kFirstPairVariant = 9;
-constexpr uint32_t kPairMaxPatterns = 8;  // patterns per group up to which pairs are the default
+constexpr int kFirstPairVariant = 9;      // direct_variant<1>; <2> and <4> follow
+constexpr uint32_t kPairMaxPatterns = 4;  // patterns per group up to which they are the default
 constexpr int kNumScanVariants = sizeof(kScanVariants) / sizeof(kScanVariants[0]);
 static_assert(kNumScanVariants <= 16, "Engine::scan_occ_ holds 16 shapes");
 
@@ -1584,19 +1517,11 @@ int Engine::run_popcount(const std::vector<Request> &reqs, std::vector<Result> &
         o_sample[v.span_tiles] = tp.add(samp);
     }
 
-    // Strand pairs for scan_pair_kernel: a group and the next one whose
+    // Strand pairs for scan_direct_kernel: a group and the next one whose
     // segments cover the same batches (the two strands of a filter) become
     // one work unit over the union of their window ranges; a group without
-    // such a partner is scanned alone.  Queue entries tag their (biased)
-    // start with the groups it passed in bits 30-31, so pairs need every
-    // biased batch-local start below 2^30.
-    bool pairs_ok = !groups.empty();
-    for (const ScanSeg &x : segs) {
-        // window starts lie in [lo - base, hi - base) of the batch, at most
-        // 31 cells before it
-        pairs_ok = pairs_ok && x.lo + kPairBias >= x.base &&
-                   x.hi - x.base + kPairBias <= (1ull << kPairTagShift);
-    }
+    // such a partner is scanned alone.
+    const bool pairs_ok = !groups.empty();
     auto make_pairs = [&](const std::vector<ScanGroup> &G, const std::vector<ScanSeg> &S,
                           std::vector<ScanPair> &pairs, std::vector<PairSeg> &ps) {
         std::vector<char> used(G.size(), 0);
@@ -1997,23 +1922,32 @@ int Engine::run_popcount(const std::vector<Request> &reqs, std::vector<Result> &
                                 std::to_string(max_l) + "-mm" + std::to_string(max_mm);
         // tuning pays off only when the search is much larger than its sample
         const bool worth = full_tiles >= 8 * tune_tiles * groups.size();
-        // the default: strand pairs for few patterns per group (the fixed
-        // work per tile dominates there), else the per-warp lean tile
+        // the default: strand pairs compared directly for few patterns per
+        // group (the fixed work per tile dominates there), else the per-warp
+        // lean tile.  A direct shape holds a fixed number of patterns per
+        // group and cannot run larger groups.
         uint32_t max_group_pats = 0;
         for (const ScanGroup &g : groups) max_group_pats = std::max(max_group_pats, g.pat_end - g.pat_begin);
-        const int v_default = pairs_ok && max_group_pats <= kPairMaxPatterns ? kFirstPairVariant : 0;
+        auto usable = [&](int k) {
+            const ScanVariant &x = kScanVariants[k];
+            return !x.paired || (pairs_ok && max_group_pats <= x.max_pats);
+        };
+        int v_default = 0;
+        if (max_group_pats <= kPairMaxPatterns)
+            for (int k = kFirstPairVariant; k < kNumScanVariants && !v_default; ++k)
+                if (usable(k)) v_default = k;
         int vi = v_default;
         const char *force = std::getenv("COF_SCAN_VARIANT");  // testing: pin a shape
         if (force && *force) {
             vi = std::max(0, std::min(kNumScanVariants - 1, std::atoi(force)));
-            if (kScanVariants[vi].paired && !pairs_ok) vi = 0;
+            if (!usable(vi)) vi = 0;
         } else if (!tuner_.lookup(key, vi) && tuner_.enabled() && worth) {
             if (launch(kScanVariants[vi], true)) return err.code;  // warm-up
             float t[kNumScanVariants];
             for (int k = 0; k < kNumScanVariants; ++k) t[k] = 1e30f;
             for (int rep = 0; rep < 2; ++rep) {  // interleaved repeats, best of two
                 for (int k = 0; k < kNumScanVariants; ++k) {
-                    if (kScanVariants[k].paired && !pairs_ok) continue;
+                    if (!usable(k)) continue;
                     CU(cudaEventRecord(d.ev[1], s));
                     if (launch(kScanVariants[k], true)) return err.code;
                     CU(cudaEventRecord(d.ev[2], s));
@@ -2028,15 +1962,19 @@ int Engine::run_popcount(const std::vector<Request> &reqs, std::vector<Result> &
                 if (k != v_default && t[k] < 0.97f * t[vi]) vi = k;
             tuner_.store(key, vi);
         }
-        if (kScanVariants[vi].paired && !pairs_ok) vi = 0;  // a cached choice from another genome
+        if (!usable(vi)) vi = v_default;  // a cached choice for larger groups
         const ScanVariant &v = kScanVariants[vi];
         times_.scan_variant = vi;
         static const char *const kMinName[] = {"", "", "", "", "min3-"};
-        times_.scan_shape = std::string(v.paired ? "pair-" : "") + (v.per_warp ? "warp-" : "") +
-                            (v.lean ? "lean-" : "") +
-                            kMinName[v.pair] + "cpt" + std::to_string(v.cpt) + "-warps" + std::to_string(v.warps) +
-                            "-minb" + std::to_string(v.min_blocks) + "-span" +
-                            std::to_string(v.span_tiles);
+        if (v.paired)
+            times_.scan_shape = "pair-direct-np" + std::to_string(v.max_pats) + "-warps" +
+                                std::to_string(v.warps) + "-minb" + std::to_string(v.min_blocks) +
+                                "-span" + std::to_string(v.span_tiles);
+        else
+            times_.scan_shape = std::string(v.per_warp ? "warp-" : "") + (v.lean ? "lean-" : "") +
+                                kMinName[v.pair] + "cpt" + std::to_string(v.cpt) + "-warps" +
+                                std::to_string(v.warps) + "-minb" + std::to_string(v.min_blocks) +
+                                "-span" + std::to_string(v.span_tiles);
         vsel = &v;
     }
     if (!slices.empty()) {

@@ -155,9 +155,17 @@ def test_cli_matches_oracle_cli(cof_mod, oracle_mod, golden, tmp_path):
         assert "=== Cas-OFFinder Rust ===" in log and "Matches found: 117" in log
 
 
-# per-warp work items: 0-4 and 8; CTA work items: 5-7; strand pairs: 9-10
-N_SCAN_VARIANTS = 11
-PAIR_VARIANTS = (9, 10)
+# per-warp work items: 0-4 and 8; CTA work items: 5-7; strand pairs compared
+# directly, holding 1, 2 or 4 patterns per group: 9-11 (a request whose
+# groups are larger runs the default shape instead)
+N_SCAN_VARIANTS = 12
+PAIR_VARIANTS = {9: 1, 10: 2, 11: 4}
+
+
+def _expected_variant(variant, patterns_per_group):
+    if variant in PAIR_VARIANTS and patterns_per_group > PAIR_VARIANTS[variant]:
+        return 0
+    return variant
 
 
 @pytest.mark.parametrize("variant", range(N_SCAN_VARIANTS))
@@ -172,10 +180,10 @@ def test_every_scan_tile_shape(cof_mod, oracle_mod, golden, variant, monkeypatch
     text, _ = g2.search(case["filter"], case["patterns"], case["mm"], chunks_per_search=case["cps"])
     ref, _ = o.search(case["filter"], case["patterns"], case["mm"], chunks_per_search=case["cps"])
     assert _rows(text) == _rows(ref)
-    assert g2.tuning()["variant"] == variant
+    assert g2.tuning()["variant"] == _expected_variant(variant, len(case["patterns"]))
 
 
-@pytest.mark.parametrize("variant", [0, 3, 5, 9])
+@pytest.mark.parametrize("variant", [0, 3, 5])
 def test_patterns_beyond_the_shared_memory_table(cof_mod, oracle_mod, variant, monkeypatch):
     # 1500 guides: 3000 patterns in two strand groups; the per-warp scan
     # stages the first 1024 or 2048 patterns, so later groups read their
@@ -194,28 +202,29 @@ def test_patterns_beyond_the_shared_memory_table(cof_mod, oracle_mod, variant, m
     assert g.tuning()["variant"] == variant
 
 
-@pytest.mark.parametrize("variant", PAIR_VARIANTS)
+@pytest.mark.parametrize("variant", sorted(PAIR_VARIANTS))
 @pytest.mark.parametrize("cps", [0, 3])
 def test_strand_pairs_in_a_mixed_batch(cof_mod, oracle_mod, variant, cps, monkeypatch):
-    # the strand-pair scan takes both strand groups of a filter as one work
-    # item (and a group without a partner alone): a batch of requests with
-    # 3' and 5' PAMs, no PAM, a long pattern, IUPAC guides and different
-    # lengths and thresholds gives every request's rows, equal to its own
-    # oracle run
+    # the direct strand-pair scan takes both strand groups of a filter as
+    # one work item (and a group without a partner alone), with the groups'
+    # patterns in registers: a batch of requests with 3' and 5' PAMs, no
+    # PAM, a 40-cell pattern, IUPAC guides and different lengths and
+    # thresholds gives every request's rows, equal to its own oracle run
     monkeypatch.setenv("COF_SCAN_VARIANT", str(variant))
     rng = random.Random(900 + variant + cps)
     _, records = randgen.random_genome(rng, 3, 20000, 40000)
+    n_pat = PAIR_VARIANTS[variant]
     reqs = []
     for filt, mk, mm in randgen.REQUEST_SHAPES:
-        pats = [mk("".join(rng.choice("ACGT") for _ in range(25))) for _ in range(2)]
+        pats = [mk("".join(rng.choice("ACGT") for _ in range(25))) for _ in range(n_pat)]
         for p in pats:
             randgen.plant_sites(rng, records, p.upper(), filt, 8, 2)
         reqs.append(dict(search_filter=filt, patterns=pats, max_mismatches=mm,
                          chunks_per_search=cps))
     g40 = "".join(rng.choice("ACGT") for _ in range(37))
-    reqs.append(dict(search_filter="N" * 38 + "RG", patterns=[g40 + "NNN"], max_mismatches=5,
+    reqs.append(dict(search_filter="N" * 38 + "AG", patterns=[g40 + "NNN"], max_mismatches=5,
                      chunks_per_search=cps))
-    randgen.plant_sites(rng, records, g40 + "NNN", "N" * 38 + "RG", 8, 3)
+    randgen.plant_sites(rng, records, g40 + "NNN", "N" * 38 + "AG", 8, 3)
     g, o = _both(cof_mod, oracle_mod, randgen.chunk_records(rng, records, 2500))
     res = g.search_batch(reqs)
     assert g.tuning()["variant"] == variant and g.tuning()["last"].startswith("pair-")
@@ -508,7 +517,7 @@ def test_chunk_added_after_fasta_load(cof_mod, oracle_mod, tmp_path):
     assert na == nref > 0 and sorted(ra.split("\n")) == sorted(ref.split("\n"))
 
 
-@pytest.mark.parametrize("variant", [0, 5, 9])
+@pytest.mark.parametrize("variant", [0, 5, 11])
 def test_more_batches_than_one_scan_group_holds(cof_mod, oracle_mod, variant, monkeypatch):
     # ~300 batches (2 chunks each): more batch segments than a scan group
     # stages, as with chunks_per_search 64 (the CLI's C) on a large genome
