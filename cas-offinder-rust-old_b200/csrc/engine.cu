@@ -630,31 +630,6 @@ scan_warp_kernel(ScanParams P) {
 // direct scan of strand pairs (few patterns per group)
 // ---------------------------------------------------------------------------
 
-// The PAM prefilter of one group over a lane's 32 window starts.
-__device__ __forceinline__ uint32_t pam_mask(const ScanGroup *G, uint32_t m, uint32_t h0,
-                                             uint32_t h1, uint32_t l0, uint32_t l1, uint32_t s0,
-                                             uint32_t s1) {
-    const uint32_t n_pam = G->n_pam;
-    for (uint32_t c = 0; c < n_pam && m; ++c) {
-        const PamCell pc = G->pam[c];
-        const uint32_t h = __funnelshift_r(h0, h1, pc.cell);
-        const uint32_t l = __funnelshift_r(l0, l1, pc.cell);
-        const uint32_t sv = __funnelshift_r(s0, s1, pc.cell);
-        const uint32_t t0 = (l & pc.fc) | (~l & pc.fa);
-        const uint32_t t1 = (l & pc.ft) | (~l & pc.fg);
-        m &= ((h & t1) | (~h & t0)) & ~sv;
-    }
-    return m;
-}
-
-// Window starts 32w + k in [lo, hi) of a lane's word starting at p0.
-__device__ __forceinline__ uint32_t range_mask(uint64_t p0, uint64_t lo, uint64_t hi) {
-    uint32_t m = 0xFFFFFFFFu;
-    if (p0 < lo) m = (lo - p0 >= 32) ? 0u : (m << (uint32_t)(lo - p0));
-    if (p0 + 32 > hi) m = (hi <= p0) ? 0u : (m & (0xFFFFFFFFu >> (uint32_t)(32 - (hi - p0))));
-    return m;
-}
-
 // The patterns of one group (at most kNP), in registers: scan form, the
 // window cell of each pattern's first cell (its care class offset) and its
 // index in the pattern table.  Unused slots never match (k = -1).
@@ -688,13 +663,17 @@ __device__ __forceinline__ void load_reg_pats(const ScanGroup *G, const FastPatt
 }
 
 // Every PAM-passing start of a lane's word (mask m) against the group's
-// patterns, straight from the lane's plane words: no queue, no loads.
+// patterns, straight from the lane's plane words: no queue, no loads.  The
+// warp steps together (a vote per step), one start per lane per step: left
+// to diverge, lanes with different start counts ran their loops apart, with
+// about 6 of 32 lanes active per instruction.
 template <int kNP>
 __device__ __forceinline__ void compare_direct(uint32_t m, const RegPats<kNP> &R, uint32_t h0,
                                                uint32_t h1, uint32_t l0, uint32_t l1,
                                                uint32_t s0, uint32_t s1, uint32_t off0,
                                                uint32_t batch, const ScanParams &P) {
-    while (m) {
+    while (__any_sync(0xFFFFFFFFu, m)) {
+        if (!m) continue;
         const uint32_t k = __ffs(m) - 1;
         m &= m - 1;
         const uint32_t wh = __funnelshift_r(h0, h1, k), wl = __funnelshift_r(l0, l1, k),
@@ -717,14 +696,46 @@ __device__ __forceinline__ void compare_direct(uint32_t m, const RegPats<kNP> &R
 // registers.  With few patterns the queue of scan_warp_kernel costs more
 // than the comparisons it batches: a queued window is stored, reloaded and
 // masked per care class, while here it costs three funnel shifts.
+constexpr uint32_t kDirectPamCells = 8;  // PAM cells per group a direct scan stages
+
+// The PAM prefilter of a group whose cells a warp staged in shared memory
+// (code masks fa fc fg ft, and window cells).
+__device__ __forceinline__ uint32_t pam_mask_staged(const uint4 *cm, const uint32_t *ci,
+                                                    uint32_t n, uint32_t m, uint32_t h0,
+                                                    uint32_t h1, uint32_t l0, uint32_t l1,
+                                                    uint32_t s0, uint32_t s1) {
+    for (uint32_t c = 0; c < n; ++c) {
+        const uint4 f = cm[c];  // fa, fc, fg, ft
+        const uint32_t cell = ci[c];
+        const uint32_t h = __funnelshift_r(h0, h1, cell);
+        const uint32_t l = __funnelshift_r(l0, l1, cell);
+        const uint32_t sv = __funnelshift_r(s0, s1, cell);
+        const uint32_t t0 = (l & f.y) | (~l & f.x);
+        const uint32_t t1 = (l & f.w) | (~l & f.z);
+        m &= ((h & t1) | (~h & t0)) & ~sv;
+    }
+    return m;
+}
+
+// Starts 0..31 of a lane whose first start is p (relative to its segment's
+// first plane word) that lie in [lo, hi).
+__device__ __forceinline__ uint32_t range_mask32(uint32_t p, uint32_t lo, uint32_t hi) {
+    uint32_t m = 0xFFFFFFFFu;
+    if (p < lo) m = (lo - p >= 32) ? 0u : (m << (lo - p));
+    if (p + 32 > hi) m = (hi <= p) ? 0u : (m & (0xFFFFFFFFu >> (32 - (hi - p))));
+    return m;
+}
+
 template <int kNP, int kScanWarps, int kMinBlocks>
 __global__ void __launch_bounds__(kScanWarps * 32, kMinBlocks)
 scan_direct_kernel(ScanParams P) {
-    const int lane = threadIdx.x & 31;
+    __shared__ uint4 s_cm[kScanWarps][2][kDirectPamCells];
+    __shared__ uint32_t s_ci[kScanWarps][2][kDirectPamCells];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     unsigned long long ncand = 0, npairs = 0;
-    uint32_t cur = 0xFFFFFFFFu, nseg = 0, npat0 = 0, npat1 = 0;
+    uint32_t cur = 0xFFFFFFFFu, nseg = 0, npat0 = 0, npat1 = 0, npam0 = 0, npam1 = 0;
     uint64_t p_tiles = 0;
-    const ScanGroup *G0 = nullptr, *G1 = nullptr;
+    bool two = false;
     const PairSeg *segs = P.psegs;
     RegPats<kNP> R0, R1;
     const uint64_t total_items = P.item_begin[P.n_pairs];
@@ -742,12 +753,27 @@ scan_direct_kernel(ScanParams P) {
         if (lo != cur) {
             cur = lo;
             const ScanPair pr = P.pairs[lo];
-            G0 = P.groups + pr.g[0];
-            G1 = pr.g[1] == 0xFFFFFFFFu ? nullptr : P.groups + pr.g[1];
+            const ScanGroup *G0 = P.groups + pr.g[0];
+            const ScanGroup *G1 = pr.g[1] == 0xFFFFFFFFu ? nullptr : P.groups + pr.g[1];
+            two = G1 != nullptr;
             npat0 = G0->pat_end - G0->pat_begin;
-            npat1 = G1 ? G1->pat_end - G1->pat_begin : 0;
+            npat1 = two ? G1->pat_end - G1->pat_begin : 0;
+            npam0 = G0->n_pam;
+            npam1 = two ? G1->n_pam : 0;
             load_reg_pats<kNP>(G0, P.pats, R0);
             load_reg_pats<kNP>(G1, P.pats, R1);
+            __syncwarp();
+            if ((uint32_t)lane < npam0) {
+                const PamCell c = G0->pam[lane];
+                s_cm[warp][0][lane] = make_uint4(c.fa, c.fc, c.fg, c.ft);
+                s_ci[warp][0][lane] = c.cell;
+            }
+            if ((uint32_t)lane < npam1) {
+                const PamCell c = G1->pam[lane];
+                s_cm[warp][1][lane] = make_uint4(c.fa, c.fc, c.fg, c.ft);
+                s_ci[warp][1][lane] = c.cell;
+            }
+            __syncwarp();
             segs = P.psegs + pr.seg_begin;
             nseg = pr.seg_end - pr.seg_begin;
             const PairSeg &last = segs[nseg - 1];
@@ -756,27 +782,58 @@ scan_direct_kernel(ScanParams P) {
         }
         const uint64_t t_begin = (it - P.item_begin[lo]) * P.span_tiles;
         const uint64_t t_end = min(t_begin + P.span_tiles, p_tiles);
+        // the current segment, as offsets from its first plane word's
+        // first start (32-bit: a segment spans one batch)
         uint32_t sidx = 0;
+        while (sidx + 1 < nseg && t_begin >= segs[sidx + 1].tile_begin) ++sidx;
+        uint64_t seg_w0 = 0, seg_t0 = 0, next_t = 0;
+        uint32_t lo0 = 0, hi0 = 0, lo1 = 0, hi1 = 0, offb = 0, batch = 0;
+        bool fresh = true;
+        uint32_t c_cand = 0, c_pairs = 0;
         for (uint64_t tile = t_begin; tile < t_end; ++tile) {
-            while (sidx + 1 < nseg && tile >= segs[sidx + 1].tile_begin) ++sidx;
-            const PairSeg &sg = segs[sidx];
-            const uint64_t w = sg.w0 + (tile - sg.tile_begin) * 32 + lane;
+            if (fresh || tile >= next_t) {
+                if (!fresh) ++sidx;
+                fresh = false;
+                const PairSeg &sg = segs[sidx];
+                seg_w0 = sg.w0;
+                seg_t0 = sg.tile_begin;
+                next_t = sidx + 1 < nseg ? segs[sidx + 1].tile_begin : ~0ull;
+                const uint64_t p0s = sg.w0 * 32;
+                lo0 = (uint32_t)(sg.lo[0] - p0s);
+                hi0 = (uint32_t)(sg.hi[0] - p0s);
+                lo1 = two ? (uint32_t)(sg.lo[1] - p0s) : 0u;
+                hi1 = two ? (uint32_t)(sg.hi[1] - p0s) : 0u;
+                offb = (uint32_t)(p0s - sg.base);
+                batch = sg.batch;
+            }
+            const uint32_t trel = (uint32_t)(tile - seg_t0);
+            const uint64_t w = seg_w0 + (uint64_t)trel * 32 + lane;
             const uint32_t h0 = __ldg(P.H + w), h1 = __ldg(P.H + w + 1);
             const uint32_t l0 = __ldg(P.L + w), l1 = __ldg(P.L + w + 1);
             const uint32_t s0 = __ldg(P.S + w), s1 = __ldg(P.S + w + 1);
-            const uint64_t p0 = w * 32;
-            const uint32_t m0 = pam_mask(G0, range_mask(p0, sg.lo[0], sg.hi[0]), h0, h1, l0, l1, s0, s1);
-            const uint32_t m1 =
-                G1 ? pam_mask(G1, range_mask(p0, sg.lo[1], sg.hi[1]), h0, h1, l0, l1, s0, s1) : 0u;
+            const uint32_t t0 = trel * 1024u;  // the tile's first start
+            const uint32_t pl = t0 + (uint32_t)lane * 32u;
+            // a tile inside both ranges (nearly all) skips the range masks
+            const uint32_t r0 = t0 >= lo0 && t0 + 1024u <= hi0 ? 0xFFFFFFFFu : range_mask32(pl, lo0, hi0);
+            const uint32_t m0 = pam_mask_staged(s_cm[warp][0], s_ci[warp][0], npam0, r0, h0, h1,
+                                                l0, l1, s0, s1);
+            uint32_t m1 = 0;
+            if (two) {
+                const uint32_t r1 = t0 >= lo1 && t0 + 1024u <= hi1 ? 0xFFFFFFFFu : range_mask32(pl, lo1, hi1);
+                m1 = pam_mask_staged(s_cm[warp][1], s_ci[warp][1], npam1, r1, h0, h1, l0, l1, s0,
+                                     s1);
+            }
             const uint32_t n0 = __popc(m0), n1 = __popc(m1);
-            ncand += n0 + n1;
-            npairs += (unsigned long long)n0 * npat0 + (unsigned long long)n1 * npat1;
+            c_cand += n0 + n1;
+            c_pairs += n0 * npat0 + n1 * npat1;
             // batch-local start of bit 0 (a window may begin before its
             // batch; the class offset brings every hit's start back into it)
-            const uint32_t off0 = (uint32_t)(p0 - sg.base);
-            compare_direct<kNP>(m0, R0, h0, h1, l0, l1, s0, s1, off0, sg.batch, P);
-            compare_direct<kNP>(m1, R1, h0, h1, l0, l1, s0, s1, off0, sg.batch, P);
+            const uint32_t off0 = offb + pl;
+            compare_direct<kNP>(m0, R0, h0, h1, l0, l1, s0, s1, off0, batch, P);
+            compare_direct<kNP>(m1, R1, h0, h1, l0, l1, s0, s1, off0, batch, P);
         }
+        ncand += c_cand;
+        npairs += c_pairs;
     }
     for (int o = 16; o; o >>= 1) {
         ncand += __shfl_down_sync(0xFFFFFFFFu, ncand, o);
@@ -833,12 +890,13 @@ const ScanVariant kScanVariants[] = {
     variant<8, 8, 3>(64), variant<4, 8, 4>(64), variant<4, 16, 2>(128),
     // the default shape without the lean tile (more patterns per group)
     warp_variant<8, 8, 4, 4, 1024>(8),
-    // strand pairs compared directly (the default for up to 4 patterns per
-    // group): 1, 2 and 4 patterns in registers
-    direct_variant<1, 8, 4>(8), direct_variant<2, 8, 3>(8), direct_variant<4, 8, 3>(8),
+    // strand pairs compared directly (the default for up to 2 patterns per
+    // group; at 3.1 Gbp: 1 guide 1.86 ms against 2.80, 2 guides 2.78 against
+    // 2.92; with 4 patterns in registers 3.67 against 3.17 ms)
+    direct_variant<1, 8, 4>(8), direct_variant<2, 8, 4>(8),
 };
-constexpr int kFirstPairVariant = 9;      // direct_variant<1>; <2> and <4> follow
-constexpr uint32_t kPairMaxPatterns = 4;  // patterns per group up to which they are the default
+constexpr int kFirstPairVariant = 9;      // direct_variant<1>; <2> follows
+constexpr uint32_t kPairMaxPatterns = 2;  // patterns per group up to which they are the default
 constexpr int kNumScanVariants = sizeof(kScanVariants) / sizeof(kScanVariants[0]);
 static_assert(kNumScanVariants <= 16, "Engine::scan_occ_ holds 16 shapes");
 
@@ -1928,9 +1986,12 @@ int Engine::run_popcount(const std::vector<Request> &reqs, std::vector<Result> &
         // group and cannot run larger groups.
         uint32_t max_group_pats = 0;
         for (const ScanGroup &g : groups) max_group_pats = std::max(max_group_pats, g.pat_end - g.pat_begin);
+        uint32_t max_group_pam = 0;
+        for (const ScanGroup &g : groups) max_group_pam = std::max(max_group_pam, g.n_pam);
         auto usable = [&](int k) {
             const ScanVariant &x = kScanVariants[k];
-            return !x.paired || (pairs_ok && max_group_pats <= x.max_pats);
+            return !x.paired || (pairs_ok && max_group_pats <= x.max_pats &&
+                                 max_group_pam <= kDirectPamCells);
         };
         int v_default = 0;
         if (max_group_pats <= kPairMaxPatterns)
