@@ -68,7 +68,10 @@ def parse():
                     help="skip the 1-guide scan measurement (few_guide)")
     ap.add_argument("--no-ref-gpu", action="store_true",
                     help="--impl reference: skip timing the reference's own GPU kernel")
-    ap.add_argument("--serving-requests", type=int, default=64)
+    ap.add_argument("--serving-requests", type=int, default=1000)
+    ap.add_argument("--serving-c5", action="store_true",
+                    help="only the serving stream at its stated sizes (10,000 requests at "
+                         "500/s, 1,000 at 50/s and 200/s) over the resident genome")
     ap.add_argument("--serving-rate", type=float, default=200.0, help="arrivals per second")
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the batched mixed-PAM, serving, bulge and whole-process CLI "
@@ -290,7 +293,21 @@ def serving_requests(n, seed=5, max_guides=500, max_mm=4):
     return out
 
 
-def bench_serving(cof, g, n_nt, n_req, rate, seed=7, max_guides=500, max_mm=4, reqs=None):
+SERVING_MODES = (
+    # (name, max_requests_per_pass, ring_slices)
+    ("plain", 1, 1),            # one request per whole-genome pass
+    ("batched_passes", 0, 1),   # arrivals wait for the running pass, then share the next
+    ("batched", 0, 0),          # the ring: arrivals join at the next slice boundary
+)
+
+
+def bench_serving(cof, g, n_nt, n_req, rate, seed=7, max_guides=500, max_mm=4, reqs=None,
+                  modes=SERVING_MODES):
+    """A Poisson stream of requests through the server (cof_server_*), once
+    per mode: the plain loop (one request per whole-genome pass), batching
+    by whole passes, and the ring (continuous batching: the genome walked in
+    slices, arrivals admitted at every slice boundary).  value = the
+    stream's Gbp*guides / makespan; latency from submit to completion."""
     import numpy as np
     given = reqs is not None
     if not given:
@@ -299,12 +316,13 @@ def bench_serving(cof, g, n_nt, n_req, rate, seed=7, max_guides=500, max_mm=4, r
     arrivals = np.cumsum(rng.exponential(1.0 / rate, size=n_req))
     work = sum(n_nt * 1e-9 * len(r["patterns"]) for r in reqs)
     res = {}
-    # both modes run the default scan tile shape: first-time autotuning of a
-    # new request shape would otherwise be charged to whichever mode meets it
+    # every mode runs the default scan tile shape: first-time autotuning of
+    # a new request shape would otherwise be charged to whichever mode meets it
     prev = os.environ.get("COF_AUTOTUNE")
     os.environ["COF_AUTOTUNE"] = "0"
-    for mode, per_pass in (("plain", 1), ("batched", 0)):
-        srv = cof.Server(g, max_requests_per_pass=per_pass)
+    rows = {}
+    for mode, per_pass, ring in modes:
+        srv = cof.Server(g, max_requests_per_pass=per_pass, ring_slices=ring)
         t0 = time.perf_counter()
         tickets = []
         for a, r in zip(arrivals, reqs):
@@ -312,25 +330,51 @@ def bench_serving(cof, g, n_nt, n_req, rate, seed=7, max_guides=500, max_mm=4, r
             if dt > 0:
                 time.sleep(dt)
             tickets.append(srv.submit(**r))
-        lats = [srv.wait(t, as_text=None)[2] for t in tickets]
+        out = [srv.wait(t, as_text=None) for t in tickets]
         span = time.perf_counter() - t0
         st = srv.stats()
         srv.close()
-        lats.sort()
+        rows[mode] = [o[1] for o in out]
+        lats = sorted(o[2] for o in out)
         res[mode] = {"value": work / span, "unit": UNIT, "makespan_s": span,
                      "p50_ms": lats[len(lats) // 2],
                      "p99_ms": lats[min(len(lats) - 1, int(0.99 * len(lats)))],
-                     "passes": st["passes"], "largest_pass": st["largest_pass"]}
+                     "steps": st["passes"], "most_active": st["largest_pass"]}
     if prev is None:
         os.environ.pop("COF_AUTOTUNE", None)
     else:
         os.environ["COF_AUTOTUNE"] = prev
-    res["speedup"] = res["batched"]["value"] / res["plain"]["value"]
+    names = [m[0] for m in modes]
+    if len({tuple(v) for v in rows.values()}) != 1:
+        raise RuntimeError("serving modes returned different row counts")
+    if "plain" in names:
+        for m in names:
+            if m != "plain":
+                res[f"speedup_{m}"] = res[m]["value"] / res["plain"]["value"]
+        if "batched" in names:
+            res["speedup"] = res["batched"]["value"] / res["plain"]["value"]
+    res["requests"] = n_req
+    res["rate_per_s"] = rate
     if not given:
         res["workload"] = (f"{n_req} requests, Poisson arrivals at {rate:g}/s, guides log-uniform "
                            f"1..{max_guides} (17-25 nt), PAM NRG/NNGRRT/TTTN/NNNRRT, "
                            f"mm 0..{max_mm}, no bulges")
     return res
+
+
+def bench_serving_c5(cof, g, n_nt):
+    """The serving stream at its stated sizes: 10,000 requests at 500/s,
+    and 1,000 each at 50/s and 200/s, of the serving mix (guides 1..500
+    log-uniform, 17-25 nt, four PAMs, mm 0..4, no bulges)."""
+    out = {}
+    for n_req, rate, seed in ((1000, 50.0, 11), (1000, 200.0, 12), (10000, 500.0, 13)):
+        reqs = serving_requests(n_req, seed=seed)
+        r = bench_serving(cof, g, n_nt, n_req, rate, seed=seed + 100, reqs=reqs)
+        r["workload"] = (f"{n_req} requests, Poisson arrivals at {rate:g}/s, guides log-uniform "
+                         f"1..500 (17-25 nt), PAM NRG/NNGRRT/TTTN/NNNRRT, mm 0..4, no bulges")
+        out[f"{n_req}_at_{rate:g}"] = r
+        print(json.dumps({f"serving_c5_{n_req}_at_{rate:g}": r}), flush=True)
+    return out
 
 
 def bench_serving_bulge(cof, device, n_req=96, rate=4000.0, seed=9, scale=0.02):
@@ -755,6 +799,14 @@ def main():
     torch.cuda.synchronize()
     t_upload = time.perf_counter() - t0
 
+    if args.serving_c5:
+        if rank == 0:
+            bench_serving_c5(cof, g, n_nt)
+        g.close()
+        if dist:
+            dist.destroy_process_group()
+        return
+
     peaks = measure_peaks(local)
     req = dict(search_filter=cfg["filter"], patterns=cfg["patterns"],
                max_mismatches=cfg["max_mismatches"])
@@ -833,8 +885,8 @@ def main():
     if not args.no_extras and world == 1:
         line["batched_mixed_pam"] = bench_mixed_pam(g, n_nt, max(3, args.steps // 2))
         line["serving"] = bench_serving(cof, g, n_nt, args.serving_requests, args.serving_rate)
-        line["serving_small_requests"] = bench_serving(cof, g, n_nt, 4 * args.serving_requests,
-                                                       2000.0, seed=8, max_guides=4, max_mm=3)
+        line["serving_small_requests"] = bench_serving(cof, g, n_nt, 256, 2000.0, seed=8,
+                                                       max_guides=4, max_mm=3)
         line["bulge"] = bench_bulge(cof, local, 3, args.bulge_scale)
         line["bulge_full"] = bench_bulge_full(cof, local, 2)
         line["serving_bulge_mix"] = bench_serving_bulge(cof, local)

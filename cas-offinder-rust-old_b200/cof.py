@@ -103,7 +103,8 @@ _SINK = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.POINTER(_Piece))
 
 class _ServerConfig(ctypes.Structure):
     _fields_ = [("max_requests_per_pass", ctypes.c_uint32),
-                ("memory_budget_bytes", ctypes.c_uint64)]
+                ("memory_budget_bytes", ctypes.c_uint64),
+                ("ring_slices", ctypes.c_uint32)]
 
 
 _lib = None
@@ -363,11 +364,13 @@ def search(devices, max_mismatches, max_dna_bulges, max_rna_bulges, search_filte
 
 class Server:
     """Continuous-batching request loop over a resident Genome
-    (cof_server_*).  max_requests_per_pass=1 is the plain loop."""
+    (cof_server_*): the genome is walked as a ring of ring_slices slices (0:
+    about one per 512 Mnt), arrivals join at slice boundaries.
+    max_requests_per_pass=1 is the plain one-request-per-pass loop."""
 
-    def __init__(self, genome, max_requests_per_pass=0, memory_budget_bytes=0):
+    def __init__(self, genome, max_requests_per_pass=0, memory_budget_bytes=0, ring_slices=0):
         self.genome = genome
-        cfg = _ServerConfig(max_requests_per_pass, memory_budget_bytes)
+        cfg = _ServerConfig(max_requests_per_pass, memory_budget_bytes, ring_slices)
         h = ctypes.c_void_p()
         _check(_lib.cof_server_create(genome._h, ctypes.byref(cfg), ctypes.byref(h)))
         self._h = h
@@ -399,6 +402,8 @@ class Server:
         return data, n, lat.value
 
     def stats(self):
+        """steps (slice searches), completed, queued, and the most requests
+        active in one step."""
         s = (ctypes.c_uint64 * 4)()
         _check(_lib.cof_server_stats(self._h, s))
         return dict(passes=s[0], completed=s[1], queued=s[2], largest_pass=s[3])

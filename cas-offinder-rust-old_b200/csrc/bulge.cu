@@ -1273,7 +1273,7 @@ void build_eq16(const std::string &p, uint32_t eq_lo[16], uint32_t eq_hi[16]) {
 }  // namespace
 
 int Engine::run_bulge(const std::vector<Request> &reqs, std::vector<Result> &out, Error &err,
-                      const Sink *sink) {
+                      const Sink *sink, const SearchRange &range) {
     DeviceGenome &d = *dev_;
     const HostGenome &h = host_;
     const Bit4Tables &t = bit4();
@@ -1293,10 +1293,12 @@ int Engine::run_bulge(const std::vector<Request> &reqs, std::vector<Result> &out
         x.nch = (uint32_t)(b.last - b.first + 1);
         x.active_start = b.has_head ? (uint32_t)(2 * (h.boff[b.first + 1] - h.boff[b.first])) : 0;
         batches.push_back(x);
-        // active end positions (search.rs:913-927, :1087-1092)
-        for (uint64_t a = x.base + x.active_start; a < x.base + x.valid; a += kTile)
-            tiles.push_back(MyersTile{a, std::min<uint64_t>(a + kTile, x.base + x.valid),
-                                      (uint32_t)bi, 0, 0});
+        // active end positions (search.rs:913-927, :1087-1092) inside the
+        // searched range
+        const uint64_t e_lo = std::max(x.base + x.active_start, range.lo);
+        const uint64_t e_hi = std::min<uint64_t>(x.base + x.valid, range.hi);
+        for (uint64_t a = e_lo; a < e_hi; a += kTile)
+            tiles.push_back(MyersTile{a, std::min<uint64_t>(a + kTile, e_hi), (uint32_t)bi, 0, 0});
     }
     std::vector<MyersReqDev> rdev;
     std::vector<MyersPattern> pats;

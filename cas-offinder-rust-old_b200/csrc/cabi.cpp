@@ -90,9 +90,9 @@ int set_last_error(int code, const std::string &msg) { return fail(code, msg); }
 // that the next search on this genome overwrites, so it becomes owned
 // before the lock is let go.
 int genome_search(cof_genome *g, const std::vector<Request> &reqs, std::vector<Result> &out,
-                  Error &err) {
+                  Error &err, const SearchRange *range) {
     std::lock_guard<std::mutex> lk(g->mu);
-    const int rc = g->engine.search(reqs, out, err);
+    const int rc = g->engine.search(reqs, out, err, nullptr, range);
     if (rc) return rc;
     for (Result &r : out) {
         if (r.text && r.text != r.owned.data() && r.text != r.pooled.p) {
@@ -103,6 +103,9 @@ int genome_search(cof_genome *g, const std::vector<Request> &reqs, std::vector<R
     return rc;
 }
 uint64_t genome_nucl(const cof_genome *g) { return g->engine.host().n_nucl(); }
+// Length of the genome's chunk stream (2 x its bytes: odd chunks leave a
+// pad nibble), the coordinate space of SearchRange.
+uint64_t genome_stream_nt(const cof_genome *g) { return 2 * g->engine.host().n_bytes(); }
 int genome_free_device_bytes(cof_genome *g, uint64_t *free_bytes, Error &err) {
     std::lock_guard<std::mutex> lk(g->mu);
     if (g->engine.upload(err)) return err.code;

@@ -232,6 +232,16 @@ struct Sink {
     bool records = false;  // pieces carry MatchRec records
 };
 
+// Part of the genome a search covers, in global nucleotide coordinates of
+// the chunk stream: pattern starts [lo, hi) on the popcount path (rows and
+// raw Match lines), alignment end positions [lo, hi) on the bulge path.
+// Searches over consecutive ranges partition a whole search's rows; on the
+// popcount path their texts, concatenated in range order, are the whole
+// search's text.
+struct SearchRange {
+    uint64_t lo = 0, hi = ~0ull;
+};
+
 // Per-stage device timings of the last search (milliseconds, CUDA events).
 struct StageTimes {
     double scan_ms = 0, verify_ms = 0, format_ms = 0, d2h_ms = 0, total_ms = 0;
@@ -276,7 +286,7 @@ class Engine {
     // With a sink, the rows are handed to it piece by piece and `out` only
     // receives each request's row count.
     int search(const std::vector<Request> &reqs, std::vector<Result> &out, Error &err,
-               const Sink *sink = nullptr);
+               const Sink *sink = nullptr, const SearchRange *range = nullptr);
     int free_device_bytes(uint64_t *free_bytes, Error &err);
     const StageTimes &last_times() const { return times_; }
     Tuner &tuner() { return tuner_; }
@@ -284,10 +294,10 @@ class Engine {
 
   private:
     int run_popcount(const std::vector<Request> &reqs, std::vector<Result> &out, Error &err,
-                     const Sink *sink);
+                     const Sink *sink, const SearchRange &range);
     int run_bulge(const std::vector<Request> &reqs, std::vector<Result> &out, Error &err,
-                  const Sink *sink);
-    int run_raw(const Request &req, Result &out, Error &err);
+                  const Sink *sink, const SearchRange &range);
+    int run_raw(const Request &req, Result &out, Error &err, const SearchRange &range);
     int device_;
     uint64_t slice_text_hint_ = 0;  // bytes of the last sliced result (+2 %)
     int scan_occ_[16] = {};          // resident CTAs per SM of each scan shape (0: not set up)

@@ -909,10 +909,10 @@ __global__ void verify_kernel(GenomeDev G, const BatchDev *__restrict__ batches,
                               const uint32_t *__restrict__ fast2exact,
                               const RequestDev *__restrict__ reqs, const Hit *__restrict__ hits,
                               const Counters *__restrict__ scan_ctr, uint32_t hit_cap,
-                              uint32_t sg_bits, uint32_t e_bits,
-                              Row *__restrict__ rows, uint64_t *__restrict__ keys,
-                              uint32_t *__restrict__ vals, Counters *ctr,
-                              uint32_t *__restrict__ req_rows) {
+                              uint32_t sg_bits, uint32_t e_bits, uint64_t range_lo,
+                              uint64_t range_hi, Row *__restrict__ rows,
+                              uint64_t *__restrict__ keys, uint32_t *__restrict__ vals,
+                              Counters *ctr, uint32_t *__restrict__ req_rows) {
     // row sort key: request, then genome position, then the pattern's index
     // within its request (sg < 2^sg_bits, index < 2^e_bits)
     // the block steps through the hits together, so every lane of a warp
@@ -944,6 +944,9 @@ __global__ void verify_kernel(GenomeDev G, const BatchDev *__restrict__ batches,
             const uint32_t msmin = B.active_start > L - 1 ? B.active_start - (L - 1) : 0;
             if (h.s_local < msmin || h.s_local >= B.valid) break;
             const uint64_t sg = B.base + h.s_local;
+            // a scan group's window range is the union over its lengths:
+            // keep this pattern's starts inside the searched range
+            if (sg < range_lo || sg >= range_hi) break;
             // search_chunk_cpu count on the N-masked batch buffer (zero past
             // the batch's valid bytes)
             uint8_t g[kMaxPatternLen];
@@ -1223,8 +1226,10 @@ int Engine::free_device_bytes(uint64_t *free_bytes, Error &err) {
 }
 
 int Engine::search(const std::vector<Request> &reqs, std::vector<Result> &out, Error &err,
-                   const Sink *sink) {
+                   const Sink *sink, const SearchRange *range) {
     times_ = StageTimes();
+    const SearchRange whole;
+    const SearchRange &rg = range ? *range : whole;
     out.clear();
     out.resize(reqs.size());
     if (reqs.empty()) return kOk;
@@ -1244,7 +1249,7 @@ int Engine::search(const std::vector<Request> &reqs, std::vector<Result> &out, E
     for (size_t i = 0; i < reqs.size(); ++i) {
         if (reqs[i].raw && !reqs[i].max_db && !reqs[i].max_rb) {
             // search()'s raw stream: every window, no PAM prefilter
-            if (run_raw(reqs[i], out[i], err)) return err.code;
+            if (run_raw(reqs[i], out[i], err, rg)) return err.code;
             if (out[i].text) out[i].text = out[i].owned.data();
             if (sink) {  // one piece, without match records
                 Piece pc;
@@ -1285,13 +1290,13 @@ int Engine::search(const std::vector<Request> &reqs, std::vector<Result> &out, E
     if (!pr.empty()) {
         std::vector<Result> po;
         Sink sub;
-        if (run_popcount(pr, po, err, sub_sink(pi, sub))) return err.code;
+        if (run_popcount(pr, po, err, sub_sink(pi, sub), rg)) return err.code;
         for (size_t k = 0; k < pi.size(); ++k) out[pi[k]] = std::move(po[k]);
     }
     if (!br.empty()) {
         std::vector<Result> bo;
         Sink sub;
-        if (run_bulge(br, bo, err, sub_sink(bi, sub))) return err.code;
+        if (run_bulge(br, bo, err, sub_sink(bi, sub), rg)) return err.code;
         for (size_t k = 0; k < bi.size(); ++k) out[bi[k]] = std::move(bo[k]);
     }
     CU(cudaEventRecord(d.ev[9], d.stream));
@@ -1304,7 +1309,7 @@ int Engine::search(const std::vector<Request> &reqs, std::vector<Result> &out, E
 }
 
 int Engine::run_popcount(const std::vector<Request> &reqs, std::vector<Result> &out, Error &err,
-                         const Sink *sink) {
+                         const Sink *sink, const SearchRange &range) {
     out.clear();
     out.resize(reqs.size());
     DeviceGenome &d = *dev_;
@@ -1450,12 +1455,15 @@ int Engine::run_popcount(const std::vector<Request> &reqs, std::vector<Result> &
             for (const auto &lo_ : lens) {
                 const uint32_t L = lo_.first, o = lo_.second;
                 const uint64_t msmin = c1 > L - 1 ? c1 - (L - 1) : 0;
-                if (msmin >= b.valid) continue;
+                // this length's pattern starts in the batch and the range
+                const uint64_t s_lo = std::max(b.base + msmin, range.lo);
+                const uint64_t s_hi = std::min<uint64_t>(b.base + b.valid, range.hi);
+                if (s_hi <= s_lo) continue;
                 // shifted window start of pattern start s: s + kScanWindow - o
                 // (a 32-bit difference: L for an END anchor of any length)
                 const uint32_t shift = kScanWindow - o;
-                lo = std::min<uint64_t>(lo, b.base + msmin + shift);
-                hi = std::max<uint64_t>(hi, b.base + b.valid + shift);
+                lo = std::min<uint64_t>(lo, s_lo + shift);
+                hi = std::max<uint64_t>(hi, s_hi + shift);
             }
             if (hi <= lo) continue;
             ScanSeg sgm{};
@@ -1684,7 +1692,8 @@ int Engine::run_popcount(const std::vector<Request> &reqs, std::vector<Result> &
         const char *force = std::getenv("COF_SLICE_NT");  // tests: slice small genomes too
         if (force) slice_nt = std::max<uint64_t>(1024, std::strtoull(force, nullptr, 10));
         const uint64_t total_nt = 2 * h.boff.back();
-        bool ok = reqs.size() == 1 && !groups.empty() && total_nt >= 2 * slice_nt;
+        const bool whole = range.lo == 0 && range.hi == ~0ull;
+        bool ok = whole && reqs.size() == 1 && !groups.empty() && total_nt >= 2 * slice_nt;
         if (ok && !force) {
             // slice only when the text is expected to be large enough for
             // its copy to outweigh the slices' own cost (about 0.2 ms each).
@@ -1867,8 +1876,8 @@ int Engine::run_popcount(const std::vector<Request> &reqs, std::vector<Result> &
                 verify_kernel<<<d.n_sm * 8, 256, 0, s>>>(
                     d.view(), (const BatchDev *)tab(o_batch), (const ExactPattern *)tab(o_ep),
                     (const uint32_t *)tab(o_f2e), (const RequestDev *)tab(o_rdev), d.hits.p, d.ctr.p,
-                    (uint32_t)std::min<size_t>(d.hits.cap, 0xFFFFFFF0u), sg_bits, e_bits, d.rows.p,
-                    d.keys.p, d.vals.p, d.ctr.p, d.req_rows.p);
+                    (uint32_t)std::min<size_t>(d.hits.cap, 0xFFFFFFF0u), sg_bits, e_bits, range.lo,
+                    range.hi, d.rows.p, d.keys.p, d.vals.p, d.ctr.p, d.req_rows.p);
                 CU(cudaGetLastError());
                 ++times_.kernel_launches;
             }

@@ -172,7 +172,7 @@ __global__ void raw_write_kernel(GenomeDev G, const Row *__restrict__ rows, cons
 
 }  // namespace
 
-int Engine::run_raw(const Request &r, Result &out, Error &err) {
+int Engine::run_raw(const Request &r, Result &out, Error &err, const SearchRange &range) {
     DeviceGenome &d = *dev_;
     const HostGenome &h = host_;
     const Bit4Tables &t = bit4();
@@ -193,8 +193,8 @@ int Engine::run_raw(const Request &r, Result &out, Error &err) {
         const uint64_t c1 = b.has_head ? 2 * (h.boff[b.first + 1] - h.boff[b.first]) : 0;
         const uint64_t msmin = c1 > L - 1 ? c1 - (L - 1) : 0;  // search.rs:540-546
         RawSeg sg{};
-        sg.lo = x.base + msmin;
-        sg.hi = x.base + x.valid;
+        sg.lo = std::max(x.base + msmin, range.lo);
+        sg.hi = std::min<uint64_t>(x.base + x.valid, range.hi);
         if (sg.hi <= sg.lo) continue;
         sg.base = x.base;
         sg.clip = x.base + x.valid;

@@ -2,13 +2,17 @@
 // (cof_server_*, declared in include/cof.h).  No reference counterpart: the
 // reference runs one filter per process (cli_utils.rs:97-108).
 //
-// A worker thread owns the GPU work.  Each pass takes the queued requests in
+// A worker thread owns the GPU work.  It walks the genome as a ring of
+// slices, one slice per step.  Before each step it admits queued requests in
 // arrival order while their estimated device memory for candidate and row
-// buffers fits the budget (and while the pass has room, if a per-pass request
-// limit is set), runs them as one batched search (one launch per kernel
-// stage, scan groups shared by requests with the same filter), copies every
-// request's rows into its own result and wakes its waiter.  Requests that
-// arrive while a pass is on the GPU are admitted by the next pass.
+// buffers fits the budget (and while the step has room, if a per-pass
+// request limit is set); the step then searches its slice for every active
+// request as one batched pass (one launch per kernel stage, scan groups
+// shared by requests with the same filter).  A request that arrives while
+// others are on the GPU thus joins them at the next slice boundary instead
+// of waiting for a whole pass, and its work shares their launches.  After
+// one full turn of the ring its slices' rows, joined in genome order, are
+// its result, and its waiter is woken.
 #include <algorithm>
 #include <chrono>
 #include <condition_variable>
@@ -27,8 +31,9 @@
 struct cof_genome;  // cabi.cpp
 namespace cof {
 int genome_search(cof_genome *g, const std::vector<Request> &reqs, std::vector<Result> &out,
-                  Error &err);
+                  Error &err, const SearchRange *range);
 uint64_t genome_nucl(const cof_genome *g);
+uint64_t genome_stream_nt(const cof_genome *g);
 int genome_free_device_bytes(cof_genome *g, uint64_t *free_bytes, Error &err);
 }  // namespace cof
 
@@ -59,6 +64,14 @@ struct Done {
     uint64_t pass = 0;
 };
 
+// A request on the ring: the slices searched so far, each slice's rows.
+struct Active {
+    Pending p;
+    uint32_t searched = 0;
+    std::vector<cof::Result> piece;  // per slice
+    double device_ms = 0;
+};
+
 }  // namespace
 
 struct cof_server {
@@ -84,56 +97,112 @@ struct cof_server {
         return (uint64_t)(48.0 * per * mbp * (double)r.patterns.size()) + (1u << 20);
     }
 
+    // The ring: n_slices slices of the chunk stream, cut[j] the first
+    // coordinate of slice j.
+    uint32_t n_slices = 1;
+    std::vector<uint64_t> cut;
+
+    // A finished request's result: its slices' rows in genome order.
+    static Done assemble(Active &a, uint64_t step, Clock::time_point now) {
+        Done d;
+        d.pass = step;
+        d.device_ms = a.device_ms;
+        d.latency_ms = ms_since(a.p.t_submit, now);
+        auto src = [](const cof::Result &r) -> const char * {
+            return r.pooled.p ? r.pooled.p : r.owned.data();
+        };
+        if (a.piece.size() == 1) {
+            cof::Result &r = a.piece[0];
+            d.text_len = r.text_len;
+            d.n_rows = r.n_rows;
+            if (r.pooled.p) d.pooled = std::move(r.pooled);
+            else d.text = std::move(r.owned);
+            return d;
+        }
+        size_t total = 0;
+        for (const cof::Result &r : a.piece) {
+            total += r.text_len;
+            d.n_rows += r.n_rows;
+        }
+        d.pooled.p = cof::PinnedPool::get().acquire(total + 1);
+        if (!d.pooled.p) {
+            d.status = COF_E_OOM;
+            d.err = "out of page-locked host memory for a result";
+            return d;
+        }
+        size_t at = 0;
+        for (cof::Result &r : a.piece) {
+            if (r.text_len) std::memcpy(d.pooled.p + at, src(r), r.text_len);
+            at += r.text_len;
+            r.pooled.reset();
+            r.owned.clear();
+        }
+        d.pooled.p[total] = 0;
+        d.text_len = total;
+        return d;
+    }
+
     void loop() {
+        std::vector<Active> active;
+        uint32_t cur = 0;  // the slice the next step searches
         std::unique_lock<std::mutex> lk(mu);
         while (true) {
-            cv_work.wait(lk, [&] { return stop || !queue.empty(); });
-            if (stop && queue.empty()) return;
-            // admission: arrival order, memory budget, per-pass limit; the
-            // first request is always admitted so that none can starve
-            std::vector<Pending> batch;
+            cv_work.wait(lk, [&] { return stop || !queue.empty() || !active.empty(); });
+            if (stop && queue.empty() && active.empty()) return;
+            // admission at this slice boundary: arrival order, memory
+            // budget, per-step limit; with nothing active the first queued
+            // request is always admitted so that none can starve
             uint64_t bytes = 0;
+            for (const Active &x : active) bytes += x.p.est_bytes;
             while (!queue.empty()) {
                 const Pending &p = queue.front();
-                if (!batch.empty() && (bytes + p.est_bytes > budget ||
-                                       (max_per_pass && batch.size() >= max_per_pass)))
+                if (!active.empty() && (bytes + p.est_bytes > budget ||
+                                        (max_per_pass && active.size() >= max_per_pass)))
                     break;
-                if (!batch.empty() && p.req.cps != batch[0].req.cps) break;
+                if (!active.empty() && p.req.cps != active[0].p.req.cps) break;
                 bytes += p.est_bytes;
-                batch.push_back(std::move(queue.front()));
+                Active x;
+                x.p = std::move(queue.front());
                 queue.pop_front();
+                x.piece.resize(n_slices);
+                active.push_back(std::move(x));
             }
-            const uint64_t pass = ++passes;
-            max_pass_size = std::max<uint64_t>(max_pass_size, batch.size());
+            const uint64_t step = ++passes;
+            max_pass_size = std::max<uint64_t>(max_pass_size, active.size());
             lk.unlock();
             std::vector<cof::Request> reqs;
-            for (auto &p : batch) reqs.push_back(p.req);
+            for (const Active &x : active) reqs.push_back(x.p.req);
             std::vector<cof::Result> res;
             cof::Error err;
-            const int rc = cof::genome_search(g, reqs, res, err);
-            std::vector<Done> out(batch.size());
+            const cof::SearchRange rg{cut[cur], cur + 1 == n_slices ? ~0ull : cut[cur + 1]};
+            const int rc = cof::genome_search(g, reqs, res, err, n_slices > 1 ? &rg : nullptr);
             const auto now = Clock::now();
-            for (size_t i = 0; i < batch.size(); ++i) {
-                Done &d = out[i];
-                d.status = rc;
-                d.pass = pass;
-                if (rc) {
+            std::vector<std::pair<uint64_t, Done>> fin;
+            std::vector<Active> keep;
+            for (size_t i = 0; i < active.size(); ++i) {
+                Active &x = active[i];
+                if (rc) {  // the step failed: every request on the ring fails
+                    Done d;
+                    d.status = rc;
                     d.err = err.msg;
-                } else {
-                    if (res[i].pooled.p && res[i].text == res[i].pooled.p)
-                        d.pooled = std::move(res[i].pooled);
-                    else
-                        d.text.assign(res[i].text ? res[i].text : "", res[i].text_len);
-                    d.text_len = res[i].text_len;
-                    d.n_rows = res[i].n_rows;
-                    d.device_ms = res[i].device_ms;
+                    d.pass = step;
+                    d.latency_ms = ms_since(x.p.t_submit, now);
+                    fin.emplace_back(x.p.ticket, std::move(d));
+                    continue;
                 }
-                d.latency_ms = ms_since(batch[i].t_submit, now);
+                x.device_ms += res[i].device_ms;
+                x.piece[cur] = std::move(res[i]);
+                if (++x.searched == n_slices)
+                    fin.emplace_back(x.p.ticket, assemble(x, step, now));
+                else
+                    keep.push_back(std::move(x));
             }
+            active = std::move(keep);
+            cur = (cur + 1) % n_slices;
             lk.lock();
-            for (size_t i = 0; i < batch.size(); ++i) done[batch[i].ticket] = std::move(out[i]);
-            completed += batch.size();
-            cv_done.notify_all();
+            for (auto &f : fin) done[f.first] = std::move(f.second);
+            completed += fin.size();
+            if (!fin.empty()) cv_done.notify_all();
         }
     }
 };
@@ -162,6 +231,15 @@ COF_API int cof_server_create(cof_genome *g, const cof_server_config *cfg, cof_s
         budget = free_b / 2;  // half of what is free once the genome is resident
     }
     s->budget = budget;
+    // the ring: about one slice per 512 Mnt unless set; whole-genome passes
+    // for the plain one-request-per-pass loop
+    const uint64_t nt = cof::genome_stream_nt(g);
+    uint32_t k = cfg ? cfg->ring_slices : 0;
+    if (k == 0) k = (uint32_t)std::min<uint64_t>(16, std::max<uint64_t>(1, (nt + (512ull << 20) - 1) >> 29));
+    if (s->max_per_pass == 1) k = 1;
+    k = (uint32_t)std::min<uint64_t>(k, std::max<uint64_t>(1, nt));
+    s->n_slices = k;
+    for (uint32_t j = 0; j < k; ++j) s->cut.push_back(nt * j / k);
     s->worker = std::thread([s] { s->loop(); });
     *out = s;
     return COF_OK;

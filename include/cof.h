@@ -219,18 +219,27 @@ COF_API const char *cof_genome_record_name(const cof_genome *g, uint32_t record)
 COF_API uint32_t cof_genome_n_records(const cof_genome *g);
 
 /* Continuous-batching request server over a resident genome.  No reference
- * counterpart.  A worker thread repeatedly admits queued requests in arrival
- * order while their estimated device memory for candidate and row buffers
- * fits memory_budget_bytes (0 = half of the device memory free after the
- * genome upload) and, if max_requests_per_pass > 0, at most that many; runs
- * them as one cof_search_batch pass; and completes their tickets.  Requests
- * submitted while a pass runs join the next pass.  max_requests_per_pass = 1
- * gives the plain one-request-per-pass loop.  Direct searches on the same
- * genome are serialised with the server's passes. */
+ * counterpart.  A worker thread walks the genome as a ring of ring_slices
+ * slices, one slice per step: every step searches one slice for all active
+ * requests in one batched pass (cof_search_batch restricted to the slice's
+ * pattern starts, or alignment ends with bulges).  Before each step it
+ * admits queued requests in arrival order while their estimated device
+ * memory for candidate and row buffers fits memory_budget_bytes (0 = half
+ * of the device memory free after the genome upload) and, if
+ * max_requests_per_pass > 0, while the active requests number at most that
+ * many.  So a request that arrives while others are on the GPU joins them
+ * at the next slice boundary, and completes after one full turn of the
+ * ring, its slices' rows joined in genome order: the text cof_search gives
+ * (byte for byte on the popcount path; the same rows on the bulge path).
+ * ring_slices 0 picks about one slice per 512 Mnt (at most 16); 1 runs
+ * whole-genome passes.  max_requests_per_pass = 1 gives the plain
+ * one-request-per-pass loop (whole-genome passes).  Direct searches on the
+ * same genome are serialised with the server's steps. */
 typedef struct cof_server cof_server;
 typedef struct {
     uint32_t max_requests_per_pass;
     uint64_t memory_budget_bytes;
+    uint32_t ring_slices;
 } cof_server_config;
 
 COF_API int cof_server_create(cof_genome *g, const cof_server_config *cfg, cof_server **out);
@@ -241,7 +250,9 @@ COF_API int cof_server_submit(cof_server *s, const cof_request *req, uint64_t *t
  * *latency_ms (submit to completion, host clock) and forgets the ticket. */
 COF_API int cof_server_wait(cof_server *s, uint64_t ticket, int64_t timeout_ms, cof_result *out,
                             double *latency_ms);
-/* stats4 = {passes, completed requests, queued requests, largest pass}. */
+/* stats4 = {steps (slice searches; whole-genome passes when the ring has
+ * one slice), completed requests, queued requests, most requests active in
+ * one step}. */
 COF_API int cof_server_stats(cof_server *s, uint64_t *stats4);
 /* Finishes the queued requests, stops the worker and frees the server. */
 COF_API void cof_server_free(cof_server *s);
