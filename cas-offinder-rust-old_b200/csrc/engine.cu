@@ -890,12 +890,15 @@ const ScanVariant kScanVariants[] = {
     variant<8, 8, 3>(64), variant<4, 8, 4>(64), variant<4, 16, 2>(128),
     // the default shape without the lean tile (more patterns per group)
     warp_variant<8, 8, 4, 4, 1024>(8),
-    // strand pairs compared directly (the default for up to 2 patterns per
-    // group; at 3.1 Gbp: 1 guide 1.86 ms against 2.80, 2 guides 2.78 against
-    // 2.92; with 4 patterns in registers 3.67 against 3.17 ms)
-    direct_variant<1, 8, 4>(8), direct_variant<2, 8, 4>(8),
+    // strand pairs compared directly, the default for up to 2 patterns per
+    // group.  Scan at 3.1 Gbp: 1 guide 1.60 ms at six CTAs per SM (1.66 at
+    // five, 1.86 at four) against 2.80 ms for the lean tile; 2 guides 2.25
+    // (2.31, 2.45) against 2.92.  With 4 patterns in registers 3.23 against
+    // 3.17 ms, so none is compiled.
+    direct_variant<1, 8, 6>(8), direct_variant<2, 8, 6>(8),
+    direct_variant<1, 8, 5>(8), direct_variant<2, 8, 5>(8),
 };
-constexpr int kFirstPairVariant = 9;      // direct_variant<1>; <2> follows
+constexpr int kFirstPairVariant = 9;      // the first usable one from here is the default
 constexpr uint32_t kPairMaxPatterns = 2;  // patterns per group up to which they are the default
 constexpr int kNumScanVariants = sizeof(kScanVariants) / sizeof(kScanVariants[0]);
 static_assert(kNumScanVariants <= 16, "Engine::scan_occ_ holds 16 shapes");

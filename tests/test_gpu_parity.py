@@ -156,10 +156,10 @@ def test_cli_matches_oracle_cli(cof_mod, oracle_mod, golden, tmp_path):
 
 
 # per-warp work items: 0-4 and 8; CTA work items: 5-7; strand pairs compared
-# directly, holding 1 or 2 patterns per group: 9-10 (a request whose groups
+# directly, holding 1 or 2 patterns per group: 9-12 (a request whose groups
 # are larger runs the default shape instead)
-N_SCAN_VARIANTS = 11
-PAIR_VARIANTS = {9: 1, 10: 2}
+N_SCAN_VARIANTS = 13
+PAIR_VARIANTS = {9: 1, 10: 2, 11: 1, 12: 2}
 
 
 def _expected_variant(variant, patterns_per_group):
