@@ -642,7 +642,10 @@ __host__ __device__ constexpr size_t tb_warp_bytes(uint32_t tbl_words, uint32_t 
            ~(size_t)15;
 }
 
-template <int NW, int NO>
+// kBand: the budget DP comes from the candidate's band table in band_tbl
+// (budget_band_kernel<.., true>: band_stride words per candidate of the
+// chunk) instead of the wavefront below; a handed-on subtree reloads it.
+template <int NW, int NO, bool kBand>
 __global__ void __launch_bounds__(kTbWarps * 32)
 traceback_warp_kernel(GenomeDev G, const BatchDev *__restrict__ batches,
                       const MyersPattern *__restrict__ pats, const MyersReqDev *__restrict__ reqs,
@@ -650,7 +653,8 @@ traceback_warp_kernel(GenomeDev G, const BatchDev *__restrict__ batches,
                       const TbItem<NO> *__restrict__ items, uint32_t n_items, TbItem<NO> *spill,
                       uint32_t spill_cap, uint32_t iter_budget, uint32_t tbl_words,
                       uint32_t stk_cap, uint32_t margin, MyersRow *rows, uint32_t row_cap,
-                      uint64_t *keys, uint32_t *vals, Counters *ctr, uint32_t *req_rows) {
+                      uint64_t *keys, uint32_t *vals, Counters *ctr, uint32_t *req_rows,
+                      const uint64_t *__restrict__ band_tbl, uint32_t band_stride) {
     using Node = TbNode<NO>;
     extern __shared__ __align__(16) unsigned char tb_smem[];
     const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -690,17 +694,26 @@ traceback_warp_kernel(GenomeDev G, const BatchDev *__restrict__ batches,
             sisn[k] = P.isn[k];
             seff[k] = P.eff[k];
         }
+        const uint32_t bw = R.db + R.rb + 1;               // band cells per row
+        const int blo = (int)n - (int)L - (int)R.db;        // j - i of band cell 0
         uint64_t valid[NW];
 #pragma unroll
         for (int w = 0; w < NW; ++w) valid[w] = R.m_valid[w];
-        for (uint32_t k = lane; k < cols; k += 32) {  // row 0: F = 0 for every budget
+        if (kBand) {
+            const uint64_t *src = band_tbl + (uint64_t)ci * band_stride;
+            const uint32_t words = (L + 1) * bw * NW;
+            for (uint32_t k = lane; k < words; k += 32) tbl[k] = src[k];
+            __syncwarp();
+        } else {
+            for (uint32_t k = lane; k < cols; k += 32) {  // row 0: F = 0 for every budget
 #pragma unroll
-            for (int w = 0; w < NW; ++w) tbl[k * NW + w] = valid[w];
+                for (int w = 0; w < NW; ++w) tbl[k * NW + w] = valid[w];
+            }
+            __syncwarp();
         }
-        __syncwarp();
 
         // -- 1. budget DP wavefront, 32 pattern rows per pass
-        for (uint32_t r0 = 0; r0 < L; r0 += 32) {
+        for (uint32_t r0 = 0; !kBand && r0 < L; r0 += 32) {
             const uint32_t i = r0 + lane + 1;
             const bool row_on = i <= L;
             uint8_t pbi = 0, effi = 0;
@@ -754,7 +767,13 @@ traceback_warp_kernel(GenomeDev G, const BatchDev *__restrict__ batches,
         // F[b](ii, jj) <= mm - m ?
         auto feas = [&](uint32_t ii, uint32_t jj, uint32_t b, uint32_t m) -> bool {
             const uint32_t bit = b * T + (mm - m);
-            return (tbl[(ii * cols + jj) * NW + (bit >> 6)] >> (bit & 63)) & 1u;
+            uint32_t cell = ii * cols + jj;
+            if (kBand) {  // a cell off the band lies on no path within the caps
+                const int kk = (int)jj - (int)ii - blo;
+                if (kk < 0 || kk >= (int)bw) return false;
+                cell = ii * bw + (uint32_t)kk;
+            }
+            return (tbl[cell * NW + (bit >> 6)] >> (bit & 63)) & 1u;
         };
         if (!items) {
             if (!feas(L, n, R.db * rb1 + R.rb, 0)) continue;  // no alignment within the caps
@@ -1057,6 +1076,142 @@ budget_filter_kernel(GenomeDev G, const BatchDev *__restrict__ batches,
     }
 }
 
+// The budget pre-test on the band of the DP that alignments within the caps
+// can touch.  A path from the root (L, n) back to row 0 changes its
+// diagonal j - i by +1 per RNA bulge and -1 per DNA bulge, so every cell of
+// an alignment with at most db DNA and rb RNA bulges has
+// n - L - db <= j - i <= n - L + rb: db + rb + 1 cells per row (5 of the
+// 26 at L = 23, db = rb = 2).  Cells outside the band lie on no such path;
+// taking them as dead changes no value that a path within the caps reads,
+// so the test is exact and does a fifth of the work.  kBandMax: widest
+// band (db + rb + 1) this kernel takes.
+constexpr uint32_t kBandMax = 16;
+
+//
+// kTable: the same band DP for candidates known to pass (the traceback's
+// survivors), without the early exit, writing every row's band cells to the
+// candidate's table in tbl (tbl_stride words per candidate:
+// [(i * band + k) * NW + w]); the traceback then reads the table instead of
+// computing the DP again.
+template <int NW, int TW, bool kTable>
+__global__ void __launch_bounds__(kBfThreads)
+budget_band_kernel(GenomeDev G, const BatchDev *__restrict__ batches,
+                   const MyersPattern *__restrict__ pats, const MyersReqDev *__restrict__ reqs,
+                   const MyersCand *__restrict__ cand, uint32_t n_cand,
+                   MyersCand *__restrict__ out, uint32_t *n_out, uint64_t *__restrict__ tbl,
+                   uint32_t tbl_stride) {
+    extern __shared__ uint64_t bb_row[];  // [band cell * NW + w][thread]
+    const uint32_t tid = threadIdx.x;
+    auto Rw = [&](uint32_t k, int w) -> uint64_t & {
+        return bb_row[(k * NW + w) * kBfThreads + tid];
+    };
+    for (uint32_t base = blockIdx.x * kBfThreads; base < n_cand; base += gridDim.x * kBfThreads) {
+        const uint32_t ci = base + tid;
+        bool keep = false;
+        MyersCand c{0, 0, 0, 0};
+        if (ci < n_cand) {
+            c = cand[ci];
+            const BatchDev B = batches[c.batch];
+            const MyersPattern &P = pats[c.pattern];
+            const MyersReqDev &R = reqs[P.request];
+            const uint32_t L = P.L, t = c.t_local, T = R.T;
+            const uint32_t n = min(R.W, t + 1);
+            const uint32_t dsh = T * (R.rb + 1);
+            const uint32_t top = ((R.db + 1) * (R.rb + 1) - 1) * T + R.mm;  // root bit
+            const uint32_t bw = R.db + R.rb + 1;                         // band width
+            const int lo = (int)n - (int)L - (int)R.db;                  // j - i of band cell 0
+            uint64_t fullg[NW], valid[NW];
+#pragma unroll
+            for (int w = 0; w < NW; ++w) {
+                fullg[w] = R.m_full[w];
+                valid[w] = R.m_valid[w];
+            }
+            // the window's n text cells, cell k in bits 4 (k % 16) of word k / 16
+            const uint64_t tbase = B.base + t + 1 - n;
+            uint64_t tw0 = 0, tw1 = 0, tw2 = 0, tw3 = 0, tw4 = 0;
+            for (uint32_t k = 0; k < n; ++k) {
+                const uint64_t x = (uint64_t)nib(G.bit4, tbase + k) << (4 * (k & 15));
+                if (k < 16) tw0 |= x;
+                else if (k < 32) tw1 |= x;
+                else if (TW == 3 || k < 48) tw2 |= x;
+                else if (k < 64) tw3 |= x;
+                else tw4 |= x;
+            }
+            auto word = [&](int q) -> uint64_t {
+                return q == 0 ? tw0 : q == 1 ? tw1 : q == 2 ? tw2
+                     : (TW == 5 && q == 3) ? tw3 : (TW == 5 && q == 4) ? tw4 : 0ull;
+            };
+            // 16 text cells from cell cs on (cells below 0 read 0)
+            auto text16 = [&](int cs) -> uint64_t {
+                if (cs < 0) return cs <= -16 ? 0ull : tw0 << (4 * -cs);
+                const int q = cs >> 4, b = 4 * (cs & 15);
+                const uint64_t a = word(q), h = word(q + 1);
+                return b ? (a >> b) | (h << (64 - b)) : a;
+            };
+            uint64_t *tb = kTable ? tbl + (uint64_t)ci * tbl_stride : nullptr;
+            for (uint32_t k = 0; k < bw; ++k) {  // row 0: F = 0 for every budget
+                const int j = lo + (int)k;
+#pragma unroll
+                for (int w = 0; w < NW; ++w) {
+                    Rw(k, w) = (j >= 0 && j <= (int)n) ? valid[w] : 0;
+                    if (kTable) tb[k * NW + w] = Rw(k, w);
+                }
+            }
+            keep = true;
+            for (uint32_t i = 1; i <= L && (kTable || keep); ++i) {
+                const uint8_t pb = P.b4[i - 1], ef = P.eff[i - 1];
+                const bool isn1 = P.isn[i - 1], isn0 = i < L && P.isn[i],
+                           isn2 = i >= 2 && P.isn[i - 2];
+                const bool rna_ok = R.rb > 0 && !isn1 && !isn0 && !isn2;
+                const bool dna_ok = R.db > 0 && i < L && !(isn1 && isn0);
+                const int j0 = (int)i + lo;                   // column of band cell 0
+                const uint64_t tx16 = text16(j0 - 1);          // text cells j - 1
+                uint64_t left[NW], row_or = 0;
+#pragma unroll
+                for (int w = 0; w < NW; ++w) left[w] = 0;
+                for (uint32_t k = 0; k < bw; ++k) {
+                    const int j = j0 + (int)k;
+                    uint64_t dg[NW], up[NW], v[NW];
+#pragma unroll
+                    for (int w = 0; w < NW; ++w) {
+                        dg[w] = Rw(k, w);                          // (i - 1, j - 1)
+                        up[w] = k + 1 < bw ? Rw(k + 1, w) : 0ull;  // (i - 1, j)
+                        v[w] = 0;
+                    }
+                    if (j == 0) {  // column 0: only an RNA bulge from the cell above
+                        budget_cell<NW>(up, up, up, false, 0, rna_ok, false, T, dsh, R, v);
+                    } else if (j > 0 && j <= (int)n) {
+                        const uint8_t tx = (uint8_t)((tx16 >> (4 * k)) & 0xF);
+                        if (tx != 0) {  // a node over a padding cell is dead
+                            const uint32_t mc = loose(pb, tx) ? 0u : 1u;
+                            const bool dok = !(mc && isn1) && filt_ok(ef, tx);
+                            budget_cell<NW>(dg, up, left, dok, mc, rna_ok, dna_ok, T, dsh, R, v);
+                        }
+                    }
+#pragma unroll
+                    for (int w = 0; w < NW; ++w) {
+                        Rw(k, w) = v[w];
+                        left[w] = v[w];
+                        row_or |= v[w] & fullg[w];
+                        if (kTable) tb[(i * bw + k) * NW + w] = v[w];
+                    }
+                }
+                if (!row_or) keep = false;
+            }
+            // the root (L, n) is band cell db
+            if (keep) keep = (Rw(R.db, (int)(top >> 6)) >> (top & 63)) & 1u;
+        }
+        if (kTable) continue;
+        const unsigned full = 0xFFFFFFFFu;
+        const unsigned m = __ballot_sync(full, keep);
+        const uint32_t lane = tid & 31;
+        uint32_t o = 0;
+        if (lane == 0 && m) o = atomicAdd(n_out, (uint32_t)__popc(m));
+        o = __shfl_sync(full, o, 0);
+        if (keep) out[o + __popc(m & ((1u << lane) - 1u))] = c;
+    }
+}
+
 __device__ __forceinline__ uint64_t mpos_out(const MyersRow &w, const MyersReqDev &R,
                                              uint32_t strand) {
     if (!strand) return w.pos;
@@ -1229,15 +1384,18 @@ struct TbLaunch {
     uint32_t *vals;
     Counters *ctr;
     uint32_t *req_rows;
+    const uint64_t *band_tbl;  // the chunk's band tables (kBand)
+    uint32_t band_stride;
 };
 
-template <int NW, int NO>
+template <int NW, int NO, bool kBand>
 void launch_tb(const TbLaunch &a) {
-    traceback_warp_kernel<NW, NO><<<a.grid, a.threads, a.smem, a.s>>>(
+    traceback_warp_kernel<NW, NO, kBand><<<a.grid, a.threads, a.smem, a.s>>>(
         a.G, a.batches, a.pats, a.reqs, a.cand, a.n_cand,
         reinterpret_cast<const TbItem<NO> *>(a.items), a.n_items,
         reinterpret_cast<TbItem<NO> *>(a.spill), a.spill_cap, a.iter_budget, a.tbl_words,
-        a.stk_cap, a.margin, a.rows, a.row_cap, a.keys, a.vals, a.ctr, a.req_rows);
+        a.stk_cap, a.margin, a.rows, a.row_cap, a.keys, a.vals, a.ctr, a.req_rows, a.band_tbl,
+        a.band_stride);
 }
 
 // Myers Eq table of one pattern (build_peq, myers.rs:32-50, and the eq rule
@@ -1505,10 +1663,20 @@ int Engine::run_bulge(const std::vector<Request> &reqs, std::vector<Result> &out
         if (rd.nbits > kTbMaxBits) warp_tb = false;
         nw = std::max(nw, (rd.nbits + 63) / 64);
     }
-    uint32_t tbl_words = 0;  // 64-bit words of one warp's table
-    for (const MyersReqDev &rd : rdev) tbl_words = std::max(tbl_words, (rd.L + 1) * (rd.W + 1) * nw);
     if (const char *e = std::getenv("COF_BULGE_WARP"))
         if (e[0] == '0') warp_tb = false;
+    // the band of the budget DP that alignments within the caps can touch
+    // (db + rb + 1 cells per row): the pre-test computes only the band, and
+    // the warp traceback reads each survivor's band table from a kernel
+    // that writes them per chunk (COF_BULGE_BAND=0: whole tables)
+    uint32_t band = 0;
+    for (const MyersReqDev &rd : rdev) band = std::max(band, rd.db + rd.rb + 1);
+    bool banded = band <= kBandMax;
+    if (const char *e = std::getenv("COF_BULGE_BAND"))
+        if (e[0] == '0') banded = false;
+    uint32_t tbl_words = 0;  // 64-bit words of one warp's table
+    for (const MyersReqDev &rd : rdev)
+        tbl_words = std::max(tbl_words, (rd.L + 1) * (banded ? rd.db + rd.rb + 1 : rd.W + 1) * nw);
     // nodes with two op words for windows of more than 48 cells; a stack of
     // the walk margin plus kTbSpare slots
     const bool wide_nodes = wmax > 48;
@@ -1527,13 +1695,20 @@ int Engine::run_bulge(const std::vector<Request> &reqs, std::vector<Result> &out
         1, std::min<size_t>(kTbWarps, (size_t)smem_optin / warp_bytes));
     if (warp_tb && warp_bytes > (size_t)smem_optin) warp_tb = false;
     const size_t tb_smem = (size_t)tb_wpb * warp_bytes;
-    const void *tb_fn = wide_nodes ? (nw == 1 ? (const void *)traceback_warp_kernel<1, 2>
-                                              : (const void *)traceback_warp_kernel<2, 2>)
-                                   : (nw == 1 ? (const void *)traceback_warp_kernel<1, 1>
-                                              : (const void *)traceback_warp_kernel<2, 1>);
+    const void *tb_fn =
+        banded ? (wide_nodes ? (nw == 1 ? (const void *)traceback_warp_kernel<1, 2, true>
+                                        : (const void *)traceback_warp_kernel<2, 2, true>)
+                             : (nw == 1 ? (const void *)traceback_warp_kernel<1, 1, true>
+                                        : (const void *)traceback_warp_kernel<2, 1, true>))
+               : (wide_nodes ? (nw == 1 ? (const void *)traceback_warp_kernel<1, 2, false>
+                                        : (const void *)traceback_warp_kernel<2, 2, false>)
+                             : (nw == 1 ? (const void *)traceback_warp_kernel<1, 1, false>
+                                        : (const void *)traceback_warp_kernel<2, 1, false>));
     void (*tb_launch)(const TbLaunch &) =
-        wide_nodes ? (nw == 1 ? launch_tb<1, 2> : launch_tb<2, 2>)
-                   : (nw == 1 ? launch_tb<1, 1> : launch_tb<2, 1>);
+        banded ? (wide_nodes ? (nw == 1 ? launch_tb<1, 2, true> : launch_tb<2, 2, true>)
+                             : (nw == 1 ? launch_tb<1, 1, true> : launch_tb<2, 1, true>))
+               : (wide_nodes ? (nw == 1 ? launch_tb<1, 2, false> : launch_tb<2, 2, false>)
+                             : (nw == 1 ? launch_tb<1, 1, false> : launch_tb<2, 1, false>));
     int tb_blocks_per_sm = 1;
     if (warp_tb) {
         CU(cudaFuncSetAttribute(tb_fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tb_smem));
@@ -1546,20 +1721,34 @@ int Engine::run_bulge(const std::vector<Request> &reqs, std::vector<Result> &out
     const MyersCand *cands = d.mcand.p;
     uint32_t n_work = n_cand;
     if (warp_tb && n_cand) {
-        const size_t bf_smem = (size_t)(wmax + 1) * nw * kBfThreads * 8;
         if (d.mcand2.ensure(n_cand, err)) return err.code;
-        auto kfn = wmax > 48 ? (nw == 1 ? budget_filter_kernel<1, 5> : budget_filter_kernel<2, 5>)
-                             : (nw == 1 ? budget_filter_kernel<1, 3> : budget_filter_kernel<2, 3>);
-        CU(cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bf_smem));
+        const size_t bf_smem = (size_t)(banded ? band : wmax + 1) * nw * kBfThreads * 8;
+        const void *fn = banded ? (wmax > 48 ? (nw == 1 ? (const void *)budget_band_kernel<1, 5, false>
+                                                        : (const void *)budget_band_kernel<2, 5, false>)
+                                             : (nw == 1 ? (const void *)budget_band_kernel<1, 3, false>
+                                                        : (const void *)budget_band_kernel<2, 3, false>))
+                                : (wmax > 48 ? (nw == 1 ? (const void *)budget_filter_kernel<1, 5>
+                                                        : (const void *)budget_filter_kernel<2, 5>)
+                                             : (nw == 1 ? (const void *)budget_filter_kernel<1, 3>
+                                                        : (const void *)budget_filter_kernel<2, 3>));
+        CU(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bf_smem));
         int bf_per_sm = 1;
-        CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bf_per_sm, kfn, kBfThreads, bf_smem));
+        CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bf_per_sm, fn, kBfThreads, bf_smem));
         CU(cudaMemsetAsync(&d.ctr.p->rows, 0, 4, s));
         CU(cudaEventRecord(d.ev[3], s));
         const unsigned bg = (unsigned)std::max<uint64_t>(
             1, std::min<uint64_t>((n_cand + kBfThreads - 1) / kBfThreads,
                                   (uint64_t)d.n_sm * std::max(1, bf_per_sm)));
-        kfn<<<bg, kBfThreads, bf_smem, s>>>(d.view(), dB, dP, dR, d.mcand.p, n_cand, d.mcand2.p,
-                                           &d.ctr.p->rows);
+        const GenomeDev gv = d.view();
+        const MyersCand *cin = d.mcand.p;
+        MyersCand *cout = d.mcand2.p;
+        uint32_t *nout = &d.ctr.p->rows;
+        uint64_t *no_tbl = nullptr;
+        uint32_t no_stride = 0;
+        void *args[] = {(void *)&gv,  (void *)&dB,   (void *)&dP,     (void *)&dR,
+                        (void *)&cin, (void *)&n_cand, (void *)&cout, (void *)&nout,
+                        (void *)&no_tbl, (void *)&no_stride};
+        CU(cudaLaunchKernel(fn, dim3(bg), dim3(kBfThreads), args, bf_smem, s));
         CU(cudaGetLastError());
         CU(cudaEventRecord(d.ev[4], s));
         ++times_.kernel_launches;
@@ -1578,7 +1767,13 @@ int Engine::run_bulge(const std::vector<Request> &reqs, std::vector<Result> &out
     // rows) first walks a probe chunk; the later chunks are sized from its
     // rows per candidate to fill most of the row buffer, and a chunk that
     // overflows it is cut in proportion to its row count and walked again.
-    uint32_t chunk = std::max<uint32_t>(1, std::min<uint32_t>(n_work, kBulgeChunkMax));
+    // with band tables, a chunk's tables (tbl_words words per candidate)
+    // stay within 4 GiB of device memory
+    const uint32_t chunk_max = (warp_tb && banded)
+        ? (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(kBulgeChunkMax,
+                                                           (uint64_t(4) << 30) / (tbl_words * 8ull)))
+        : kBulgeChunkMax;
+    uint32_t chunk = std::max<uint32_t>(1, std::min<uint32_t>(n_work, chunk_max));
     bool probe = n_work > 4 * kBulgeProbe;
     if (probe) chunk = std::min(chunk, kBulgeProbe);
     if (const char *e = std::getenv("COF_BULGE_CHUNK")) {
@@ -1592,6 +1787,20 @@ int Engine::run_bulge(const std::vector<Request> &reqs, std::vector<Result> &out
         CU(cudaMemsetAsync(d.ctr.p, 0, sizeof(Counters), s));
         CU(cudaMemsetAsync(d.req_rows.p, 0, reqs.size() * 4, s));
         CU(cudaEventRecord(d.ev[3], s));
+        if (warp_tb && banded) {
+            // the chunk's band tables, one thread per surviving candidate
+            if (d.bandtbl.ensure((size_t)cn * tbl_words, err)) return err.code;
+            auto tfn = wmax > 48 ? (nw == 1 ? budget_band_kernel<1, 5, true> : budget_band_kernel<2, 5, true>)
+                                 : (nw == 1 ? budget_band_kernel<1, 3, true> : budget_band_kernel<2, 3, true>);
+            const size_t tsm = (size_t)band * nw * kBfThreads * 8;
+            CU(cudaFuncSetAttribute(tfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tsm));
+            const unsigned tg = (unsigned)std::max<uint64_t>(
+                1, std::min<uint64_t>((cn + kBfThreads - 1) / kBfThreads, (uint64_t)d.n_sm * 16));
+            tfn<<<tg, kBfThreads, tsm, s>>>(d.view(), dB, dP, dR, cands + c0, cn, nullptr, nullptr,
+                                            d.bandtbl.p, tbl_words);
+            CU(cudaGetLastError());
+            ++times_.kernel_launches;
+        }
         if (warp_tb) {
             // pass 0 walks every candidate; a warp that spends kTbBudget
             // iterations on one tree hands its remaining stack on, and the
@@ -1612,7 +1821,7 @@ int Engine::run_bulge(const std::vector<Request> &reqs, std::vector<Result> &out
                 TbLaunch a{tb, tb_wpb * 32, tb_smem, s, d.view(), dB, dP, dR, cands + c0, cn,
                            in, n_in, last ? nullptr : out_q, kTbQueue, tb_budget, tbl_words,
                            stk_cap, tb_mrg, d.mrows.p, (uint32_t)row_cap, d.keys.p, d.vals.p,
-                           d.ctr.p, d.req_rows.p};
+                           d.ctr.p, d.req_rows.p, banded ? d.bandtbl.p : nullptr, tbl_words};
                 tb_launch(a);
                 CU(cudaGetLastError());
                 ++times_.kernel_launches;
@@ -1658,7 +1867,7 @@ int Engine::run_bulge(const std::vector<Request> &reqs, std::vector<Result> &out
         const uint32_t nr = hc.rows;
         if (probe) {  // size the remaining chunks from the probe's rows per candidate
             const double per = std::max(1.0, (double)nr) / (double)cn;
-            chunk = (uint32_t)std::max(1.0, std::min((double)kBulgeChunkMax, row_fill / per));
+            chunk = (uint32_t)std::max(1.0, std::min((double)chunk_max, row_fill / per));
             probe = false;
         }
         times_.rows += nr;

@@ -222,6 +222,7 @@ class DeviceGenome {
     DevBuf<unsigned char> tb_items;  // two queues of handed-on traceback subtrees
     DevBuf<MatchRec> recs;           // match records of a streamed piece
     DevBuf<uint32_t> req_first;      // first sorted row of each request in a piece
+    DevBuf<uint64_t> bandtbl;        // band tables of a bulge chunk's survivors
 
     ~DeviceGenome() {
         bit4.release(); planes.release(); boff.release(); start.release(); end.release();
@@ -229,7 +230,7 @@ class DeviceGenome {
         hits.release(); rows.release(); keys.release(); keys2.release(); offs.release();
         vals.release(); vals2.release(); lens.release(); req_rows.release(); ctr.release();
         text.release(); cub_tmp.release(); mcand.release(); mcand2.release(); mrows.release();
-        tb_items.release(); recs.release(); req_first.release();
+        tb_items.release(); recs.release(); req_first.release(); bandtbl.release();
         for (auto &e : ev)
             if (e) cudaEventDestroy(e);
         if (fmt_done) cudaEventDestroy(fmt_done);

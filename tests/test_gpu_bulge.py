@@ -119,6 +119,31 @@ def test_warp_traceback_equals_thread_traceback(cof_mod, oracle_mod, monkeypatch
         assert nref == n and sorted(ref.splitlines()) == sorted(text.splitlines())
 
 
+@pytest.mark.parametrize("mm,db,rb", [(4, 2, 2), (3, 1, 1), (2, 3, 0), (2, 0, 3), (3, 3, 3)])
+def test_band_dp_equals_whole_table(cof_mod, oracle_mod, monkeypatch, mm, db, rb):
+    # the budget pre-test and the traceback read only the band of the DP
+    # that alignments within the caps can touch (db + rb + 1 cells per row);
+    # their rows must equal those of the whole-table kernels
+    # (COF_BULGE_BAND=0) and of the oracle, also near record and batch
+    # starts, where the window is shorter than L + db
+    import synth
+    cfg = synth.config_bulge(seed=7, scale=0.0004, n_guides=4, planted=6)
+    g = cof_mod.Genome()
+    cfg["genome"].load_into(g)
+    args = (cfg["filter"], cfg["patterns"], mm, db, rb)
+    monkeypatch.delenv("COF_BULGE_BAND", raising=False)
+    text, n = g.search(*args, chunks_per_search=3)
+    monkeypatch.setenv("COF_BULGE_BAND", "0")
+    text0, n0 = g.search(*args, chunks_per_search=3)
+    assert n == n0 > 0
+    assert sorted(text.splitlines()) == sorted(text0.splitlines())
+    o = oracle_mod.OracleGenome()
+    for name, data, s, e in cfg["genome"].chunks():
+        o.add_chunk(name, data, s, e)
+    ref, nref = o.search(*args, chunks_per_search=3)
+    assert nref == n and sorted(ref.splitlines()) == sorted(text.splitlines())
+
+
 @pytest.mark.parametrize("per_chunk", [1, 7, 64])
 def test_many_traceback_chunks(cof_mod, oracle_mod, monkeypatch, per_chunk):
     # the surviving candidates are walked in chunks whose row texts follow
