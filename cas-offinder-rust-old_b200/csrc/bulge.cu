@@ -520,7 +520,7 @@ traceback_kernel(GenomeDev G, const BatchDev *__restrict__ batches,
 constexpr int kTbWarps = 4;                  // warps per block (fewer for large tables)
 constexpr uint32_t kTbSpare = 80;            // stack slots beyond the walk margin
 constexpr uint32_t kTbMaxBits = 128;         // budget bits per cell (NW <= 2)
-constexpr uint32_t kTbBudget = 384;          // iterations on one tree before handing it on
+constexpr uint32_t kTbBudget = 128;          // iterations on one tree before handing it on
 constexpr uint32_t kTbQueue = 1u << 21;      // subtrees per hand-on queue
 constexpr int kTbMaxPasses = 24;             // the last pass finishes every tree
 constexpr uint32_t kTbText = 80;             // staged window text bytes (>= kMaxCells)
@@ -646,7 +646,7 @@ __host__ __device__ constexpr size_t tb_warp_bytes(uint32_t tbl_words, uint32_t 
 // (budget_band_kernel<.., true>: band_stride words per candidate of the
 // chunk) instead of the wavefront below; a handed-on subtree reloads it.
 template <int NW, int NO, bool kBand>
-__global__ void __launch_bounds__(kTbWarps * 32)
+__global__ void __launch_bounds__(kTbWarps * 32, 8)
 traceback_warp_kernel(GenomeDev G, const BatchDev *__restrict__ batches,
                       const MyersPattern *__restrict__ pats, const MyersReqDev *__restrict__ reqs,
                       const MyersCand *__restrict__ cand, uint32_t n_cand,
