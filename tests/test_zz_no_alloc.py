@@ -14,6 +14,7 @@ The buffers below are allocated by the test (the caller) before anything is
 measured; the entry point itself allocates nothing.  This file sorts last so
 that a run stopping at its first failure has run every other test first."""
 import ctypes
+import gc
 import random
 
 import pytest
@@ -111,12 +112,22 @@ def test_noalloc_matches_oracle_and_cof_search(cof_mod, oracle_mod, shape):
     cap = nref + 16
     seq_dev = torch.frombuffer(bytearray(_pack(seq)), dtype=torch.uint8).cuda()
     bufs = [torch.full((3 * cap,), -1, dtype=torch.int32, device="cuda") for _ in range(3)]
+    # genomes of earlier tests that the garbage collector frees in the middle
+    # of the measurement would raise the free memory: collect them first and
+    # keep the collector off while the calls are measured
+    gc.collect()
     torch.cuda.synchronize()
-    free = []
-    for rows in bufs:
-        rc, n_rows = _call(cof_mod, rows, seq_dev, len(seq), filt, full, mm, cap)
-        torch.cuda.synchronize()
-        free.append(torch.cuda.mem_get_info()[0])
+    free, results = [], []
+    gc.disable()
+    try:
+        for rows in bufs:
+            rc, n_rows = _call(cof_mod, rows, seq_dev, len(seq), filt, full, mm, cap)
+            torch.cuda.synchronize()
+            free.append(torch.cuda.mem_get_info()[0])
+            results.append((rc, n_rows, rows))
+    finally:
+        gc.enable()
+    for rc, n_rows, rows in results:
         assert rc == 0, cof_mod.load_library().cof_last_error().decode()
         assert n_rows == nref
         got = {tuple(x) for x in rows[:3 * n_rows].view(-1, 3).cpu().tolist()}
