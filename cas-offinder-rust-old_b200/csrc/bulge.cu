@@ -1789,7 +1789,10 @@ int Engine::run_bulge(const std::vector<Request> &reqs, std::vector<Result> &out
         CU(cudaEventRecord(d.ev[3], s));
         if (warp_tb && banded) {
             // the chunk's band tables, one thread per surviving candidate
-            if (d.bandtbl.ensure((size_t)cn * tbl_words, err)) return err.code;
+            // at least 8 MiB, so that a stream of small requests of varying
+            // size does not reallocate it (an allocation waits for the device)
+            if (d.bandtbl.ensure(std::max<size_t>((size_t)cn * tbl_words, size_t(1) << 20), err))
+                return err.code;
             auto tfn = wmax > 48 ? (nw == 1 ? budget_band_kernel<1, 5, true> : budget_band_kernel<2, 5, true>)
                                  : (nw == 1 ? budget_band_kernel<1, 3, true> : budget_band_kernel<2, 3, true>);
             const size_t tsm = (size_t)band * nw * kBfThreads * 8;
