@@ -954,6 +954,423 @@ traceback_warp_kernel(GenomeDev G, const BatchDev *__restrict__ batches,
     }
 }
 
+// traceback_slots_kernel: the band-table traceback with several candidates
+// resident in one warp.  traceback_warp_kernel pops up to 32 nodes of one
+// tree per step, but a tree's frontier is seldom that wide (every walk
+// starts from a single root, and most candidates have a few alignments),
+// so about half of its lanes idle.  Here a warp keeps up to n_slots
+// candidates loaded -- band table, window text, pattern cells and a
+// context record per slot, in shared memory -- and their nodes share one
+// stack, each node's st carrying its slot in bits 28-31.  A step pops up
+// to 32 nodes of any of the trees.  Whenever the stack holds fewer than
+// refill_below nodes, free slots take the next candidates (or handed-on
+// subtrees) of the work queue (refill_below + n_slots <= kTbSlotSpare keeps
+// the roots within the stack's spare slots); a slot is free again once no
+// node of its tree is left (a live-node count per slot).  A slot loaded
+// iter_budget steps ago hands its remaining nodes to the hand-on queue, as
+// traceback_warp_kernel does with its one tree; the other slots' nodes
+// stay.  Nodes are expanded, pruned and written as rows exactly as in
+// traceback_warp_kernel<.., true>; only the warp step that expands a node
+// differs, and the rows are sorted afterwards.
+constexpr uint32_t kTbSlotsMax = 4;     // most candidates resident per warp
+constexpr uint32_t kTbSlots = 3;        // the default (10 Mbp bulge set: 3 slots 9.99 ms
+                                        // device total, 4 slots 10.14, 2 slots 10.38)
+constexpr uint32_t kTbSlotSpare = 128;  // stack slots beyond the walk margin
+constexpr uint32_t kTbRefill = 32;      // refill free slots below this many stacked nodes
+constexpr uint32_t kTbSlotBits = 28;    // st bits below the slot index
+
+// one slot's context: the values of its candidate that a node's expansion
+// reads (window, pattern and request limits, chunks for the leaf rule)
+struct __align__(16) TbSlot {
+    uint64_t wstart;           // global nucleotide index of window text cell 0
+    uint32_t ci;               // candidate index (hand-on items)
+    uint32_t pattern, request;
+    uint32_t k_lo, k_hi;       // owning chunks of the window's first and last cell
+    uint32_t b_first, b_last;  // the batch's first and last chunk
+    uint32_t it0;              // the warp step the slot was loaded at
+    uint16_t L, n;             // pattern cells, window text cells
+    int16_t blo;               // j - i of band cell 0
+    uint8_t mm, T, db, rb, bw, pad;
+};
+
+__host__ __device__ constexpr size_t tb_al16(size_t x) { return (x + 15) & ~(size_t)15; }
+
+// byte offsets inside one warp's shared memory: the node stack, the slot
+// records, the band tables, the live-node counts, the window texts and the
+// pattern arrays (b4, isn, eff: kTbPat bytes each per slot)
+struct TbSlotLayout {
+    size_t stk, rec, tbl, live, text, pat, total;
+};
+__host__ __device__ inline TbSlotLayout tb_slot_layout(size_t node_bytes, uint32_t tbl_words,
+                                                       uint32_t cap, uint32_t slots) {
+    TbSlotLayout o{};
+    o.stk = 0;
+    o.rec = tb_al16((size_t)cap * node_bytes);
+    o.tbl = o.rec + tb_al16((size_t)slots * sizeof(TbSlot));
+    o.live = o.tbl + tb_al16((size_t)slots * tbl_words * 8);
+    o.text = o.live + tb_al16((size_t)slots * 4);
+    o.pat = o.text + tb_al16((size_t)slots * kTbText);
+    o.total = o.pat + tb_al16((size_t)slots * 3 * kTbPat);
+    return o;
+}
+
+// the chunk of batch chunks [first, last] that holds global nucleotide start
+__device__ __forceinline__ uint32_t tb_chunk_of(const GenomeDev &G, uint32_t first, uint32_t last,
+                                                uint64_t start) {
+    const uint64_t gbyte = start >> 1;
+    uint32_t lo = first, hi = last + 1;
+    while (hi - lo > 1) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (G.boff[mid] <= gbyte) lo = mid; else hi = mid;
+    }
+    return lo;
+}
+
+template <int NW, int NO>
+__global__ void __launch_bounds__(kTbWarps * 32, 6)
+traceback_slots_kernel(GenomeDev G, const BatchDev *__restrict__ batches,
+                       const MyersPattern *__restrict__ pats, const MyersReqDev *__restrict__ reqs,
+                       const MyersCand *__restrict__ cand, uint32_t n_cand,
+                       const TbItem<NO> *__restrict__ items, uint32_t n_items, TbItem<NO> *spill,
+                       uint32_t spill_cap, uint32_t iter_budget, uint32_t tbl_words,
+                       uint32_t stk_cap, uint32_t margin, uint32_t n_slots,
+                       uint32_t refill_below, MyersRow *rows,
+                       uint32_t row_cap, uint64_t *keys, uint32_t *vals, Counters *ctr,
+                       uint32_t *req_rows, const uint64_t *__restrict__ band_tbl,
+                       uint32_t band_stride) {
+    using Node = TbNode<NO>;
+    extern __shared__ __align__(16) unsigned char tb_smem[];
+    const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const TbSlotLayout lay = tb_slot_layout(sizeof(Node), tbl_words, stk_cap, n_slots);
+    unsigned char *wbase = tb_smem + warp * lay.total;
+    Node *stk = reinterpret_cast<Node *>(wbase + lay.stk);
+    TbSlot *srec = reinterpret_cast<TbSlot *>(wbase + lay.rec);
+    uint64_t *stbl = reinterpret_cast<uint64_t *>(wbase + lay.tbl);
+    int *live = reinterpret_cast<int *>(wbase + lay.live);
+    uint8_t *stext = wbase + lay.text;
+    uint8_t *spat = wbase + lay.pat;
+    const unsigned full = 0xFFFFFFFFu;
+    const uint32_t all_slots = (1u << n_slots) - 1u;
+    const uint32_t lanes_below = (1u << lane) - 1u;
+    const uint32_t n_work = items ? n_items : n_cand;
+
+    // warp-uniform state: nodes on the stack, occupied slots, steps taken
+    uint32_t size = 0, used = 0, iters = 0;
+    bool drained = false;  // the work queue is exhausted
+    bool may_spill = iter_budget != 0 && spill != nullptr;
+
+    // loads work item wi into free slot s and pushes its root; false for
+    // an empty hand-on entry or a root with no alignment within the caps
+    auto load = [&](uint32_t s, uint32_t wi) -> bool {
+        uint32_t ci = wi;
+        Node root{};
+        if (items) {
+            const TbItem<NO> it = items[wi];
+            if (it.cand == ~0u) return false;
+            ci = it.cand;
+            root = it.node;
+        }
+        const MyersCand c = cand[ci];
+        const BatchDev B = batches[c.batch];
+        const MyersPattern &P = pats[c.pattern];
+        const uint32_t req = P.request;
+        const MyersReqDev &R = reqs[req];
+        const uint32_t L = P.L, t = c.t_local;
+        const uint32_t n = min(R.W, t + 1);
+        const uint32_t bw = R.db + R.rb + 1;
+        const uint64_t wstart = B.base + t + 1 - n;
+        uint8_t *tx = stext + s * kTbText;
+        for (uint32_t k = lane; k < n; k += 32) tx[k] = nib(G.bit4, wstart + k);
+        uint8_t *pp = spat + s * (3 * kTbPat);
+        for (uint32_t k = lane; k < L; k += 32) {
+            pp[k] = P.b4[k];
+            pp[kTbPat + k] = P.isn[k];
+            pp[2 * kTbPat + k] = P.eff[k];
+        }
+        uint64_t *tbl = stbl + (size_t)s * tbl_words;
+        const uint64_t *src = band_tbl + (uint64_t)ci * band_stride;
+        const uint32_t words = (L + 1) * bw * NW;
+        for (uint32_t k = lane; k < words; k += 32) tbl[k] = src[k];
+        if (lane == 0) {
+            TbSlot o;
+            o.wstart = wstart;
+            o.ci = ci;
+            o.pattern = c.pattern;
+            o.request = req;
+            o.b_first = B.first;
+            o.b_last = B.first + B.nch - 1;
+            o.k_lo = tb_chunk_of(G, o.b_first, o.b_last, wstart);
+            o.k_hi = tb_chunk_of(G, o.b_first, o.b_last, B.base + t + 1);
+            o.it0 = iters;
+            o.L = (uint16_t)L;
+            o.n = (uint16_t)n;
+            o.blo = (int16_t)((int)n - (int)L - (int)R.db);
+            o.mm = (uint8_t)R.mm;
+            o.T = (uint8_t)R.T;
+            o.db = (uint8_t)R.db;
+            o.rb = (uint8_t)R.rb;
+            o.bw = (uint8_t)bw;
+            o.pad = 0;
+            srec[s] = o;
+        }
+        __syncwarp();
+        if (!items) {
+            // the root cell (L, n): full budget at mm; n - L - blo = db
+            // is its band cell
+            const uint32_t bit = (R.db * (R.rb + 1) + R.rb) * R.T + R.mm;
+            const uint64_t w = tbl[(L * bw + R.db) * NW + (bit >> 6)];
+            if (!((w >> (bit & 63)) & 1u)) return false;
+            root = Node{};
+            root.st = tb_st(L, n, 0, 0, 0);
+        }
+        if (lane == 0) {
+            root.st = (root.st & ((1u << kTbSlotBits) - 1u)) | (s << kTbSlotBits);
+            stk[size] = root;
+            live[s] = 1;
+        }
+        ++size;
+        return true;
+    };
+
+    for (;;) {
+        // -- refill: free slots take work while the stack is thin
+        if (!drained && size < refill_below && used != all_slots) {
+            const uint32_t want = n_slots - __popc(used);
+            uint32_t w0 = 0;
+            if (lane == 0)
+                w0 = (uint32_t)min(atomicAdd(&ctr->next_item, (unsigned long long)want),
+                                   (unsigned long long)n_work);
+            w0 = __shfl_sync(full, w0, 0);
+            const uint32_t got = min(want, n_work - w0);
+            if (got < want) drained = true;
+            for (uint32_t q = 0; q < got; ++q) {
+                const uint32_t s = __ffs(~used & all_slots) - 1;
+                if (load(s, w0 + q)) used |= 1u << s;
+            }
+            __syncwarp();
+        }
+        if (size == 0) {
+            if (drained) break;
+            continue;
+        }
+
+        // -- one step: pop k nodes (as traceback_warp_kernel: with
+        // size + 2k <= cap - margin the stack cannot overflow, and below
+        // that a one-node walk adds <= margin slots), expand them
+        ++iters;
+        const int room = (int)stk_cap - (int)margin - (int)size;
+        const uint32_t k = room >= 2 ? min(min(32u, size), (uint32_t)room / 2) : 1u;
+        const bool have = lane < k;
+        Node nd{};
+        if (have) nd = stk[size - 1 - lane];
+        size -= k;
+        __syncwarp();
+        struct Kid { uint32_t st, op; bool on; };
+        struct Leaf { uint64_t start, pos; uint32_t chunk, m, d, r, op; bool on; };
+        Kid ka{0, 0, false}, kb{0, 0, false}, kc{0, 0, false};
+        Leaf la{0, 0, 0, 0, 0, 0, 0, false}, lb{0, 0, 0, 0, 0, 0, 0, false};
+        uint32_t dep = 0, s = 0, pattern = 0, req = 0;
+        if (have) {
+            const uint32_t st = nd.st;
+            s = st >> kTbSlotBits;
+            const TbSlot &S = srec[s];
+            const uint32_t L = S.L, mm = S.mm, T = S.T, db = S.db, rb = S.rb;
+            const uint32_t bw = S.bw, rb1 = rb + 1;
+            const int blo = S.blo;
+            pattern = S.pattern;
+            req = S.request;
+            const uint8_t *tx = stext + s * kTbText;
+            const uint8_t *pb4 = spat + s * (3 * kTbPat), *pisn = pb4 + kTbPat, *peff = pisn + kTbPat;
+            const uint64_t *tbl = stbl + (size_t)s * tbl_words;
+            const uint32_t sbits = s << kTbSlotBits;
+            // F[b](ii, jj) <= mm - m ?  (a cell off the band lies on no
+            // path within the caps)
+            auto feas = [&](uint32_t ii, uint32_t jj, uint32_t b, uint32_t m) -> bool {
+                const int kk = (int)jj - (int)ii - blo;
+                if (kk < 0 || kk >= (int)bw) return false;
+                const uint32_t bit = b * T + (mm - m);
+                return (tbl[(ii * bw + (uint32_t)kk) * NW + (bit >> 6)] >> (bit & 63)) & 1u;
+            };
+            const uint32_t ni = st & 127, nj = (st >> 7) & 127, m = (st >> 14) & 63;
+            const uint32_t d = (st >> 20) & 15, r = (st >> 24) & 15;
+            dep = L - ni + d;
+            // convert_matches_myers: owning chunk and record-end drop
+            auto leaf = [&](Leaf &o, uint32_t jf, uint32_t lm, uint32_t ld, uint32_t lr,
+                            uint32_t op) {
+                const uint64_t start = S.wstart + jf;
+                const uint32_t k_lo = S.k_lo, k_hi = S.k_hi;
+                const uint32_t lo = k_lo == k_hi ? k_lo : tb_chunk_of(G, S.b_first, S.b_last, start);
+                const uint64_t pos = G.start[lo] + (start - 2 * G.boff[lo]);
+                const bool end_chrom = (lo == S.b_last) || G.start[lo + 1] == 0;
+                if (end_chrom && pos + (uint64_t)L + ld - lr > G.end[lo]) return;
+                o = Leaf{start, pos, lo, lm, ld, lr, op, true};
+            };
+            // diagonal: match / substitution
+            if (nj >= 1) {
+                const uint8_t t1 = tx[nj - 1];
+                const uint32_t mc = loose(pb4[ni - 1], t1) ? 0u : 1u;
+                if (!(mc && pisn[ni - 1]) && filt_ok(peff[ni - 1], t1) && m + mc <= mm) {
+                    if (ni == 1)
+                        leaf(la, nj - 1, m + mc, d, r, mc);
+                    else if (feas(ni - 1, nj - 1, (db - d) * rb1 + (rb - r), m + mc))
+                        ka = Kid{tb_st(ni - 1, nj - 1, m + mc, d, r) | sbits, mc, true};
+                }
+            }
+            // RNA bulge: pattern cell skipped
+            if (r < rb) {
+                const bool isn0 = ni < L && pisn[ni], isn2 = ni >= 2 && pisn[ni - 2];
+                if (!pisn[ni - 1] && !isn0 && !isn2) {
+                    if (ni == 1)
+                        leaf(lb, nj, m, d, r + 1, 3);
+                    else if (feas(ni - 1, nj, (db - d) * rb1 + (rb - r - 1), m))
+                        kb = Kid{tb_st(ni - 1, nj, m, d, r + 1) | sbits, 3, true};
+                }
+            }
+            // DNA bulge: text cell skipped
+            if (d < db && nj >= 1 && ni < L && !(pisn[ni - 1] && pisn[ni])) {
+                if (feas(ni, nj - 1, (db - d - 1) * rb1 + (rb - r), m))
+                    kc = Kid{tb_st(ni, nj - 1, m, d + 1, r) | sbits, 2, true};
+            }
+        }
+        // nd's ops with op at depth dep
+        auto ops_with = [&](uint32_t op, Node &o) {
+#pragma unroll
+            for (int q = 0; q < NO; ++q) o.ops[q] = nd.ops[q];
+            o.ops_hi = nd.ops_hi;
+            if (dep < 32) o.ops[0] |= (uint64_t)op << (2 * dep);
+            else if (NO == 2 && dep < 64) o.ops[NO - 1] |= (uint64_t)op << (2 * (dep - 32));
+            else o.ops_hi |= op << (2 * (dep - 32 * NO));
+        };
+        const uint32_t nc = (uint32_t)ka.on + kb.on + kc.on;
+        const uint32_t ne = (uint32_t)la.on + lb.on;
+        // push the children
+        uint32_t incl = nc;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(full, incl, o);
+            if ((int)lane >= o) incl += y;
+        }
+        const uint32_t tot = __shfl_sync(full, incl, 31);
+        uint32_t at = size + incl - nc;
+        auto push = [&](const Kid &k2) {
+            if (!k2.on) return;
+            Node o;
+            ops_with(k2.op, o);
+            o.st = k2.st;
+            stk[at++] = o;
+        };
+        push(ka);
+        push(kb);
+        push(kc);
+        size += tot;
+        if (have) atomicAdd(&live[s], (int)nc - 1);
+        // write the rows: one row-counter update per warp, one request
+        // count per warp when every writing lane has the same request
+        uint32_t einc = ne;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(full, einc, o);
+            if ((int)lane >= o) einc += y;
+        }
+        const uint32_t etot = __shfl_sync(full, einc, 31);
+        if (etot) {
+            uint32_t base = 0;
+            if (lane == 0) base = atomicAdd(&ctr->rows, etot);
+            base = __shfl_sync(full, base, 0);
+            const uint32_t writers = __ballot_sync(full, ne != 0);
+            const uint32_t req0 = __shfl_sync(full, req, __ffs(writers) - 1);
+            if (__all_sync(full, ne == 0 || req == req0)) {
+                if (lane == 0) atomicAdd(&req_rows[req0], etot);
+            } else if (ne) {
+                atomicAdd(&req_rows[req], ne);
+            }
+            uint32_t rr = base + einc - ne;
+            auto put = [&](const Leaf &l2) {
+                if (!l2.on) return;
+                if (rr < row_cap) {
+                    Node o;
+                    ops_with(l2.op, o);
+                    const uint32_t n_ops = dep + 1;
+                    MyersRow w;
+                    w.start = l2.start;
+                    w.pos = l2.pos;
+                    // steps 0..31, 32..63, 64..79 of the walk-back ops
+                    const uint64_t a1 = NO == 1 ? (uint64_t)o.ops_hi : o.ops[NO - 1];
+                    const uint32_t a2 = NO == 1 ? 0u : o.ops_hi;
+                    ops_forward(o.ops[0], a1, a2, n_ops, w.ops[0], w.ops[1], w.ops_hi);
+                    w.chunk = l2.chunk;
+                    w.pattern = pattern;
+                    w.n_ops = (uint8_t)n_ops;
+                    w.mm = (uint8_t)l2.m;
+                    w.db = (uint8_t)l2.d;
+                    w.rb = (uint8_t)l2.r;
+                    rows[rr] = w;
+                    keys[rr] = ((uint64_t)pattern << 34) | l2.start;
+                    vals[rr] = rr;
+                } else {
+                    ctr->overflow = 1;
+                }
+                ++rr;
+            };
+            put(la);
+            put(lb);
+        }
+        __syncwarp();
+
+        // -- slots whose trees are done are free again
+        const bool mine = lane < n_slots && ((used >> lane) & 1u);
+        const uint32_t done = __ballot_sync(full, mine && live[lane] == 0);
+        used &= ~done;
+        if (!may_spill) continue;
+        // -- slots loaded iter_budget steps ago hand their nodes on
+        const uint32_t over = __ballot_sync(
+            full, mine && !((done >> lane) & 1u) && iters - srec[lane].it0 >= iter_budget);
+        if (!over) continue;
+        const uint32_t cnt = __reduce_add_sync(full, ((over >> lane) & 1u) ? (uint32_t)live[lane] : 0u);
+        uint32_t sb = 0;
+        if (lane == 0) sb = atomicAdd(&ctr->hits, cnt);
+        sb = __shfl_sync(full, sb, 0);
+        if ((uint64_t)sb + cnt <= spill_cap) {
+            // compact the stack in place: the handed-on nodes go to the
+            // queue, the others keep their order (a chunk is read before
+            // any of it is overwritten, and writes land at or below it)
+            uint32_t kept = 0, sent = 0;
+            for (uint32_t b0 = 0; b0 < size; b0 += 32) {
+                const uint32_t idx = b0 + lane;
+                const bool in = idx < size;
+                Node x{};
+                if (in) x = stk[idx];
+                const bool go = in && ((over >> (x.st >> kTbSlotBits)) & 1u);
+                const bool keep = in && !go;
+                const uint32_t gm = __ballot_sync(full, go), km = __ballot_sync(full, keep);
+                __syncwarp();
+                // (the live counts make exactly cnt such nodes; the bound
+                // keeps the writes inside the reserved entries regardless)
+                const uint32_t q = sent + __popc(gm & lanes_below);
+                if (go && q < cnt) {
+                    TbItem<NO> it;
+                    it.cand = srec[x.st >> kTbSlotBits].ci;
+                    it.pad = 0;
+                    it.node = x;
+                    it.node.st &= (1u << kTbSlotBits) - 1u;
+                    spill[sb + q] = it;
+                }
+                if (keep) stk[kept + __popc(km & lanes_below)] = x;
+                sent += __popc(gm);
+                kept += __popc(km);
+                __syncwarp();
+            }
+            size = kept;
+            used &= ~over;
+            if ((over >> lane) & 1u) live[lane] = 0;
+        } else {
+            for (uint32_t q = sb + lane; q < spill_cap && q < sb + cnt; q += 32) spill[q].cand = ~0u;
+            may_spill = false;  // queue full: this warp finishes its trees
+        }
+        __syncwarp();
+    }
+}
+
 // Exact pre-test of the warp traceback, one thread per candidate: the
 // budget DP row by row (pattern cell i) with the previous row kept in
 // shared memory, interleaved by thread so that a warp's accesses hit
@@ -1386,6 +1803,8 @@ struct TbLaunch {
     uint32_t *req_rows;
     const uint64_t *band_tbl;  // the chunk's band tables (kBand)
     uint32_t band_stride;
+    uint32_t n_slots;          // candidates resident per warp (0: one tree per warp)
+    uint32_t refill_below;     // free slots take work while the stack holds fewer nodes
 };
 
 template <int NW, int NO, bool kBand>
@@ -1396,6 +1815,17 @@ void launch_tb(const TbLaunch &a) {
         reinterpret_cast<TbItem<NO> *>(a.spill), a.spill_cap, a.iter_budget, a.tbl_words,
         a.stk_cap, a.margin, a.rows, a.row_cap, a.keys, a.vals, a.ctr, a.req_rows, a.band_tbl,
         a.band_stride);
+}
+
+template <int NW, int NO>
+void launch_tb_slots(const TbLaunch &a) {
+    traceback_slots_kernel<NW, NO><<<a.grid, a.threads, a.smem, a.s>>>(
+        a.G, a.batches, a.pats, a.reqs, a.cand, a.n_cand,
+        reinterpret_cast<const TbItem<NO> *>(a.items), a.n_items,
+        reinterpret_cast<TbItem<NO> *>(a.spill), a.spill_cap, a.iter_budget, a.tbl_words,
+        a.stk_cap, a.margin, a.n_slots, a.refill_below, a.rows, a.row_cap, a.keys, a.vals, a.ctr,
+        a.req_rows,
+        a.band_tbl, a.band_stride);
 }
 
 // Myers Eq table of one pattern (build_peq, myers.rs:32-50, and the eq rule
@@ -1677,38 +2107,62 @@ int Engine::run_bulge(const std::vector<Request> &reqs, std::vector<Result> &out
     uint32_t tbl_words = 0;  // 64-bit words of one warp's table
     for (const MyersReqDev &rd : rdev)
         tbl_words = std::max(tbl_words, (rd.L + 1) * (banded ? rd.db + rd.rb + 1 : rd.W + 1) * nw);
-    // nodes with two op words for windows of more than 48 cells; a stack of
-    // the walk margin plus kTbSpare slots
+    // nodes with two op words for windows of more than 48 cells
     const bool wide_nodes = wmax > 48;
     const size_t item_bytes = wide_nodes ? sizeof(TbItem<2>) : sizeof(TbItem<1>);
-    const uint32_t tb_mrg = tb_margin(wmax), stk_cap = tb_mrg + kTbSpare;
+    const uint32_t tb_mrg = tb_margin(wmax);
+    // with band tables, kTbSlots candidates are resident per warp
+    // (traceback_slots_kernel); COF_TB_SLOTS sets 1..kTbSlotsMax, or 0 for
+    // one tree per warp (traceback_warp_kernel)
+    uint32_t tb_slots = banded ? kTbSlots : 0;
+    if (const char *e = std::getenv("COF_TB_SLOTS"))
+        if (banded) tb_slots = (uint32_t)std::min<long>(kTbSlotsMax, std::max(0L, std::atol(e)));
+    // free slots take work while the stack holds fewer than tb_refill
+    // nodes (COF_TB_REFILL)
+    uint32_t tb_refill = kTbRefill;
+    if (const char *e = std::getenv("COF_TB_REFILL"))
+        tb_refill = (uint32_t)std::min<int>(kTbSlotSpare - kTbSlotsMax, std::max(1, std::atoi(e)));
+    // a stack of the walk margin plus the spare slots
+    const uint32_t stk_cap = tb_mrg + (tb_slots ? kTbSlotSpare : kTbSpare);
     if (warp_tb && d.tb_items.ensure(2 * (size_t)kTbQueue * item_bytes, err)) return err.code;
     uint32_t tb_budget = kTbBudget;  // COF_TB_BUDGET: iterations before a tree is handed on
     if (const char *e = std::getenv("COF_TB_BUDGET")) tb_budget = (uint32_t)std::max(1, std::atoi(e));
-    const size_t warp_bytes = wide_nodes ? tb_warp_bytes<2>(tbl_words, stk_cap)
-                                         : tb_warp_bytes<1>(tbl_words, stk_cap);
-    // warps per block: kTbWarps, fewer when their tables exceed a block's
-    // shared memory (patterns of more than 32 cells with two-word cells)
     int smem_optin = 0;
     CU(cudaDeviceGetAttribute(&smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, d.device));
+    const size_t node_bytes = wide_nodes ? sizeof(TbNode<2>) : sizeof(TbNode<1>);
+    auto warp_bytes_for = [&](uint32_t slots) -> size_t {
+        if (slots) return tb_slot_layout(node_bytes, tbl_words, stk_cap, slots).total;
+        return wide_nodes ? tb_warp_bytes<2>(tbl_words, stk_cap) : tb_warp_bytes<1>(tbl_words, stk_cap);
+    };
+    // fewer slots while kTbWarps warps of them exceed a block's shared memory
+    while (tb_slots > 1 && warp_bytes_for(tb_slots) * kTbWarps > (size_t)smem_optin) --tb_slots;
+    const size_t warp_bytes = warp_bytes_for(tb_slots);
+    // warps per block: kTbWarps, fewer when their tables exceed a block's
+    // shared memory (patterns of more than 32 cells with two-word cells)
     const uint32_t tb_wpb = (uint32_t)std::max<size_t>(
         1, std::min<size_t>(kTbWarps, (size_t)smem_optin / warp_bytes));
     if (warp_tb && warp_bytes > (size_t)smem_optin) warp_tb = false;
     const size_t tb_smem = (size_t)tb_wpb * warp_bytes;
     const void *tb_fn =
-        banded ? (wide_nodes ? (nw == 1 ? (const void *)traceback_warp_kernel<1, 2, true>
-                                        : (const void *)traceback_warp_kernel<2, 2, true>)
-                             : (nw == 1 ? (const void *)traceback_warp_kernel<1, 1, true>
-                                        : (const void *)traceback_warp_kernel<2, 1, true>))
-               : (wide_nodes ? (nw == 1 ? (const void *)traceback_warp_kernel<1, 2, false>
-                                        : (const void *)traceback_warp_kernel<2, 2, false>)
-                             : (nw == 1 ? (const void *)traceback_warp_kernel<1, 1, false>
-                                        : (const void *)traceback_warp_kernel<2, 1, false>));
+        tb_slots ? (wide_nodes ? (nw == 1 ? (const void *)traceback_slots_kernel<1, 2>
+                                          : (const void *)traceback_slots_kernel<2, 2>)
+                               : (nw == 1 ? (const void *)traceback_slots_kernel<1, 1>
+                                          : (const void *)traceback_slots_kernel<2, 1>))
+        : banded ? (wide_nodes ? (nw == 1 ? (const void *)traceback_warp_kernel<1, 2, true>
+                                          : (const void *)traceback_warp_kernel<2, 2, true>)
+                               : (nw == 1 ? (const void *)traceback_warp_kernel<1, 1, true>
+                                          : (const void *)traceback_warp_kernel<2, 1, true>))
+                 : (wide_nodes ? (nw == 1 ? (const void *)traceback_warp_kernel<1, 2, false>
+                                          : (const void *)traceback_warp_kernel<2, 2, false>)
+                               : (nw == 1 ? (const void *)traceback_warp_kernel<1, 1, false>
+                                          : (const void *)traceback_warp_kernel<2, 1, false>));
     void (*tb_launch)(const TbLaunch &) =
-        banded ? (wide_nodes ? (nw == 1 ? launch_tb<1, 2, true> : launch_tb<2, 2, true>)
-                             : (nw == 1 ? launch_tb<1, 1, true> : launch_tb<2, 1, true>))
-               : (wide_nodes ? (nw == 1 ? launch_tb<1, 2, false> : launch_tb<2, 2, false>)
-                             : (nw == 1 ? launch_tb<1, 1, false> : launch_tb<2, 1, false>));
+        tb_slots ? (wide_nodes ? (nw == 1 ? launch_tb_slots<1, 2> : launch_tb_slots<2, 2>)
+                               : (nw == 1 ? launch_tb_slots<1, 1> : launch_tb_slots<2, 1>))
+        : banded ? (wide_nodes ? (nw == 1 ? launch_tb<1, 2, true> : launch_tb<2, 2, true>)
+                               : (nw == 1 ? launch_tb<1, 1, true> : launch_tb<2, 1, true>))
+                 : (wide_nodes ? (nw == 1 ? launch_tb<1, 2, false> : launch_tb<2, 2, false>)
+                               : (nw == 1 ? launch_tb<1, 1, false> : launch_tb<2, 1, false>));
     int tb_blocks_per_sm = 1;
     if (warp_tb) {
         CU(cudaFuncSetAttribute(tb_fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tb_smem));
@@ -1824,7 +2278,8 @@ int Engine::run_bulge(const std::vector<Request> &reqs, std::vector<Result> &out
                 TbLaunch a{tb, tb_wpb * 32, tb_smem, s, d.view(), dB, dP, dR, cands + c0, cn,
                            in, n_in, last ? nullptr : out_q, kTbQueue, tb_budget, tbl_words,
                            stk_cap, tb_mrg, d.mrows.p, (uint32_t)row_cap, d.keys.p, d.vals.p,
-                           d.ctr.p, d.req_rows.p, banded ? d.bandtbl.p : nullptr, tbl_words};
+                           d.ctr.p, d.req_rows.p, banded ? d.bandtbl.p : nullptr, tbl_words,
+                           tb_slots, tb_refill};
                 tb_launch(a);
                 CU(cudaGetLastError());
                 ++times_.kernel_launches;

@@ -144,6 +144,40 @@ def test_band_dp_equals_whole_table(cof_mod, oracle_mod, monkeypatch, mm, db, rb
     assert nref == n and sorted(ref.splitlines()) == sorted(text.splitlines())
 
 
+@pytest.mark.parametrize("slots,budget,chunk", [(4, 0, 0), (2, 0, 0), (1, 0, 0), (4, 1, 0),
+                                                (3, 2, 0), (4, 3, 5)])
+def test_slot_traceback_equals_one_tree_per_warp(cof_mod, oracle_mod, monkeypatch, slots, budget,
+                                                 chunk):
+    # traceback_slots_kernel keeps several candidates' trees in one warp's
+    # stack; its rows must equal those of one tree per warp
+    # (COF_TB_SLOTS=0) and of the oracle.  Budgets of 1-3 steps make slots
+    # hand their nodes on after almost every step (hand-on passes up to the
+    # last, which finishes every tree); small candidate chunks make many
+    # launches with few candidates
+    import synth
+    cfg = synth.config_bulge(seed=5, scale=0.0004, n_guides=6, planted=8)
+    g = cof_mod.Genome()
+    cfg["genome"].load_into(g)
+    args = (cfg["filter"], cfg["patterns"], 4, 2, 2)
+    monkeypatch.setenv("COF_TB_SLOTS", "0")
+    text0, n0 = g.search(*args)
+    monkeypatch.setenv("COF_TB_SLOTS", str(slots))
+    if budget:
+        monkeypatch.setenv("COF_TB_BUDGET", str(budget))
+    if chunk:
+        monkeypatch.setenv("COF_BULGE_CHUNK", str(chunk))
+    text, n = g.search(*args)
+    g.close()
+    assert n == n0 > 1000
+    assert sorted(text.splitlines()) == sorted(text0.splitlines())
+    o = oracle_mod.OracleGenome()
+    for name, data, s, e in cfg["genome"].chunks():
+        o.add_chunk(name, data, s, e)
+    ref, nref = o.search(*args)
+    o.close()
+    assert nref == n and sorted(ref.splitlines()) == sorted(text.splitlines())
+
+
 @pytest.mark.parametrize("per_chunk", [1, 7, 64])
 def test_many_traceback_chunks(cof_mod, oracle_mod, monkeypatch, per_chunk):
     # the surviving candidates are walked in chunks whose row texts follow
