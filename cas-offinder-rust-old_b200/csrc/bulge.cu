@@ -124,6 +124,21 @@ __device__ __forceinline__ int myers_step(Word eq, Word &vp, Word &vn, Word mask
     return (int)((hp >> sh) & 1u) - (int)((hn >> sh) & 1u);
 }
 
+// myers_step without the pattern mask: bits above the pattern's last cell
+// hold garbage that never reaches the score bit sh (the step only carries
+// toward higher bits)
+template <typename Word>
+__device__ __forceinline__ int myers_step_unmasked(Word eq, Word &vp, Word &vn, uint32_t sh) {
+    const Word x = eq | vn;
+    const Word d0 = (((x & vp) + vp) ^ vp) | x;
+    const Word hn = vp & d0;
+    const Word hp = vn | ~(vp | d0);
+    const Word xs = hp << 1;
+    vn = xs & d0;
+    vp = (hn << 1) | ~(xs | d0);
+    return (int)((hp >> sh) & 1u) - (int)((hn >> sh) & 1u);
+}
+
 // the Word-wide Eq vector of genome nibble b
 template <typename Word>
 __device__ __forceinline__ Word eq_word(const MyersPattern &P, uint32_t b) {
@@ -198,6 +213,7 @@ constexpr uint32_t kMfThreads = 256;
 constexpr uint32_t kMfMaxTiles = 32;           // tiles per block
 constexpr uint32_t kMfMaxForms = 8;            // PAM forms per launch
 constexpr uint32_t kMfQWords = kTile / 32 + 2; // Q bits: 1024 ends + <= 16 span shifts
+constexpr uint32_t kMfStage = 3072;            // candidates staged per block and round
 
 struct PamForm {
     uint32_t pam_off, pam_n, span_lo, span_hi;  // spans span_lo..span_hi
@@ -214,11 +230,17 @@ myers_tile_kernel(const uint8_t *__restrict__ bit4, const BatchDev *__restrict__
     extern __shared__ __align__(16) uint32_t mf_smem[];
     uint32_t *q_bits = mf_smem;                            // [tpb][n_forms][kMfQWords]
     uint32_t *ok_bits = q_bits + tpb * n_forms * kMfQWords; // [tpb][n_forms][32]
-    // [n_pat][16] when staged; 8-byte aligned (kMfQWords and 32 words are even)
+    // [16][n_pat] when staged (lanes of one tile read one nibble's row:
+    // no bank conflicts); 8-byte aligned (kMfQWords and 32 words are even)
     Word *seq = reinterpret_cast<Word *>(ok_bits + tpb * n_forms * 32);
     const bool staged = n_pat <= (uint32_t)kSmemMyers;
+    // a round's candidates (tile-local end, tile << 24 | pattern), then
+    // the stage's fill count and the round's base in the candidate list
+    uint2 *stage = reinterpret_cast<uint2 *>(seq + (staged ? n_pat * 16 : 0));
+    uint32_t *stage_n = reinterpret_cast<uint32_t *>(stage + kMfStage);
+    uint32_t *stage_base = stage_n + 1;
     if (staged)
-        for (uint32_t i = threadIdx.x; i < n_pat * 16; i += blockDim.x) seq[i] = eq_word<Word>(pats[i / 16], i % 16);
+        for (uint32_t i = threadIdx.x; i < n_pat * 16; i += blockDim.x) seq[i] = eq_word<Word>(pats[i % n_pat], i / n_pat);
     for (uint64_t tb = blockIdx.x; tb * tpb < n_tiles; tb += gridDim.x) {
         const uint64_t tile0 = tb * tpb;
         const uint32_t nt = (uint32_t)(n_tiles - tile0 < tpb ? n_tiles - tile0 : tpb);
@@ -261,44 +283,106 @@ myers_tile_kernel(const uint8_t *__restrict__ bit4, const BatchDev *__restrict__
             ok_bits[i] = v;
         }
         __syncthreads();
-        // streaming Myers per (tile, pattern)
-        for (uint32_t i = threadIdx.x; i < nt * n_pat; i += blockDim.x) {
-            const uint32_t tl = i / n_pat, p = i % n_pat;
-            const MyersTile T = tiles[tile0 + tl];
-            const BatchDev B = batches[T.batch];
-            const MyersPattern &P = pats[p];
-            const Word *eq = staged ? seq + 16 * p
-                                    : (sizeof(Word) == 4 ? reinterpret_cast<const Word *>(P.eq_lo) : nullptr);
-            const uint32_t *okw = ok_bits + (tl * n_forms + P.pad) * 32;
-            const uint32_t L = P.L;
-            const Word mask = myers_mask<Word>(L);
-            const uint32_t sh = L - 1;
-            Word vp = mask, vn = 0;
-            int score = (int)L;
-            const uint64_t ws = T.t0 >= warm ? ((T.t0 - warm) & ~15ull) : 0;
-            unsigned long long word = 0;
-            uint32_t okb = 0;
-            for (uint64_t q = ws; q < T.t1; ++q) {
-                if ((q & 15) == 0 || q == ws)
-                    word = __ldg(reinterpret_cast<const unsigned long long *>(bit4 + ((q >> 1) & ~7ull)));
-                const uint32_t b = (uint32_t)(word >> ((q & 15) * 4)) & 0xF;
-                Word e;
-                if constexpr (sizeof(Word) == 4) e = eq[b];
-                else e = staged ? eq[b] : eq_word<Word>(P, b);
-                score += myers_step<Word>(e, vp, vn, mask, sh);
-                if (q >= T.t0) {
-                    const uint32_t r = (uint32_t)(q - T.t0);
-                    if ((r & 31) == 0) okb = okw[r >> 5];
-                    if (((okb >> (r & 31)) & 1u) && score <= (int)P.E) {
-                        const uint32_t tlc = (uint32_t)(q - B.base);
+        // streaming Myers per (tile, pattern), in rounds of one item per
+        // thread.  A round's candidates are staged in shared memory and
+        // appended with one global atomic: one counter shared by every SM,
+        // taken once per candidate, serialised the whole sweep.
+        for (uint32_t round0 = 0; round0 < nt * n_pat; round0 += blockDim.x) {
+            if (threadIdx.x == 0) *stage_n = 0;
+            __syncthreads();
+            const uint32_t i = round0 + threadIdx.x;
+            if (i < nt * n_pat) {
+                const uint32_t tl = i / n_pat, p = i % n_pat;
+                const MyersTile T = tiles[tile0 + tl];
+                const BatchDev B = batches[T.batch];
+                const MyersPattern &P = pats[p];
+                const uint32_t *okw = ok_bits + (tl * n_forms + P.pad) * 32;
+                const uint32_t L = P.L;
+                const uint32_t sh = L - 1;
+                const int E = (int)P.E;
+                // The Eq lookup reads the staged table ([16][n_pat]: the lanes of
+                // one tile read one row, without bank conflicts) straight from
+                // shared memory; a pointer that could point to either table
+                // would make every lookup a generic load, which waits like a
+                // global one.
+                // No mask on vp / vn: every operation of the step (bitwise
+                // logic, the add, left shifts) carries information only toward
+                // higher bits, so the bits above L - 1 never reach bit L - 1,
+                // the only one the score reads.
+                Word vp = ~(Word)0, vn = 0;
+                int score = (int)L;
+                const uint64_t t0 = T.t0, t1 = T.t1;
+                // whole 16-cell genome words from ws (a multiple of 16) on:
+                // the warm-up words before t0 run the sweep alone, the others
+                // also collect a bit per cell whose score is within E.  Each
+                // word is loaded one word ahead, under the 16 steps before.
+                const uint64_t ws = t0 >= warm ? ((t0 - warm) & ~15ull) : 0;
+                const unsigned long long *gw = reinterpret_cast<const unsigned long long *>(bit4);
+                unsigned long long ahead = __ldg(gw + (ws >> 4));
+                for (uint64_t qw = ws; qw < t1; qw += 16) {
+                    const unsigned long long word = ahead;
+                    if (qw + 16 < t1) ahead = __ldg(gw + ((qw + 16) >> 4));
+                    uint32_t within = 0;
+                    if (qw + 16 <= t0) {
+#pragma unroll
+                        for (uint32_t k = 0; k < 16; ++k) {
+                            const uint32_t b = (uint32_t)(word >> (4 * k)) & 0xF;
+                            const Word e = staged ? seq[b * n_pat + p] : eq_word<Word>(P, b);
+                            score += myers_step_unmasked<Word>(e, vp, vn, sh);
+                        }
+                        continue;
+                    }
+#pragma unroll
+                    for (uint32_t k = 0; k < 16; ++k) {
+                        const uint32_t b = (uint32_t)(word >> (4 * k)) & 0xF;
+                        const Word e = staged ? seq[b * n_pat + p] : eq_word<Word>(P, b);
+                        score += myers_step_unmasked<Word>(e, vp, vn, sh);
+                        within |= ((uint32_t)(score - E - 1) >> 31) << k;  // score <= E
+                    }
+                    // cells of the tile only: [t0, t1)
+                    if (qw < t0) within &= ~0u << (uint32_t)(t0 - qw);
+                    if (qw + 16 > t1) within &= (1u << (uint32_t)(t1 - qw)) - 1u;
+                    if (!within) continue;
+                    // pam_ok bits of cells qw .. qw + 15 (tile offsets r0 .. r0 + 15)
+                    const int r0 = (int)(qw - t0);
+                    uint32_t okb;
+                    if (r0 >= 0) {
+                        const uint32_t wi = (uint32_t)r0 >> 5;
+                        const uint32_t hi = wi + 1 < 32 ? okw[wi + 1] : 0u;
+                        okb = __funnelshift_r(okw[wi], hi, (uint32_t)r0 & 31);
+                    } else {
+                        okb = okw[0] << (uint32_t)(-r0);
+                    }
+                    uint32_t hits = within & okb & 0xFFFFu;
+                    while (hits) {
+                        const uint32_t k = __ffs(hits) - 1;
+                        hits &= hits - 1;
+                        const uint32_t tlc = (uint32_t)(qw + k - B.base);
                         if (tlc + 1 >= L) {
-                            const uint32_t c = append_slot(&ctr->hits);
-                            if (c < cap) cand[c] = MyersCand{tlc, T.batch, p, 0};
-                            else ctr->overflow = 1;
+                            const uint32_t slot = atomicAdd(stage_n, 1u);
+                            if (slot < kMfStage) {
+                                stage[slot] = make_uint2(tlc, (tl << 24) | p);
+                            } else {  // stage full: straight to the list
+                                const uint32_t c = atomicAdd(&ctr->hits, 1u);
+                                if (c < cap) cand[c] = MyersCand{tlc, T.batch, p, 0};
+                                else ctr->overflow = 1;
+                            }
                         }
                     }
                 }
             }
+            __syncthreads();
+            const uint32_t ns = min(*stage_n, kMfStage);
+            if (threadIdx.x == 0) *stage_base = ns ? atomicAdd(&ctr->hits, ns) : 0u;
+            __syncthreads();
+            const uint32_t gb = *stage_base;
+            for (uint32_t k = threadIdx.x; k < ns; k += blockDim.x) {
+                const uint2 e = stage[k];
+                const uint64_t c = (uint64_t)gb + k;
+                if (c < cap) cand[c] = MyersCand{e.x, tiles[tile0 + (e.y >> 24)].batch, e.y & 0xFFFFFFu, 0};
+                else ctr->overflow = 1;
+            }
+            __syncthreads();  // the stage is read before the next round resets it
         }
     }
 }
@@ -1998,6 +2082,10 @@ int Engine::run_bulge(const std::vector<Request> &reqs, std::vector<Result> &out
     // stage 1: streaming Myers + PAM -> candidates
     Counters hc{};
     const uint32_t n_pat = (uint32_t)pats.size();
+    if (n_pat >= (1u << 24)) {  // staged candidates keep the pattern in 24 bits
+        err = {kUnsupported, "more than 16 M bulge patterns in one pass"};
+        return err.code;
+    }
     for (int attempt = 0; attempt < 2; ++attempt) {
         CU(cudaMemsetAsync(d.ctr.p, 0, sizeof(Counters), s));
         CU(cudaEventRecord(d.ev[1], s));
@@ -2012,7 +2100,8 @@ int Engine::run_bulge(const std::vector<Request> &reqs, std::vector<Result> &out
             const size_t eq_bytes = wide ? 8 : 4;
             auto smem_of = [&](uint32_t t) {
                 return (size_t)t * forms.size() * (kMfQWords + 32) * 4 +
-                       (n_pat <= (uint32_t)kSmemMyers ? (size_t)n_pat * 16 * eq_bytes : 0);
+                       (n_pat <= (uint32_t)kSmemMyers ? (size_t)n_pat * 16 * eq_bytes : 0) +
+                       (size_t)kMfStage * 8 + 8;
             };
             uint32_t tpb = 1;
             uint64_t best = ~0ull;
