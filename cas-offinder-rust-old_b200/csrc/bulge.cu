@@ -226,7 +226,8 @@ myers_tile_kernel(const uint8_t *__restrict__ bit4, const BatchDev *__restrict__
                   const MyersTile *__restrict__ tiles, uint64_t n_tiles,
                   const MyersPattern *__restrict__ pats, uint32_t n_pat,
                   const PamForm *__restrict__ forms, uint32_t n_forms, uint32_t tpb,
-                  uint32_t warm, MyersCand *cand, uint32_t cap, Counters *ctr) {
+                  uint32_t warm, MyersCand *cand, uint32_t cap, Counters *ctr,
+                  uint32_t stage_cap) {
     extern __shared__ __align__(16) uint32_t mf_smem[];
     uint32_t *q_bits = mf_smem;                            // [tpb][n_forms][kMfQWords]
     uint32_t *ok_bits = q_bits + tpb * n_forms * kMfQWords; // [tpb][n_forms][32]
@@ -360,7 +361,7 @@ myers_tile_kernel(const uint8_t *__restrict__ bit4, const BatchDev *__restrict__
                         const uint32_t tlc = (uint32_t)(qw + k - B.base);
                         if (tlc + 1 >= L) {
                             const uint32_t slot = atomicAdd(stage_n, 1u);
-                            if (slot < kMfStage) {
+                            if (slot < stage_cap) {
                                 stage[slot] = make_uint2(tlc, (tl << 24) | p);
                             } else {  // stage full: straight to the list
                                 const uint32_t c = atomicAdd(&ctr->hits, 1u);
@@ -372,7 +373,7 @@ myers_tile_kernel(const uint8_t *__restrict__ bit4, const BatchDev *__restrict__
                 }
             }
             __syncthreads();
-            const uint32_t ns = min(*stage_n, kMfStage);
+            const uint32_t ns = min(*stage_n, stage_cap);
             if (threadIdx.x == 0) *stage_base = ns ? atomicAdd(&ctr->hits, ns) : 0u;
             __syncthreads();
             const uint32_t gb = *stage_base;
@@ -2097,6 +2098,11 @@ int Engine::run_bulge(const std::vector<Request> &reqs, std::vector<Result> &out
             // n_sm x (blocks per SM); take the tpb with the fewest
             // waves x rounds (ties: more tiles per block)
             auto mf_fn = wide ? myers_tile_kernel<uint64_t> : myers_tile_kernel<uint32_t>;
+            // candidates staged per block round (COF_MYERS_STAGE lowers it:
+            // tests of the overflow to direct appends)
+            uint32_t stage_cap = kMfStage;
+            if (const char *e = std::getenv("COF_MYERS_STAGE"))
+                stage_cap = (uint32_t)std::min<long>(kMfStage, std::max(0L, std::atol(e)));
             const size_t eq_bytes = wide ? 8 : 4;
             auto smem_of = [&](uint32_t t) {
                 return (size_t)t * forms.size() * (kMfQWords + 32) * 4 +
@@ -2130,7 +2136,7 @@ int Engine::run_bulge(const std::vector<Request> &reqs, std::vector<Result> &out
             mf_fn<<<blocks, kMfThreads, smem, s>>>(
                 d.bit4.p, dB, (const MyersTile *)tab(o_t), tiles.size(), dP, n_pat,
                 (const PamForm *)tab(o_f), (uint32_t)forms.size(), tpb, warm, d.mcand.p, cap,
-                d.ctr.p);
+                d.ctr.p, stage_cap);
         } else {
             const uint64_t items = (uint64_t)tiles.size() * n_pat;
             const unsigned blocks = (unsigned)std::max<uint64_t>(

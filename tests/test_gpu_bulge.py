@@ -178,6 +178,35 @@ def test_slot_traceback_equals_one_tree_per_warp(cof_mod, oracle_mod, monkeypatc
     assert nref == n and sorted(ref.splitlines()) == sorted(text.splitlines())
 
 
+@pytest.mark.parametrize("stage", [0, 7, 100])
+def test_myers_stage_overflow(cof_mod, oracle_mod, monkeypatch, stage):
+    # myers_tile_kernel stages a round's candidates in shared memory and
+    # appends them with one atomic; candidates past the stage go straight
+    # to the list.  A stage of 0 / 7 / 100 candidates (COF_MYERS_STAGE; the
+    # default holds 3072) sends most of them that way: the rows must not
+    # change
+    import synth
+    cfg = synth.config_bulge(seed=8, scale=0.0004, n_guides=6, planted=8)
+    g = cof_mod.Genome()
+    cfg["genome"].load_into(g)
+    args = (cfg["filter"], cfg["patterns"], 4, 2, 2)
+    monkeypatch.delenv("COF_MYERS_STAGE", raising=False)
+    text0, n0 = g.search(*args)
+    cand0 = g.last_stats()["candidates"]
+    monkeypatch.setenv("COF_MYERS_STAGE", str(stage))
+    text, n = g.search(*args)
+    assert g.last_stats()["candidates"] == cand0 > 10000
+    g.close()
+    assert n == n0 > 1000
+    assert sorted(text.splitlines()) == sorted(text0.splitlines())
+    o = oracle_mod.OracleGenome()
+    for name, data, s, e in cfg["genome"].chunks():
+        o.add_chunk(name, data, s, e)
+    ref, nref = o.search(*args)
+    o.close()
+    assert nref == n and sorted(ref.splitlines()) == sorted(text.splitlines())
+
+
 @pytest.mark.parametrize("per_chunk", [1, 7, 64])
 def test_many_traceback_chunks(cof_mod, oracle_mod, monkeypatch, per_chunk):
     # the surviving candidates are walked in chunks whose row texts follow
