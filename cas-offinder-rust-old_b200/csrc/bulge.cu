@@ -1044,9 +1044,9 @@ traceback_warp_kernel(GenomeDev G, const BatchDev *__restrict__ batches,
 // tree per step, but a tree's frontier is seldom that wide (every walk
 // starts from a single root, and most candidates have a few alignments),
 // so about half of its lanes idle.  Here a warp keeps up to n_slots
-// candidates loaded -- band table, window text, pattern cells and a
-// context record per slot, in shared memory -- and their nodes share one
-// stack, each node's st carrying its slot in bits 28-31.  A step pops up
+// candidates loaded -- window text, pattern cells, a context record and
+// (unless kGT) the band table per slot, in shared memory -- and their nodes
+// share one stack, each node's st carrying its slot in bits 28-31.  A step pops up
 // to 32 nodes of any of the trees.  Whenever the stack holds fewer than
 // refill_below nodes, free slots take the next candidates (or handed-on
 // subtrees) of the work queue (refill_below + n_slots <= kTbSlotSpare keeps
@@ -1057,9 +1057,13 @@ traceback_warp_kernel(GenomeDev G, const BatchDev *__restrict__ batches,
 // stay.  Nodes are expanded, pruned and written as rows exactly as in
 // traceback_warp_kernel<.., true>; only the warp step that expands a node
 // differs, and the rows are sorted afterwards.
-constexpr uint32_t kTbSlotsMax = 4;     // most candidates resident per warp
-constexpr uint32_t kTbSlots = 3;        // the default (10 Mbp bulge set: 3 slots 9.99 ms
-                                        // device total, 4 slots 10.14, 2 slots 10.38)
+constexpr uint32_t kTbSlotsMax = 8;     // most candidates resident per warp
+// the defaults.  Band tables read from global memory: 6 slots (10 Mbp bulge
+// set, device total: 3 slots 8.75 ms, 4: 8.58, 6: 8.34, 8: 8.55).  Tables
+// copied into the slots: 3 (2: 10.38, 3: 9.99, 4: 10.14 with the earlier
+// Myers filter; 3: 8.66 with the current one).
+constexpr uint32_t kTbSlotsGlobal = 6;
+constexpr uint32_t kTbSlotsShared = 3;
 constexpr uint32_t kTbSlotSpare = 128;  // stack slots beyond the walk margin
 constexpr uint32_t kTbRefill = 32;      // refill free slots below this many stacked nodes
 constexpr uint32_t kTbSlotBits = 28;    // st bits below the slot index
@@ -1111,7 +1115,10 @@ __device__ __forceinline__ uint32_t tb_chunk_of(const GenomeDev &G, uint32_t fir
     return lo;
 }
 
-template <int NW, int NO>
+// kGT: the band tables are read where budget_band_kernel<.., true> wrote
+// them, in global memory (through L1), instead of being copied into the
+// slot; a slot then needs a few hundred bytes, so more slots fit.
+template <int NW, int NO, bool kGT>
 __global__ void __launch_bounds__(kTbWarps * 32, 6)
 traceback_slots_kernel(GenomeDev G, const BatchDev *__restrict__ batches,
                        const MyersPattern *__restrict__ pats, const MyersReqDev *__restrict__ reqs,
@@ -1126,7 +1133,7 @@ traceback_slots_kernel(GenomeDev G, const BatchDev *__restrict__ batches,
     using Node = TbNode<NO>;
     extern __shared__ __align__(16) unsigned char tb_smem[];
     const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const TbSlotLayout lay = tb_slot_layout(sizeof(Node), tbl_words, stk_cap, n_slots);
+    const TbSlotLayout lay = tb_slot_layout(sizeof(Node), kGT ? 0u : tbl_words, stk_cap, n_slots);
     unsigned char *wbase = tb_smem + warp * lay.total;
     Node *stk = reinterpret_cast<Node *>(wbase + lay.stk);
     TbSlot *srec = reinterpret_cast<TbSlot *>(wbase + lay.rec);
@@ -1172,10 +1179,12 @@ traceback_slots_kernel(GenomeDev G, const BatchDev *__restrict__ batches,
             pp[kTbPat + k] = P.isn[k];
             pp[2 * kTbPat + k] = P.eff[k];
         }
-        uint64_t *tbl = stbl + (size_t)s * tbl_words;
         const uint64_t *src = band_tbl + (uint64_t)ci * band_stride;
-        const uint32_t words = (L + 1) * bw * NW;
-        for (uint32_t k = lane; k < words; k += 32) tbl[k] = src[k];
+        if (!kGT) {
+            uint64_t *tbl = stbl + (size_t)s * tbl_words;
+            const uint32_t words = (L + 1) * bw * NW;
+            for (uint32_t k = lane; k < words; k += 32) tbl[k] = src[k];
+        }
         if (lane == 0) {
             TbSlot o;
             o.wstart = wstart;
@@ -1203,7 +1212,8 @@ traceback_slots_kernel(GenomeDev G, const BatchDev *__restrict__ batches,
             // the root cell (L, n): full budget at mm; n - L - blo = db
             // is its band cell
             const uint32_t bit = (R.db * (R.rb + 1) + R.rb) * R.T + R.mm;
-            const uint64_t w = tbl[(L * bw + R.db) * NW + (bit >> 6)];
+            const uint32_t at = (L * bw + R.db) * NW + (bit >> 6);
+            const uint64_t w = kGT ? src[at] : stbl[(size_t)s * tbl_words + at];
             if (!((w >> (bit & 63)) & 1u)) return false;
             root = Node{};
             root.st = tb_st(L, n, 0, 0, 0);
@@ -1266,7 +1276,8 @@ traceback_slots_kernel(GenomeDev G, const BatchDev *__restrict__ batches,
             req = S.request;
             const uint8_t *tx = stext + s * kTbText;
             const uint8_t *pb4 = spat + s * (3 * kTbPat), *pisn = pb4 + kTbPat, *peff = pisn + kTbPat;
-            const uint64_t *tbl = stbl + (size_t)s * tbl_words;
+            const uint64_t *tbl = kGT ? band_tbl + (uint64_t)S.ci * band_stride
+                                      : stbl + (size_t)s * tbl_words;
             const uint32_t sbits = s << kTbSlotBits;
             // F[b](ii, jj) <= mm - m ?  (a cell off the band lies on no
             // path within the caps)
@@ -1902,9 +1913,9 @@ void launch_tb(const TbLaunch &a) {
         a.band_stride);
 }
 
-template <int NW, int NO>
+template <int NW, int NO, bool kGT>
 void launch_tb_slots(const TbLaunch &a) {
-    traceback_slots_kernel<NW, NO><<<a.grid, a.threads, a.smem, a.s>>>(
+    traceback_slots_kernel<NW, NO, kGT><<<a.grid, a.threads, a.smem, a.s>>>(
         a.G, a.batches, a.pats, a.reqs, a.cand, a.n_cand,
         reinterpret_cast<const TbItem<NO> *>(a.items), a.n_items,
         reinterpret_cast<TbItem<NO> *>(a.spill), a.spill_cap, a.iter_budget, a.tbl_words,
@@ -2206,12 +2217,16 @@ int Engine::run_bulge(const std::vector<Request> &reqs, std::vector<Result> &out
     const bool wide_nodes = wmax > 48;
     const size_t item_bytes = wide_nodes ? sizeof(TbItem<2>) : sizeof(TbItem<1>);
     const uint32_t tb_mrg = tb_margin(wmax);
-    // with band tables, kTbSlots candidates are resident per warp
-    // (traceback_slots_kernel); COF_TB_SLOTS sets 1..kTbSlotsMax, or 0 for
-    // one tree per warp (traceback_warp_kernel)
-    uint32_t tb_slots = banded ? kTbSlots : 0;
+    // with band tables, several candidates are resident per warp
+    // (traceback_slots_kernel), reading their tables from global memory
+    // (COF_TB_GLOBAL=0: copied into the slots); COF_TB_SLOTS sets
+    // 1..kTbSlotsMax, or 0 for one tree per warp (traceback_warp_kernel)
+    bool tb_global = true;
+    if (const char *e = std::getenv("COF_TB_GLOBAL")) tb_global = e[0] != '0';
+    uint32_t tb_slots = banded ? (tb_global ? kTbSlotsGlobal : kTbSlotsShared) : 0;
     if (const char *e = std::getenv("COF_TB_SLOTS"))
         if (banded) tb_slots = (uint32_t)std::min<long>(kTbSlotsMax, std::max(0L, std::atol(e)));
+    if (!tb_slots) tb_global = false;
     // free slots take work while the stack holds fewer than tb_refill
     // nodes (COF_TB_REFILL)
     uint32_t tb_refill = kTbRefill;
@@ -2226,7 +2241,7 @@ int Engine::run_bulge(const std::vector<Request> &reqs, std::vector<Result> &out
     CU(cudaDeviceGetAttribute(&smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, d.device));
     const size_t node_bytes = wide_nodes ? sizeof(TbNode<2>) : sizeof(TbNode<1>);
     auto warp_bytes_for = [&](uint32_t slots) -> size_t {
-        if (slots) return tb_slot_layout(node_bytes, tbl_words, stk_cap, slots).total;
+        if (slots) return tb_slot_layout(node_bytes, tb_global ? 0u : tbl_words, stk_cap, slots).total;
         return wide_nodes ? tb_warp_bytes<2>(tbl_words, stk_cap) : tb_warp_bytes<1>(tbl_words, stk_cap);
     };
     // fewer slots while kTbWarps warps of them exceed a block's shared memory
@@ -2239,10 +2254,15 @@ int Engine::run_bulge(const std::vector<Request> &reqs, std::vector<Result> &out
     if (warp_tb && warp_bytes > (size_t)smem_optin) warp_tb = false;
     const size_t tb_smem = (size_t)tb_wpb * warp_bytes;
     const void *tb_fn =
-        tb_slots ? (wide_nodes ? (nw == 1 ? (const void *)traceback_slots_kernel<1, 2>
-                                          : (const void *)traceback_slots_kernel<2, 2>)
-                               : (nw == 1 ? (const void *)traceback_slots_kernel<1, 1>
-                                          : (const void *)traceback_slots_kernel<2, 1>))
+        tb_slots ? (tb_global
+                        ? (wide_nodes ? (nw == 1 ? (const void *)traceback_slots_kernel<1, 2, true>
+                                                 : (const void *)traceback_slots_kernel<2, 2, true>)
+                                      : (nw == 1 ? (const void *)traceback_slots_kernel<1, 1, true>
+                                                 : (const void *)traceback_slots_kernel<2, 1, true>))
+                        : (wide_nodes ? (nw == 1 ? (const void *)traceback_slots_kernel<1, 2, false>
+                                                 : (const void *)traceback_slots_kernel<2, 2, false>)
+                                      : (nw == 1 ? (const void *)traceback_slots_kernel<1, 1, false>
+                                                 : (const void *)traceback_slots_kernel<2, 1, false>)))
         : banded ? (wide_nodes ? (nw == 1 ? (const void *)traceback_warp_kernel<1, 2, true>
                                           : (const void *)traceback_warp_kernel<2, 2, true>)
                                : (nw == 1 ? (const void *)traceback_warp_kernel<1, 1, true>
@@ -2252,8 +2272,11 @@ int Engine::run_bulge(const std::vector<Request> &reqs, std::vector<Result> &out
                                : (nw == 1 ? (const void *)traceback_warp_kernel<1, 1, false>
                                           : (const void *)traceback_warp_kernel<2, 1, false>));
     void (*tb_launch)(const TbLaunch &) =
-        tb_slots ? (wide_nodes ? (nw == 1 ? launch_tb_slots<1, 2> : launch_tb_slots<2, 2>)
-                               : (nw == 1 ? launch_tb_slots<1, 1> : launch_tb_slots<2, 1>))
+        tb_slots ? (tb_global
+                        ? (wide_nodes ? (nw == 1 ? launch_tb_slots<1, 2, true> : launch_tb_slots<2, 2, true>)
+                                      : (nw == 1 ? launch_tb_slots<1, 1, true> : launch_tb_slots<2, 1, true>))
+                        : (wide_nodes ? (nw == 1 ? launch_tb_slots<1, 2, false> : launch_tb_slots<2, 2, false>)
+                                      : (nw == 1 ? launch_tb_slots<1, 1, false> : launch_tb_slots<2, 1, false>)))
         : banded ? (wide_nodes ? (nw == 1 ? launch_tb<1, 2, true> : launch_tb<2, 2, true>)
                                : (nw == 1 ? launch_tb<1, 1, true> : launch_tb<2, 1, true>))
                  : (wide_nodes ? (nw == 1 ? launch_tb<1, 2, false> : launch_tb<2, 2, false>)

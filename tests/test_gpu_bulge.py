@@ -144,16 +144,19 @@ def test_band_dp_equals_whole_table(cof_mod, oracle_mod, monkeypatch, mm, db, rb
     assert nref == n and sorted(ref.splitlines()) == sorted(text.splitlines())
 
 
-@pytest.mark.parametrize("slots,budget,chunk", [(4, 0, 0), (2, 0, 0), (1, 0, 0), (4, 1, 0),
-                                                (3, 2, 0), (4, 3, 5)])
+@pytest.mark.parametrize("slots,budget,chunk,tables", [
+    (6, 0, 0, "global"), (8, 1, 0, "global"), (1, 2, 0, "global"), (6, 3, 5, "global"),
+    (4, 0, 0, "shared"), (2, 0, 0, "shared"), (1, 0, 0, "shared"), (4, 1, 0, "shared"),
+    (3, 2, 0, "shared"), (4, 3, 5, "shared")])
 def test_slot_traceback_equals_one_tree_per_warp(cof_mod, oracle_mod, monkeypatch, slots, budget,
-                                                 chunk):
+                                                 chunk, tables):
     # traceback_slots_kernel keeps several candidates' trees in one warp's
-    # stack; its rows must equal those of one tree per warp
-    # (COF_TB_SLOTS=0) and of the oracle.  Budgets of 1-3 steps make slots
-    # hand their nodes on after almost every step (hand-on passes up to the
-    # last, which finishes every tree); small candidate chunks make many
-    # launches with few candidates
+    # stack, reading their band tables from global memory or from copies in
+    # the slots (COF_TB_GLOBAL=0); its rows must equal those of one tree
+    # per warp (COF_TB_SLOTS=0) and of the oracle.  Budgets of 1-3 steps
+    # make slots hand their nodes on after almost every step (hand-on
+    # passes up to the last, which finishes every tree); small candidate
+    # chunks make many launches with few candidates
     import synth
     cfg = synth.config_bulge(seed=5, scale=0.0004, n_guides=6, planted=8)
     g = cof_mod.Genome()
@@ -162,6 +165,7 @@ def test_slot_traceback_equals_one_tree_per_warp(cof_mod, oracle_mod, monkeypatc
     monkeypatch.setenv("COF_TB_SLOTS", "0")
     text0, n0 = g.search(*args)
     monkeypatch.setenv("COF_TB_SLOTS", str(slots))
+    monkeypatch.setenv("COF_TB_GLOBAL", "1" if tables == "global" else "0")
     if budget:
         monkeypatch.setenv("COF_TB_BUDGET", str(budget))
     if chunk:
