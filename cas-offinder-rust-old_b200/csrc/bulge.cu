@@ -509,7 +509,7 @@ traceback_kernel(GenomeDev G, const BatchDev *__restrict__ batches,
                                 w.rb = f.rb;
                                 w.ops_hi = o2;
                                 rows[r] = w;
-                                keys[r] = ((uint64_t)c.pattern << 34) | start;
+                                keys[r] = ((uint64_t)c.pattern << G.key_shift) | start;
                                 vals[r] = r;
                                 atomicAdd(&req_rows[P.request], 1u);
                             } else {
@@ -1024,7 +1024,7 @@ traceback_warp_kernel(GenomeDev G, const BatchDev *__restrict__ batches,
                         w.db = (uint8_t)l2.d;
                         w.rb = (uint8_t)l2.r;
                         rows[rr] = w;
-                        keys[rr] = ((uint64_t)c.pattern << 34) | l2.start;
+                        keys[rr] = ((uint64_t)c.pattern << G.key_shift) | l2.start;
                         vals[rr] = rr;
                     } else {
                         ctr->overflow = 1;
@@ -1401,7 +1401,7 @@ traceback_slots_kernel(GenomeDev G, const BatchDev *__restrict__ batches,
                     w.db = (uint8_t)l2.d;
                     w.rb = (uint8_t)l2.r;
                     rows[rr] = w;
-                    keys[rr] = ((uint64_t)pattern << 34) | l2.start;
+                    keys[rr] = ((uint64_t)pattern << G.key_shift) | l2.start;
                     vals[rr] = rr;
                 } else {
                     ctr->overflow = 1;
@@ -1803,17 +1803,26 @@ mrow_write_kernel(GenomeDev G, const MyersRow *__restrict__ rows,
             // aligned strings in alignment order (traceback.rs:267-298), then
             // reverse-complemented for reverse-strand patterns
             uint32_t pi = 0;
+            // genome cells from w.start on, through a 16-cell word cursor
+            // (the buffer is padded past the last cell by more than a word)
+            const unsigned long long *gwords = reinterpret_cast<const unsigned long long *>(G.bit4);
             uint64_t gi = w.start;
+            unsigned long long gword = __ldg(gwords + (gi >> 4));
+            auto gnext = [&]() -> uint8_t {
+                const uint8_t v = (uint8_t)((gword >> (4 * (gi & 15))) & 0xF);
+                if ((++gi & 15) == 0) gword = __ldg(gwords + (gi >> 4));
+                return v;
+            };
             for (uint32_t k = 0; k < no; ++k) {
                 const uint32_t op = mrow_op(w, k);
                 uint8_t pv = 0, gv = 0;
                 bool pgap = false, ggap = false;
                 if (op <= 1) {
                     pv = P.b4[pi++];
-                    gv = nib(G.bit4, gi++);
+                    gv = gnext();
                 } else if (op == 2) {
                     pgap = true;
-                    gv = nib(G.bit4, gi++);
+                    gv = gnext();
                 } else {
                     pv = P.b4[pi++];
                     ggap = true;
@@ -2450,13 +2459,17 @@ int Engine::run_bulge(const std::vector<Request> &reqs, std::vector<Result> &out
         if (nr) {
             CU(cudaEventRecord(d.ev[5], s));
             size_t tmp = 0, tmp2 = 0;
+            // key bits in use: the start's, then the pattern index's
+            int key_bits = (int)d.key_shift();
+            for (size_t np = pats.size(); np > 1; np = (np + 1) / 2) ++key_bits;
+            key_bits = std::min(key_bits, 64);
             CU(cub::DeviceRadixSort::SortPairs(nullptr, tmp, d.keys.p, d.keys2.p, d.vals.p,
-                                               d.vals2.p, (int)nr, 0, 64, s));
+                                               d.vals2.p, (int)nr, 0, key_bits, s));
             CU(cub::DeviceScan::ExclusiveSum(nullptr, tmp2, d.lens.p, d.offs.p, (int)nr + 1, s));
             if (d.cub_tmp.ensure(std::max(tmp, tmp2), err)) return err.code;
             tmp = d.cub_tmp.cap;
             CU(cub::DeviceRadixSort::SortPairs(d.cub_tmp.p, tmp, d.keys.p, d.keys2.p, d.vals.p,
-                                               d.vals2.p, (int)nr, 0, 64, s));
+                                               d.vals2.p, (int)nr, 0, key_bits, s));
             const unsigned fb = (unsigned)std::min<uint64_t>((nr + 255) / 256, (uint64_t)d.n_sm * 8);
             mrow_len_kernel<<<fb, 256, 0, s>>>(d.view(), d.mrows.p, d.vals2.p, nr, dP, dR, d.lens.p);
             CU(cudaGetLastError());

@@ -110,6 +110,9 @@ struct GenomeDev {
     const char *names;
     const uint32_t *name_off;
     uint64_t n_chunks;
+    // bulge row sort keys: pattern << key_shift | global start, with
+    // 2^key_shift above every start, so the sort covers only the bits in use
+    uint32_t key_shift;
 };
 
 __device__ __forceinline__ uint32_t ndigits(uint64_t v) {
@@ -238,8 +241,16 @@ class DeviceGenome {
         if (copy_stream) cudaStreamDestroy(copy_stream);
         if (stream) cudaStreamDestroy(stream);
     }
+    // bits of the largest global nucleotide index (the plane words cover
+    // every start)
+    uint32_t key_shift() const {
+        uint32_t b = 1;
+        while (b < 63 && (1ull << b) <= n_words * 32) ++b;
+        return b;
+    }
     GenomeDev view() const {
-        return GenomeDev{bit4.p, boff.p, start.p, end.p, name_idx.p, names.p, name_off.p, n_chunks};
+        return GenomeDev{bit4.p, boff.p,   start.p,  end.p,       name_idx.p,
+                         names.p, name_off.p, n_chunks, key_shift()};
     }
 };
 
