@@ -1639,17 +1639,31 @@ budget_band_kernel(GenomeDev G, const BatchDev *__restrict__ batches,
                 fullg[w] = R.m_full[w];
                 valid[w] = R.m_valid[w];
             }
-            // the window's n text cells, cell k in bits 4 (k % 16) of word k / 16
+            // the window's n text cells, cell k in bits 4 (k % 16) of word
+            // k / 16 (cells from n on 0), from aligned 16-cell genome words
+            // (the buffer is padded past the last cell by more than a word)
             const uint64_t tbase = B.base + t + 1 - n;
-            uint64_t tw0 = 0, tw1 = 0, tw2 = 0, tw3 = 0, tw4 = 0;
-            for (uint32_t k = 0; k < n; ++k) {
-                const uint64_t x = (uint64_t)nib(G.bit4, tbase + k) << (4 * (k & 15));
-                if (k < 16) tw0 |= x;
-                else if (k < 32) tw1 |= x;
-                else if (TW == 3 || k < 48) tw2 |= x;
-                else if (k < 64) tw3 |= x;
-                else tw4 |= x;
+            const unsigned long long *gwp = reinterpret_cast<const unsigned long long *>(G.bit4);
+            const uint64_t q0 = tbase >> 4;
+            const uint32_t sh = 4 * (uint32_t)(tbase & 15);
+            uint64_t tw[TW];
+            {
+                uint64_t a = __ldg(gwp + q0);
+#pragma unroll
+                for (int q = 0; q < TW; ++q) {
+                    uint64_t x = 0;
+                    if (16u * q < n) {
+                        const uint64_t b = __ldg(gwp + q0 + q + 1);
+                        x = sh ? (a >> sh) | (b << (64 - sh)) : a;
+                        a = b;
+                        if (16u * (q + 1) > n) x &= (1ull << (4 * (n - 16u * q))) - 1ull;
+                    }
+                    tw[q] = x;
+                }
             }
+            const uint64_t tw0 = tw[0], tw1 = tw[1], tw2 = tw[2];
+            const uint64_t tw3 = TW == 5 ? tw[TW == 5 ? 3 : 0] : 0ull;
+            const uint64_t tw4 = TW == 5 ? tw[TW == 5 ? 4 : 0] : 0ull;
             auto word = [&](int q) -> uint64_t {
                 return q == 0 ? tw0 : q == 1 ? tw1 : q == 2 ? tw2
                      : (TW == 5 && q == 3) ? tw3 : (TW == 5 && q == 4) ? tw4 : 0ull;
