@@ -1058,10 +1058,12 @@ traceback_warp_kernel(GenomeDev G, const BatchDev *__restrict__ batches,
 // traceback_warp_kernel<.., true>; only the warp step that expands a node
 // differs, and the rows are sorted afterwards.
 constexpr uint32_t kTbSlotsMax = 8;     // most candidates resident per warp
-// the defaults.  Band tables read from global memory: 6 slots (10 Mbp bulge
-// set, device total: 3 slots 8.75 ms, 4: 8.58, 6: 8.34, 8: 8.55).  Tables
-// copied into the slots: 3 (2: 10.38, 3: 9.99, 4: 10.14 with the earlier
-// Myers filter; 3: 8.66 with the current one).
+// the defaults.  Tables copied into the slots: 3 (10 Mbp bulge set, device
+// total: 2: 10.38, 3: 9.99, 4: 10.14 with the earlier Myers filter; 3: 8.66
+// with the current one).  Band tables read from global memory (through L1
+// and L2): 6 (3: 8.75, 4: 8.58, 6: 8.34, 8: 8.55), but a chunk of a large
+// set holds gigabytes of tables, far past L2, and the 500 Mbp set's
+// traceback took 846 ms against 614 with copied tables.
 constexpr uint32_t kTbSlotsGlobal = 6;
 constexpr uint32_t kTbSlotsShared = 3;
 constexpr uint32_t kTbSlotSpare = 128;  // stack slots beyond the walk margin
@@ -2241,11 +2243,11 @@ int Engine::run_bulge(const std::vector<Request> &reqs, std::vector<Result> &out
     const size_t item_bytes = wide_nodes ? sizeof(TbItem<2>) : sizeof(TbItem<1>);
     const uint32_t tb_mrg = tb_margin(wmax);
     // with band tables, several candidates are resident per warp
-    // (traceback_slots_kernel), reading their tables from global memory
-    // (COF_TB_GLOBAL=0: copied into the slots); COF_TB_SLOTS sets
+    // (traceback_slots_kernel), their tables copied into the slots
+    // (COF_TB_GLOBAL=1: read from global memory); COF_TB_SLOTS sets
     // 1..kTbSlotsMax, or 0 for one tree per warp (traceback_warp_kernel)
-    bool tb_global = true;
-    if (const char *e = std::getenv("COF_TB_GLOBAL")) tb_global = e[0] != '0';
+    bool tb_global = false;
+    if (const char *e = std::getenv("COF_TB_GLOBAL")) tb_global = e[0] == '1';
     uint32_t tb_slots = banded ? (tb_global ? kTbSlotsGlobal : kTbSlotsShared) : 0;
     if (const char *e = std::getenv("COF_TB_SLOTS"))
         if (banded) tb_slots = (uint32_t)std::min<long>(kTbSlotsMax, std::max(0L, std::atol(e)));
