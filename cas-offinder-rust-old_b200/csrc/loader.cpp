@@ -758,7 +758,7 @@ int make_request(const char *filter, size_t pattern_len, const char *const *patt
     }
     bool myers = db > 0 || rb > 0;
     if (pattern_len > kMaxPatternLen)
-        return bad("pattern length above 64 is not supported by this build", kUnsupported);
+        return bad("pattern length above 64 is not supported (at most 64 cells)", kUnsupported);
     if (!myers && mm >= pattern_len)
         return bad("max_mismatches must be below the pattern length");
     if (myers && (db > 8 || rb > 8 || mm + db + rb > 30))

@@ -47,7 +47,7 @@ extern "C" {
 #define COF_E_OOM (-2)         /* device or host allocation failed         */
 #define COF_E_CUDA (-3)        /* CUDA runtime error                       */
 #define COF_E_IO (-4)          /* genome file could not be read            */
-#define COF_E_UNSUPPORTED (-5) /* valid input outside this build's limits  */
+#define COF_E_UNSUPPORTED (-5) /* valid input outside the library's limits */
 #define COF_E_STATE (-6)       /* call order (e.g. add_chunk after upload) */
 #define COF_E_TIMEOUT (-7)     /* a bounded device wait gave up            */
 #define COF_E_CANCELLED (-8)   /* a result sink stopped the search         */
