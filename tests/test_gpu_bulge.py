@@ -92,6 +92,41 @@ def test_mixed_popcount_and_bulge_batch(cof_mod, oracle_mod):
         assert n == ns == nref
 
 
+def test_bulge_eq_tables_and_pam_forms_beyond_staging(cof_mod, oracle_mod):
+    # myers_tile_kernel stages the Eq tables of at most 512 patterns in
+    # shared memory (more are read from the patterns in global memory) and
+    # tests at most 8 PAM forms per launch (more go to myers_filter_kernel,
+    # which tests the PAM per lane): one request of 300 guides (600
+    # patterns), and one pass of five PAM shapes on both strands (10 forms),
+    # each request's rows equal to the oracle's
+    rng = random.Random(515)
+    _, records = randgen.random_genome(rng, 2, 8000, 12000)
+    filt0, mk0, _ = randgen.REQUEST_SHAPES[0]
+    big_pats = [mk0("".join(rng.choice("ACGT") for _ in range(25))) for _ in range(300)]
+    for p in big_pats[:6]:
+        randgen.plant_sites(rng, records, p, filt0, 3, 2)
+    big = dict(search_filter=filt0, patterns=big_pats, max_mismatches=2, max_dna_bulges=1,
+               max_rna_bulges=1)
+    mixed = []
+    for filt, mk, mm in [randgen.REQUEST_SHAPES[i] for i in (0, 1, 2, 4, 5)]:
+        pats = [mk("".join(rng.choice("ACGT") for _ in range(25))) for _ in range(2)]
+        for p in pats:
+            randgen.plant_sites(rng, records, p, filt, 3, 2)
+        mixed.append(dict(search_filter=filt, patterns=pats, max_mismatches=min(mm, 3),
+                          max_dna_bulges=1, max_rna_bulges=1))
+    g, o = _both(cof_mod, oracle_mod, randgen.chunk_records(rng, records, 700))
+    total = 0
+    for batch in ([big], mixed):
+        for r, (text, n) in zip(batch, g.search_batch(batch)):
+            ref, nref = o.search(r["search_filter"], r["patterns"], r["max_mismatches"],
+                                 r["max_dna_bulges"], r["max_rna_bulges"])
+            assert n == nref and _rows(text) == _rows(ref)
+            total += n
+    g.close()
+    o.close()
+    assert total > 100
+
+
 @pytest.mark.parametrize("n_guides,planted", [(4, 5), (20, 30)])
 def test_warp_traceback_equals_thread_traceback(cof_mod, oracle_mod, monkeypatch, n_guides,
                                                 planted):
