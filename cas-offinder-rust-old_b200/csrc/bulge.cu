@@ -207,8 +207,10 @@ __global__ void myers_filter_kernel(const uint8_t *__restrict__ bit4,
 // for every form, Q(y) = "the PAM cells starting at batch cell y are all
 // good" and from it pam_ok(t) = OR over spans of Q(t + 1 - span + pam_off)
 // for the tile's end positions t, into shared memory.  Then every
-// (tile, pattern) thread runs the streaming Myers sweep and tests one bit
-// per position instead of the reference's per-position cell loads.
+// (tile, pattern) thread runs the streaming Myers sweep a 16-cell genome
+// word at a time and meets each word's "score <= E" bits with 16 pam_ok
+// bits, instead of the reference's per-position cell loads; a round's
+// candidates are staged in shared memory and appended with one atomic.
 constexpr uint32_t kMfThreads = 256;
 constexpr uint32_t kMfMaxTiles = 32;           // tiles per block
 constexpr uint32_t kMfMaxForms = 8;            // PAM forms per launch
