@@ -126,6 +126,34 @@ def test_bad_requests_rejected(cof_mod, golden):
     assert e.value.code == cof_mod.COF_E_UNSUPPORTED
 
 
+def test_stream_argument_errors(cof_mod, golden):
+    # cof_search_stream rejects a null genome or sink, an unknown stream
+    # flag and a bad request before any device work (no GPU needed); the
+    # sink is never called
+    import ctypes
+    lib = cof_mod.load_library()
+    g = cof_mod.Genome(os.path.join(golden, "upstream1000.fa"))
+    good = dict(search_filter="N" * 24, patterns=["CCGTGGTTCAACATTTGCTTAGCA"], max_mismatches=3)
+    calls = []
+    sink = cof_mod._SINK(lambda _u, _p: calls.append(1) or 0)
+    reqs, _keep = g.prepare([good])
+    n = (ctypes.c_uint64 * 1)()
+    assert lib.cof_search_stream(None, reqs, 1, 0, sink, None, n) == cof_mod.COF_E_BADINPUT
+    assert lib.cof_search_stream(g._h, reqs, 1, 0, cof_mod._SINK(), None, n) == cof_mod.COF_E_BADINPUT
+    assert lib.cof_search_stream(g._h, None, 1, 0, sink, None, n) == cof_mod.COF_E_BADINPUT
+    assert lib.cof_search_stream(g._h, reqs, 1, 0x80, sink, None, n) == cof_mod.COF_E_BADINPUT
+    assert b"stream flag" in lib.cof_last_error()
+    with pytest.raises(cof_mod.CofError) as e:
+        g.search_stream([dict(good, search_filter="NNNN")], lambda *a: 0)
+    assert e.value.code == cof_mod.COF_E_BADINPUT
+    assert calls == []
+    # the record-name calls answer for a null genome too
+    assert lib.cof_genome_n_records(None) == 0
+    assert lib.cof_genome_record_name(None, 0) is None
+    assert lib.cof_genome_record_name(g._h, g.n_records) is None
+    g.close()
+
+
 def test_bad_genome_files(cof_mod, tmp_path):
     p = tmp_path / "bad.fa"
     p.write_text("ACGT\n>x\nACGT\n")  # sequence before the first header
