@@ -193,6 +193,32 @@ def test_no_gpu_fails_loudly(cof_mod, golden):
     assert e.value.code in (cof_mod.COF_E_CUDA, cof_mod.COF_E_OOM)
 
 
+def test_server_argument_errors(cof_mod, golden):
+    # with a memory budget given, a server is created without touching the
+    # device; a bad request is refused at submit, an unknown ticket at wait
+    import ctypes
+    lib = cof_mod.load_library()
+    g = cof_mod.Genome(os.path.join(golden, "upstream1000.fa"))
+    h = ctypes.c_void_p()
+    assert lib.cof_server_create(None, None, ctypes.byref(h)) == cof_mod.COF_E_BADINPUT
+    srv = cof_mod.Server(g, memory_budget_bytes=1 << 30, ring_slices=3)
+    with pytest.raises(cof_mod.CofError) as e:
+        srv.submit("NNNN", ["ACGTA"], 1)
+    assert e.value.code == cof_mod.COF_E_BADINPUT
+    with pytest.raises(cof_mod.CofError) as e:
+        srv.wait(12345)
+    assert e.value.code == cof_mod.COF_E_BADINPUT
+    assert srv.stats()["queued"] == 0
+    if not _gpu_usable():
+        # no GPU: the request completes with the CUDA error, it does not hang
+        t = srv.submit("N" * 24, ["CCGTGGTTCAACATTTGCTTAGCA"], 3)
+        with pytest.raises(cof_mod.CofError) as e:
+            srv.wait(t, timeout_ms=120000)
+        assert e.value.code in (cof_mod.COF_E_CUDA, cof_mod.COF_E_OOM)
+    srv.close()
+    g.close()
+
+
 def test_cli_input_errors(cof_mod, tmp_path):
     cli = os.path.join(os.path.dirname(cof_mod.LIB_PATH), "cof-offinder")
     cases = {
