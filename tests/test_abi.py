@@ -219,6 +219,41 @@ def test_server_argument_errors(cof_mod, golden):
     g.close()
 
 
+@pytest.mark.skipif(_gpu_usable(), reason="passes a placeholder device address; never run with a GPU")
+def test_noalloc_argument_checks(cof_mod):
+    # cof_search_seq_noalloc checks its arguments before any CUDA call.  The
+    # device buffers here are a placeholder address, which every case below
+    # rejects before it could be used (and no GPU is present)
+    import ctypes
+    lib = cof_mod.load_library()
+    fake = 1 << 20  # 16-byte aligned
+    n_rows = ctypes.c_uint32(0)
+    pats2 = [b"ACGTACGTACGTNNN", b"NNNACGTACGTACGT"]
+
+    def call(seq=fake, n_nucl=8000, filt=b"N" * 15, pats=pats2, npat=None, mm=2, rows=fake,
+             cap=10):
+        arr = (ctypes.c_char_p * len(pats))(*pats)
+        rc = lib.cof_search_seq_noalloc(seq, n_nucl, filt, arr, len(pats) if npat is None else npat,
+                                        mm, rows, cap, ctypes.byref(n_rows), None)
+        return rc, lib.cof_last_error()
+
+    bad, uns = cof_mod.COF_E_BADINPUT, cof_mod.COF_E_UNSUPPORTED
+    assert call(seq=None)[0] == bad
+    assert call(rows=None)[0] == bad  # rows_cap > 0 needs a row buffer
+    assert call(seq=fake + 4) == (bad, b"d_bit4 must be 16-byte aligned")
+    assert call(filt=b"")[0] == uns
+    assert call(filt=b"N" * 33, pats=[b"A" * 33, b"T" * 33])[0] == uns
+    assert call(pats=pats2 * 257)[0] == uns and b"n_patterns" in call(pats=pats2 * 257)[1]
+    assert call(npat=0)[0] == uns
+    rc, msg = call(pats=pats2 + [pats2[0]])
+    assert rc == bad and b"even" in msg
+    assert call(n_nucl=1 << 31)[0] == uns
+    assert call(mm=15)[0] == bad
+    assert call(filt=b"N" * 14 + b"X")[0] == bad
+    assert call(pats=[b"ACGT", b"ACGT"])[0] == bad  # length differs from the filter
+    assert call(pats=[b"ACGTACGTACGTNN!", pats2[1]])[0] == bad
+
+
 def test_cli_input_errors(cof_mod, tmp_path):
     cli = os.path.join(os.path.dirname(cof_mod.LIB_PATH), "cof-offinder")
     cases = {
