@@ -34,11 +34,11 @@ def test_myers_tile_kernel_smem_worst_case():
 
 
 def test_slot_traceback_fits_a_block():
-    # four warps of the largest slot layout: the stack (margin + spare
-    # nodes of 24 bytes for windows over 48 cells), slot records, band
-    # tables of the widest band at 64 cells with two-word cells, texts and
-    # pattern arrays; the host lowers the slot count when this does not fit,
-    # and at three slots it must fit
+    # the largest slot layout: the stack (margin + spare nodes of 24 bytes
+    # for windows over 48 cells), slot records, band tables of the widest
+    # band at 64 cells with two-word cells, texts and pattern arrays.  The
+    # host lowers the slots, then the warps per block, while a block does
+    # not fit; one warp of the default three slots must always fit
     spare, slots = _const("kTbSlotSpare"), _const("kTbSlotsShared")
     band_max = _const("kBandMax")
     text, pat = _const("kTbText"), _const("kTbPat")
